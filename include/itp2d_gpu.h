@@ -1,0 +1,167 @@
+/*
+ * itp2d_gpu.h -- C ABI of the B200 (sm_100a) implementation of the itp2d
+ * imaginary-time-propagation hot path.
+ *
+ * One context holds one set of k states of an sx*sy grid resident in device
+ * memory (state n at offset n*sx*sy, x fastest, complex values), the
+ * potential, and the split-operator tables for the current time step. The
+ * three seams of the reference driver map to one call each:
+ *
+ *   ITPSystem::propagate          (itpsystem.cpp:243-256)  -> itp2d_propagate
+ *   StateSet::orthonormalize      (stateset.cpp:136-232)   -> itp2d_orthonormalize
+ *   ITPSystem::calculate_energies (itpsystem.cpp:473-511)  -> itp2d_energies
+ *
+ * Conventions: every function returns an int status (ITP2D_OK = 0); no C++
+ * exception crosses this boundary. A context is bound to one CUDA stream and
+ * is not re-entrant: calls on one context must not overlap (the library
+ * serialises them with a per-context mutex). Host arrays are plain doubles:
+ * complex values are interleaved (re, im).
+ */
+#ifndef ITP2D_GPU_H
+#define ITP2D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The C++ host layer maps them to the reference exceptions
+ * (exceptions.hpp:37-254): NONPOSITIVE -> NonPositiveEigenvalue,
+ * NONNORMAL -> NonNormalEigenvalue, EIGENSOLVER -> EigensolverError. */
+enum {
+	ITP2D_OK = 0,
+	ITP2D_E_INVALID = 1,                /* bad argument or unsupported size */
+	ITP2D_E_CUDA = 2,                   /* a CUDA runtime call failed */
+	ITP2D_E_OOM = 3,                    /* device allocation failed */
+	ITP2D_E_NONPOSITIVE_EIGENVALUE = 4, /* overlap eigenvalue <= 0 (stateset.cpp:163-167) */
+	ITP2D_E_NONNORMAL_EIGENVALUE = 5,   /* overlap eigenvalue not FP_NORMAL (stateset.cpp:168-172) */
+	ITP2D_E_EIGENSOLVER = 6,            /* eigensolver did not converge (eigensolver.hpp:80-84) */
+	ITP2D_E_TIMEOUT = 7,                /* a bounded device wait ran out */
+	ITP2D_E_UNSUPPORTED = 8             /* combination not built (for example a grid size) */
+};
+
+/* Boundary conditions, enum BoundaryType of itp2d_common.hpp:50. */
+enum { ITP2D_PERIODIC = 0, ITP2D_DIRICHLET = 1 };
+
+/* Arithmetic of the propagation sweeps and energies. */
+enum { ITP2D_FP64 = 0, ITP2D_FP32 = 1 };
+
+/* Orthonormalisation algorithm, enum OrthoAlgorithm of itp2d_common.hpp:53.
+ * Both select the same out-of-place device path; the argument is accepted
+ * for interface compatibility. */
+enum { ITP2D_ORTHO_DEFAULT = 0, ITP2D_ORTHO_HIGHMEM = 1 };
+
+/* Transform kinds in the order of enum Transform (transformer.hpp:32-34). */
+enum {
+	ITP2D_FFT = 0, ITP2D_IFFT, ITP2D_FFTX, ITP2D_IFFTX, ITP2D_FFTY, ITP2D_IFFTY,
+	ITP2D_DST, ITP2D_IDST, ITP2D_DSTX, ITP2D_IDSTX, ITP2D_DSTY, ITP2D_IDSTY,
+	ITP2D_DCT, ITP2D_IDCT, ITP2D_DCTX, ITP2D_IDCTX, ITP2D_DCTY, ITP2D_IDCTY
+};
+
+typedef struct itp2d_ctx itp2d_ctx;
+
+/* Creates a context for num_states states on an sx*sy grid with spacing dx
+ * (DataLayout, datalayout.cpp:21-36; Parameters::get_grid_delta,
+ * parameters.hpp:97). B is the magnetic field (linear gauge, kinetic.hpp:24-29),
+ * halforder the multi-product half order m (MultiProductSplit,
+ * multiproductsplit.cpp:23-41; forced to 1 when the potential is null).
+ * cuda_stream is a cudaStream_t or NULL for a stream owned by the context.
+ * Replaces the allocation part of the ITPSystem constructor
+ * (itpsystem.cpp:23-139) and StateSet::StateSet (stateset.cpp:23-44). */
+int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary,
+		double B, int halforder, int precision, void* cuda_stream,
+		itp2d_ctx** out);
+
+/* Frees every device allocation of the context. */
+int itp2d_ctx_destroy(itp2d_ctx* ctx);
+
+/* Sets the potential V (sx*sy doubles, y-major) or the null potential when
+ * V is NULL. Replaces Potential (potential.cpp:21-63) as seen by
+ * ExpPotential and the Hamiltonian. Tables are rebuilt for the current time
+ * step. */
+int itp2d_set_potential(itp2d_ctx* ctx, const double* V);
+
+/* Sets the imaginary time step eps and rebuilds every exponential table:
+ * MultiProductSplit::set_time_step (multiproductsplit.cpp:43-47). */
+int itp2d_set_time_step(itp2d_ctx* ctx, double eps);
+
+/* Copies all states host -> device / device -> host
+ * (k*sy*sx interleaved complex doubles, StateArray layout statearray.cpp:21-75). */
+int itp2d_upload_states(itp2d_ctx* ctx, const double* states);
+int itp2d_download_states(itp2d_ctx* ctx, double* states);
+
+/* Device pointer to the state array (double2 or float2 per element,
+ * depending on the precision), valid until the next orthonormalisation,
+ * which swaps buffers. */
+int itp2d_device_states(itp2d_ctx* ctx, void** dev_ptr);
+
+/* Applies the multi-product split evolution operator to every state:
+ * ITPSystem::propagate (itpsystem.cpp:243-256) with MultiProductSplit
+ * (multiproductsplit.cpp:23-41), SecondOrderSplit (secondordersplit.cpp:21-49),
+ * ExpKinetic (expkinetic.cpp:138-197), ExpPotential (exppotential.hpp:56-65). */
+int itp2d_propagate(itp2d_ctx* ctx);
+
+/* Canonical subspace orthonormalisation of the state set,
+ * StateSet::orthonormalize (stateset.cpp:136-232): S = Psi^H Psi dx^2,
+ * S = U diag(l) U^H with ascending l, psi'_n = sum_i U_{i,n} l_n^{-1/2} psi_i.
+ * On ITP2D_E_NONPOSITIVE_EIGENVALUE / ITP2D_E_NONNORMAL_EIGENVALUE the
+ * states are left unchanged and (*bad_index, *bad_value) name the first
+ * offending eigenvalue in ascending order. algo: ITP2D_ORTHO_*. Either out
+ * pointer may be NULL. */
+int itp2d_orthonormalize(itp2d_ctx* ctx, int algo, int* bad_index, double* bad_value);
+
+/* Per-state energy and deviation in storage order:
+ * Operator::mean_and_standard_deviation (operators.cpp:40-50) for H = T + V
+ * (itpsystem.cpp:116-119): E = Re<psi|H psi>, sigma = Re sqrt(<H^2> - <H>^2)
+ * with <H^2> = <H psi|H psi>. sigma_residual = ||H psi - E psi|| (no
+ * cancellation floor). Arrays hold num_states doubles; sigma_residual and
+ * E_imag may be NULL. */
+int itp2d_energies(itp2d_ctx* ctx, double* E, double* sigma, double* sigma_residual, double* E_imag);
+
+/* states <- H states (Hamiltonian OperatorSum of itpsystem.cpp:116-119),
+ * the operator application tested by test_hamiltonian.cpp:40-106. */
+int itp2d_apply_hamiltonian(itp2d_ctx* ctx);
+
+/* states <- Transformer::transform(states, kind), unnormalised
+ * (transformer.hpp:132-158). kind: ITP2D_FFT ... ITP2D_IDCTY. */
+int itp2d_transform(itp2d_ctx* ctx, int kind);
+
+/* Switches the arithmetic of the sweeps and energies (ITP2D_FP64 or
+ * ITP2D_FP32), converting the resident states on the device and rebuilding
+ * the tables. The FP32 form switches to FP64 at its accuracy floor to refine
+ * the eigenpairs; no reference counterpart (the reference is FP64 only). */
+int itp2d_set_precision(itp2d_ctx* ctx, int precision);
+
+/* Waits for the context's stream. */
+int itp2d_synchronize(itp2d_ctx* ctx);
+
+/* Number of kernel launches issued by this context since creation. */
+long long itp2d_launch_count(itp2d_ctx* ctx);
+
+/* Accumulated device milliseconds per phase, measured with CUDA events on
+ * the context's stream: [0] propagate, [1] overlap, [2] eigensolve,
+ * [3] rotation, [4] energies. Timing is enabled by itp2d_set_timing(ctx, 1)
+ * and costs one event pair per phase. */
+int itp2d_set_timing(itp2d_ctx* ctx, int enable);
+int itp2d_phase_times(itp2d_ctx* ctx, double* ms5);
+
+/* Jacobi sweeps used by the last orthonormalisation. */
+int itp2d_last_sweeps(itp2d_ctx* ctx);
+
+/* Eigen-decomposition of an n x n complex Hermitian matrix on the device,
+ * the drop-in for EigenSolver::solve (ZHEEV("V","U"), eigensolver.hpp:80-84).
+ * A is column-major interleaved complex (A[j*n+i] = element (i, j)); only
+ * the upper triangle i <= j is read. On return evals holds the eigenvalues in
+ * ascending order and evecs[m*n+i] element i of eigenvector m (the layout of
+ * EigenSolver::eigenvector, eigensolver.hpp:60). Eigenvector phases are
+ * those of the Jacobi method, not LAPACK's. Allocates temporary device
+ * memory; runs on the default stream. */
+int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs);
+
+/* Short description of a status code. */
+const char* itp2d_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ITP2D_GPU_H */

@@ -1,0 +1,97 @@
+/*
+ * itp2d_host.h -- C ABI of the native ITP driver that runs on top of
+ * itp2d_gpu.h. It mirrors the reference ITPSystem (itpsystem.hpp:55-156):
+ * Parameters in, step() until finished, sorted energies and deviations out.
+ * The C++ classes behind it (itp2d_b200/host/itp2d_host.hpp) keep the
+ * reference names: Parameters, ConvergenceTest and its six tests, ITPSystem.
+ */
+#ifndef ITP2D_HOST_H
+#define ITP2D_HOST_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Mirrors the Parameters setters of parameters.hpp:37-211 that the hot path
+ * reads. Strings use the reference's mini-language, for example
+ * "harmonic(1)", "abschange(1e-10)", "relstdev(1e-3,1e-4)" (parser.cpp:26-60,
+ * convergence.cpp:28-55). */
+typedef struct {
+	int sx, sy;
+	double length;          /* lenx; dx = length / sx (parameters.hpp:97) */
+	int boundary;           /* ITP2D_PERIODIC or ITP2D_DIRICHLET */
+	double B;
+	int halforder;          /* order = 2 * halforder */
+	int num_states;         /* N */
+	int wanted;             /* needed_to_converge */
+	int ignore_lowest;
+	int num_eps;            /* leading time steps (add_eps_value) */
+	double eps[16];
+	double eps_divisor;
+	int exhaust_eps;
+	int max_steps;
+	double min_eps;
+	unsigned long seed;
+	int ortho_algorithm;    /* ITP2D_ORTHO_DEFAULT / ITP2D_ORTHO_HIGHMEM */
+	int recover;
+	int precision;          /* ITP2D_FP64 or ITP2D_FP32 (sweeps; FP64 refinement, see below) */
+	double fp32_switch;     /* FP32 form: switch sweeps to FP64 once every wanted state has
+	                           |dE| per step below this (0: never switch) */
+	char potential[128];
+	char timestep_test[128];
+	char final_test[128];
+} itp2d_parameters;
+
+typedef struct itp2d_system itp2d_system;
+
+/* Reference defaults (parameters.cpp:25-55). */
+void itp2d_parameters_default(itp2d_parameters* p);
+
+/* Builds the system: grid, potential (+ optional extra_potential array added
+ * like the reference's user noise hook, itpsystem.cpp:63-64), evolution
+ * operator tables, and initial states (init_states: num_states*sy*sx
+ * interleaved complex doubles, or NULL for seeded complex Gaussian noise
+ * normalised per state, stateset.cpp:124-131). cuda_stream may be NULL. */
+int itp2d_system_create(const itp2d_parameters* p, const double* extra_potential, const double* init_states,
+		void* cuda_stream, itp2d_system** out);
+int itp2d_system_destroy(itp2d_system* s);
+
+/* One ITP iteration, ITPSystem::step (itpsystem.cpp:407-470). */
+int itp2d_system_step(itp2d_system* s);
+/* step() until finished or max_iterations more iterations were taken;
+ * returns ITP2D_OK (check itp2d_system_error_flag). */
+int itp2d_system_run(itp2d_system* s, int max_iterations);
+
+int itp2d_system_is_finished(const itp2d_system* s);
+int itp2d_system_error_flag(const itp2d_system* s);
+int itp2d_system_total_steps(const itp2d_system* s);
+int itp2d_system_num_converged(const itp2d_system* s);
+double itp2d_system_eps(const itp2d_system* s);
+/* 1 while the sweeps run in FP32 (FP32 form before its switch to FP64). */
+int itp2d_system_in_fp32(const itp2d_system* s);
+
+/* Latest energies sorted ascending with their deviations and storage
+ * indices (ITPSystem::calculate_energies, itpsystem.cpp:473-511). Returns the
+ * count (0 before the first step). residual may be NULL. */
+int itp2d_system_energies(const itp2d_system* s, double* E, double* sigma, double* residual, int* index);
+/* Energies of step `step` (0-based) of the history, sorted. */
+int itp2d_system_energy_history(const itp2d_system* s, int step, double* E);
+
+int itp2d_system_download_states(itp2d_system* s, double* states);
+
+/* Seconds: [0] total, [1] propagation, [2] orthonormalisation, [3] overlap
+ * (dot), [4] eigensolve, [5] lincomb, [6] energies + convergence tests. The
+ * device phases [3..5] come from CUDA events. */
+int itp2d_system_times(itp2d_system* s, double* t7);
+
+/* Last error message of the driver (exception text), or "". */
+const char* itp2d_system_last_error(const itp2d_system* s);
+
+/* The device context owned by the system (for itp2d_gpu.h calls). */
+struct itp2d_ctx* itp2d_system_context(itp2d_system* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ITP2D_HOST_H */

@@ -1,0 +1,195 @@
+"""ctypes binding of the C ABI in include/itp2d_gpu.h (libitp2d_b200.so).
+
+This is a thin host-side mirror used by the tests and the benchmark; the
+native C++ host layer (itp2d_b200/host) sits on the same ABI. Every call
+raises ``ITP2DError`` on a non-zero status; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libitp2d_b200.so")
+HEADER = os.path.join(ROOT, "include", "itp2d_gpu.h")
+
+OK = 0
+E_INVALID, E_CUDA, E_OOM = 1, 2, 3
+E_NONPOSITIVE_EIGENVALUE, E_NONNORMAL_EIGENVALUE, E_EIGENSOLVER = 4, 5, 6
+E_TIMEOUT, E_UNSUPPORTED = 7, 8
+PERIODIC, DIRICHLET = 0, 1
+FP64, FP32 = 0, 1
+ORTHO_DEFAULT, ORTHO_HIGHMEM = 0, 1
+TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
+              "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
+
+_lib = None
+
+
+class ITP2DError(RuntimeError):
+    def __init__(self, status: int, what: str, bad_index: int = -1, bad_value: float = 0.0):
+        msg = lib().itp2d_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})")
+        self.status, self.bad_index, self.bad_value = status, bad_index, bad_value
+
+
+def header_symbols() -> list:
+    """Function names declared in include/itp2d_gpu.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*\**\s+\**(itp2d_[a-z0-9_]+)\s*\(",
+                                 txt, flags=re.M)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ITP2DError(E_INVALID, f"{LIB_PATH} missing; build it with python -m itp2d_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d, dp, ip = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.itp2d_ctx_create.argtypes = [i, i, d, i, i, d, i, i, vp, C.POINTER(vp)]
+        L.itp2d_ctx_destroy.argtypes = [vp]
+        L.itp2d_set_potential.argtypes = [vp, dp]
+        L.itp2d_set_time_step.argtypes = [vp, d]
+        L.itp2d_upload_states.argtypes = [vp, dp]
+        L.itp2d_download_states.argtypes = [vp, dp]
+        L.itp2d_device_states.argtypes = [vp, C.POINTER(vp)]
+        L.itp2d_propagate.argtypes = [vp]
+        L.itp2d_orthonormalize.argtypes = [vp, i, ip, dp]
+        L.itp2d_energies.argtypes = [vp, dp, dp, dp, dp]
+        L.itp2d_apply_hamiltonian.argtypes = [vp]
+        L.itp2d_transform.argtypes = [vp, i]
+        L.itp2d_synchronize.argtypes = [vp]
+        L.itp2d_launch_count.argtypes = [vp]
+        L.itp2d_launch_count.restype = C.c_longlong
+        L.itp2d_set_timing.argtypes = [vp, i]
+        L.itp2d_phase_times.argtypes = [vp, dp]
+        L.itp2d_last_sweeps.argtypes = [vp]
+        L.itp2d_hermitian_eigensolve.argtypes = [i, dp, dp, dp]
+        L.itp2d_status_string.argtypes = [i]
+        L.itp2d_status_string.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(st, what):
+    if st != OK:
+        raise ITP2DError(st, what)
+
+
+def hermitian_eigensolve(A: np.ndarray):
+    """Eigenvalues (ascending) and eigenvectors (columns) of a Hermitian
+    matrix through itp2d_hermitian_eigensolve; reads the upper triangle."""
+    n = A.shape[0]
+    a = np.ascontiguousarray(np.asarray(A, dtype=np.complex128).T)  # column-major
+    ev = np.empty(n)
+    vec = np.empty((n, n), dtype=np.complex128)
+    _check(lib().itp2d_hermitian_eigensolve(n, _dp(a.view(np.float64)), _dp(ev), _dp(vec.view(np.float64))),
+           "itp2d_hermitian_eigensolve")
+    return ev, vec.T.copy()
+
+
+class Context:
+    """One device-resident state set (the three seams of ITPSystem::step)."""
+
+    def __init__(self, sx, sy, dx, num_states, boundary=PERIODIC, B=0.0, halforder=1, precision=FP64,
+                 stream=None):
+        self.sx, self.sy, self.dx, self.k = sx, sy, float(dx), num_states
+        self.precision = precision
+        h = C.c_void_p()
+        st = lib().itp2d_ctx_create(sx, sy, float(dx), num_states, boundary, float(B), halforder, precision,
+                                    C.c_void_p(stream) if stream else None, C.byref(h))
+        _check(st, "itp2d_ctx_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().itp2d_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_potential(self, V):
+        if V is None:
+            _check(lib().itp2d_set_potential(self.h, None), "itp2d_set_potential")
+            return
+        a = np.ascontiguousarray(V, dtype=np.float64).reshape(-1)
+        assert a.size == self.sx * self.sy
+        _check(lib().itp2d_set_potential(self.h, _dp(a)), "itp2d_set_potential")
+
+    def set_time_step(self, eps):
+        _check(lib().itp2d_set_time_step(self.h, float(eps)), "itp2d_set_time_step")
+
+    def upload(self, psi):
+        a = np.ascontiguousarray(psi, dtype=np.complex128)
+        assert a.shape == (self.k, self.sy, self.sx), a.shape
+        _check(lib().itp2d_upload_states(self.h, _dp(a.view(np.float64))), "itp2d_upload_states")
+
+    def download(self):
+        out = np.empty((self.k, self.sy, self.sx), dtype=np.complex128)
+        _check(lib().itp2d_download_states(self.h, _dp(out.view(np.float64))), "itp2d_download_states")
+        return out
+
+    def device_states(self) -> int:
+        p = C.c_void_p()
+        _check(lib().itp2d_device_states(self.h, C.byref(p)), "itp2d_device_states")
+        return p.value
+
+    def propagate(self):
+        _check(lib().itp2d_propagate(self.h), "itp2d_propagate")
+
+    def orthonormalize(self, algo=ORTHO_DEFAULT):
+        bi, bv = C.c_int(-1), C.c_double(0.0)
+        st = lib().itp2d_orthonormalize(self.h, algo, C.byref(bi), C.byref(bv))
+        if st != OK:
+            raise ITP2DError(st, "itp2d_orthonormalize", bi.value, bv.value)
+
+    def energies(self):
+        E, s, r, ei = (np.empty(self.k) for _ in range(4))
+        _check(lib().itp2d_energies(self.h, _dp(E), _dp(s), _dp(r), _dp(ei)), "itp2d_energies")
+        return E, s, r, ei
+
+    def apply_hamiltonian(self):
+        _check(lib().itp2d_apply_hamiltonian(self.h), "itp2d_apply_hamiltonian")
+
+    def transform(self, kind):
+        if isinstance(kind, str):
+            kind = TRANSFORMS.index(kind)
+        _check(lib().itp2d_transform(self.h, kind), "itp2d_transform")
+
+    def synchronize(self):
+        _check(lib().itp2d_synchronize(self.h), "itp2d_synchronize")
+
+    @property
+    def launches(self) -> int:
+        return lib().itp2d_launch_count(self.h)
+
+    def set_timing(self, on=True):
+        _check(lib().itp2d_set_timing(self.h, int(on)), "itp2d_set_timing")
+
+    def phase_times(self) -> dict:
+        t = np.zeros(5)
+        _check(lib().itp2d_phase_times(self.h, _dp(t)), "itp2d_phase_times")
+        return dict(zip(["propagate", "overlap", "eigensolve", "rotation", "energies"], t.tolist()))
+
+    @property
+    def last_sweeps(self) -> int:
+        return lib().itp2d_last_sweeps(self.h)

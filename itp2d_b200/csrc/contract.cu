@@ -1,0 +1,315 @@
+// Dense contractions of the orthonormalisation on FP64 tensor cores.
+//
+//   overlap:  S_ij = dx^2 sum_g conj(psi_i[g]) psi_j[g]     (stateset.cpp:146-154)
+//   rotation: out_n[g] = sum_i W[i][n] psi_i[g]             (stateset.cpp:214-228)
+//
+// tcgen05 has no f64 kind, so the FP64 path issues DMMA (mma.sync m8n8k4 f64)
+// from register fragments staged through shared memory. A complex product is
+// four real MMAs. The overlap computes only upper-triangle 64x64 tiles and
+// splits the long g dimension across CTAs; a second kernel sums the splits in
+// a fixed order and fills the Hermitian matrix from the upper triangle, as
+// ZHEEV("U") reads it (eigensolver.hpp:44-53).
+#include "contract.cuh"
+
+#include <algorithm>
+
+namespace itp2d {
+
+namespace {
+
+constexpr int kBM = 64;   // tile rows
+constexpr int kBN = 64;   // tile cols
+constexpr int kBK = 16;   // k step
+constexpr int kPad = 20;  // padded row length (doubles) of a staged plane: conflict-free fragments
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+			: "+d"(d0), "+d"(d1)
+			: "d"(a), "d"(b));
+}
+
+// Shared-memory planes: [64][kPad] doubles each.
+struct Stage {
+	double ar[kBM * kPad];
+	double ai[kBM * kPad];
+	double br[kBN * kPad];
+	double bi[kBN * kPad];
+};
+
+// Overlap: A rows i (conjugated side) and B rows j, both rows of psi (k x G).
+template <class T>
+__global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi, int k, long long G,
+		const int2* __restrict__ pairs, long long chunk, double2* __restrict__ part) {
+	__shared__ __align__(16) Stage st;
+	const int2 tp = pairs[blockIdx.x];
+	const int i0 = tp.x * kBM, j0 = tp.y * kBN;
+	const long long g0 = (long long)blockIdx.y * chunk;
+	const long long g1 = min(G, g0 + chunk);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int wi = warp >> 2;  // 0..1 : 32 rows each
+	const int wj = warp & 3;   // 0..3 : 16 cols each
+	double accr[4][2][2], acci[4][2][2];
+#pragma unroll
+	for (int a = 0; a < 4; a++)
+#pragma unroll
+		for (int b = 0; b < 2; b++) {
+			accr[a][b][0] = accr[a][b][1] = 0.0;
+			acci[a][b][0] = acci[a][b][1] = 0.0;
+		}
+	// loader mapping: row = tid / 4, 4 consecutive complex at seg*4
+	const int lrow = tid >> 2, lseg = (tid & 3) * 4;
+	for (long long g = g0; g < g1; g += kBK) {
+		{
+			const int ia = i0 + lrow, jb = j0 + lrow;
+#pragma unroll
+			for (int q = 0; q < 4; q++) {
+				const long long gg = g + lseg + q;
+				double2 va = make_double2(0, 0), vb = make_double2(0, 0);
+				if (gg < g1) {
+					if (ia < k) { const T t = psi[(long long)ia * G + gg]; va = make_double2(t.x, t.y); }
+					if (jb < k) { const T t = psi[(long long)jb * G + gg]; vb = make_double2(t.x, t.y); }
+				}
+				st.ar[lrow * kPad + lseg + q] = va.x;
+				st.ai[lrow * kPad + lseg + q] = va.y;
+				st.br[lrow * kPad + lseg + q] = vb.x;
+				st.bi[lrow * kPad + lseg + q] = vb.y;
+			}
+		}
+		__syncthreads();
+#pragma unroll
+		for (int kk = 0; kk < kBK; kk += 4) {
+			double far[4], fai[4], fbr[2], fbi[2];
+#pragma unroll
+			for (int a = 0; a < 4; a++) {
+				const int r = wi * 32 + a * 8 + (lane >> 2);
+				far[a] = st.ar[r * kPad + kk + (lane & 3)];
+				fai[a] = st.ai[r * kPad + kk + (lane & 3)];
+			}
+#pragma unroll
+			for (int b = 0; b < 2; b++) {
+				const int c = wj * 16 + b * 8 + (lane >> 2);
+				fbr[b] = st.br[c * kPad + kk + (lane & 3)];
+				fbi[b] = st.bi[c * kPad + kk + (lane & 3)];
+			}
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 2; b++) {
+					// conj(a) b = (ar br + ai bi) + i (ar bi - ai br)
+					dmma(accr[a][b][0], accr[a][b][1], far[a], fbr[b]);
+					dmma(accr[a][b][0], accr[a][b][1], fai[a], fbi[b]);
+					dmma(acci[a][b][0], acci[a][b][1], far[a], fbi[b]);
+					dmma(acci[a][b][0], acci[a][b][1], -fai[a], fbr[b]);
+				}
+		}
+		__syncthreads();
+	}
+	// write the partial tile: part[split][i][j]
+	double2* out = part + (size_t)blockIdx.y * k * k;
+#pragma unroll
+	for (int a = 0; a < 4; a++)
+#pragma unroll
+		for (int b = 0; b < 2; b++) {
+			const int i = i0 + wi * 32 + a * 8 + (lane >> 2);
+			const int j = j0 + wj * 16 + b * 8 + 2 * (lane & 3);
+			if (i < k) {
+				if (j < k) out[(size_t)i * k + j] = make_double2(accr[a][b][0], acci[a][b][0]);
+				if (j + 1 < k) out[(size_t)i * k + j + 1] = make_double2(accr[a][b][1], acci[a][b][1]);
+			}
+		}
+}
+
+// Sum the splits (fixed order), scale, and build the Hermitian matrix from the
+// upper triangle. One thread per (i, j) with i <= j of the full matrix.
+__global__ void overlap_finish_kernel(const double2* __restrict__ part, int k, int nsplit, double dx2,
+		double2* __restrict__ S) {
+	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= (long long)k * k) return;
+	const int i = (int)(idx / k), j = (int)(idx % k);
+	if (i > j) return;
+	double sr = 0.0, si = 0.0;
+	for (int s = 0; s < nsplit; s++) {
+		const double2 v = part[(size_t)s * k * k + idx];
+		sr += v.x;
+		si += v.y;
+	}
+	sr *= dx2;
+	si *= dx2;
+	if (i == j) {
+		S[idx] = make_double2(sr, 0.0);
+	} else {
+		S[idx] = make_double2(sr, si);
+		S[(size_t)j * k + i] = make_double2(sr, -si);
+	}
+}
+
+// Rotation: out[n][g] = sum_i W[i][n] psi[i][g]; tile 64 n x 64 g.
+template <class T>
+__global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__ W, const T* __restrict__ psi,
+		int k, long long G, T* __restrict__ out) {
+	__shared__ __align__(16) Stage st;  // a*: [n][i], b*: [g][i]
+	const int n0 = blockIdx.x * kBM;
+	const long long g0 = (long long)blockIdx.y * kBN;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int wn = warp >> 2, wg = warp & 3;
+	double accr[4][2][2], acci[4][2][2];
+#pragma unroll
+	for (int a = 0; a < 4; a++)
+#pragma unroll
+		for (int b = 0; b < 2; b++) {
+			accr[a][b][0] = accr[a][b][1] = 0.0;
+			acci[a][b][0] = acci[a][b][1] = 0.0;
+		}
+	for (int i0 = 0; i0 < k; i0 += kBK) {
+		// W tile: 16 i x 64 n, contiguous in n. 1024 elements, 4 per thread.
+#pragma unroll
+		for (int q = 0; q < 4; q++) {
+			const int e = tid + q * 256;
+			const int ii = e >> 6, nn = e & 63;
+			const int i = i0 + ii, n = n0 + nn;
+			double2 v = make_double2(0, 0);
+			if (i < k && n < k) v = W[(size_t)i * k + n];
+			st.ar[nn * kPad + ii] = v.x;
+			st.ai[nn * kPad + ii] = v.y;
+		}
+		// psi tile: 16 i x 64 g, contiguous in g.
+#pragma unroll
+		for (int q = 0; q < 4; q++) {
+			const int e = tid + q * 256;
+			const int ii = e >> 6, gg = e & 63;
+			const int i = i0 + ii;
+			const long long g = g0 + gg;
+			double2 v = make_double2(0, 0);
+			if (i < k && g < G) { const T t = psi[(long long)i * G + g]; v = make_double2(t.x, t.y); }
+			st.br[gg * kPad + ii] = v.x;
+			st.bi[gg * kPad + ii] = v.y;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int kk = 0; kk < kBK; kk += 4) {
+			double far[4], fai[4], fbr[2], fbi[2];
+#pragma unroll
+			for (int a = 0; a < 4; a++) {
+				const int r = wn * 32 + a * 8 + (lane >> 2);
+				far[a] = st.ar[r * kPad + kk + (lane & 3)];
+				fai[a] = st.ai[r * kPad + kk + (lane & 3)];
+			}
+#pragma unroll
+			for (int b = 0; b < 2; b++) {
+				const int c = wg * 16 + b * 8 + (lane >> 2);
+				fbr[b] = st.br[c * kPad + kk + (lane & 3)];
+				fbi[b] = st.bi[c * kPad + kk + (lane & 3)];
+			}
+#pragma unroll
+			for (int a = 0; a < 4; a++)
+#pragma unroll
+				for (int b = 0; b < 2; b++) {
+					// (ar + i ai)(br + i bi)
+					dmma(accr[a][b][0], accr[a][b][1], far[a], fbr[b]);
+					dmma(accr[a][b][0], accr[a][b][1], -fai[a], fbi[b]);
+					dmma(acci[a][b][0], acci[a][b][1], far[a], fbi[b]);
+					dmma(acci[a][b][0], acci[a][b][1], fai[a], fbr[b]);
+				}
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int a = 0; a < 4; a++)
+#pragma unroll
+		for (int b = 0; b < 2; b++) {
+			const int n = n0 + wn * 32 + a * 8 + (lane >> 2);
+			const long long g = g0 + wg * 16 + b * 8 + 2 * (lane & 3);
+			if (n < k) {
+				T o;
+				if (g < G) { o.x = accr[a][b][0]; o.y = acci[a][b][0]; out[(long long)n * G + g] = o; }
+				if (g + 1 < G) { o.x = accr[a][b][1]; o.y = acci[a][b][1]; out[(long long)n * G + g + 1] = o; }
+			}
+		}
+}
+
+// Norm of a single state (the N = 1 branch of stateset.cpp:138-144).
+template <class T>
+__global__ void norm1_kernel(const T* __restrict__ psi, long long G, double dx, double* out) {
+	__shared__ double red[32];
+	double s = 0.0;
+	for (long long g = threadIdx.x; g < G; g += blockDim.x) {
+		const T v = psi[g];
+		s += (double)v.x * v.x + (double)v.y * v.y;
+	}
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+		*out = sqrt(t) * dx;
+	}
+}
+
+template <class T>
+__global__ void scale1_kernel(T* psi, long long G, const double* nrm) {
+	const double f = 1.0 / *nrm;
+	for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += (long long)gridDim.x * blockDim.x) {
+		T v = psi[g];
+		v.x = v.x * f;
+		v.y = v.y * f;
+		psi[g] = v;
+	}
+}
+
+template <class TI, class TO>
+__global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, long long n) {
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+		const TI v = in[i];
+		TO o;
+		o.x = v.x;
+		o.y = v.y;
+		out[i] = o;
+	}
+}
+
+}  // namespace
+
+int overlap_tiles(int k) { return (k + kBM - 1) / kBM; }
+
+template <class T>
+void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
+		double2* part, double dx2, double2* S, cudaStream_t s) {
+	long long chunk = (G + nsplit - 1) / nsplit;
+	chunk = ((chunk + kBK - 1) / kBK) * kBK;
+	const int used = (int)((G + chunk - 1) / chunk);
+	overlap_kernel<T><<<dim3(npairs, used), 256, 0, s>>>(psi, k, G, pairs, chunk, part);
+	const long long kk = (long long)k * k;
+	overlap_finish_kernel<<<(unsigned)((kk + 255) / 256), 256, 0, s>>>(part, k, used, dx2, S);
+}
+
+template <class T>
+void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s) {
+	const dim3 grid((k + kBM - 1) / kBM, (unsigned)((G + kBN - 1) / kBN));
+	rotate_kernel<T><<<grid, 256, 0, s>>>(W, psi, k, G, out);
+}
+
+template <class T>
+void launch_normalize1(T* psi, long long G, double dx, double* tmp, cudaStream_t s) {
+	norm1_kernel<T><<<1, 1024, 0, s>>>(psi, G, dx, tmp);
+	scale1_kernel<T><<<148, 256, 0, s>>>(psi, G, tmp);
+}
+
+void launch_convert(const void* in, int in_fp64, void* out, long long n, cudaStream_t s) {
+	const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148 * 16);
+	if (in_fp64)
+		convert_kernel<double2, float2><<<blocks, 256, 0, s>>>((const double2*)in, (float2*)out, n);
+	else
+		convert_kernel<float2, double2><<<blocks, 256, 0, s>>>((const float2*)in, (double2*)out, n);
+}
+
+template void launch_overlap<double2>(const double2*, int, long long, const int2*, int, int, double2*, double,
+		double2*, cudaStream_t);
+template void launch_overlap<float2>(const float2*, int, long long, const int2*, int, int, double2*, double,
+		double2*, cudaStream_t);
+template void launch_rotate<double2>(const double2*, const double2*, int, long long, double2*, cudaStream_t);
+template void launch_rotate<float2>(const double2*, const float2*, int, long long, float2*, cudaStream_t);
+template void launch_normalize1<double2>(double2*, long long, double, double*, cudaStream_t);
+template void launch_normalize1<float2>(float2*, long long, double, double*, cudaStream_t);
+
+}  // namespace itp2d

@@ -1,0 +1,51 @@
+// Orthonormalisation contractions and eigensolver entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace itp2d {
+
+int overlap_tiles(int k);
+// T = double2 (FP64 states) or float2 (FP32 states); products and sums in FP64.
+template <class T>
+void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
+		double2* part, double dx2, double2* S, cudaStream_t s);
+template <class T>
+void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s);
+template <class T>
+void launch_normalize1(T* psi, long long G, double dx, double* tmp, cudaStream_t s);
+// Converts n complex values between double2 (in_fp64 = 1) and float2.
+void launch_convert(const void* in, int in_fp64, void* out, long long n, cudaStream_t s);
+
+// Status block written by the eigensolver (device memory).
+struct EigStatus {
+	int status;      // 0 ok, ITP2D_E_* otherwise
+	int bad_index;   // first offending eigenvalue (ascending order)
+	int sweeps;      // Jacobi sweeps used
+	int pad;
+	double bad_value;
+};
+
+struct JacobiWork {
+	double2* A0;      // k x k working matrix (input S, overwritten)
+	double2* A1;      // k x k second buffer
+	double2* V;       // k x k eigenvectors (columns)
+	double* evals;    // k
+	int* perm;        // k
+	int* counters;    // max_sweeps + 4 ints
+	int max_sweeps;
+};
+
+// Eigen-decomposition of the Hermitian S (k x k, row-major, full storage) by
+// parallel cyclic Jacobi, then W[:, n] = V[:, p(n)] / sqrt(l_n) with l
+// ascending, and the eigenvalue checks of stateset.cpp:158-173. S is
+// consumed. Returns a CUDA error code of the launches (status goes to *st).
+cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms,
+		cudaStream_t s);
+// Eigenvalues (ascending, w.evals), permutation (w.perm) and eigenvectors
+// (columns of w.V, kp x kp with kp = k rounded up to even) without the
+// overlap checks unless check != 0.
+cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
+size_t jacobi_counters(int max_sweeps);
+
+}  // namespace itp2d

@@ -1,0 +1,972 @@
+// Context and C ABI (include/itp2d_gpu.h) of the itp2d B200 hot path.
+//
+// Host-side plan building, table construction and the launch sequences of the
+// three seams. Tables are computed on the host in double precision with the
+// same formulas as the reference (ExpPotential exppotential.cpp:55-63,
+// ExpKinetic expkinetic.cpp:65-136, Kinetic kinetic.cpp:25-83, Transformer
+// k-tables and normalisations transformer.cpp:66-90) and uploaded once per
+// time step.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/itp2d_gpu.h"
+#include "common.cuh"
+#include "contract.cuh"
+#include "split.cuh"
+
+using namespace itp2d;
+
+namespace {
+
+enum Phase { kPropagate = 0, kOverlap = 1, kEigen = 2, kRotate = 3, kEnergies = 4 };
+
+struct DevBuf {
+	void* p = nullptr;
+	size_t n = 0;
+};
+
+struct MemberTables {
+	double c = 1.0;        // multi-product coefficient c_t
+	int t = 1;             // exponent (member index)
+	void* vh = nullptr;    // exp(-eps_t V / 2)
+	void* vp = nullptr;    // c_t exp(-eps_t V / 2)
+	void* vsq = nullptr;   // exp(-eps_t V)
+	void* kmul = nullptr;  // B = 0: 2-D kinetic multiplier
+	void* kx = nullptr;    // B != 0: X(k_x, y)
+	void* ky = nullptr;    // B != 0: Y(k_y)
+};
+
+struct PlanStore {
+	LinePlan lp{};
+	void* tw = nullptr;
+	void* ext = nullptr;
+	bool ready = false;
+};
+
+}  // namespace
+
+struct itp2d_ctx {
+	std::mutex mu;
+	int sx = 0, sy = 0, k = 0, boundary = 0, halforder = 1, m = 1, precision = 0;
+	double dx = 0, B = 0, eps = 0;
+	long long G = 0;
+	size_t es = 16;  // bytes per complex element
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	int num_sms = 148;
+	void* psi = nullptr;
+	void* acc = nullptr;
+	void* work = nullptr;
+	std::vector<double> V;
+	bool null_pot = true;
+	bool eps_set = false;
+	PlanStore planstore[2][2][3];  // [precision][axis x=0/y=1][kind]
+	std::vector<void*> table_allocs;  // tables in the working precision (freed on a precision switch)
+	std::vector<MemberTables> members;
+	void* eV = nullptr;     // potential in working precision (energies)
+	void* eT2 = nullptr;    // B = 0: 0.5 k^2 norm
+	void* eTx = nullptr;    // B != 0: 0.5 (k_x - B y)^2 / sx
+	void* eTy = nullptr;    // B != 0: 0.5 k_y^2 / sy
+	// orthonormalisation
+	double2* S = nullptr;
+	double2* part = nullptr;
+	double2* W = nullptr;
+	int2* pairs = nullptr;
+	int npairs = 0, nsplit = 1;
+	JacobiWork jw{};
+	EigStatus* dstat = nullptr;
+	EigStatus* hstat = nullptr;
+	double* dnorm = nullptr;
+	int last_sweeps = 0;
+	// energies
+	double* sums = nullptr;
+	double* dE = nullptr;
+	double* dsig = nullptr;
+	double* dres = nullptr;
+	double* dEi = nullptr;
+	double* dEshift = nullptr;
+	double* hbuf = nullptr;  // pinned, 4k doubles
+	long long launches = 0;
+	bool timing = false;
+	double phase_ms[5] = {0, 0, 0, 0, 0};
+	std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+	std::vector<void*> allocs;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+	if (e == cudaSuccess) return ITP2D_OK;
+	if (e == cudaErrorMemoryAllocation) return ITP2D_E_OOM;
+	return ITP2D_E_CUDA;
+}
+
+#define ITP2D_TRY(expr)                          \
+	do {                                         \
+		cudaError_t e_ = (expr);                 \
+		if (e_ != cudaSuccess) return cuda_status(e_); \
+	} while (0)
+
+bool smooth7(int n) {
+	if (n < 1) return false;
+	for (int p : {2, 3, 5, 7})
+		while (n % p == 0) n /= p;
+	return n == 1;
+}
+
+void factor(int n, FftPlan& p) {
+	p.n = n;
+	p.nstages = 0;
+	while (n > 1) {
+		int r;
+		if (n % 8 == 0) r = 8;
+		else if (n % 4 == 0) r = 4;
+		else if (n % 2 == 0) r = 2;
+		else if (n % 3 == 0) r = 3;
+		else if (n % 5 == 0) r = 5;
+		else r = 7;
+		p.radix[p.nstages++] = r;
+		n /= r;
+	}
+}
+
+template <class R>
+std::vector<c2<R>> make_twiddles(int n) {
+	std::vector<c2<R>> tw(n);
+	for (int t = 0; t < n; t++) {
+		const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
+		tw[t] = mk<R>((R)(double)cosl(a), (R)(double)(-sinl(a)));
+	}
+	return tw;
+}
+
+template <class R>
+std::vector<c2<R>> make_ext(int N) {
+	std::vector<c2<R>> e(2 * N + 1);
+	for (int m = 0; m <= 2 * N; m++) {
+		const long double a = 3.14159265358979323846264338327950288L * (long double)m / (long double)(2 * N);
+		e[m] = mk<R>((R)(double)cosl(a), (R)(double)(-sinl(a)));
+	}
+	return e;
+}
+
+void* dalloc(itp2d_ctx* c, size_t bytes, cudaError_t* err) {
+	void* p = nullptr;
+	*err = cudaMalloc(&p, bytes ? bytes : 16);
+	if (*err == cudaSuccess) c->allocs.push_back(p);
+	return p;
+}
+
+template <class R>
+int build_plan(itp2d_ctx* c, int axis, int kind) {
+	PlanStore& ps = c->planstore[c->precision][axis][kind];
+	if (ps.ready) return ITP2D_OK;
+	const int N = axis == 0 ? c->sx : c->sy;
+	const int n = kind == 0 ? N : 2 * N;
+	ps.lp.N = N;
+	ps.lp.kind = kind;
+	factor(n, ps.lp.fft);
+	cudaError_t e;
+	auto tw = make_twiddles<R>(n);
+	ps.tw = dalloc(c, tw.size() * sizeof(c2<R>), &e);
+	if (e != cudaSuccess) return cuda_status(e);
+	ITP2D_TRY(cudaMemcpy(ps.tw, tw.data(), tw.size() * sizeof(c2<R>), cudaMemcpyHostToDevice));
+	ps.lp.fft.tw = ps.tw;
+	if (kind != 0) {
+		auto ex = make_ext<R>(N);
+		ps.ext = dalloc(c, ex.size() * sizeof(c2<R>), &e);
+		if (e != cudaSuccess) return cuda_status(e);
+		ITP2D_TRY(cudaMemcpy(ps.ext, ex.data(), ex.size() * sizeof(c2<R>), cudaMemcpyHostToDevice));
+	}
+	ps.lp.ext = ps.ext;
+	ps.ready = true;
+	return ITP2D_OK;
+}
+
+int build_plans(itp2d_ctx* c, int axis, int kind) {
+	return c->precision == ITP2D_FP64 ? build_plan<double>(c, axis, kind) : build_plan<float>(c, axis, kind);
+}
+
+const LinePlan& plan(const itp2d_ctx* c, int axis, int kind) { return c->planstore[c->precision][axis][kind].lp; }
+
+// Uploads a double host table in the working precision into dst (allocating on first use).
+int upload_table(itp2d_ctx* c, void** dst, const std::vector<double>& h) {
+	const size_t n = h.size();
+	if (!*dst) {
+		const cudaError_t e = cudaMalloc(dst, n * c->es / 2);
+		if (e != cudaSuccess) {
+			*dst = nullptr;
+			return cuda_status(e);
+		}
+		c->table_allocs.push_back(*dst);
+	}
+	if (c->precision == ITP2D_FP64) {
+		ITP2D_TRY(cudaMemcpy(*dst, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+	} else {
+		std::vector<float> f(n);
+		for (size_t i = 0; i < n; i++) f[i] = (float)h[i];
+		ITP2D_TRY(cudaMemcpy(*dst, f.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+	}
+	return ITP2D_OK;
+}
+
+// Transformer k-tables and normalisations (transformer.cpp:66-90).
+struct KTables {
+	std::vector<double> kx, ky, posy;
+	double norm, normx, normy;
+};
+
+KTables ktables(const itp2d_ctx* c) {
+	KTables t;
+	const double lenx = (double)c->sx * c->dx, leny = (double)c->sy * c->dx;
+	const double mx = M_PI / lenx, my = M_PI / leny;
+	t.kx.resize(c->sx);
+	t.ky.resize(c->sy);
+	t.posy.resize(c->sy);
+	const bool per = c->boundary == ITP2D_PERIODIC;
+	for (int x = 0; x < c->sx; x++)
+		t.kx[x] = per ? (double)((x < c->sx / 2) ? x : x - c->sx) * 2 * mx : (double)(x + 1) * mx;
+	for (int y = 0; y < c->sy; y++) {
+		t.ky[y] = per ? (double)((y < c->sy / 2) ? y : y - c->sy) * 2 * my : (double)(y + 1) * my;
+		t.posy[y] = (double)(2 * y + 1 - c->sy) * 0.5 * c->dx;
+	}
+	if (per) {
+		t.norm = 1.0 / (double)(c->sx * c->sy);
+		t.normx = 1.0 / (double)c->sx;
+		t.normy = 1.0 / (double)c->sy;
+	} else {
+		t.norm = 1.0 / (double)(4 * c->sx * c->sy);
+		t.normx = 1.0 / (double)(2 * c->sx);
+		t.normy = 1.0 / (double)(2 * c->sy);
+	}
+	return t;
+}
+
+// Multi-product coefficients c_t = t^{2(m-1)} / prod_{n != t}(t^2 - n^2)
+// (multiproductsplit.cpp:49-59).
+std::vector<double> mp_coefficients(int m) {
+	std::vector<double> c(m);
+	for (int t = 1; t <= m; t++) {
+		int denom = 1;
+		for (int n = 1; n <= m; n++)
+			if (n != t) denom *= (t * t - n * n);
+		c[t - 1] = std::pow((double)t, 2 * (m - 1)) / denom;
+	}
+	return c;
+}
+
+// Exponential kinetic tables of ExpKinetic::calculate_multipliers
+// (expkinetic.cpp:65-136) for time step e, coefficient coeff, prefactor p.
+int kinetic_exp_tables(itp2d_ctx* c, MemberTables& mt, double e, double coeff, double prefactor) {
+	const KTables kt = ktables(c);
+	const int sx = c->sx, sy = c->sy;
+	if (c->B == 0) {
+		std::vector<double> mul((size_t)sx * sy);
+		const double A = coeff * e * 0.5;
+		const double p = prefactor * kt.norm;
+		for (int y = 0; y < sy; y++)
+			for (int x = 0; x < sx; x++)
+				mul[(size_t)y * sx + x] = p * std::exp(A * (kt.kx[x] * kt.kx[x] + kt.ky[y] * kt.ky[y]));
+		return upload_table(c, &mt.kmul, mul);
+	}
+	const double normfacx = std::sqrt(kt.normx);  // periodic: applied twice
+	const double z = c->B * e;
+	const double Cy = (std::fabs(z) < 1e-6) ? 1 + std::pow(z, 2) / 6 + std::pow(z, 4) / 120 : std::sinh(z) / z;
+	const double Cx = (std::fabs(z) < 1e-6) ? 0.5 - std::pow(z, 2) / 24 + std::pow(z, 4) / 240 : std::tanh(z / 2) / z;
+	const double Ax = coeff * e * 0.5 * Cx;
+	const double Ay = coeff * e * 0.5 * Cy;
+	const double px = normfacx;
+	const double py = prefactor * kt.normy;
+	std::vector<double> X((size_t)sx * sy), Y(sy);
+	for (int y = 0; y < sy; y++) {
+		const double dy = kt.posy[y];
+		Y[y] = py * std::exp(Ay * kt.ky[y] * kt.ky[y]);
+		for (int x = 0; x < sx; x++) {
+			const double q = kt.kx[x] - c->B * dy;
+			X[(size_t)y * sx + x] = px * std::exp(Ax * q * q);
+		}
+	}
+	int st = upload_table(c, &mt.kx, X);
+	if (st) return st;
+	return upload_table(c, &mt.ky, Y);
+}
+
+int potential_table(itp2d_ctx* c, void** dst, double e, double coeff, double prefactor) {
+	std::vector<double> v(c->V.size());
+	for (size_t i = 0; i < v.size(); i++) v[i] = prefactor * std::exp(e * coeff * c->V[i]);
+	return upload_table(c, dst, v);
+}
+
+// Rebuilds every table for the current eps (SecondOrderSplit members of
+// secondordersplit.cpp:21-49 inside MultiProductSplit).
+int rebuild_tables(itp2d_ctx* c) {
+	c->m = c->null_pot ? 1 : c->halforder;
+	const std::vector<double> coef = mp_coefficients(c->m);
+	if ((int)c->members.size() < c->m) c->members.resize(c->m);
+	for (int t = 1; t <= c->m; t++) {
+		MemberTables& mt = c->members[t - 1];
+		mt.t = t;
+		mt.c = coef[t - 1];
+		const double et = c->eps / (double)t;
+		int st;
+		if (c->null_pot) {
+			st = kinetic_exp_tables(c, mt, et, -1.0 * t, mt.c);
+			if (st) return st;
+			continue;
+		}
+		st = kinetic_exp_tables(c, mt, et, -1.0, 1.0);
+		if (st) return st;
+		st = potential_table(c, &mt.vh, et, -0.5, 1.0);
+		if (st) return st;
+		st = potential_table(c, &mt.vp, et, -0.5, mt.c);
+		if (st) return st;
+		if (t >= 2) {
+			st = potential_table(c, &mt.vsq, et, -1.0, 1.0);
+			if (st) return st;
+		}
+	}
+	return ITP2D_OK;
+}
+
+// Kinetic (Hamiltonian) tables of kinetic.cpp:25-83 and the potential.
+int rebuild_energy_tables(itp2d_ctx* c) {
+	const KTables kt = ktables(c);
+	const int sx = c->sx, sy = c->sy;
+	int st;
+	if (c->B == 0) {
+		std::vector<double> t2((size_t)sx * sy);
+		for (int y = 0; y < sy; y++)
+			for (int x = 0; x < sx; x++)
+				t2[(size_t)y * sx + x] = 0.5 * (kt.kx[x] * kt.kx[x] + kt.ky[y] * kt.ky[y]) * kt.norm;
+		st = upload_table(c, &c->eT2, t2);
+		if (st) return st;
+	} else {
+		std::vector<double> tx((size_t)sx * sy), ty(sy);
+		for (int y = 0; y < sy; y++) {
+			ty[y] = 0.5 * kt.ky[y] * kt.ky[y] * kt.normy;
+			for (int x = 0; x < sx; x++) {
+				const double q = kt.kx[x] - c->B * kt.posy[y];
+				tx[(size_t)y * sx + x] = 0.5 * q * q * kt.normx;
+			}
+		}
+		st = upload_table(c, &c->eTx, tx);
+		if (st) return st;
+		st = upload_table(c, &c->eTy, ty);
+		if (st) return st;
+	}
+	if (!c->null_pot) {
+		st = upload_table(c, &c->eV, c->V);
+		if (st) return st;
+	}
+	return ITP2D_OK;
+}
+
+struct PhaseTimer {
+	itp2d_ctx* c;
+	int phase;
+	cudaEvent_t a = nullptr, b = nullptr;
+	PhaseTimer(itp2d_ctx* c_, int ph) : c(c_), phase(ph) {
+		if (c->timing) {
+			cudaEventCreate(&a);
+			cudaEventCreate(&b);
+			cudaEventRecord(a, c->stream);
+		}
+	}
+	~PhaseTimer() {
+		if (c->timing) {
+			cudaEventRecord(b, c->stream);
+			c->pending.push_back({phase, {a, b}});
+		}
+	}
+};
+
+void flush_timers(itp2d_ctx* c) {
+	for (auto& p : c->pending) {
+		cudaEventSynchronize(p.second.second);
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+		c->phase_ms[p.first] += ms;
+		cudaEventDestroy(p.second.first);
+		cudaEventDestroy(p.second.second);
+	}
+	c->pending.clear();
+}
+
+int line_len(const LinePlan& lp) { return lp.kind == 0 ? lp.N : 2 * lp.N; }
+
+template <class R>
+void row_pass(itp2d_ctx* c, const LinePlan& lp, const void* in, void* out, const void* acc, const void* pre,
+		const void* mid, const void* post, int do_inv, int do_fwd) {
+	RowPassArgs a;
+	a.in = in; a.out = out; a.acc = acc;
+	a.mul_pre = pre; a.mul_mid = mid; a.mul_post = post;
+	a.do_inv = do_inv; a.do_fwd = do_fwd;
+	a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+	a.rows_per_tile = row_tile_rows(line_len(lp), sizeof(c2<R>), c->sy);
+	a.lp = lp;
+	launch_row_pass<R>(a, c->k, nullptr, c->stream);
+	c->launches++;
+}
+
+template <class R>
+void col_pass(itp2d_ctx* c, const LinePlan& lp, void* data, const void* mul2d, const void* mul1d, int mode) {
+	ColPassArgs a;
+	a.data = data; a.mul2d = mul2d; a.mul1d = mul1d; a.mode = mode;
+	a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+	a.cols_per_tile = col_tile_cols(line_len(lp), sizeof(c2<R>), c->sx);
+	a.lp = lp;
+	launch_col_pass<R>(a, c->k, nullptr, c->stream);
+	c->launches++;
+}
+
+// One SecondOrderSplit member t applied to `src`, result in `dst`, optionally
+// added to `acc` (dst may equal src or acc). Pass structure: the first row pass
+// applies V/2 and the forward x transform, each column pass the y transform
+// pair with the kinetic multiplier, each interior row pass the inverse x
+// transform, V and the forward x transform, and the last row pass the inverse
+// x transform and c_t V/2.
+template <class R>
+void apply_member(itp2d_ctx* c, const MemberTables& mt, const void* src, void* dst, const void* acc) {
+	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
+	const LinePlan& lx = plan(c, 0, kind);
+	const LinePlan& ly = plan(c, 1, kind);
+	const void* X = mt.kx;  // null for B = 0
+	const void* vfirst = c->null_pot ? nullptr : mt.vh;
+	const void* vlast = c->null_pot ? nullptr : mt.vp;
+	row_pass<R>(c, lx, src, dst, nullptr, nullptr, vfirst, X, 0, 1);
+	for (int r = 1; r <= mt.t; r++) {
+		col_pass<R>(c, ly, dst, c->B == 0 ? mt.kmul : nullptr, c->B == 0 ? nullptr : mt.ky, 0);
+		if (r < mt.t) row_pass<R>(c, lx, dst, dst, nullptr, X, mt.vsq, X, 1, 1);
+	}
+	row_pass<R>(c, lx, dst, dst, acc, X, vlast, nullptr, 1, 0);
+}
+
+// Multi-product propagation (MultiProductSplit over OperatorSum,
+// operatorsum.cpp:61-86): member 1 goes out of place into acc; each later
+// member reads the original psi and its last row pass adds into acc, so the
+// sum is formed in the reference order (m1 + m2) + m3. The last member may work
+// in place on psi because nothing reads the original afterwards.
+template <class R>
+int propagate_fused(itp2d_ctx* c) {
+	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
+	const LinePlan& lx = plan(c, 0, kind);
+	const LinePlan& ly = plan(c, 1, kind);
+	if (c->m == 1) {
+		apply_member<R>(c, c->members[0], c->psi, c->psi, nullptr);
+		return ITP2D_OK;
+	}
+	apply_member<R>(c, c->members[0], c->psi, c->acc, nullptr);
+	for (int t = 2; t <= c->m; t++) {
+		const MemberTables& mt = c->members[t - 1];
+		void* buf = (t == c->m) ? c->psi : c->work;
+		const void* X = mt.kx;
+		row_pass<R>(c, lx, c->psi, buf, nullptr, nullptr, mt.vh, X, 0, 1);
+		for (int r = 1; r <= mt.t; r++) {
+			col_pass<R>(c, ly, buf, c->B == 0 ? mt.kmul : nullptr, c->B == 0 ? nullptr : mt.ky, 0);
+			if (r < mt.t) row_pass<R>(c, lx, buf, buf, nullptr, X, mt.vsq, X, 1, 1);
+		}
+		// acc = member_t + acc
+		row_pass<R>(c, lx, buf, c->acc, c->acc, X, mt.vp, nullptr, 1, 0);
+	}
+	void* t = c->psi;
+	c->psi = c->acc;
+	c->acc = t;
+	return ITP2D_OK;
+}
+
+template <class R>
+int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
+	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
+	const LinePlan& lx = plan(c, 0, kind);
+	const LinePlan& ly = plan(c, 1, kind);
+	const void* V = c->null_pot ? nullptr : c->eV;
+	if (c->B == 0) {
+		// acc = F_x psi; acc = F_y^-1 T F_y acc; h = F_x^-1 acc + V psi
+		row_pass<R>(c, lx, c->psi, c->acc, nullptr, nullptr, nullptr, nullptr, 0, 1);
+		col_pass<R>(c, ly, c->acc, c->eT2, nullptr, 0);
+		EnergyRowArgs a;
+		a.src_t = c->acc; a.psi = c->psi; a.tmul = nullptr; a.V = V;
+		a.h_out = h_out; a.sums = want_sums ? c->sums : nullptr; a.Eshift = c->dEshift;
+		a.do_fwd = 0; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+		a.rows_per_tile = row_tile_rows(line_len(lx), sizeof(c2<R>), c->sy);
+		a.lp = lx;
+		launch_energy_row<R>(a, c->k, nullptr, c->stream);
+		c->launches++;
+		if (want_sums) {
+			const int nt = (c->sy + a.rows_per_tile - 1) / a.rows_per_tile;
+			launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->dE, c->dsig, c->dres, c->dEi,
+					c->stream);
+			c->launches++;
+		}
+		return ITP2D_OK;
+	}
+	// periodic, B != 0: acc = T_x psi + V psi; h = T_y psi + acc
+	EnergyRowArgs a;
+	a.src_t = c->psi; a.psi = c->psi; a.tmul = c->eTx; a.V = V;
+	a.h_out = c->acc; a.sums = nullptr; a.Eshift = nullptr;
+	a.do_fwd = 1; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+	a.rows_per_tile = row_tile_rows(line_len(lx), sizeof(c2<R>), c->sy);
+	a.lp = lx;
+	launch_energy_row<R>(a, c->k, nullptr, c->stream);
+	c->launches++;
+	EnergyColArgs b;
+	b.psi = c->psi; b.add_in = c->acc; b.ty = c->eTy;
+	b.h_out = h_out; b.sums = want_sums ? c->sums : nullptr; b.Eshift = c->dEshift;
+	b.sx = c->sx; b.sy = c->sy; b.G = c->G;
+	b.cols_per_tile = col_tile_cols(line_len(ly), sizeof(c2<R>), c->sx);
+	b.lp = ly;
+	launch_energy_col<R>(b, c->k, nullptr, c->stream);
+	c->launches++;
+	if (want_sums) {
+		const int nt = (c->sx + b.cols_per_tile - 1) / b.cols_per_tile;
+		launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->dE, c->dsig, c->dres, c->dEi,
+				c->stream);
+		c->launches++;
+	}
+	return ITP2D_OK;
+}
+
+template <class R>
+int transform_impl(itp2d_ctx* c, int kind_code) {
+	// axis selection and direction per enum Transform (transformer.hpp:32-34)
+	const int family = kind_code / 6;  // 0 FFT, 1 DST, 2 DCT
+	const int sub = kind_code % 6;     // 0 2-D, 1 inv 2-D, 2 x, 3 inv x, 4 y, 5 inv y
+	const bool inv = (sub & 1) != 0;
+	const bool dox = sub <= 3;
+	const bool doy = sub <= 1 || sub >= 4;
+	int st = build_plans(c, 0, family);
+	if (st) return st;
+	st = build_plans(c, 1, family);
+	if (st) return st;
+	const LinePlan& lx = plan(c, 0, family);
+	const LinePlan& ly = plan(c, 1, family);
+	if (dox) row_pass<R>(c, lx, c->psi, c->psi, nullptr, nullptr, nullptr, nullptr, inv ? 1 : 0, inv ? 0 : 1);
+	if (doy) col_pass<R>(c, ly, c->psi, nullptr, nullptr, inv ? 2 : 1);
+	return ITP2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* itp2d_status_string(int s) {
+	switch (s) {
+		case ITP2D_OK: return "ok";
+		case ITP2D_E_INVALID: return "invalid argument";
+		case ITP2D_E_CUDA: return "CUDA error";
+		case ITP2D_E_OOM: return "device out of memory";
+		case ITP2D_E_NONPOSITIVE_EIGENVALUE: return "non-positive overlap eigenvalue";
+		case ITP2D_E_NONNORMAL_EIGENVALUE: return "non-normal overlap eigenvalue";
+		case ITP2D_E_EIGENSOLVER: return "eigensolver did not converge";
+		case ITP2D_E_TIMEOUT: return "device wait timed out";
+		case ITP2D_E_UNSUPPORTED: return "unsupported configuration";
+		default: return "unknown status";
+	}
+}
+
+int itp2d_ctx_destroy(itp2d_ctx* c) {
+	if (!c) return ITP2D_E_INVALID;
+	if (c->stream) cudaStreamSynchronize(c->stream);
+	flush_timers(c);
+	for (void* p : c->allocs) cudaFree(p);
+	for (void* p : c->table_allocs) cudaFree(p);
+	if (c->hstat) cudaFreeHost(c->hstat);
+	if (c->hbuf) cudaFreeHost(c->hbuf);
+	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+	delete c;
+	return ITP2D_OK;
+}
+
+int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, double B, int halforder,
+		int precision, void* cuda_stream, itp2d_ctx** out) {
+	if (!out || sx < 2 || sy < 2 || num_states < 1 || !(dx > 0) || halforder < 1 || halforder > 8)
+		return ITP2D_E_INVALID;
+	if (boundary != ITP2D_PERIODIC && boundary != ITP2D_DIRICHLET) return ITP2D_E_INVALID;
+	if (precision != ITP2D_FP64 && precision != ITP2D_FP32) return ITP2D_E_INVALID;
+	if (!smooth7(sx) || !smooth7(sy) || sx > 4096 || sy > 4096) return ITP2D_E_UNSUPPORTED;
+	if (boundary == ITP2D_DIRICHLET && B != 0) return ITP2D_E_UNSUPPORTED;
+	*out = nullptr;
+	itp2d_ctx* c = new (std::nothrow) itp2d_ctx();
+	if (!c) return ITP2D_E_OOM;
+	c->sx = sx; c->sy = sy; c->dx = dx; c->k = num_states; c->boundary = boundary; c->B = B;
+	c->halforder = halforder; c->precision = precision;
+	c->G = (long long)sx * sy;
+	c->es = precision == ITP2D_FP64 ? 16 : 8;
+	c->V.assign((size_t)c->G, 0.0);
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
+	if (e != cudaSuccess) { delete c; return cuda_status(e); }
+	if (cuda_stream) {
+		c->stream = (cudaStream_t)cuda_stream;
+	} else {
+		e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+		if (e != cudaSuccess) { delete c; return cuda_status(e); }
+		c->own_stream = true;
+	}
+	const size_t sbytes = (size_t)c->G * c->k * c->es;
+	const int k = c->k;
+	c->psi = dalloc(c, sbytes, &e);
+	if (e == cudaSuccess) c->acc = dalloc(c, sbytes, &e);
+	if (e == cudaSuccess && halforder >= 3) c->work = dalloc(c, sbytes, &e);
+	// overlap / eigensolver buffers
+	const int nt = overlap_tiles(k);
+	c->npairs = nt * (nt + 1) / 2;
+	c->nsplit = std::max(1, std::min((4 * c->num_sms + c->npairs - 1) / c->npairs, (int)std::max(1LL, c->G / 512)));
+	const int kp = (k + 1) & ~1;
+	if (e == cudaSuccess) c->S = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
+	if (e == cudaSuccess) c->part = (double2*)dalloc(c, (size_t)c->nsplit * k * k * sizeof(double2), &e);
+	if (e == cudaSuccess) c->W = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
+	if (e == cudaSuccess) c->pairs = (int2*)dalloc(c, (size_t)c->npairs * sizeof(int2), &e);
+	c->jw.max_sweeps = 60;
+	if (e == cudaSuccess) c->jw.A0 = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
+	if (e == cudaSuccess) c->jw.A1 = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
+	if (e == cudaSuccess) c->jw.V = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
+	if (e == cudaSuccess) c->jw.evals = (double*)dalloc(c, (size_t)k * sizeof(double), &e);
+	if (e == cudaSuccess) c->jw.perm = (int*)dalloc(c, (size_t)k * sizeof(int), &e);
+	if (e == cudaSuccess) c->jw.counters = (int*)dalloc(c, jacobi_counters(c->jw.max_sweeps) * sizeof(int), &e);
+	if (e == cudaSuccess) c->dstat = (EigStatus*)dalloc(c, sizeof(EigStatus), &e);
+	if (e == cudaSuccess) c->dnorm = (double*)dalloc(c, sizeof(double), &e);
+	// energies
+	const int ntiles = std::max(sx, sy);  // upper bound of row or column tiles
+	if (e == cudaSuccess) c->sums = (double*)dalloc(c, (size_t)k * ntiles * 5 * sizeof(double), &e);
+	if (e == cudaSuccess) c->dE = (double*)dalloc(c, (size_t)5 * k * sizeof(double), &e);
+	if (e == cudaSuccess) {
+		c->dsig = c->dE + k;
+		c->dres = c->dE + 2 * k;
+		c->dEi = c->dE + 3 * k;
+		c->dEshift = c->dE + 4 * k;
+		e = cudaMemset(c->dE, 0, (size_t)5 * k * sizeof(double));
+	}
+	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hstat, sizeof(EigStatus));
+	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hbuf, (size_t)4 * k * sizeof(double));
+	if (e == cudaSuccess) {
+		std::vector<int2> pr;
+		for (int i = 0; i < nt; i++)
+			for (int j = i; j < nt; j++) pr.push_back(make_int2(i, j));
+		e = cudaMemcpy(c->pairs, pr.data(), pr.size() * sizeof(int2), cudaMemcpyHostToDevice);
+	}
+	if (e != cudaSuccess) {
+		const int st = cuda_status(e);
+		itp2d_ctx_destroy(c);
+		return st;
+	}
+	const int kind = boundary == ITP2D_PERIODIC ? 0 : 1;
+	int st = build_plans(c, 0, kind);
+	if (!st) st = build_plans(c, 1, kind);
+	if (!st) st = rebuild_energy_tables(c);  // null potential until set
+	if (st) {
+		itp2d_ctx_destroy(c);
+		return st;
+	}
+	*out = c;
+	return ITP2D_OK;
+}
+
+int itp2d_set_potential(itp2d_ctx* c, const double* V) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (V) {
+		std::memcpy(c->V.data(), V, (size_t)c->G * sizeof(double));
+		c->null_pot = false;
+	} else {
+		std::fill(c->V.begin(), c->V.end(), 0.0);
+		c->null_pot = true;
+	}
+	int st = rebuild_energy_tables(c);
+	if (st) return st;
+	if (c->eps_set) return rebuild_tables(c);
+	return ITP2D_OK;
+}
+
+int itp2d_set_time_step(itp2d_ctx* c, double eps) {
+	if (!c || !(eps > 0)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->eps = eps;
+	c->eps_set = true;
+	return rebuild_tables(c);
+}
+
+int itp2d_upload_states(itp2d_ctx* c, const double* h) {
+	if (!c || !h) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	const size_t n = (size_t)c->G * c->k;
+	if (c->precision == ITP2D_FP64) {
+		ITP2D_TRY(cudaMemcpyAsync(c->psi, h, n * 16, cudaMemcpyHostToDevice, c->stream));
+	} else {
+		std::vector<float> f(2 * n);
+		for (size_t i = 0; i < 2 * n; i++) f[i] = (float)h[i];
+		ITP2D_TRY(cudaMemcpyAsync(c->psi, f.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_download_states(itp2d_ctx* c, double* h) {
+	if (!c || !h) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	const size_t n = (size_t)c->G * c->k;
+	if (c->precision == ITP2D_FP64) {
+		ITP2D_TRY(cudaMemcpyAsync(h, c->psi, n * 16, cudaMemcpyDeviceToHost, c->stream));
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	} else {
+		std::vector<float> f(2 * n);
+		ITP2D_TRY(cudaMemcpyAsync(f.data(), c->psi, n * 8, cudaMemcpyDeviceToHost, c->stream));
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		for (size_t i = 0; i < 2 * n; i++) h[i] = f[i];
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_device_states(itp2d_ctx* c, void** p) {
+	if (!c || !p) return ITP2D_E_INVALID;
+	*p = c->psi;
+	return ITP2D_OK;
+}
+
+int itp2d_propagate(itp2d_ctx* c) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (!c->eps_set) return ITP2D_E_INVALID;
+	PhaseTimer t(c, kPropagate);
+	if (c->precision == ITP2D_FP64) propagate_fused<double>(c);
+	else propagate_fused<float>(c);
+	return cuda_status(cudaGetLastError());
+}
+
+int itp2d_energies(itp2d_ctx* c, double* E, double* sigma, double* sres, double* Eimag) {
+	if (!c || !E || !sigma) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	{
+		PhaseTimer t(c, kEnergies);
+		if (c->precision == ITP2D_FP64) energies_impl<double>(c, nullptr, true);
+		else energies_impl<float>(c, nullptr, true);
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaMemcpyAsync(c->hbuf, c->dE, (size_t)4 * c->k * sizeof(double), cudaMemcpyDeviceToHost,
+				c->stream));
+		// the current energies are the shift of the next residual evaluation
+		ITP2D_TRY(cudaMemcpyAsync(c->dEshift, c->dE, (size_t)c->k * sizeof(double), cudaMemcpyDeviceToDevice,
+				c->stream));
+	}
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	const int k = c->k;
+	std::memcpy(E, c->hbuf, k * sizeof(double));
+	std::memcpy(sigma, c->hbuf + k, k * sizeof(double));
+	if (sres) std::memcpy(sres, c->hbuf + 2 * k, k * sizeof(double));
+	if (Eimag) std::memcpy(Eimag, c->hbuf + 3 * k, k * sizeof(double));
+	return ITP2D_OK;
+}
+
+int itp2d_apply_hamiltonian(itp2d_ctx* c) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	// h is written into the second buffer, which then becomes the state array
+	// (the field path reuses acc as its intermediate; every kernel reads an
+	// element of acc before the same thread overwrites it)
+	void* h = c->acc;
+	if (c->precision == ITP2D_FP64) energies_impl<double>(c, h, false);
+	else energies_impl<float>(c, h, false);
+	void* t = c->psi;
+	c->psi = c->acc;
+	c->acc = t;
+	return cuda_status(cudaGetLastError());
+}
+
+int itp2d_transform(itp2d_ctx* c, int kind) {
+	if (!c || kind < 0 || kind > ITP2D_IDCTY) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	int st = c->precision == ITP2D_FP64 ? transform_impl<double>(c, kind) : transform_impl<float>(c, kind);
+	if (st) return st;
+	return cuda_status(cudaGetLastError());
+}
+
+int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_value) {
+	if (!c || (algo != ITP2D_ORTHO_DEFAULT && algo != ITP2D_ORTHO_HIGHMEM)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (bad_index) *bad_index = -1;
+	if (bad_value) *bad_value = 0.0;
+	const bool f64 = c->precision == ITP2D_FP64;
+	if (c->k == 1) {
+		if (f64) launch_normalize1((double2*)c->psi, c->G, c->dx, c->dnorm, c->stream);
+		else launch_normalize1((float2*)c->psi, c->G, c->dx, c->dnorm, c->stream);
+		c->launches += 2;
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		return ITP2D_OK;
+	}
+	{
+		PhaseTimer t(c, kOverlap);
+		if (f64)
+			launch_overlap((const double2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
+					c->dx * c->dx, c->S, c->stream);
+		else
+			launch_overlap((const float2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
+					c->dx * c->dx, c->S, c->stream);
+		c->launches += 2;
+	}
+	{
+		PhaseTimer t(c, kEigen);
+		ITP2D_TRY(launch_eigensolve(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
+		c->launches += 6;
+	}
+	{
+		PhaseTimer t(c, kRotate);
+		if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
+		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
+		c->launches += 1;
+	}
+	ITP2D_TRY(cudaGetLastError());
+	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	const EigStatus s = *c->hstat;
+	c->last_sweeps = s.sweeps;
+	if (s.status != ITP2D_OK) {
+		if (bad_index) *bad_index = s.bad_index;
+		if (bad_value) *bad_value = s.bad_value;
+		return s.status;
+	}
+	void* t = c->psi;
+	c->psi = c->acc;
+	c->acc = t;
+	return ITP2D_OK;
+}
+
+int itp2d_set_precision(itp2d_ctx* c, int precision) {
+	if (!c || (precision != ITP2D_FP64 && precision != ITP2D_FP32)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (precision == c->precision) return ITP2D_OK;
+	const size_t n = (size_t)c->G * c->k;
+	const size_t es_new = precision == ITP2D_FP64 ? 16 : 8;
+	void* np = nullptr;
+	ITP2D_TRY(cudaMalloc(&np, n * es_new));
+	launch_convert(c->psi, c->precision == ITP2D_FP64 ? 1 : 0, np, (long long)n, c->stream);
+	c->launches++;
+	cudaError_t e = cudaStreamSynchronize(c->stream);
+	if (e != cudaSuccess) {
+		cudaFree(np);
+		return cuda_status(e);
+	}
+	// replace the state buffers
+	auto drop = [&](void* p) {
+		if (!p) return;
+		for (auto& a : c->allocs)
+			if (a == p) a = nullptr;
+		cudaFree(p);
+	};
+	drop(c->psi);
+	drop(c->acc);
+	drop(c->work);
+	c->psi = np;
+	c->allocs.push_back(np);
+	c->acc = c->work = nullptr;
+	e = cudaMalloc(&c->acc, n * es_new);
+	if (e == cudaSuccess) c->allocs.push_back(c->acc);
+	if (e == cudaSuccess && c->halforder >= 3) {
+		e = cudaMalloc(&c->work, n * es_new);
+		if (e == cudaSuccess) c->allocs.push_back(c->work);
+	}
+	if (e != cudaSuccess) return cuda_status(e);
+	// tables in the new precision
+	for (void* p : c->table_allocs) cudaFree(p);
+	c->table_allocs.clear();
+	for (auto& m : c->members) m = MemberTables();
+	c->eV = c->eT2 = c->eTx = c->eTy = nullptr;
+	c->precision = precision;
+	c->es = es_new;
+	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
+	int st = build_plans(c, 0, kind);
+	if (!st) st = build_plans(c, 1, kind);
+	if (!st) st = rebuild_energy_tables(c);
+	if (!st && c->eps_set) st = rebuild_tables(c);
+	return st;
+}
+
+int itp2d_synchronize(itp2d_ctx* c) {
+	if (!c) return ITP2D_E_INVALID;
+	return cuda_status(cudaStreamSynchronize(c->stream));
+}
+
+long long itp2d_launch_count(itp2d_ctx* c) { return c ? c->launches : -1; }
+
+int itp2d_set_timing(itp2d_ctx* c, int enable) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->timing = enable != 0;
+	return ITP2D_OK;
+}
+
+int itp2d_phase_times(itp2d_ctx* c, double* ms5) {
+	if (!c || !ms5) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	flush_timers(c);
+	for (int i = 0; i < 5; i++) ms5[i] = c->phase_ms[i];
+	return ITP2D_OK;
+}
+
+int itp2d_last_sweeps(itp2d_ctx* c) { return c ? c->last_sweeps : -1; }
+
+int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs) {
+	if (n < 1 || !A || !evals || !evecs) return ITP2D_E_INVALID;
+	const int kp = (n + 1) & ~1;
+	std::vector<double2> S((size_t)n * n);
+	for (int i = 0; i < n; i++)
+		for (int j = i; j < n; j++) {
+			const double re = A[2 * ((size_t)j * n + i)], im = A[2 * ((size_t)j * n + i) + 1];
+			S[(size_t)i * n + j] = make_double2(re, i == j ? 0.0 : im);
+			S[(size_t)j * n + i] = make_double2(re, i == j ? 0.0 : -im);
+		}
+	int dev = 0, sms = 148;
+	ITP2D_TRY(cudaGetDevice(&dev));
+	ITP2D_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	JacobiWork w{};
+	w.max_sweeps = 60;
+	std::vector<void*> bufs;
+	auto al = [&](size_t b) -> void* {
+		void* p = nullptr;
+		if (cudaMalloc(&p, b) != cudaSuccess) return nullptr;
+		bufs.push_back(p);
+		return p;
+	};
+	double2* dS = (double2*)al(S.size() * sizeof(double2));
+	w.A0 = (double2*)al((size_t)kp * kp * sizeof(double2));
+	w.A1 = (double2*)al((size_t)kp * kp * sizeof(double2));
+	w.V = (double2*)al((size_t)kp * kp * sizeof(double2));
+	w.evals = (double*)al((size_t)n * sizeof(double));
+	w.perm = (int*)al((size_t)n * sizeof(int));
+	w.counters = (int*)al(jacobi_counters(w.max_sweeps) * sizeof(int));
+	EigStatus* dst = (EigStatus*)al(sizeof(EigStatus));
+	int status = ITP2D_OK;
+	if (!dS || !w.A0 || !w.A1 || !w.V || !w.evals || !w.perm || !w.counters || !dst) status = ITP2D_E_OOM;
+	std::vector<double2> V;
+	std::vector<int> perm(n);
+	EigStatus hs{};
+	if (status == ITP2D_OK) {
+		cudaError_t e = cudaMemcpy(dS, S.data(), S.size() * sizeof(double2), cudaMemcpyHostToDevice);
+		if (e == cudaSuccess) e = launch_eigh(dS, n, w, dst, sms, 0, 0);
+		if (e == cudaSuccess) e = cudaDeviceSynchronize();
+		V.resize((size_t)kp * kp);
+		if (e == cudaSuccess) e = cudaMemcpy(V.data(), w.V, V.size() * sizeof(double2), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess) e = cudaMemcpy(evals, w.evals, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess) e = cudaMemcpy(perm.data(), w.perm, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost);
+		if (e == cudaSuccess) e = cudaMemcpy(&hs, dst, sizeof(EigStatus), cudaMemcpyDeviceToHost);
+		status = cuda_status(e);
+		if (status == ITP2D_OK && hs.status != ITP2D_OK) status = hs.status;
+	}
+	if (status == ITP2D_OK) {
+		for (int m = 0; m < n; m++)
+			for (int i = 0; i < n; i++) {
+				const double2 v = V[(size_t)i * kp + perm[m]];
+				evecs[2 * ((size_t)m * n + i)] = v.x;
+				evecs[2 * ((size_t)m * n + i) + 1] = v.y;
+			}
+	}
+	for (void* p : bufs) cudaFree(p);
+	return status;
+}
+
+}  // extern "C"

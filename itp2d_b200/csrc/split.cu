@@ -1,0 +1,409 @@
+// Split-operator row/column passes and Hamiltonian energy passes.
+//
+// Each CTA stages one tile (a few rows, or a few columns of one state) in
+// shared memory, transforms it along x or y (fft.cuh), applies the fused
+// pointwise tables and writes it back: one HBM round trip per pass. The grid
+// is (k states, tiles) with the state index fastest so that CTAs running at the
+// same time read the same rows of the (state-independent) tables from L2.
+#include "fft.cuh"
+#include "split.cuh"
+
+#include <algorithm>
+
+namespace itp2d {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTileBytes = 32768;  // shared-memory bytes per ping-pong buffer
+
+template <class R>
+__device__ __forceinline__ void load_twiddles(c2<R>* tw, const LinePlan& lp) {
+	const c2<R>* g = reinterpret_cast<const c2<R>*>(lp.fft.tw);
+	for (int i = threadIdx.x; i < lp.fft.n; i += blockDim.x) tw[i] = g[i];
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) row_pass_kernel(RowPassArgs a) {
+	using T = c2<R>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
+	const int rows = a.rows_per_tile;
+	T* buf0 = reinterpret_cast<T*>(smem_raw);
+	T* buf1 = buf0 + rows * L;
+	T* tw = buf1 + rows * L;
+	load_twiddles<R>(tw, a.lp);
+
+	const long long state = blockIdx.x;
+	const int row0 = blockIdx.y * rows;
+	const int nrows = min(rows, a.sy - row0);
+	const int sx = a.sx;
+	const long long base = state * a.G + (long long)row0 * sx;
+	const T* in = reinterpret_cast<const T*>(a.in) + base;
+	const R* mpre = reinterpret_cast<const R*>(a.mul_pre);
+	const R* mmid = reinterpret_cast<const R*>(a.mul_mid);
+	const R* mpost = reinterpret_cast<const R*>(a.mul_post);
+	const int toff = row0 * sx;  // table offset of this tile
+	const int cnt = nrows * sx;
+
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / sx;
+		const int x = i - r * sx;
+		T v = in[i];
+		if (a.do_inv) {
+			if (mpre) v = cscale(v, mpre[toff + i]);
+		} else if (mmid) {
+			v = cscale(v, mmid[toff + i]);
+		}
+		buf0[r * L + x] = v;
+	}
+	__syncthreads();
+
+	T* cur = buf0;
+	T* oth = buf1;
+	if (a.do_inv) {
+		cur = line_transform<R, false>(buf0, buf1, a.lp, tw, nrows, 1, L, true);
+		oth = (cur == buf0) ? buf1 : buf0;
+		if (mmid) {
+			for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+				const int r = i / sx;
+				const int x = i - r * sx;
+				cur[r * L + x] = cscale(cur[r * L + x], mmid[toff + i]);
+			}
+			__syncthreads();
+		}
+	}
+	if (a.do_fwd) cur = line_transform<R, false>(cur, oth, a.lp, tw, nrows, 1, L, false);
+
+	T* out = reinterpret_cast<T*>(a.out) + base;
+	const T* acc = reinterpret_cast<const T*>(a.acc);
+	if (acc) acc += base;
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / sx;
+		const int x = i - r * sx;
+		T v = cur[r * L + x];
+		if (a.do_fwd && mpost) v = cscale(v, mpost[toff + i]);
+		if (acc) v = cadd(v, acc[i]);
+		out[i] = v;
+	}
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) col_pass_kernel(ColPassArgs a) {
+	using T = c2<R>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
+	const int C = a.cols_per_tile;
+	T* buf0 = reinterpret_cast<T*>(smem_raw);
+	T* buf1 = buf0 + L * C;
+	T* tw = buf1 + L * C;
+	load_twiddles<R>(tw, a.lp);
+
+	const long long state = blockIdx.x;
+	const int col0 = blockIdx.y * C;
+	const int ncols = min(C, a.sx - col0);
+	const int sx = a.sx, sy = a.sy;
+	T* data = reinterpret_cast<T*>(a.data) + state * a.G + col0;
+
+	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+		const int y = i / C;
+		const int c = i - y * C;
+		buf0[y * C + c] = (c < ncols) ? data[(long long)y * sx + c] : mk<R>(0, 0);
+	}
+	__syncthreads();
+
+	T* cur = buf0;
+	T* oth = buf1;
+	if (a.mode == 0 || a.mode == 1) {
+		cur = line_transform<R, true>(cur, oth, a.lp, tw, C, C, 1, false);
+		oth = (cur == buf0) ? buf1 : buf0;
+	}
+	if (a.mode == 0) {
+		const R* m2 = reinterpret_cast<const R*>(a.mul2d);
+		const R* m1 = reinterpret_cast<const R*>(a.mul1d);
+		for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+			const int y = i / C;
+			const int c = i - y * C;
+			if (c < ncols) {
+				const R f = m2 ? m2[y * sx + col0 + c] : m1[y];
+				cur[y * C + c] = cscale(cur[y * C + c], f);
+			}
+		}
+		__syncthreads();
+	}
+	if (a.mode == 0 || a.mode == 2) cur = line_transform<R, true>(cur, oth, a.lp, tw, C, C, 1, true);
+
+	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+		const int y = i / C;
+		const int c = i - y * C;
+		if (c < ncols) data[(long long)y * sx + c] = cur[y * C + c];
+	}
+}
+
+// Deterministic block reduction of NV doubles; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double* v, double* red) {
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int j = 0; j < NV; j++)
+		for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+	if (lane == 0)
+		for (int j = 0; j < NV; j++) red[warp * NV + j] = v[j];
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		const int nw = blockDim.x >> 5;
+		for (int j = 0; j < NV; j++) {
+			double s = 0.0;
+			for (int w = 0; w < nw; w++) s += red[w * NV + j];
+			v[j] = s;
+		}
+	}
+}
+
+template <class T>
+__device__ __forceinline__ void accumulate_sums(double* s, T psi, T h, double es) {
+	const double pr = psi.x, pi = psi.y, hr = h.x, hi = h.y;
+	s[0] += pr * hr + pi * hi;  // Re conj(psi) h
+	s[1] += pr * hi - pi * hr;  // Im conj(psi) h
+	s[2] += hr * hr + hi * hi;
+	const double dr = hr - es * pr, di = hi - es * pi;
+	s[3] += dr * dr + di * di;
+	s[4] += pr * pr + pi * pi;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) energy_row_kernel(EnergyRowArgs a) {
+	using T = c2<R>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
+	const int rows = a.rows_per_tile;
+	T* buf0 = reinterpret_cast<T*>(smem_raw);
+	T* buf1 = buf0 + rows * L;
+	T* tw = buf1 + rows * L;
+	double* red = reinterpret_cast<double*>(tw + a.lp.fft.n);
+	load_twiddles<R>(tw, a.lp);
+
+	const long long state = blockIdx.x;
+	const int row0 = blockIdx.y * rows;
+	const int nrows = min(rows, a.sy - row0);
+	const int sx = a.sx;
+	const long long base = state * a.G + (long long)row0 * sx;
+	const int toff = row0 * sx;
+	const int cnt = nrows * sx;
+	const T* src = reinterpret_cast<const T*>(a.src_t) + base;
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / sx;
+		buf0[r * L + (i - r * sx)] = src[i];
+	}
+	__syncthreads();
+	T* cur = buf0;
+	T* oth = buf1;
+	if (a.do_fwd) {
+		cur = line_transform<R, false>(cur, oth, a.lp, tw, nrows, 1, L, false);
+		oth = (cur == buf0) ? buf1 : buf0;
+		const R* tm = reinterpret_cast<const R*>(a.tmul);
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / sx;
+			const int x = i - r * sx;
+			cur[r * L + x] = cscale(cur[r * L + x], tm[toff + i]);
+		}
+		__syncthreads();
+	}
+	cur = line_transform<R, false>(cur, oth, a.lp, tw, nrows, 1, L, true);
+
+	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
+	const R* V = reinterpret_cast<const R*>(a.V);
+	T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
+	const double es = a.Eshift ? a.Eshift[state] : 0.0;
+	double s[5] = {0, 0, 0, 0, 0};
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / sx;
+		const int x = i - r * sx;
+		T h = cur[r * L + x];
+		const T p = psi[i];
+		if (V) {
+			const R v = V[toff + i];
+			h.x += v * p.x;
+			h.y += v * p.y;
+		}
+		if (hout) hout[i] = h;
+		if (a.sums) accumulate_sums(s, p, h, es);
+	}
+	if (a.sums) {
+		block_reduce<5>(s, red);
+		if (threadIdx.x == 0) {
+			double* o = a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5;
+			for (int j = 0; j < 5; j++) o[j] = s[j];
+		}
+	}
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) energy_col_kernel(EnergyColArgs a) {
+	using T = c2<R>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
+	const int C = a.cols_per_tile;
+	T* buf0 = reinterpret_cast<T*>(smem_raw);
+	T* buf1 = buf0 + L * C;
+	T* tw = buf1 + L * C;
+	double* red = reinterpret_cast<double*>(tw + a.lp.fft.n);
+	load_twiddles<R>(tw, a.lp);
+
+	const long long state = blockIdx.x;
+	const int col0 = blockIdx.y * C;
+	const int ncols = min(C, a.sx - col0);
+	const int sx = a.sx, sy = a.sy;
+	const long long base = state * a.G + col0;
+	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
+	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+		const int y = i / C;
+		const int c = i - y * C;
+		buf0[y * C + c] = (c < ncols) ? psi[(long long)y * sx + c] : mk<R>(0, 0);
+	}
+	__syncthreads();
+	T* cur = line_transform<R, true>(buf0, buf1, a.lp, tw, C, C, 1, false);
+	T* oth = (cur == buf0) ? buf1 : buf0;
+	const R* ty = reinterpret_cast<const R*>(a.ty);
+	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+		const int y = i / C;
+		cur[i] = cscale(cur[i], ty[y]);
+	}
+	__syncthreads();
+	cur = line_transform<R, true>(cur, oth, a.lp, tw, C, C, 1, true);
+
+	const T* add = reinterpret_cast<const T*>(a.add_in) + base;
+	T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
+	const double es = a.Eshift ? a.Eshift[state] : 0.0;
+	double s[5] = {0, 0, 0, 0, 0};
+	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+		const int y = i / C;
+		const int c = i - y * C;
+		if (c < ncols) {
+			const long long off = (long long)y * sx + c;
+			const T h = cadd(cur[i], add[off]);
+			if (hout) hout[off] = h;
+			if (a.sums) accumulate_sums(s, psi[off], h, es);
+		}
+	}
+	if (a.sums) {
+		block_reduce<5>(s, red);
+		if (threadIdx.x == 0) {
+			double* o = a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5;
+			for (int j = 0; j < 5; j++) o[j] = s[j];
+		}
+	}
+}
+
+__global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int ntiles, double dx2,
+		const double* __restrict__ Eshift, double* E, double* sigma, double* sigma_res, double* E_imag) {
+	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= k) return;
+	double s[5] = {0, 0, 0, 0, 0};
+	for (int t = lane; t < ntiles; t += 32)
+		for (int j = 0; j < 5; j++) s[j] += sums[((size_t)warp * ntiles + t) * 5 + j];
+	for (int j = 0; j < 5; j++)
+		for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+	if (lane == 0) {
+		const double er = s[0] * dx2, ei = s[1] * dx2, m2 = s[2] * dx2;
+		// sigma = Re sqrt(<H^2> - <H>^2) with complex <H> (operators.cpp:46-49)
+		const double zr = m2 - (er * er - ei * ei);
+		const double zi = -2.0 * er * ei;
+		const double az = hypot(zr, zi);
+		const double sg = sqrt(fmax(0.0, 0.5 * (az + zr)));
+		const double es = Eshift ? Eshift[warp] : 0.0;
+		const double de = er - es;
+		const double res2 = s[3] * dx2 - de * de * (s[4] * dx2);
+		E[warp] = er;
+		sigma[warp] = sg;
+		if (sigma_res) sigma_res[warp] = sqrt(fmax(0.0, res2));
+		if (E_imag) E_imag[warp] = ei;
+	}
+}
+
+template <class K>
+void set_smem_limit(K kernel) {
+	static bool done = false;
+	if (!done) {
+		cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+		done = true;
+	}
+}
+
+}  // namespace
+
+int row_tile_rows(int L, int elem_bytes, int sy) {
+	int r = kTileBytes / (elem_bytes * L);
+	r = std::max(1, std::min(r, 32));
+	return std::min(r, sy);
+}
+
+int col_tile_cols(int L, int elem_bytes, int sx) {
+	int c = kTileBytes / (elem_bytes * L);
+	c = std::max(1, std::min(c, 16));
+	return std::min(c, sx);
+}
+
+size_t row_pass_smem(int L, int rows, int n_fft, int elem_bytes) {
+	return (size_t)(2 * rows * L + n_fft) * elem_bytes + 5 * sizeof(double) * (kThreads / 32);
+}
+
+size_t col_pass_smem(int L, int cols, int n_fft, int elem_bytes) {
+	return (size_t)(2 * cols * L + n_fft) * elem_bytes + 5 * sizeof(double) * (kThreads / 32);
+}
+
+template <class R>
+void launch_row_pass(const RowPassArgs& a, int k, const void*, cudaStream_t s) {
+	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
+	const dim3 grid(k, (a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
+	const size_t sm = row_pass_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	set_smem_limit(row_pass_kernel<R>);
+	row_pass_kernel<R><<<grid, kThreads, sm, s>>>(a);
+}
+
+template <class R>
+void launch_col_pass(const ColPassArgs& a, int k, const void*, cudaStream_t s) {
+	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
+	const dim3 grid(k, (a.sx + a.cols_per_tile - 1) / a.cols_per_tile);
+	const size_t sm = col_pass_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	set_smem_limit(col_pass_kernel<R>);
+	col_pass_kernel<R><<<grid, kThreads, sm, s>>>(a);
+}
+
+template <class R>
+void launch_energy_row(const EnergyRowArgs& a, int k, const void*, cudaStream_t s) {
+	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
+	const dim3 grid(k, (a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
+	const size_t sm = row_pass_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	set_smem_limit(energy_row_kernel<R>);
+	energy_row_kernel<R><<<grid, kThreads, sm, s>>>(a);
+}
+
+template <class R>
+void launch_energy_col(const EnergyColArgs& a, int k, const void*, cudaStream_t s) {
+	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
+	const dim3 grid(k, (a.sx + a.cols_per_tile - 1) / a.cols_per_tile);
+	const size_t sm = col_pass_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	set_smem_limit(energy_col_kernel<R>);
+	energy_col_kernel<R><<<grid, kThreads, sm, s>>>(a);
+}
+
+void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift,
+		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s) {
+	const int threads = 128;
+	const int blocks = (k * 32 + threads - 1) / threads;
+	energy_finish_kernel<<<blocks, threads, 0, s>>>(sums, k, ntiles, dx2, Eshift, E, sigma, sigma_res, E_imag);
+}
+
+template void launch_row_pass<double>(const RowPassArgs&, int, const void*, cudaStream_t);
+template void launch_row_pass<float>(const RowPassArgs&, int, const void*, cudaStream_t);
+template void launch_col_pass<double>(const ColPassArgs&, int, const void*, cudaStream_t);
+template void launch_col_pass<float>(const ColPassArgs&, int, const void*, cudaStream_t);
+template void launch_energy_row<double>(const EnergyRowArgs&, int, const void*, cudaStream_t);
+template void launch_energy_row<float>(const EnergyRowArgs&, int, const void*, cudaStream_t);
+template void launch_energy_col<double>(const EnergyColArgs&, int, const void*, cudaStream_t);
+template void launch_energy_col<float>(const EnergyColArgs&, int, const void*, cudaStream_t);
+
+}  // namespace itp2d

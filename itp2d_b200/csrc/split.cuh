@@ -1,0 +1,98 @@
+// Row / column pass kernels of the split-operator propagation and of the
+// Hamiltonian used for energies.
+#pragma once
+
+#include "common.cuh"
+
+namespace itp2d {
+
+// One row pass over a k x sy x sx state array:
+//   v = in[row]
+//   if do_inv:  v = Tinv_x( mul_pre .* v )        (X table then inverse transform)
+//   v = mul_mid .* v                              (potential exponential)
+//   if do_fwd:  v = mul_post .* Tfwd_x(v)         (forward transform then X table)
+//   out[row] = v (+ acc[row])
+// Tables are [sy][sx] in the working precision; null pointers skip a multiply.
+struct RowPassArgs {
+	const void* in;
+	void* out;
+	const void* acc;
+	const void* mul_pre;
+	const void* mul_mid;
+	const void* mul_post;
+	int do_inv;
+	int do_fwd;
+	int sx, sy;
+	long long G;
+	int rows_per_tile;
+	LinePlan lp;
+};
+
+// One column pass, in place:
+//   mode 0: v = Tinv_y( mul .* Tfwd_y(v) ), mul = mul2d[y][x] or mul1d[y]
+//   mode 1: v = Tfwd_y(v)      mode 2: v = Tinv_y(v)
+struct ColPassArgs {
+	void* data;
+	const void* mul2d;
+	const void* mul1d;
+	int mode;
+	int sx, sy;
+	long long G;
+	int cols_per_tile;
+	LinePlan lp;
+};
+
+// Energy pass over rows, producing h = H psi pieces and per-tile sums.
+//   src_t: array whose rows are transformed (psi or a partially transformed
+//          scratch). if do_fwd: t = Tinv_x( tmul .* Tfwd_x(src_t) )
+//          else: t = Tinv_x(src_t) (the column pass already multiplied).
+//   h = t + V .* psi (V may be null) (+ add_in when non-null)
+//   write h to h_out when non-null; when sums is non-null accumulate
+//   <psi|h>, <h|h>, <h - Eshift psi|h - Eshift psi>, <psi|psi> per tile.
+struct EnergyRowArgs {
+	const void* src_t;
+	const void* psi;
+	const void* tmul;
+	const void* V;
+	void* h_out;
+	double* sums;  // [k][ntiles][5]
+	const double* Eshift;
+	int do_fwd;
+	int sx, sy;
+	long long G;
+	int rows_per_tile;
+	LinePlan lp;
+};
+
+// Energy pass over columns (periodic magnetic field): t = Tinv_y(ty .* Tfwd_y(psi)),
+// h = t + add_in; sums as above.
+struct EnergyColArgs {
+	const void* psi;
+	const void* add_in;
+	const void* ty;
+	void* h_out;
+	double* sums;
+	const double* Eshift;
+	int sx, sy;
+	long long G;
+	int cols_per_tile;
+	LinePlan lp;
+};
+
+template <class R> void launch_row_pass(const RowPassArgs& a, int k, const void* tw, cudaStream_t s);
+template <class R> void launch_col_pass(const ColPassArgs& a, int k, const void* tw, cudaStream_t s);
+template <class R> void launch_energy_row(const EnergyRowArgs& a, int k, const void* tw, cudaStream_t s);
+template <class R> void launch_energy_col(const EnergyColArgs& a, int k, const void* tw, cudaStream_t s);
+
+// Per-state reduction of the energy partial sums into E, sigma and the
+// residual deviation (deterministic order).
+void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift,
+		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s);
+
+// Tile sizes (rows or columns per CTA) for a line length L (complex entries).
+int row_tile_rows(int L, int elem_bytes, int sy);
+int col_tile_cols(int L, int elem_bytes, int sx);
+size_t row_pass_smem(int L, int rows, int n_fft, int elem_bytes);
+size_t col_pass_smem(int L, int cols, int n_fft, int elem_bytes);
+
+}  // namespace itp2d

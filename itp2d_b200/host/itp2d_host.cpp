@@ -1,0 +1,661 @@
+// Native host layer: Parameters, ConvergenceTest, ITPSystem over the device
+// C ABI, plus the extern "C" surface of include/itp2d_host.h.
+#include "itp2d_host.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <thread>
+
+namespace itp2d {
+
+namespace {
+
+double now_s() {
+	return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+std::string status_text(const std::string& where, int st) {
+	return where + ": " + itp2d_status_string(st);
+}
+
+std::string num(double v) {
+	std::ostringstream o;
+	o << v;
+	return o.str();
+}
+
+const char* kWhitespace = " \t\n";
+
+}  // namespace
+
+NonPositiveEigenvalue::NonPositiveEigenvalue(int n, double v)
+	: std::runtime_error("non-positive eigenvalue " + num(v) + " of the overlap matrix at index " + num(n)),
+	  index(n), value(v) {}
+
+NonNormalEigenvalue::NonNormalEigenvalue(int n, double v)
+	: std::runtime_error("non-normal eigenvalue " + num(v) + " of the overlap matrix at index " + num(n)),
+	  index(n), value(v) {}
+
+EigensolverError::EigensolverError(int status) : std::runtime_error(status_text("eigensolver", status)) {}
+
+DeviceError::DeviceError(const std::string& where, int st) : std::runtime_error(status_text(where, st)), status(st) {}
+
+std::pair<std::string, std::vector<double>> parse_parameter_string(const std::string& s) {
+	const size_t start = s.find_first_not_of(kWhitespace);
+	if (start == std::string::npos) throw ParseError(s);
+	const size_t last = s.find_last_not_of(kWhitespace);
+	size_t name_end = s.find_first_of(" \t\n(", start);
+	if (name_end == std::string::npos || name_end > last) name_end = last + 1;
+	std::pair<std::string, std::vector<double>> out(s.substr(start, name_end - start), std::vector<double>());
+	const size_t rest = s.find_first_not_of(kWhitespace, name_end);
+	if (rest == std::string::npos) return out;
+	if (s[rest] != '(' || s[last] != ')') throw ParseError(s);
+	std::string inner = s.substr(rest + 1, last - rest - 1);
+	if (inner.find_first_not_of(kWhitespace) == std::string::npos) return out;
+	std::istringstream in(inner);
+	while (true) {
+		double v;
+		in >> v;
+		if (in.fail()) throw ParseError(s);
+		out.second.push_back(v);
+		in >> std::ws;
+		if (in.eof()) break;
+		if (in.peek() != ',') throw ParseError(s);
+		in.get();
+	}
+	return out;
+}
+
+// ---------------- convergence tests (convergence.cpp) ----------------
+
+NoConvergenceTest::NoConvergenceTest(const std::vector<double>& params) {
+	if (!params.empty()) throw GeneralError("convergence test 'none' takes no parameters");
+	description = "none";
+}
+
+OneStepConvergenceTest::OneStepConvergenceTest(const std::vector<double>& params) {
+	if (!params.empty()) throw GeneralError("convergence test 'onestep' takes no parameters");
+	description = "one-step convergence";
+}
+
+bool OneStepConvergenceTest::test(const ITPSystem& sys, size_t n) const {
+	return sys.get_step_counter() == 1 && sys.is_timestep_converged(sys.get_sorted_index(n));
+}
+
+RelativeEnergyChangeTest::RelativeEnergyChangeTest(const std::vector<double>& params) {
+	if (params.size() != 1) throw GeneralError("relative energy change test takes exactly one parameter");
+	limit = params[0];
+	description = "relative energy change < " + num(limit);
+}
+
+bool RelativeEnergyChangeTest::test(const ITPSystem& sys, size_t n) const {
+	const auto& e = sys.get_energies();
+	if (e.size() < 2) return false;
+	const double a = e[e.size() - 1][n], b = e[e.size() - 2][n];
+	return std::fabs((a - b) / b) < limit;
+}
+
+AbsoluteEnergyChangeTest::AbsoluteEnergyChangeTest(const std::vector<double>& params) {
+	if (params.size() != 1) throw GeneralError("absolute energy change test takes exactly one parameter");
+	limit = params[0];
+	description = "absolute energy change < " + num(limit);
+}
+
+bool AbsoluteEnergyChangeTest::test(const ITPSystem& sys, size_t n) const {
+	const auto& e = sys.get_energies();
+	if (e.size() < 2) return false;
+	return std::fabs(e[e.size() - 1][n] - e[e.size() - 2][n]) < limit;
+}
+
+AbsoluteEnergyDeviationTest::AbsoluteEnergyDeviationTest(const std::vector<double>& params) {
+	if (params.size() != 1 && params.size() != 2)
+		throw GeneralError("absolute deviation test takes one or two parameters");
+	dev_limit = params[0];
+	diff_limit = params.size() == 2 ? params[1] : 0.0;
+	description = "absolute energy deviation < " + num(dev_limit) + " or absolute energy deviation change < " +
+	              num(diff_limit);
+}
+
+bool AbsoluteEnergyDeviationTest::test(const ITPSystem& sys, size_t n) const {
+	const auto& s = sys.get_standard_deviations();
+	if (s.size() < 2) return false;
+	const double a = s[s.size() - 1][n], b = s[s.size() - 2][n];
+	return a < dev_limit || std::fabs(a - b) < diff_limit;
+}
+
+RelativeEnergyDeviationTest::RelativeEnergyDeviationTest(const std::vector<double>& params) {
+	if (params.size() != 1 && params.size() != 2)
+		throw GeneralError("relative deviation test takes one or two parameters");
+	dev_limit = params[0];
+	diff_limit = params.size() == 2 ? params[1] : 0.0;
+	description = "relative energy deviation < " + num(dev_limit) + " or relative energy deviation change < " +
+	              num(diff_limit);
+}
+
+bool RelativeEnergyDeviationTest::test(const ITPSystem& sys, size_t n) const {
+	const auto& e = sys.get_energies();
+	const auto& s = sys.get_standard_deviations();
+	if (e.size() < 2) return false;
+	const size_t l = s.size() - 1;
+	const double a = s[l][n] / e[l][n], b = s[l - 1][n] / e[l - 1][n];
+	return a < dev_limit || std::fabs(a - b) < diff_limit;
+}
+
+std::unique_ptr<ConvergenceTest> parse_convergence_description(const std::string& str) {
+	const auto p = parse_parameter_string(str);
+	const std::string& n = p.first;
+	if (n == "none" || n == "no" || n == "null") return std::unique_ptr<ConvergenceTest>(new NoConvergenceTest(p.second));
+	if (n == "onestep" || n == "one-step")
+		return std::unique_ptr<ConvergenceTest>(new OneStepConvergenceTest(p.second));
+	if (n == "abschange" || n == "absEdelta")
+		return std::unique_ptr<ConvergenceTest>(new AbsoluteEnergyChangeTest(p.second));
+	if (n == "relchange" || n == "relEdelta")
+		return std::unique_ptr<ConvergenceTest>(new RelativeEnergyChangeTest(p.second));
+	if (n == "absstdev" || n == "absresidual")
+		return std::unique_ptr<ConvergenceTest>(new AbsoluteEnergyDeviationTest(p.second));
+	if (n == "relstdev" || n == "relresidual")
+		return std::unique_ptr<ConvergenceTest>(new RelativeEnergyDeviationTest(p.second));
+	throw GeneralError("unknown convergence test: " + str);
+}
+
+// ---------------- grid, potentials, parameters ----------------
+
+DataLayout::DataLayout(size_t sx, size_t sy, double d)
+	: sizex(sx), sizey(sy), N(sx * sy), dx(d), lenx((double)sx * d), leny((double)sy * d), posx(sx), posy(sy) {
+	for (size_t x = 0; x < sx; x++) posx[x] = (double)(2 * (long)x + 1 - (long)sx) * 0.5 * dx;
+	for (size_t y = 0; y < sy; y++) posy[y] = (double)(2 * (long)y + 1 - (long)sy) * 0.5 * dx;
+}
+
+bool evaluate_potential(const std::string& desc, const DataLayout& dl, std::vector<double>& out) {
+	const auto p = parse_parameter_string(desc);
+	const std::vector<double>& a = p.second;
+	out.assign(dl.N, 0.0);
+	if (p.first == "zero") return false;
+	auto at = [&](size_t i, double d) { return a.size() > i ? a[i] : d; };
+	for (size_t y = 0; y < dl.sizey; y++)
+		for (size_t x = 0; x < dl.sizex; x++) {
+			double v;
+			if (p.first == "harmonic") {
+				const double px = dl.posx[x] - at(1, 0.0), py = dl.posy[y] - at(2, 0.0);
+				v = 0.5 * at(0, 1.0) * (px * px + py * py);
+			} else if (p.first == "elliptic") {
+				const double px = dl.posx[x], py = dl.posy[y];
+				v = 0.5 * (at(0, 1.0) * px * px + at(1, 1.6180339887498948482) * py * py);
+			} else if (p.first == "gaussian" || p.first == "gaussianblob") {
+				const double px = dl.posx[x] - at(2, 0.0), py = dl.posy[y] - at(3, 0.0);
+				const double s = at(1, 1.0);
+				v = at(0, 1.0) * std::exp(-(px * px + py * py) / (2 * s * s));
+			} else {
+				throw GeneralError("potential type not available in this build: " + desc);
+			}
+			out[y * dl.sizex + x] = v;
+		}
+	return true;
+}
+
+Parameters::Parameters() { itp2d_parameters_default(&p); }
+
+void Parameters::define_grid(size_t sx, size_t sy, double lenx, int boundary) {
+	p.sx = (int)sx;
+	p.sy = (int)sy;
+	p.length = lenx;
+	p.boundary = boundary;
+}
+
+void Parameters::define_external_field(const std::string& ptype, double B) {
+	if (ptype.size() >= sizeof(p.potential)) throw GeneralError("potential description too long");
+	std::strcpy(p.potential, ptype.c_str());
+	p.B = B;
+}
+
+void Parameters::set_num_states(size_t N, size_t wanted, size_t ignore_lowest) {
+	if (ignore_lowest + wanted > N) throw GeneralError("wanted + ignored states exceed the number of states");
+	p.num_states = (int)N;
+	p.wanted = (int)wanted;
+	p.ignore_lowest = (int)ignore_lowest;
+}
+
+void Parameters::add_eps_value(double e) {
+	if (p.num_eps >= 16) throw GeneralError("at most 16 explicit time steps");
+	p.eps[p.num_eps++] = e;
+}
+
+void Parameters::set_bailout_limits(int max_steps, double min_time_step) {
+	p.max_steps = max_steps;
+	p.min_eps = min_time_step;
+}
+
+void Parameters::set_timestep_convergence_test(const std::string& s) {
+	parse_convergence_description(s);  // validate
+	std::strncpy(p.timestep_test, s.c_str(), sizeof(p.timestep_test) - 1);
+}
+
+void Parameters::set_final_convergence_test(const std::string& s) {
+	parse_convergence_description(s);
+	std::strncpy(p.final_test, s.c_str(), sizeof(p.final_test) - 1);
+}
+
+void Parameters::set_precision(int prec, double fp32_switch) {
+	p.precision = prec;
+	p.fp32_switch = fp32_switch;
+}
+
+// ---------------- ITPSystem ----------------
+
+ITPSystem::ITPSystem(const Parameters& params, void* stream)
+	: p(params.raw()), dl((size_t)p.sx, (size_t)p.sy, p.length / (double)p.sx), exhausting(p.exhaust_eps != 0) {
+	if (p.ignore_lowest + p.wanted > p.num_states) throw GeneralError("wanted + ignored states exceed N");
+	ts_test = parse_convergence_description(p.timestep_test);
+	final_test = parse_convergence_description(p.final_test);
+	null_potential = !evaluate_potential(p.potential, dl, V);
+	if (!params.user_potential.empty()) {
+		if (params.user_potential.size() != dl.N) throw GeneralError("user potential has the wrong size");
+		for (size_t i = 0; i < dl.N; i++) V[i] += params.user_potential[i];
+		null_potential = false;
+	}
+	for (int i = 0; i < p.num_eps; i++) eps_values.push_back(p.eps[i]);
+	if (!eps_values.empty()) {
+		eps = eps_values.front();
+		eps_values.pop_front();
+	} else {
+		eps = 0.5;  // Parameters::default_initial_eps
+	}
+	precision = p.precision;
+	check(itp2d_ctx_create(p.sx, p.sy, dl.dx, p.num_states, p.boundary, p.B, p.halforder, precision, stream, &ctx),
+			"itp2d_ctx_create");
+	check(itp2d_set_timing(ctx, 1), "itp2d_set_timing");
+	check(itp2d_set_potential(ctx, null_potential ? nullptr : V.data()), "itp2d_set_potential");
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
+	initial_states = params.initial_states;
+	if (!initial_states.empty() && initial_states.size() != 2 * dl.N * (size_t)p.num_states)
+		throw GeneralError("initial states have the wrong size");
+	rng_state = p.seed;
+	timestep_converged.assign(p.num_states, false);
+	finally_converged.assign(p.num_states, false);
+	init_states();
+}
+
+ITPSystem::~ITPSystem() {
+	if (ctx) itp2d_ctx_destroy(ctx);
+}
+
+void ITPSystem::check(int st, const char* where) {
+	if (st != ITP2D_OK) throw DeviceError(where, st);
+}
+
+// Complex standard-normal noise per grid point, normalised per state
+// (StateSet::init_to_gaussian_noise, stateset.cpp:124-131). The stream is a
+// counter-based hash (splitmix64) with Box-Muller, so it does not depend on
+// the number of host threads. Re-initialisation after a failed
+// orthonormalisation draws a fresh stream.
+void ITPSystem::init_states() {
+	if (!initial_states.empty()) {
+		check(itp2d_upload_states(ctx, initial_states.data()), "itp2d_upload_states");
+		initial_states.clear();  // a recovery re-randomises like the reference
+		return;
+	}
+	const size_t k = (size_t)p.num_states, G = dl.N;
+	std::vector<double> psi(2 * k * G);
+	const unsigned long base = rng_state;
+	rng_state = rng_state * 6364136223846793005ULL + 1442695040888963407ULL;
+	auto mix = [](unsigned long long z) {
+		z += 0x9E3779B97F4A7C15ULL;
+		z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+		z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+		return z ^ (z >> 31);
+	};
+	const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+	std::vector<std::thread> th;
+	for (unsigned t = 0; t < nth; t++)
+		th.emplace_back([&, t]() {
+			for (size_t n = t; n < k; n += nth) {
+				double* s = psi.data() + 2 * n * G;
+				double nrm = 0.0;
+				for (size_t i = 0; i < G; i++) {
+					const unsigned long long c = ((unsigned long long)base << 20) ^ (n * G + i);
+					const unsigned long long a = mix(2 * c), b = mix(2 * c + 1);
+					const double u1 = ((a >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+					const double u2 = (b >> 11) * (1.0 / 9007199254740992.0);
+					const double r = std::sqrt(-2.0 * std::log(u1));
+					s[2 * i] = r * std::cos(2 * M_PI * u2);
+					s[2 * i + 1] = r * std::sin(2 * M_PI * u2);
+					nrm += s[2 * i] * s[2 * i] + s[2 * i + 1] * s[2 * i + 1];
+				}
+				const double f = 1.0 / (std::sqrt(nrm) * dl.dx);
+				for (size_t i = 0; i < 2 * G; i++) s[i] *= f;
+			}
+		});
+	for (auto& x : th) x.join();
+	check(itp2d_upload_states(ctx, psi.data()), "itp2d_upload_states");
+}
+
+void ITPSystem::propagate() {
+	const double t0 = now_s();
+	check(itp2d_propagate(ctx), "itp2d_propagate");
+	t_prop += now_s() - t0;
+}
+
+void ITPSystem::orthonormalize() {
+	const double t0 = now_s();
+	int bi = -1;
+	double bv = 0;
+	const int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
+	t_ortho += now_s() - t0;
+	if (st == ITP2D_OK) return;
+	if (st == ITP2D_E_NONPOSITIVE_EIGENVALUE) {
+		// itpsystem.cpp:264-281: shrink eps and restart from noise, or stop.
+		error_text = NonPositiveEigenvalue(bi, bv).what();
+		if (p.recover) {
+			change_time_step();
+			init_states();
+		} else {
+			error_flag = true;
+			finish();
+		}
+		return;
+	}
+	if (st == ITP2D_E_NONNORMAL_EIGENVALUE) error_text = NonNormalEigenvalue(bi, bv).what();
+	else if (st == ITP2D_E_EIGENSOLVER) error_text = EigensolverError(st).what();
+	else error_text = status_text("itp2d_orthonormalize", st);
+	error_flag = true;
+	finish();
+}
+
+void ITPSystem::calculate_energies() {
+	if (total_step_counter == 0) return;
+	const double t0 = now_s();
+	const size_t k = (size_t)p.num_states;
+	std::vector<double> E(k), s(k), r(k);
+	check(itp2d_energies(ctx, E.data(), s.data(), r.data(), nullptr), "itp2d_energies");
+	sorted.resize(k);
+	for (size_t n = 0; n < k; n++) sorted[n] = Esn(std::make_pair(E[n], s[n]), n);
+	std::sort(sorted.begin(), sorted.end());
+	if (energies.size() < (size_t)total_step_counter) {
+		energies.resize(total_step_counter);
+		deviations.resize(total_step_counter);
+	}
+	std::vector<double>& ne = energies[total_step_counter - 1];
+	std::vector<double>& nd = deviations[total_step_counter - 1];
+	ne.resize(k);
+	nd.resize(k);
+	residuals.resize(k);
+	for (size_t n = 0; n < k; n++) {
+		ne[n] = sorted[n].first.first;
+		nd[n] = sorted[n].first.second;
+		residuals[n] = r[sorted[n].second];
+	}
+	t_conv += now_s() - t0;
+}
+
+void ITPSystem::check_timestep_convergence() {
+	const double t0 = now_s();
+	for (size_t n = 0; n < (size_t)p.num_states; n++)
+		if (ts_test->test(*this, n)) timestep_converged[sorted[n].second] = true;
+	bool flag = true;
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
+		if (!timestep_converged[sorted[n].second]) flag = false;
+	all_timestep_converged = flag;
+	t_conv += now_s() - t0;
+}
+
+void ITPSystem::check_final_convergence() {
+	const double t0 = now_s();
+	for (size_t n = 0; n < (size_t)p.num_states; n++) finally_converged[sorted[n].second] = final_test->test(*this, n);
+	bool flag = true;
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
+		if (!finally_converged[sorted[n].second]) flag = false;
+	all_finally_converged = flag;
+	t_conv += now_s() - t0;
+}
+
+size_t ITPSystem::how_many_finally_converged() const {
+	return (size_t)std::count(finally_converged.begin(), finally_converged.end(), true);
+}
+
+size_t ITPSystem::how_many_timestep_converged() const {
+	return (size_t)std::count(timestep_converged.begin(), timestep_converged.end(), true);
+}
+
+// itpsystem.cpp:202-233
+void ITPSystem::change_time_step() {
+	if (!eps_values.empty()) {
+		eps = eps_values.front();
+		eps_values.pop_front();
+		if (eps_values.empty()) exhausting = false;
+	} else {
+		eps /= p.eps_divisor;
+	}
+	if (eps < p.min_eps) {
+		error_text = "minimum time step reached";
+		error_flag = true;
+		finish();
+		return;
+	}
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
+	step_counter = 0;
+	all_timestep_converged = false;
+	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
+}
+
+// FP32 form: once every wanted state's energy changes by less than the switch
+// threshold per step (the FP32 sweep floor), continue in FP64, which refines
+// the eigenpairs to the FP64 fixed point.
+void ITPSystem::maybe_switch_precision() {
+	if (precision != ITP2D_FP32 || !(p.fp32_switch > 0) || energies.size() < 2) return;
+	const auto& a = energies[energies.size() - 1];
+	const auto& b = energies[energies.size() - 2];
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
+		if (!(std::fabs(a[n] - b[n]) < p.fp32_switch)) return;
+	check(itp2d_set_precision(ctx, ITP2D_FP64), "itp2d_set_precision");
+	precision = ITP2D_FP64;
+	step_counter = 0;
+	all_timestep_converged = false;
+	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
+}
+
+// itpsystem.cpp:407-470
+void ITPSystem::step() {
+	if (finished) return;
+	if (total_step_counter == 0) t_start = now_s();
+	if (total_step_counter >= p.max_steps) {
+		error_text = "maximum number of total steps reached";
+		error_flag = true;
+		finish();
+		return;
+	}
+	step_counter++;
+	total_step_counter++;
+	propagate();
+	orthonormalize();
+	calculate_energies();
+	if (finished) return;
+	const bool was_fp32 = precision == ITP2D_FP32;
+	maybe_switch_precision();
+	if (was_fp32) return;  // convergence tests run on the FP64 refinement
+	check_timestep_convergence();
+	if (all_timestep_converged) {
+		check_final_convergence();
+		if (all_finally_converged) {
+			finish();
+			return;
+		}
+		change_time_step();
+	} else if (exhausting) {
+		change_time_step();
+	}
+}
+
+void ITPSystem::finish() {
+	if (finished) return;
+	finished = true;
+	if (total_step_counter > 0) t_total = now_s() - t_start;
+}
+
+void ITPSystem::download_states(double* out) { check(itp2d_download_states(ctx, out), "itp2d_download_states"); }
+
+void ITPSystem::times(double* t) {
+	double ms[5];
+	check(itp2d_phase_times(ctx, ms), "itp2d_phase_times");
+	t[0] = finished ? t_total : (total_step_counter > 0 ? now_s() - t_start : 0.0);
+	t[1] = t_prop;
+	t[2] = t_ortho;
+	t[3] = ms[1] * 1e-3;
+	t[4] = ms[2] * 1e-3;
+	t[5] = ms[3] * 1e-3;
+	t[6] = t_conv;
+}
+
+}  // namespace itp2d
+
+// ---------------- C ABI (include/itp2d_host.h) ----------------
+
+struct itp2d_system {
+	itp2d::ITPSystem* sys = nullptr;
+	std::string err;
+};
+
+extern "C" {
+
+void itp2d_parameters_default(itp2d_parameters* p) {
+	std::memset(p, 0, sizeof(*p));
+	p->sx = p->sy = 64;
+	p->length = 12;
+	p->boundary = ITP2D_PERIODIC;
+	p->B = 0;
+	p->halforder = 5;
+	p->num_states = 25;
+	p->wanted = 16;
+	p->ignore_lowest = 0;
+	p->num_eps = 0;
+	p->eps_divisor = 5.0;
+	p->exhaust_eps = 0;
+	p->max_steps = 50;
+	p->min_eps = 1e-9;
+	p->seed = 0x20120131UL;
+	p->ortho_algorithm = ITP2D_ORTHO_DEFAULT;
+	p->recover = 0;
+	p->precision = ITP2D_FP64;
+	p->fp32_switch = 0.0;
+	std::strcpy(p->potential, "harmonic");
+	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
+	std::strcpy(p->final_test, "relstdev(1e-3,0)");
+}
+
+int itp2d_system_create(const itp2d_parameters* p, const double* extra, const double* init, void* stream,
+		itp2d_system** out) {
+	if (!p || !out) return ITP2D_E_INVALID;
+	*out = nullptr;
+	itp2d_system* s = new itp2d_system();
+	try {
+		itp2d::Parameters P;
+		P.raw() = *p;
+		const size_t G = (size_t)p->sx * (size_t)p->sy;
+		if (extra) P.user_potential.assign(extra, extra + G);
+		if (init) P.initial_states.assign(init, init + 2 * G * (size_t)p->num_states);
+		s->sys = new itp2d::ITPSystem(P, stream);
+	} catch (itp2d::DeviceError& e) {
+		const int st = e.status;
+		delete s;
+		return st;
+	} catch (std::exception&) {
+		delete s;
+		return ITP2D_E_INVALID;
+	}
+	*out = s;
+	return ITP2D_OK;
+}
+
+int itp2d_system_destroy(itp2d_system* s) {
+	if (!s) return ITP2D_E_INVALID;
+	delete s->sys;
+	delete s;
+	return ITP2D_OK;
+}
+
+int itp2d_system_step(itp2d_system* s) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	try {
+		s->sys->step();
+	} catch (itp2d::DeviceError& e) {
+		s->err = e.what();
+		return e.status;
+	} catch (std::exception& e) {
+		s->err = e.what();
+		return ITP2D_E_INVALID;
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_system_run(itp2d_system* s, int max_iterations) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	for (int i = 0; i < max_iterations && !s->sys->is_finished(); i++) {
+		const int st = itp2d_system_step(s);
+		if (st != ITP2D_OK) return st;
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_system_is_finished(const itp2d_system* s) { return s && s->sys && s->sys->is_finished() ? 1 : 0; }
+int itp2d_system_error_flag(const itp2d_system* s) { return s && s->sys && s->sys->get_error_flag() ? 1 : 0; }
+int itp2d_system_total_steps(const itp2d_system* s) { return s && s->sys ? s->sys->get_total_step_counter() : -1; }
+int itp2d_system_num_converged(const itp2d_system* s) {
+	return s && s->sys ? (int)s->sys->how_many_finally_converged() : -1;
+}
+double itp2d_system_eps(const itp2d_system* s) { return s && s->sys ? s->sys->get_eps() : 0.0; }
+int itp2d_system_in_fp32(const itp2d_system* s) { return s && s->sys && s->sys->in_fp32() ? 1 : 0; }
+
+int itp2d_system_energies(const itp2d_system* s, double* E, double* sigma, double* residual, int* index) {
+	if (!s || !s->sys) return -1;
+	const auto& e = s->sys->get_energies();
+	if (e.empty()) return 0;
+	const auto& d = s->sys->get_standard_deviations();
+	const size_t k = e.back().size();
+	for (size_t n = 0; n < k; n++) {
+		if (E) E[n] = e.back()[n];
+		if (sigma) sigma[n] = d.back()[n];
+		if (residual) residual[n] = s->sys->get_residuals()[n];
+		if (index) index[n] = (int)s->sys->get_sorted_index(n);
+	}
+	return (int)k;
+}
+
+int itp2d_system_energy_history(const itp2d_system* s, int step, double* E) {
+	if (!s || !s->sys) return -1;
+	const auto& e = s->sys->get_energies();
+	if (step < 0 || (size_t)step >= e.size()) return 0;
+	std::copy(e[step].begin(), e[step].end(), E);
+	return (int)e[step].size();
+}
+
+int itp2d_system_download_states(itp2d_system* s, double* out) {
+	if (!s || !s->sys || !out) return ITP2D_E_INVALID;
+	try {
+		s->sys->download_states(out);
+	} catch (itp2d::DeviceError& e) {
+		return e.status;
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_system_times(itp2d_system* s, double* t7) {
+	if (!s || !s->sys || !t7) return ITP2D_E_INVALID;
+	try {
+		s->sys->times(t7);
+	} catch (itp2d::DeviceError& e) {
+		return e.status;
+	}
+	return ITP2D_OK;
+}
+
+const char* itp2d_system_last_error(const itp2d_system* s) {
+	if (!s) return "";
+	if (!s->err.empty()) return s->err.c_str();
+	return s->sys ? s->sys->last_error().c_str() : "";
+}
+
+itp2d_ctx* itp2d_system_context(itp2d_system* s) { return s && s->sys ? s->sys->context() : nullptr; }
+
+}  // extern "C"

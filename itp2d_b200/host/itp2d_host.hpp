@@ -1,0 +1,222 @@
+// Native host layer of the itp2d B200 hot path: the reference's driver-level
+// API (Parameters, ConvergenceTest, ITPSystem) over the device C ABI
+// (include/itp2d_gpu.h). Only the three seams run on the device; the step
+// logic, time-step schedule, sorting and convergence tests stay on the host
+// exactly as in itpsystem.cpp:202-511 and convergence.cpp:28-199.
+#pragma once
+
+#include <list>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/itp2d_gpu.h"
+#include "../../include/itp2d_host.h"
+
+namespace itp2d {
+
+// Exceptions carrying the reference's meaning (exceptions.hpp:37-254).
+class GeneralError : public std::runtime_error {
+  public:
+	explicit GeneralError(const std::string& w) : std::runtime_error(w) {}
+};
+class ParseError : public std::runtime_error {
+  public:
+	explicit ParseError(const std::string& s) : std::runtime_error("could not parse parameter string: " + s) {}
+};
+class NonPositiveEigenvalue : public std::runtime_error {
+  public:
+	NonPositiveEigenvalue(int n, double v);
+	int index;
+	double value;
+};
+class NonNormalEigenvalue : public std::runtime_error {
+  public:
+	NonNormalEigenvalue(int n, double v);
+	int index;
+	double value;
+};
+class EigensolverError : public std::runtime_error {
+  public:
+	explicit EigensolverError(int status);
+};
+class DeviceError : public std::runtime_error {
+  public:
+	DeviceError(const std::string& where, int status);
+	int status;
+};
+
+// name(v1,v2,...) mini-language of parser.cpp:26-60.
+std::pair<std::string, std::vector<double>> parse_parameter_string(const std::string& s);
+
+class ITPSystem;
+
+// convergence.hpp:32-130
+class ConvergenceTest {
+  public:
+	virtual ~ConvergenceTest() {}
+	virtual bool test(const ITPSystem& sys, size_t n) const = 0;
+	const std::string& get_description() const { return description; }
+
+  protected:
+	std::string description;
+};
+
+class NoConvergenceTest : public ConvergenceTest {
+  public:
+	explicit NoConvergenceTest(const std::vector<double>& params);
+	bool test(const ITPSystem&, size_t) const override { return false; }
+};
+
+class OneStepConvergenceTest : public ConvergenceTest {
+  public:
+	explicit OneStepConvergenceTest(const std::vector<double>& params);
+	bool test(const ITPSystem& sys, size_t n) const override;
+};
+
+class RelativeEnergyChangeTest : public ConvergenceTest {
+  public:
+	explicit RelativeEnergyChangeTest(const std::vector<double>& params);
+	bool test(const ITPSystem& sys, size_t n) const override;
+
+  private:
+	double limit;
+};
+
+class AbsoluteEnergyChangeTest : public ConvergenceTest {
+  public:
+	explicit AbsoluteEnergyChangeTest(const std::vector<double>& params);
+	bool test(const ITPSystem& sys, size_t n) const override;
+
+  private:
+	double limit;
+};
+
+class AbsoluteEnergyDeviationTest : public ConvergenceTest {
+  public:
+	explicit AbsoluteEnergyDeviationTest(const std::vector<double>& params);
+	bool test(const ITPSystem& sys, size_t n) const override;
+
+  private:
+	double dev_limit, diff_limit;
+};
+
+class RelativeEnergyDeviationTest : public ConvergenceTest {
+  public:
+	explicit RelativeEnergyDeviationTest(const std::vector<double>& params);
+	bool test(const ITPSystem& sys, size_t n) const override;
+
+  private:
+	double dev_limit, diff_limit;
+};
+
+std::unique_ptr<ConvergenceTest> parse_convergence_description(const std::string& s);
+
+// The cell-centred grid of datalayout.cpp:21-36.
+struct DataLayout {
+	DataLayout(size_t sx, size_t sy, double dx);
+	size_t sizex, sizey, N;
+	double dx, lenx, leny;
+	std::vector<double> posx, posy;
+};
+
+// Potentials of potentialtypes.hpp that the hot-path configurations use:
+// "zero", "harmonic(A[,x0,y0])", "elliptic(Ax,Ay)", "gaussian(A,sigma[,x0,y0])".
+// Returns false for the null potential.
+bool evaluate_potential(const std::string& desc, const DataLayout& dl, std::vector<double>& out);
+
+class Parameters {
+  public:
+	Parameters();
+	void set_recover(bool v) { p.recover = v; }
+	void set_random_seed(unsigned long s) { p.seed = s; }
+	void define_grid(size_t sx, size_t sy, double lenx, int boundary = ITP2D_PERIODIC);
+	void define_external_field(const std::string& ptype, double B = 0);
+	void set_num_states(size_t N, size_t wanted, size_t ignore_lowest = 0);
+	void set_operator_splitting_halforder(int h) { p.halforder = h; }
+	void add_eps_value(double e);
+	void set_time_step_divisor(double d) { p.eps_divisor = d; }
+	void set_exhaust_eps(bool v) { p.exhaust_eps = v; }
+	void set_bailout_limits(int max_steps, double min_time_step);
+	void set_ortho_algorithm(int a) { p.ortho_algorithm = a; }
+	void set_timestep_convergence_test(const std::string& s);
+	void set_final_convergence_test(const std::string& s);
+	void set_precision(int prec, double fp32_switch = 1e-7);
+	void set_user_potential(const std::vector<double>& v) { user_potential = v; }
+	void set_initial_states(const std::vector<double>& v) { initial_states = v; }
+	const itp2d_parameters& raw() const { return p; }
+	itp2d_parameters& raw() { return p; }
+	std::vector<double> user_potential;   // added to the potential (the user noise hook)
+	std::vector<double> initial_states;   // k*sy*sx interleaved complex, empty = random
+
+  private:
+	itp2d_parameters p;
+};
+
+class ITPSystem {
+  public:
+	typedef std::pair<std::pair<double, double>, size_t> Esn;  // ((E, sigma), storage index)
+	ITPSystem(const Parameters& params, void* cuda_stream = nullptr);
+	~ITPSystem();
+	ITPSystem(const ITPSystem&) = delete;
+	ITPSystem& operator=(const ITPSystem&) = delete;
+
+	void step();
+	void finish();
+	bool is_finished() const { return finished; }
+	bool get_error_flag() const { return error_flag; }
+	int get_total_step_counter() const { return total_step_counter; }
+	int get_step_counter() const { return step_counter; }
+	double get_eps() const { return eps; }
+	bool in_fp32() const { return precision == ITP2D_FP32; }
+	size_t how_many_finally_converged() const;
+	size_t how_many_timestep_converged() const;
+	bool is_timestep_converged(size_t index) const { return timestep_converged[index]; }
+	const std::vector<std::vector<double>>& get_energies() const { return energies; }
+	const std::vector<std::vector<double>>& get_standard_deviations() const { return deviations; }
+	double get_sorted_energy(size_t n) const { return sorted[n].first.first; }
+	size_t get_sorted_index(size_t n) const { return sorted[n].second; }
+	const std::vector<double>& get_residuals() const { return residuals; }
+	const std::string& last_error() const { return error_text; }
+	itp2d_ctx* context() { return ctx; }
+	void download_states(double* out);
+	void times(double* t7);
+	const itp2d_parameters p;
+
+  private:
+	void propagate();
+	void orthonormalize();
+	void calculate_energies();
+	void check_timestep_convergence();
+	void check_final_convergence();
+	void change_time_step();
+	void init_states();
+	void maybe_switch_precision();
+	void check(int status, const char* where);
+
+	DataLayout dl;
+	std::unique_ptr<ConvergenceTest> ts_test, final_test;
+	std::vector<double> V;
+	bool null_potential = true;
+	std::vector<double> initial_states;
+	itp2d_ctx* ctx = nullptr;
+	int precision = ITP2D_FP64;
+	bool finished = false, error_flag = false;
+	bool all_timestep_converged = false, all_finally_converged = false;
+	bool exhausting;
+	int total_step_counter = 0, step_counter = 0;
+	double eps = 0;
+	std::list<double> eps_values;
+	std::vector<Esn> sorted;
+	std::vector<std::vector<double>> energies, deviations;
+	std::vector<double> residuals;
+	std::vector<bool> timestep_converged, finally_converged;
+	unsigned long rng_state;
+	double t_total = 0, t_prop = 0, t_ortho = 0, t_conv = 0;
+	double t_start = 0;
+	std::string error_text;
+};
+
+}  // namespace itp2d

@@ -1,0 +1,206 @@
+"""ctypes binding of the native ITP driver (include/itp2d_host.h).
+
+``ITPSystem(Parameters(...))`` mirrors the reference ITPSystem
+(itpsystem.hpp:55-156): ``step()`` until ``finished``, then the sorted
+energies. All work runs in libitp2d_b200.so; there is no Python fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("sx", C.c_int), ("sy", C.c_int), ("length", C.c_double), ("boundary", C.c_int), ("B", C.c_double),
+        ("halforder", C.c_int), ("num_states", C.c_int), ("wanted", C.c_int), ("ignore_lowest", C.c_int),
+        ("num_eps", C.c_int), ("eps", C.c_double * 16), ("eps_divisor", C.c_double), ("exhaust_eps", C.c_int),
+        ("max_steps", C.c_int), ("min_eps", C.c_double), ("seed", C.c_ulong), ("ortho_algorithm", C.c_int),
+        ("recover", C.c_int), ("precision", C.c_int), ("fp32_switch", C.c_double),
+        ("potential", C.c_char * 128), ("timestep_test", C.c_char * 128), ("final_test", C.c_char * 128),
+    ]
+
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = capi.lib()
+    if not _bound:
+        vp, i, d, dp, ip = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.itp2d_parameters_default.argtypes = [C.POINTER(_Params)]
+        L.itp2d_system_create.argtypes = [C.POINTER(_Params), dp, dp, vp, C.POINTER(vp)]
+        for n in ["itp2d_system_destroy", "itp2d_system_step"]:
+            getattr(L, n).argtypes = [vp]
+        L.itp2d_system_run.argtypes = [vp, i]
+        for n in ["itp2d_system_is_finished", "itp2d_system_error_flag", "itp2d_system_total_steps",
+                  "itp2d_system_num_converged", "itp2d_system_in_fp32"]:
+            getattr(L, n).argtypes = [vp]
+            getattr(L, n).restype = i
+        L.itp2d_system_eps.argtypes = [vp]
+        L.itp2d_system_eps.restype = d
+        L.itp2d_system_energies.argtypes = [vp, dp, dp, dp, ip]
+        L.itp2d_system_energy_history.argtypes = [vp, i, dp]
+        L.itp2d_system_download_states.argtypes = [vp, dp]
+        L.itp2d_system_times.argtypes = [vp, dp]
+        L.itp2d_system_last_error.argtypes = [vp]
+        L.itp2d_system_last_error.restype = C.c_char_p
+        L.itp2d_system_context.argtypes = [vp]
+        L.itp2d_system_context.restype = vp
+        _bound = True
+    return L
+
+
+@dataclass
+class Parameters:
+    """Mirror of the reference Parameters (parameters.hpp:37-211), with the
+    reference defaults (parameters.cpp:25-55)."""
+    sx: int = 64
+    sy: int = 64
+    length: float = 12.0
+    boundary: int = capi.PERIODIC
+    B: float = 0.0
+    halforder: int = 5
+    num_states: int = 25
+    wanted: int = 16
+    ignore_lowest: int = 0
+    eps: list = field(default_factory=list)
+    eps_divisor: float = 5.0
+    exhaust_eps: bool = False
+    max_steps: int = 50
+    min_eps: float = 1e-9
+    seed: int = 0x20120131
+    ortho_algorithm: int = capi.ORTHO_DEFAULT
+    recover: bool = False
+    precision: int = capi.FP64
+    fp32_switch: float = 0.0
+    potential: str = "harmonic"
+    timestep_test: str = "relstdev(1e-3,1e-4)"
+    final_test: str = "relstdev(1e-3,0)"
+
+    def _raw(self) -> _Params:
+        p = _Params()
+        _lib().itp2d_parameters_default(C.byref(p))
+        for k in ["sx", "sy", "length", "boundary", "B", "halforder", "num_states", "wanted", "ignore_lowest",
+                  "eps_divisor", "max_steps", "min_eps", "seed", "ortho_algorithm", "precision", "fp32_switch"]:
+            setattr(p, k, getattr(self, k))
+        p.exhaust_eps, p.recover = int(self.exhaust_eps), int(self.recover)
+        if len(self.eps) > 16:
+            raise ValueError("at most 16 explicit time steps")
+        p.num_eps = len(self.eps)
+        for i, e in enumerate(self.eps):
+            p.eps[i] = e
+        p.potential, p.timestep_test, p.final_test = (self.potential.encode(), self.timestep_test.encode(),
+                                                      self.final_test.encode())
+        return p
+
+
+class ITPSystem:
+    def __init__(self, params: Parameters, extra_potential=None, init_states=None, stream=None):
+        self.params = params
+        self.k = params.num_states
+        self._raw = params._raw()
+        G = params.sx * params.sy
+        ep = ip = None
+        self._keep = []
+        if extra_potential is not None:
+            a = np.ascontiguousarray(extra_potential, dtype=np.float64).reshape(-1)
+            assert a.size == G
+            self._keep.append(a)
+            ep = a.ctypes.data_as(C.POINTER(C.c_double))
+        if init_states is not None:
+            b = np.ascontiguousarray(init_states, dtype=np.complex128)
+            assert b.shape == (self.k, params.sy, params.sx)
+            self._keep.append(b)
+            ip = b.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))
+        h = C.c_void_p()
+        st = _lib().itp2d_system_create(C.byref(self._raw), ep, ip, C.c_void_p(stream) if stream else None,
+                                        C.byref(h))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_create")
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().itp2d_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self):
+        st = _lib().itp2d_system_step(self.h)
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_step: " + self.last_error)
+
+    def run(self, max_iterations=1 << 30):
+        st = _lib().itp2d_system_run(self.h, int(max_iterations))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_run: " + self.last_error)
+
+    @property
+    def finished(self) -> bool:
+        return bool(_lib().itp2d_system_is_finished(self.h))
+
+    @property
+    def error_flag(self) -> bool:
+        return bool(_lib().itp2d_system_error_flag(self.h))
+
+    @property
+    def total_steps(self) -> int:
+        return _lib().itp2d_system_total_steps(self.h)
+
+    @property
+    def num_converged(self) -> int:
+        return _lib().itp2d_system_num_converged(self.h)
+
+    @property
+    def eps(self) -> float:
+        return _lib().itp2d_system_eps(self.h)
+
+    @property
+    def in_fp32(self) -> bool:
+        return bool(_lib().itp2d_system_in_fp32(self.h))
+
+    @property
+    def last_error(self) -> str:
+        return _lib().itp2d_system_last_error(self.h).decode()
+
+    def energies(self):
+        E, s, r = np.empty(self.k), np.empty(self.k), np.empty(self.k)
+        idx = np.empty(self.k, dtype=np.int32)
+        n = _lib().itp2d_system_energies(self.h, E.ctypes.data_as(C.POINTER(C.c_double)),
+                                         s.ctypes.data_as(C.POINTER(C.c_double)),
+                                         r.ctypes.data_as(C.POINTER(C.c_double)),
+                                         idx.ctypes.data_as(C.POINTER(C.c_int)))
+        return E[:n], s[:n], r[:n], idx[:n]
+
+    def energy_history(self, step: int):
+        E = np.empty(self.k)
+        n = _lib().itp2d_system_energy_history(self.h, step, E.ctypes.data_as(C.POINTER(C.c_double)))
+        return E[:n]
+
+    def states(self):
+        out = np.empty((self.k, self.params.sy, self.params.sx), dtype=np.complex128)
+        st = _lib().itp2d_system_download_states(self.h, out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_download_states")
+        return out
+
+    def times(self) -> dict:
+        t = np.zeros(7)
+        _lib().itp2d_system_times(self.h, t.ctypes.data_as(C.POINTER(C.c_double)))
+        return dict(zip(["total", "propagation", "orthonormalization", "dot", "eigensolve", "lincomb",
+                         "convtest"], t.tolist()))
+
+    def context_handle(self) -> int:
+        return _lib().itp2d_system_context(self.h)
