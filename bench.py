@@ -1,0 +1,380 @@
+"""Benchmark: converged states per second of the itp2d imaginary-time solve on
+B200, mixed (FP32 sweeps + FP64 refinement) and plain FP64 forms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the magnetic quantum dot): V = r^2/2, B = 1 (linear gauge), periodic
+256 x 256 grid of side 14, k = 500 states from seeded complex Gaussian noise,
+4th-order multi-product split (halforder 2) at eps = 0.05, canonical
+orthonormalisation every step. A solve runs ITP iterations until the 250
+lowest states change their energy by less than 1e-9 between iterations
+(the reference's abschange(1e-9) as timestep and final test). One benchmark
+step is one such solve from the same initial states; "converged states" are
+the states passing the final test (for the mixed form, only those whose
+energy also agrees with the plain FP64 solve within 1e-9).
+
+Multi-GPU (torchrun): independent replicas, one solve per rank (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Converged states/s at |ΔE|≤1e-9, mixed vs plain FP64 (1 B200); p50/p99 solve latency"
+UNIT = "converged states/s"
+WORKLOAD = dict(sx=256, sy=256, length=14.0, B=1.0, halforder=2, num_states=500, wanted=250, eps=0.05,
+                potential="harmonic(1)", test="abschange(1e-9)", seed=20240601)
+# Solve length and converged count of the plain FP64 form on the initial states above
+# (measured by this benchmark's own FP64 solve and re-checked every run); used only to
+# extrapolate the reference CPU arm, which times a bounded sample of iterations.
+FP64_SOLVE_STEPS = 33
+FP64_CONVERGED = 285
+
+
+def initial_states(pinned=True):
+    """Seeded complex Gaussian noise normalised per state (as init_to_gaussian_noise)."""
+    w = WORKLOAD
+    rng = np.random.default_rng(w["seed"])
+    dx = w["length"] / w["sx"]
+    k, sy, sx = w["num_states"], w["sy"], w["sx"]
+    psi = np.empty((k, sy, sx), dtype=np.complex128)
+    for n in range(k):
+        a = rng.standard_normal((sy, sx)) + 1j * rng.standard_normal((sy, sx))
+        psi[n] = a / (np.sqrt(np.sum(np.abs(a) ** 2)) * dx)
+    if pinned:
+        import torch
+        t = torch.empty(psi.size * 2, dtype=torch.float64, pin_memory=True)
+        buf = t.numpy().view(np.complex128).reshape(psi.shape)
+        buf[...] = psi
+        return buf, t
+    return psi, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.dev = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.dev), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def params(form: str):
+    from itp2d_b200 import capi, system
+    w = WORKLOAD
+    return system.Parameters(sx=w["sx"], sy=w["sy"], length=w["length"], B=w["B"], halforder=w["halforder"],
+                             num_states=w["num_states"], wanted=w["wanted"], eps=[w["eps"]],
+                             timestep_test=w["test"], final_test=w["test"], max_steps=5000,
+                             potential=w["potential"],
+                             precision=capi.FP32 if form == "mixed" else capi.FP64,
+                             fp32_switch=1e-6 if form == "mixed" else 0.0)
+
+
+def alg_bytes_split(w, b):
+    """Algorithmic bytes of one propagation step: k G b [2 m(m+2) + (m-1)]."""
+    m, G = w["halforder"], w["sx"] * w["sy"]
+    return w["num_states"] * G * b * (2 * m * (m + 2) + (m - 1))
+
+
+def run_form(form, psi, K, W, torch, stream, e2e_buf):
+    """W warm-up solves, K timed solves (inputs resident), K end-to-end solves."""
+    from itp2d_b200 import capi, system
+    w = WORKLOAD
+    k = w["num_states"]
+    s = system.ITPSystem(params(form), init_states=psi, stream=stream.cuda_stream)
+    ctx = s.context_handle()
+    L = capi.lib()
+    ms = np.zeros(5)
+
+    def phases():
+        L.itp2d_phase_times(ctx, ms.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
+        return ms.copy()
+
+    for _ in range(W):
+        s.reset(psi)
+        s.run()
+    torch.cuda.synchronize()
+    # timed: inputs resident in HBM (the reset that uploads them is outside)
+    times, steps, conv, lat = [], [], [], []
+    p0, l0 = phases(), L.itp2d_launch_count(ctx)
+    for _ in range(K):
+        s.reset(psi)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.run()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = ev0.elapsed_time(ev1) * 1e-3
+        times.append(t)
+        steps.append(s.total_steps)
+        conv.append(s.num_converged)
+        assert not s.error_flag, s.last_error
+    p1, l1 = phases(), L.itp2d_launch_count(ctx)
+    E, sig, res, idx = s.energies()
+    # end to end: host inputs copied in, energies and states copied out, per solve
+    e2e_times = []
+    Eh = np.empty(k)
+    for _ in range(K):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.reset(psi)           # H2D of the initial states from pinned memory
+        s.run()
+        Eh[:] = s.energies()[0]
+        L.itp2d_system_download_states(s.h, e2e_buf.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    return dict(times=times, steps=steps, conv=conv, phases_ms=(p1 - p0) / K, launches=(l1 - l0) / K,
+                E=E, converged_mask=None, e2e_times=e2e_times, system=s)
+
+
+def cpu_reference_sample(psi, iters=1, threads=None):
+    """The itp2d reference (oracle/_ref) timed on the host cores for `iters`
+    ITP iterations of the workload; returns seconds per iteration."""
+    from oracle import refkit as R
+    w = WORKLOAD
+    if not R.available():
+        return None
+    threads = threads or os.cpu_count() or 1
+    ref = R.RefSystem(w["sx"], w["sy"], w["length"], 0, w["B"], w["halforder"], w["num_states"], w["wanted"],
+                      [w["eps"]], eps_divisor=5.0, timestep_test=w["test"], final_test=w["test"],
+                      potential=w["potential"], init_states=psi, threads=threads, highmem=False)
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        ref.step()
+    dt = (time.perf_counter() - t0) / iters
+    ph = ref.times()
+    ref.close()
+    return dict(sec_per_iter=dt, threads=threads, phases=ph)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    psi, _ = initial_states(pinned=False)
+    from oracle import refkit as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libitp2d_ref.so not built"}))
+        return
+    for _ in range(args.warmup):
+        cpu_reference_sample(psi, 1)
+    samples = [cpu_reference_sample(psi, 1)["sec_per_iter"] for _ in range(args.steps)]
+    t_iter = statistics.mean(samples)
+    v = FP64_CONVERGED / (FP64_SOLVE_STEPS * t_iter)
+    cores = os.cpu_count()
+    sample = (f"{args.steps} single ITP iterations (propagate + orthonormalise + energies) of the workload, "
+              f"{t_iter:.2f} s each; converged states/s extrapolated as {FP64_CONVERGED} converged states over "
+              f"{FP64_SOLVE_STEPS} iterations of the same algorithm")
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_iter * FP64_SOLVE_STEPS * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": config_block("reference CPU (OpenMP, OpenBLAS ZGEMM/ZHEEV, substitute FFT)"),
+           "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def config_block(form):
+    w = WORKLOAD
+    return {"workload": f"magnetic dot: V=r^2/2, B={w['B']}, periodic {w['sx']}x{w['sy']}, L={w['length']}, "
+                        f"k={w['num_states']} states, 4th-order multi-product split, eps={w['eps']}, "
+                        f"solve until the {w['wanted']} lowest pass {w['test']}",
+            "form": form, "global_batch": w["num_states"], "grid": [w["sx"], w["sy"]],
+            "parallelism": "replicas", "l2": "inputs (524 MB of states) exceed the 126 MB L2"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-iters", type=int, default=1)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from itp2d_b200 import capi
+    capi.lib()
+    stream = torch.cuda.Stream()
+    psi, pin = initial_states(pinned=True)
+    w = WORKLOAD
+    k, G = w["num_states"], w["sx"] * w["sy"]
+    e2e_buf = np.empty(2 * k * G)
+    import torch as _t
+    e2e_pin = _t.empty(2 * k * G, dtype=_t.float64, pin_memory=True)
+    e2e_buf = e2e_pin.numpy()
+    fp64_peak = capi.device_fp64_peak()
+
+    results = {}
+    with torch.cuda.stream(stream):
+        with ClockSampler(local) as clk:
+            if dist:
+                dist.barrier()
+            for form in ["fp64", "mixed"]:
+                results[form] = run_form(form, psi, args.steps, args.warmup, torch, stream, e2e_buf)
+            if dist:
+                dist.barrier()
+    clocks = clk.summary()
+
+    r64, rmx = results["fp64"], results["mixed"]
+    # mixed converged states: pass the final test and agree with FP64 within 1e-9
+    E64, Emx = r64["E"], rmx["E"]
+    agree = int(np.sum(np.abs(Emx - E64) <= 1e-9))
+    conv_mx = min(rmx["conv"][-1], agree)
+
+    def agg(r, conv):
+        t = max(r["times"]) if dist is None else None
+        tsum = sum(r["times"])
+        if dist:
+            tt = torch.tensor([tsum], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tsum = float(tt.item())
+        n = len(r["times"])
+        per_solve = tsum / n
+        return conv * world / per_solve, per_solve
+
+    v64, s64 = agg(r64, r64["conv"][-1])
+    vmx, smx = agg(rmx, conv_mx)
+    head = "mixed" if vmx >= v64 else "fp64"
+    value, per_solve = (vmx, smx) if head == "mixed" else (v64, s64)
+    rh = results[head]
+    conv_h = conv_mx if head == "mixed" else r64["conv"][-1]
+
+    # roofline of the dominant phase (per-solve device times)
+    ph = rh["phases_ms"]
+    names = ["propagate", "overlap", "eigensolve", "rotation", "energies"]
+    nsteps = statistics.mean(rh["steps"])
+    hbm = None
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        peak_src = "measured"
+    except Exception:
+        hbm, peak_src = 6650.0, "fallback"
+    b = 16  # plain FP64 bytes per complex (the mixed form's FP32 share is reported per phase)
+    roof = {}
+    alg = {
+        "propagate": ("hbm", alg_bytes_split(w, b) * nsteps / 1e9, "GB"),
+        "energies": ("hbm", 5 * k * G * b * nsteps / 1e9, "GB"),
+        "overlap": ("tensor", 4 * k * k * G * nsteps / 1e12, "TFLOP"),
+        "rotation": ("tensor", 8 * k * k * G * nsteps / 1e12, "TFLOP"),
+        "eigensolve": ("tensor", 10 * k ** 3 * nsteps / 1e12, "TFLOP"),
+    }
+    for i, n in enumerate(names):
+        bound, amount, u = alg[n]
+        sec = ph[i] * 1e-3
+        ach = amount / sec if sec > 0 else 0.0
+        peak = hbm if bound == "hbm" else fp64_peak
+        unit = "GB/s" if bound == "hbm" else "TFLOP/s"
+        roof[n] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
+                   "frac": ach / peak if peak else None, "ms_per_solve": ph[i]}
+    dom = max(names, key=lambda n: roof[n]["ms_per_solve"])
+    roofline = dict(roof[dom])
+    roofline.update({"kernel": dom, "traffic": None,
+                     "peak_source": peak_src if roof[dom]["bound"] == "hbm" else "FP64 DMMA measured in-run"})
+
+    cpu = None
+    if rank == 0:
+        cs = cpu_reference_sample(np.ascontiguousarray(psi), args.cpu_iters)
+        if cs:
+            cpu = {"value": FP64_CONVERGED / (FP64_SOLVE_STEPS * cs["sec_per_iter"]), "unit": UNIT,
+                   "cores": cs["threads"], "kind": "reference",
+                   "sample": f"{args.cpu_iters} ITP iteration(s) of the workload with the reference compiled "
+                             f"from its sources (substitute FFT, OpenBLAS, default orthonormalisation), "
+                             f"{cs['sec_per_iter']:.2f} s/iteration, "
+                             f"extrapolated over {FP64_SOLVE_STEPS} iterations / {FP64_CONVERGED} converged states"}
+
+    e2e_solve = statistics.mean(rh["e2e_times"])
+    h2d = k * G * 16
+    d2h = k * G * 16 + 3 * k * 8
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+        "config": config_block(head),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": conv_h * world / e2e_solve, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(rh["launches"] * args.steps),
+        "clocks": clocks,
+        "forms": {
+            "fp64": {"value": v64, "converged": r64["conv"][-1], "iterations": r64["steps"][-1],
+                     "sec_per_solve": s64},
+            "mixed": {"value": vmx, "converged": conv_mx, "iterations": rmx["steps"][-1], "sec_per_solve": smx,
+                      "max_abs_dE_vs_fp64_wanted": float(np.max(np.abs(Emx[:w["wanted"]] - E64[:w["wanted"]])))},
+        },
+        "latency_s": {"p50": statistics.median(rh["times"]), "p99": max(rh["times"])},
+        "phases": roof,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

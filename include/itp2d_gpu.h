@@ -157,6 +157,11 @@ int itp2d_last_sweeps(itp2d_ctx* ctx);
  * memory; runs on the default stream. */
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs);
 
+/* Measures the FP64 tensor-core (DMMA) throughput of the current device in
+ * TFLOP/s with a register-only kernel: the roofline denominator of the FP64
+ * contractions. Diagnostic; no reference counterpart. */
+int itp2d_device_fp64_peak(double* tflops);
+
 /* Short description of a status code. */
 const char* itp2d_status_string(int status);
 

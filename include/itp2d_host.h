@@ -56,6 +56,11 @@ int itp2d_system_create(const itp2d_parameters* p, const double* extra_potential
 		void* cuda_stream, itp2d_system** out);
 int itp2d_system_destroy(itp2d_system* s);
 
+/* Restarts the solve from new initial states (NULL: fresh seeded noise) with
+ * the parameters' first time step, precision and empty histories, reusing
+ * every device allocation. */
+int itp2d_system_reset(itp2d_system* s, const double* init_states);
+
 /* One ITP iteration, ITPSystem::step (itpsystem.cpp:407-470). */
 int itp2d_system_step(itp2d_system* s);
 /* step() until finished or max_iterations more iterations were taken;

@@ -70,6 +70,7 @@ def lib():
         L.itp2d_phase_times.argtypes = [vp, dp]
         L.itp2d_last_sweeps.argtypes = [vp]
         L.itp2d_hermitian_eigensolve.argtypes = [i, dp, dp, dp]
+        L.itp2d_device_fp64_peak.argtypes = [dp]
         L.itp2d_status_string.argtypes = [i]
         L.itp2d_status_string.restype = C.c_char_p
         _lib = L
@@ -83,6 +84,13 @@ def _dp(a):
 def _check(st, what):
     if st != OK:
         raise ITP2DError(st, what)
+
+
+def device_fp64_peak() -> float:
+    """Measured FP64 DMMA TFLOP/s of the current device."""
+    t = C.c_double(0.0)
+    _check(lib().itp2d_device_fp64_peak(C.byref(t)), "itp2d_device_fp64_peak")
+    return t.value
 
 
 def hermitian_eigensolve(A: np.ndarray):

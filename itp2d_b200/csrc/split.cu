@@ -9,6 +9,8 @@
 #include "split.cuh"
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 
 namespace itp2d {
 
@@ -323,13 +325,15 @@ __global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int
 	}
 }
 
+// Opts a kernel into the full 227 KB of dynamic shared memory once per
+// kernel (keyed by its address: float and double instantiations share a type).
 template <class K>
 void set_smem_limit(K kernel) {
-	static bool done = false;
-	if (!done) {
+	static std::mutex mu;
+	static std::set<const void*> done;
+	std::lock_guard<std::mutex> g(mu);
+	if (done.insert((const void*)kernel).second)
 		cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-		done = true;
-	}
 }
 
 }  // namespace

@@ -494,6 +494,36 @@ void ITPSystem::finish() {
 	if (total_step_counter > 0) t_total = now_s() - t_start;
 }
 
+void ITPSystem::reset(const double* init) {
+	finished = error_flag = false;
+	all_timestep_converged = all_finally_converged = false;
+	exhausting = p.exhaust_eps != 0;
+	total_step_counter = step_counter = 0;
+	t_total = t_prop = t_ortho = t_conv = 0;
+	energies.clear();
+	deviations.clear();
+	sorted.clear();
+	residuals.clear();
+	error_text.clear();
+	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
+	std::fill(finally_converged.begin(), finally_converged.end(), false);
+	eps_values.clear();
+	for (int i = 0; i < p.num_eps; i++) eps_values.push_back(p.eps[i]);
+	if (!eps_values.empty()) {
+		eps = eps_values.front();
+		eps_values.pop_front();
+	} else {
+		eps = 0.5;
+	}
+	if (precision != p.precision) {
+		check(itp2d_set_precision(ctx, p.precision), "itp2d_set_precision");
+		precision = p.precision;
+	}
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
+	if (init) initial_states.assign(init, init + 2 * dl.N * (size_t)p.num_states);
+	init_states();
+}
+
 void ITPSystem::download_states(double* out) { check(itp2d_download_states(ctx, out), "itp2d_download_states"); }
 
 void ITPSystem::times(double* t) {
@@ -572,6 +602,20 @@ int itp2d_system_destroy(itp2d_system* s) {
 	if (!s) return ITP2D_E_INVALID;
 	delete s->sys;
 	delete s;
+	return ITP2D_OK;
+}
+
+int itp2d_system_reset(itp2d_system* s, const double* init) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	try {
+		s->sys->reset(init);
+	} catch (itp2d::DeviceError& e) {
+		s->err = e.what();
+		return e.status;
+	} catch (std::exception& e) {
+		s->err = e.what();
+		return ITP2D_E_INVALID;
+	}
 	return ITP2D_OK;
 }
 

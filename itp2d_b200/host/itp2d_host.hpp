@@ -165,6 +165,7 @@ class ITPSystem {
 
 	void step();
 	void finish();
+	void reset(const double* init_states);
 	bool is_finished() const { return finished; }
 	bool get_error_flag() const { return error_flag; }
 	int get_total_step_counter() const { return total_step_counter; }

@@ -38,6 +38,7 @@ def _lib():
         for n in ["itp2d_system_destroy", "itp2d_system_step"]:
             getattr(L, n).argtypes = [vp]
         L.itp2d_system_run.argtypes = [vp, i]
+        L.itp2d_system_reset.argtypes = [vp, dp]
         for n in ["itp2d_system_is_finished", "itp2d_system_error_flag", "itp2d_system_total_steps",
                   "itp2d_system_num_converged", "itp2d_system_in_fp32"]:
             getattr(L, n).argtypes = [vp]
@@ -136,6 +137,17 @@ class ITPSystem:
             self.close()
         except Exception:
             pass
+
+    def reset(self, init_states=None):
+        """Restart from new initial states (None: fresh noise), reusing device memory."""
+        ip = None
+        if init_states is not None:
+            b = np.ascontiguousarray(init_states, dtype=np.complex128)
+            assert b.shape == (self.k, self.params.sy, self.params.sx)
+            ip = b.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))
+        st = _lib().itp2d_system_reset(self.h, ip)
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_reset: " + self.last_error)
 
     def step(self):
         st = _lib().itp2d_system_step(self.h)

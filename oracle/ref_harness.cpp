@@ -303,7 +303,11 @@ void refsys_get_states(void* h, double* out) {
 /* Phase seconds: total, propagation, ortho, dot, eigensolve, lincomb, convtest. */
 void refsys_times(void* h, double* t) {
 	ITPSystem* sys = static_cast<Sys*>(h)->sys;
-	t[0] = sys->get_total_time();
+	try {
+		t[0] = sys->get_total_time();
+	} catch (std::exception&) {
+		t[0] = -1.0;  // Timer::get_time throws while the total timer still runs
+	}
 	t[1] = sys->get_prop_time();
 	t[2] = sys->get_ortho_time();
 	t[3] = sys->get_dot_time();

@@ -24,6 +24,11 @@ def available() -> bool:
 def lib():
     global _lib
     if _lib is None:
+        # The bundled OpenBLAS is a pthreads build; the reference calls it from
+        # inside OpenMP loops, so keep BLAS single-threaded (must be set before
+        # the library initialises) and let the reference's OpenMP loops use
+        # the cores.
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
         if not available():
             raise FileNotFoundError(f"{LIB_PATH} not built (run: make -C oracle)")
         L = C.CDLL(LIB_PATH)
