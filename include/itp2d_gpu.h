@@ -157,6 +157,22 @@ int itp2d_last_sweeps(itp2d_ctx* ctx);
  * memory; runs on the default stream. */
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs);
 
+/* Largest n accepted by itp2d_hermitian_eigensolve_noalloc. */
+#define ITP2D_NOALLOC_MAX_N 128
+
+/* The same eigen-decomposition as itp2d_hermitian_eigensolve (same
+ * arguments, layouts and results), for callers that cannot allocate memory:
+ * applications whose memory manager owns the whole device, or loops that
+ * cannot afford the synchronisation of cudaMalloc/cudaFree. It allocates
+ * nothing; its temporaries live in one fixed device array of this library
+ * (about 1.6 MB, resident on every GPU that loads the library until exit).
+ * n above ITP2D_NOALLOC_MAX_N returns ITP2D_E_INVALID. All calls share that
+ * array, so calls that overlap on the GPU race: serialise them. The first
+ * call on a device looks up the array's address for that device; make it
+ * before any stream capture begins. Runs on the default stream.
+ * No counterpart in the reference. */
+int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double* evals, double* evecs);
+
 /* Measures the FP64 tensor-core (DMMA) throughput of the current device in
  * TFLOP/s with a register-only kernel: the roofline denominator of the FP64
  * contractions. Diagnostic; no reference counterpart. */
