@@ -1,0 +1,378 @@
+// Block Jacobi eigensolver for the overlap matrix at large k.
+//
+// Same decomposition as the scalar kernel in jacobi.cu (and the same output
+// conventions), organised for fewer grid-wide rounds: the padded index range
+// is cut into blocks of BS, blocks are paired round-robin (k/BS - 1 rounds per
+// sweep), and each round has two phases separated by grid barriers:
+//   1. one CTA per block pair sweeps the 2BS x 2BS Hermitian subproblem in
+//      shared memory with cyclic Jacobi (CTA barriers only), leaving its
+//      2BS x 2BS unitary Q in global memory and the rotated subproblem in
+//      the output matrix;
+//   2. every other 2BS x 2BS block of A becomes Q_r^H A_rc Q_c and every slab
+//      of 2BS rows of V becomes V Q_c, both as FP64 DMMA products staged in shared
+//      memory (three MS x MS complex operands).
+// Each round gives every subproblem one inner sweep (block Jacobi with a
+// single inner sweep); a rotation is applied when |A_pq| > tol sqrt(|A_pp A_qq|).
+// Rotations whose relative off-diagonal |A_pq| / sqrt(|A_pp A_qq|) is at the
+// rounding level of the phase-2 products (below 1e-13) do not count against
+// convergence; the iteration stops after a sweep whose largest counted
+// rotation tangent is below 1e-10 (or that counted none).
+#include <cooperative_groups.h>
+
+#include "../../include/itp2d_gpu.h"
+#include "contract.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace itp2d {
+
+namespace {
+
+constexpr int BS = 16;        // block size
+constexpr int MS = 32;        // subproblem size: two blocks
+constexpr int NR = MS / 2;    // rotations per inner round
+constexpr int LD = MS + 4;    // padded row length (doubles): conflict-free DMMA fragments
+constexpr int PL = MS * LD;   // doubles per plane
+constexpr int kThreads = 256;
+constexpr int kInnerMaxSweeps = 30;
+constexpr double kTauFinal = 1e-10;
+constexpr double kNoiseRel = 1e-13;  // relative off-diagonal treated as rounding noise
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+			: "+d"(d0), "+d"(d1)
+			: "d"(a), "d"(b));
+}
+
+// Round-robin pairing of npos positions (circle method): position 0 fixed.
+__device__ __forceinline__ int rr_player(int pos, int r, int npos) {
+	return pos == 0 ? 0 : ((pos - 1 + r) % (npos - 1)) + 1;
+}
+
+// Global index of local subproblem index i (< 64) for the block pair (P, Q).
+__device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * BS + i : Q * BS + (i - BS); }
+
+struct Shared {
+	double pl[6][PL];                            // planes: [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
+	double rc[NR], rs[NR], rer[NR], rei[NR], rap[NR], raq[NR];
+	int rp[NR], rq[NR], rrot[NR];
+	int cnt;                                     // rotations in the current inner sweep
+	int total;                                   // rotations of this CTA in the current outer sweep
+	unsigned long long tmax;                     // largest tangent (bits of a non-negative double)
+};
+
+// Rotation of the local pair (p, q) of the subproblem in planes (mr, mi).
+__device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
+	const double* mr = sh.pl[0];
+	const double* mi = sh.pl[1];
+	const double a = mr[p * LD + p], b = mr[q * LD + q];
+	const double cr = mr[p * LD + q], ci = mi[p * LD + q];
+	const double cabs = sqrt(cr * cr + ci * ci);
+	const double scale = sqrt(fabs(a) * fabs(b));
+	sh.rp[j] = p;
+	sh.rq[j] = q;
+	sh.rrot[j] = 0;
+	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
+	if (cabs > 0.0 && cabs > tol * scale) {
+		// tan of the smaller angle: t = |c| / (|d| + sqrt(d^2 + |c|^2)), d = (b - a) / 2
+		const double d = 0.5 * (b - a);
+		const double t = cabs / (fabs(d) + sqrt(d * d + cabs * cabs));
+		if (t != 0.0) {
+			const double st = d < 0 ? -t : t;
+			const double c = 1.0 / sqrt(t * t + 1.0);
+			const double ic = 1.0 / cabs;
+			sh.rc[j] = c;
+			sh.rs[j] = st * c;
+			sh.rer[j] = cr * ic;
+			sh.rei[j] = ci * ic;
+			sh.rap[j] = a - st * cabs;
+			sh.raq[j] = b + st * cabs;
+			sh.rrot[j] = 1;
+			if (cabs > kNoiseRel * scale) {
+				atomicAdd(&sh.cnt, 1);
+				atomicMax(&sh.tmax, (unsigned long long)__double_as_longlong(t));
+			}
+		}
+	}
+}
+
+// Rows p, q of J^H X with J = [[c, s e], [-s conj(e), c]] (correction form).
+__device__ __forceinline__ void rows2(double c, double s, double er, double ei, double& xpr, double& xpi,
+		double& xqr, double& xqi) {
+	const double tau = s / (1.0 + c);
+	// yp = xp - s (e xq + tau xp)
+	const double ypr = xpr - s * (er * xqr - ei * xqi + tau * xpr);
+	const double ypi = xpi - s * (er * xqi + ei * xqr + tau * xpi);
+	// yq = xq + s (conj(e) xp - tau xq)
+	const double yqr = xqr + s * (er * xpr + ei * xpi - tau * xqr);
+	const double yqi = xqi + s * (er * xpi - ei * xpr - tau * xqi);
+	xpr = ypr; xpi = ypi; xqr = yqr; xqi = yqi;
+}
+
+// Columns s, t of X J (correction form).
+__device__ __forceinline__ void cols2(double c, double s, double er, double ei, double& xsr, double& xsi,
+		double& xtr, double& xti) {
+	const double tau = s / (1.0 + c);
+	// ys = xs - s (conj(e) xt + tau xs)
+	const double ysr = xsr - s * (er * xtr + ei * xti + tau * xsr);
+	const double ysi = xsi - s * (er * xti - ei * xtr + tau * xsi);
+	// yt = xt + s (e xs - tau xt)
+	const double ytr = xtr + s * (er * xsr - ei * xsi - tau * xtr);
+	const double yti = xti + s * (er * xsi + ei * xsr - tau * xti);
+	xsr = ysr; xsi = ysi; xtr = ytr; xti = yti;
+}
+
+// One cyclic Jacobi sweep (63 rounds of 32 rotations) on the 64 x 64
+// subproblem in planes 0/1, accumulating Q in planes 2/3. Each round updates
+// every 2 x 2 block {p,q} x {s,t} in place as J_pq^H X J_st, so the subproblem
+// crosses shared memory once per round.
+__device__ void inner_sweep(Shared& sh, double tol) {
+	double* mr = sh.pl[0];
+	double* mi = sh.pl[1];
+	double* qr = sh.pl[2];
+	double* qi = sh.pl[3];
+	const int tid = threadIdx.x;
+	for (int r = 0; r < MS - 1; r++) {
+		if (tid < NR) {
+			const int p = rr_player(tid, r, MS), q = rr_player(MS - 1 - tid, r, MS);
+			inner_rotation(sh, tid, p, q, tol);
+		}
+		__syncthreads();
+		// NR x NR blocks of M
+		for (int e = tid; e < NR * NR; e += kThreads) {
+			const int ja = e / NR, jb = e % NR;
+			const bool ra = sh.rrot[ja], rb = sh.rrot[jb];
+			if (!ra && !rb) continue;
+			const int p = sh.rp[ja], q = sh.rq[ja], s2 = sh.rp[jb], t2 = sh.rq[jb];
+			if (ja == jb) {
+				mr[p * LD + p] = sh.rap[ja]; mi[p * LD + p] = 0.0;
+				mr[q * LD + q] = sh.raq[ja]; mi[q * LD + q] = 0.0;
+				mr[p * LD + q] = 0.0; mi[p * LD + q] = 0.0;
+				mr[q * LD + p] = 0.0; mi[q * LD + p] = 0.0;
+				continue;
+			}
+			double psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
+			double qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
+			if (ra) {
+				rows2(sh.rc[ja], sh.rs[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
+				rows2(sh.rc[ja], sh.rs[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
+			}
+			if (rb) {
+				cols2(sh.rc[jb], sh.rs[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
+				cols2(sh.rc[jb], sh.rs[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
+			}
+			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
+			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
+		}
+		// Q columns
+		for (int e = tid; e < MS * NR; e += kThreads) {
+			const int i = e / NR, j = e % NR;
+			if (!sh.rrot[j]) continue;
+			const int p = sh.rp[j], q = sh.rq[j];
+			double ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
+			cols2(sh.rc[j], sh.rs[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
+			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
+		}
+		__syncthreads();
+	}
+}
+
+// acc = A B for 32 x 32 complex operands given as plane pairs, FP64 DMMA.
+// Warp w owns output rows (w >> 1) * 8 .. +8 and columns (w & 1) * 16 .. +16
+// (two 8 x 8 tiles). A element (i, m) at a_re[i*as_i + m*as_m], B element
+// (m, l) at b_re[m*LD + l]; conjA conjugates A.
+__device__ __forceinline__ void cgemm(const double* ar, const double* ai, int as_i, int as_m, bool conjA,
+		const double* br, const double* bi, double (&cr)[2][2], double (&ci)[2][2]) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int i = (warp >> 1) * 8 + (lane >> 2);
+#pragma unroll
+	for (int b = 0; b < 2; b++) cr[b][0] = cr[b][1] = ci[b][0] = ci[b][1] = 0.0;
+#pragma unroll
+	for (int kk = 0; kk < MS; kk += 4) {
+		const int m = kk + (lane & 3);
+		const double far = ar[i * as_i + m * as_m];
+		const double fai = conjA ? -ai[i * as_i + m * as_m] : ai[i * as_i + m * as_m];
+#pragma unroll
+		for (int b = 0; b < 2; b++) {
+			const int l = (warp & 1) * 16 + b * 8 + (lane >> 2);
+			const double fbr = br[m * LD + l], fbi = bi[m * LD + l];
+			dmma(cr[b][0], cr[b][1], far, fbr);
+			dmma(cr[b][0], cr[b][1], -fai, fbi);
+			dmma(ci[b][0], ci[b][1], far, fbi);
+			dmma(ci[b][0], ci[b][1], fai, fbr);
+		}
+	}
+}
+
+// Output element coordinates of accumulator (b, h) of this thread.
+__device__ __forceinline__ void acc_rc(int b, int h, int& row, int& col) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	row = (warp >> 1) * 8 + (lane >> 2);
+	col = (warp & 1) * 16 + b * 8 + 2 * (lane & 3) + h;
+}
+
+__device__ void load_q(double* qr, double* qi, const double2* Qg) {
+	for (int e = threadIdx.x; e < MS * MS; e += kThreads) {
+		const double2 v = __ldcg(Qg + e);
+		qr[(e / MS) * LD + (e % MS)] = v.x;
+		qi[(e / MS) * LD + (e % MS)] = v.y;
+	}
+}
+
+__global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, double2* A1, double2* V, double2* Qbuf,
+		int kp, int max_sweeps, double tol, int* counters, unsigned long long* tmax) {
+	cg::grid_group grid = cg::this_grid();
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
+	const int tid = threadIdx.x;
+	const int nb = kp / BS;
+	const int np = nb / 2;
+	const int nrb = kp / MS;
+	const int nA2 = np * (np - 1);
+	const int nW = nA2 + nrb * np;
+	double2* Acur = A0;
+	double2* Anext = A1;
+
+	if (tid == 0) {
+		sh.total = 0;
+		sh.cnt = 0;
+		sh.tmax = 0ULL;
+	}
+	__syncthreads();
+
+	int sweep = 0;
+	bool converged = false;
+	for (; sweep < max_sweeps && !converged; sweep++) {
+		for (int r = 0; r < nb - 1; r++) {
+			// ---- phase 1: subproblems ----
+			for (int j = blockIdx.x; j < np; j += gridDim.x) {
+				const int P = rr_player(j, r, nb), Q = rr_player(nb - 1 - j, r, nb);
+				double* mr = sh.pl[0];
+				double* mi = sh.pl[1];
+				for (int e = tid; e < MS * MS; e += kThreads) {
+					const int i = e / MS, l = e % MS;
+					const double2 v = __ldcg(Acur + (long long)gidx(i, P, Q) * kp + gidx(l, P, Q));
+					mr[i * LD + l] = v.x;
+					mi[i * LD + l] = v.y;
+					sh.pl[2][i * LD + l] = (i == l) ? 1.0 : 0.0;
+					sh.pl[3][i * LD + l] = 0.0;
+				}
+				__syncthreads();
+				inner_sweep(sh, tol);
+				double2* Qg = Qbuf + (size_t)j * MS * MS;
+				for (int e = tid; e < MS * MS; e += kThreads) {
+					const int i = e / MS, l = e % MS;
+					Qg[e] = make_double2(sh.pl[2][i * LD + l], sh.pl[3][i * LD + l]);
+					Anext[(long long)gidx(i, P, Q) * kp + gidx(l, P, Q)] = make_double2(mr[i * LD + l], mi[i * LD + l]);
+				}
+				__syncthreads();
+			}
+			grid.sync();
+			// ---- phase 2: block products ----
+			for (int w = blockIdx.x; w < nW; w += gridDim.x) {
+				double cr[2][2], ci[2][2];
+				if (w < nA2) {
+					const int jr = w / (np - 1);
+					int jc = w % (np - 1);
+					if (jc >= jr) jc++;
+					const int Pr = rr_player(jr, r, nb), Qr = rr_player(nb - 1 - jr, r, nb);
+					const int Pc = rr_player(jc, r, nb), Qc = rr_player(nb - 1 - jc, r, nb);
+					for (int e = tid; e < MS * MS; e += kThreads) {
+						const int i = e / MS, l = e % MS;
+						const double2 v = __ldcg(Acur + (long long)gidx(i, Pr, Qr) * kp + gidx(l, Pc, Qc));
+						sh.pl[0][i * LD + l] = v.x;
+						sh.pl[1][i * LD + l] = v.y;
+					}
+					load_q(sh.pl[2], sh.pl[3], Qbuf + (size_t)jr * MS * MS);
+					load_q(sh.pl[4], sh.pl[5], Qbuf + (size_t)jc * MS * MS);
+					__syncthreads();
+					cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
+					__syncthreads();
+#pragma unroll
+					for (int b = 0; b < 2; b++)
+#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							int row, col;
+							acc_rc(b, h, row, col);
+							sh.pl[0][row * LD + col] = cr[b][h];
+							sh.pl[1][row * LD + col] = ci[b][h];
+						}
+					__syncthreads();
+					// C = Qr^H T: A(i, m) = conj(Qr(m, i))
+					cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
+#pragma unroll
+					for (int b = 0; b < 2; b++)
+#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							int row, col;
+							acc_rc(b, h, row, col);
+							Anext[(long long)gidx(row, Pr, Qr) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
+						}
+				} else {
+					const int v = w - nA2;
+					const int rb = v / np, jc = v % np;
+					const int Pc = rr_player(jc, r, nb), Qc = rr_player(nb - 1 - jc, r, nb);
+					for (int e = tid; e < MS * MS; e += kThreads) {
+						const int i = e / MS, l = e % MS;
+						const double2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
+						sh.pl[0][i * LD + l] = x.x;
+						sh.pl[1][i * LD + l] = x.y;
+					}
+					load_q(sh.pl[4], sh.pl[5], Qbuf + (size_t)jc * MS * MS);
+					__syncthreads();
+					cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
+#pragma unroll
+					for (int b = 0; b < 2; b++)
+#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							int row, col;
+							acc_rc(b, h, row, col);
+							V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
+						}
+				}
+				__syncthreads();
+			}
+			grid.sync();
+			double2* t = Acur;
+			Acur = Anext;
+			Anext = t;
+		}
+		if (tid == 0) {
+			if (sh.cnt) atomicAdd(&counters[sweep], sh.cnt);
+			if (sh.tmax) atomicMax(&tmax[sweep], sh.tmax);
+			sh.cnt = 0;
+			sh.tmax = 0ULL;
+		}
+		grid.sync();
+		const int cnt = *((volatile int*)&counters[sweep]);
+		const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmax[sweep]));
+		if (cnt == 0 || tm < kTauFinal) converged = true;
+	}
+	if (blockIdx.x == 0 && tid == 0) {
+		counters[max_sweeps] = converged ? sweep : -1;
+		counters[max_sweeps + 1] = (Acur == A0) ? 0 : 1;
+	}
+}
+
+}  // namespace
+
+int bjacobi_padded(int k) { return ((k + MS - 1) / MS) * MS; }
+size_t bjacobi_qbuf_elems(int k) { return (size_t)(bjacobi_padded(k) / MS) * MS * MS; }
+
+cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* V, double2* Qbuf, int kp, int max_sweeps, int* counters,
+		int num_sms, cudaStream_t s) {
+	const size_t smem = sizeof(Shared);
+	cudaError_t e = cudaFuncSetAttribute(bjacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	if (e != cudaSuccess) return e;
+	int per_sm = 0;
+	e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bjacobi_kernel, kThreads, smem);
+	if (e != cudaSuccess) return e;
+	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+	const int blocks = num_sms * per_sm;
+	double tol = 1e-15;
+	unsigned long long* tmax = reinterpret_cast<unsigned long long*>(counters + jacobi_tmax_offset(max_sweeps));
+	void* args[] = {&A0, &A1, &V, &Qbuf, &kp, &max_sweeps, &tol, &counters, &tmax};
+	return cudaLaunchCooperativeKernel((void*)bjacobi_kernel, dim3(blocks), dim3(kThreads), args, smem, s);
+}
+
+}  // namespace itp2d

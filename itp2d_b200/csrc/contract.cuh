@@ -32,9 +32,20 @@ struct JacobiWork {
 	double2* V;       // k x k eigenvectors (columns)
 	double* evals;    // k
 	int* perm;        // k
-	int* counters;    // max_sweeps + 4 ints
+	int* counters;    // jacobi_counter_ints(max_sweeps) ints
 	int max_sweeps;
+	double2* Qbuf = nullptr;  // block Jacobi unitaries (bjacobi_qbuf_elems); null: scalar Jacobi only
 };
+
+// Smallest k solved by block Jacobi (when JacobiWork::Qbuf is set).
+constexpr int kBlockJacobiMinK = 256;
+// Padded dimension of the block path (multiple of 64) and its Q buffer size.
+int bjacobi_padded(int k);
+size_t bjacobi_qbuf_elems(int k);
+// Padded dimension the eigensolver uses for (w, k); A0/A1/V are kp x kp.
+int jacobi_kp(const JacobiWork& w, int k);
+cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* V, double2* Qbuf, int kp, int max_sweeps, int* counters,
+		int num_sms, cudaStream_t s);
 
 // Eigen-decomposition of the Hermitian S (k x k, row-major, full storage) by
 // parallel cyclic Jacobi, then W[:, n] = V[:, p(n)] / sqrt(l_n) with l
@@ -46,6 +57,11 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 // (columns of w.V, kp x kp with kp = k rounded up to even) without the
 // overlap checks unless check != 0.
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
+// Counter block of the Jacobi kernel, in ints: per-sweep rotation counts, the
+// result fields at [max_sweeps] and [max_sweeps + 1], then per-sweep maxima of
+// the rotation tangents as 64-bit words starting at jacobi_tmax_offset().
+constexpr size_t jacobi_tmax_offset(int max_sweeps) { return ((size_t)max_sweeps + 4 + 1) & ~(size_t)1; }
+constexpr size_t jacobi_counter_ints(int max_sweeps) { return jacobi_tmax_offset(max_sweeps) + 2 * (size_t)max_sweeps + 2; }
 size_t jacobi_counters(int max_sweeps);
 
 }  // namespace itp2d

@@ -618,7 +618,7 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	const int nt = overlap_tiles(k);
 	c->npairs = nt * (nt + 1) / 2;
 	c->nsplit = std::max(1, std::min((4 * c->num_sms + c->npairs - 1) / c->npairs, (int)std::max(1LL, c->G / 512)));
-	const int kp = (k + 1) & ~1;
+	const int kp = std::max(bjacobi_padded(k), (k + 1) & ~1);  // covers the scalar and block layouts
 	if (e == cudaSuccess) c->S = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
 	if (e == cudaSuccess) c->part = (double2*)dalloc(c, (size_t)c->nsplit * k * k * sizeof(double2), &e);
 	if (e == cudaSuccess) c->W = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
@@ -627,6 +627,8 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	if (e == cudaSuccess) c->jw.A0 = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
 	if (e == cudaSuccess) c->jw.A1 = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
 	if (e == cudaSuccess) c->jw.V = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
+	if (e == cudaSuccess && k >= kBlockJacobiMinK)
+		c->jw.Qbuf = (double2*)dalloc(c, bjacobi_qbuf_elems(k) * sizeof(double2), &e);
 	if (e == cudaSuccess) c->jw.evals = (double*)dalloc(c, (size_t)k * sizeof(double), &e);
 	if (e == cudaSuccess) c->jw.perm = (int*)dalloc(c, (size_t)k * sizeof(int), &e);
 	if (e == cudaSuccess) c->jw.counters = (int*)dalloc(c, jacobi_counters(c->jw.max_sweeps) * sizeof(int), &e);
@@ -912,7 +914,7 @@ int itp2d_last_sweeps(itp2d_ctx* c) { return c ? c->last_sweeps : -1; }
 
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs) {
 	if (n < 1 || !A || !evals || !evecs) return ITP2D_E_INVALID;
-	const int kp = (n + 1) & ~1;
+	const int kp = std::max(bjacobi_padded(n), (n + 1) & ~1);
 	std::vector<double2> S((size_t)n * n);
 	for (int i = 0; i < n; i++)
 		for (int j = i; j < n; j++) {
@@ -936,12 +938,15 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
 	w.A0 = (double2*)al((size_t)kp * kp * sizeof(double2));
 	w.A1 = (double2*)al((size_t)kp * kp * sizeof(double2));
 	w.V = (double2*)al((size_t)kp * kp * sizeof(double2));
+	if (n >= kBlockJacobiMinK) w.Qbuf = (double2*)al(bjacobi_qbuf_elems(n) * sizeof(double2));
 	w.evals = (double*)al((size_t)n * sizeof(double));
 	w.perm = (int*)al((size_t)n * sizeof(int));
 	w.counters = (int*)al(jacobi_counters(w.max_sweeps) * sizeof(int));
 	EigStatus* dst = (EigStatus*)al(sizeof(EigStatus));
 	int status = ITP2D_OK;
-	if (!dS || !w.A0 || !w.A1 || !w.V || !w.evals || !w.perm || !w.counters || !dst) status = ITP2D_E_OOM;
+	if (!dS || !w.A0 || !w.A1 || !w.V || !w.evals || !w.perm || !w.counters || !dst ||
+			(n >= kBlockJacobiMinK && !w.Qbuf))
+		status = ITP2D_E_OOM;
 	std::vector<double2> V;
 	std::vector<int> perm(n);
 	EigStatus hs{};
@@ -958,9 +963,10 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
 		if (status == ITP2D_OK && hs.status != ITP2D_OK) status = hs.status;
 	}
 	if (status == ITP2D_OK) {
+		const int jkp = jacobi_kp(w, n);
 		for (int m = 0; m < n; m++)
 			for (int i = 0; i < n; i++) {
-				const double2 v = V[(size_t)i * kp + perm[m]];
+				const double2 v = V[(size_t)i * jkp + perm[m]];
 				evecs[2 * ((size_t)m * n + i)] = v.x;
 				evecs[2 * ((size_t)m * n + i) + 1] = v.y;
 			}

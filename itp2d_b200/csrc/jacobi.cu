@@ -28,7 +28,7 @@ constexpr int kThreads = 256;
 struct Rot {
 	double c, s, er, ei;  // J = [[c, s e], [-s conj(e), c]], e = er + i ei
 	double ap, aq;        // rotated diagonal
-	int p, q;
+	double t;             // |tan| of the rotation angle (0 when skipped)
 	int rotated;
 };
 
@@ -41,25 +41,23 @@ __device__ __forceinline__ double2 ldA(const double2* A, long long idx) { return
 __device__ void make_rot(Rot& R, const double2* A, int kp, int slot, int r, double tol) {
 	const int p = player(slot, r, kp);
 	const int q = player(kp - 1 - slot, r, kp);
-	R.p = p;
-	R.q = q;
 	const double a = ldA(A, (long long)p * kp + p).x;
 	const double b = ldA(A, (long long)q * kp + q).x;
 	const double2 c = ldA(A, (long long)p * kp + q);
 	const double cabs = hypot(c.x, c.y);
-	R.c = 1.0; R.s = 0.0; R.er = 1.0; R.ei = 0.0; R.ap = a; R.aq = b; R.rotated = 0;
+	R.c = 1.0; R.s = 0.0; R.er = 1.0; R.ei = 0.0; R.ap = a; R.aq = b; R.t = 0.0; R.rotated = 0;
 	if (cabs > 0.0 && cabs > tol * sqrt(fabs(a) * fabs(b))) {
 		const double th = (b - a) / (2.0 * cabs);
 		const double ath = fabs(th);
-		double t = (ath > 1e150) ? 0.5 / ath : 1.0 / (ath + sqrt(th * th + 1.0));
-		if (th < 0) t = -t;
+		const double t = (ath > 1e150) ? 0.5 / ath : 1.0 / (ath + sqrt(th * th + 1.0));
 		if (t != 0.0) {
 			R.c = 1.0 / sqrt(t * t + 1.0);
-			R.s = t * R.c;
+			R.s = (th < 0 ? -t : t) * R.c;
 			R.er = c.x / cabs;
 			R.ei = c.y / cabs;
-			R.ap = a - t * cabs;
-			R.aq = b + t * cabs;
+			R.ap = a - (th < 0 ? -t : t) * cabs;
+			R.aq = b + (th < 0 ? -t : t) * cabs;
+			R.t = t;
 			R.rotated = 1;
 		}
 	}
@@ -89,11 +87,30 @@ __device__ __forceinline__ void rot_cols(const Rot& C, double2 xs, double2 xt, d
 	yt = cadd2(xt, csc(cadd2(cm(e, xs), csc(xt, -tau)), C.s));
 }
 
+constexpr int kItems = 2;  // work items per CTA between two CTA barriers
+
+// Tangent below which a sweep is final: the next sweep could only change
+// off-diagonal elements by O(k tau^2) relative to the eigenvalue gaps.
+constexpr double kTauFinal = 1e-10;
+
+// One cooperative launch = the whole eigensolve. Per round, each CTA takes up
+// to kItems work items (an A tile of TP x TP pair blocks, or a V tile of
+// kVRows rows x TP pairs), issues all of their global loads together with the
+// loads of the rotation inputs, then applies the rotations after one CTA
+// barrier; the round ends with one grid barrier.
 __global__ void __launch_bounds__(kThreads) jacobi_kernel(double2* A0, double2* A1, double2* V, int kp,
-		int max_sweeps, double tol, int* counters) {
+		int max_sweeps, double tol, int* counters, unsigned long long* tmax) {
 	cg::grid_group grid = cg::this_grid();
-	__shared__ Rot rr[TP];
-	__shared__ Rot rc[TP];
+	__shared__ Rot rr[kItems][TP];
+	__shared__ Rot rc[kItems][TP];
+	__shared__ int s_cnt;                 // rotations applied by this CTA in the sweep
+	__shared__ unsigned long long s_tmax;  // largest tangent (bit pattern of a non-negative double)
+	const int tid = threadIdx.x;
+	if (tid == 0) {
+		s_cnt = 0;
+		s_tmax = 0ULL;
+	}
+	__syncthreads();
 	const int np = kp / 2;
 	const int nt = (np + TP - 1) / TP;
 	const int nA = nt * nt;
@@ -102,91 +119,138 @@ __global__ void __launch_bounds__(kThreads) jacobi_kernel(double2* A0, double2* 
 	double2* Acur = A0;
 	double2* Anext = A1;
 	int sweep = 0;
-	for (; sweep < max_sweeps; sweep++) {
+	bool converged = false;
+	for (; sweep < max_sweeps && !converged; sweep++) {
 		for (int r = 0; r < kp - 1; r++) {
-			for (int w = blockIdx.x; w < nW; w += gridDim.x) {
-				if (w < nA) {
-					const int TI = w / nt, TJ = w % nt;
-					if (threadIdx.x < TP) {
-						const int sl = TI * TP + threadIdx.x;
-						if (sl < np) make_rot(rr[threadIdx.x], Acur, kp, sl, r, tol);
-					} else if (threadIdx.x < 2 * TP) {
-						const int sl = TJ * TP + threadIdx.x - TP;
-						if (sl < np) make_rot(rc[threadIdx.x - TP], Acur, kp, sl, r, tol);
+			for (int w0 = blockIdx.x * kItems; w0 < nW; w0 += gridDim.x * kItems) {
+				double2 x[kItems][4];
+				// phase 1: rotation set-up and all loads
+#pragma unroll
+				for (int it = 0; it < kItems; it++) {
+					const int w = w0 + it;
+					if (w >= nW) break;
+					if (w < nA) {
+						const int TI = w / nt, TJ = w % nt;
+						if (tid < TP) {
+							const int sl = TI * TP + tid;
+							if (sl < np) make_rot(rr[it][tid], Acur, kp, sl, r, tol);
+						} else if (tid < 2 * TP) {
+							const int sl = TJ * TP + tid - TP;
+							if (sl < np) make_rot(rc[it][tid - TP], Acur, kp, sl, r, tol);
+						}
+						const int sa = TI * TP + tid / TP, sb = TJ * TP + tid % TP;
+						if (sa < np && sb < np) {
+							const int p = player(sa, r, kp), q = player(kp - 1 - sa, r, kp);
+							const int s2 = player(sb, r, kp), t2 = player(kp - 1 - sb, r, kp);
+							if (sa == sb) {
+								x[it][0] = ldA(Acur, (long long)p * kp + q);
+								x[it][1] = ldA(Acur, (long long)q * kp + p);
+							} else {
+								x[it][0] = ldA(Acur, (long long)p * kp + s2);
+								x[it][1] = ldA(Acur, (long long)p * kp + t2);
+								x[it][2] = ldA(Acur, (long long)q * kp + s2);
+								x[it][3] = ldA(Acur, (long long)q * kp + t2);
+							}
+						}
+					} else {
+						const int v = w - nA;
+						const int RC = v / nt, TJ = v % nt;
+						if (tid < TP) {
+							const int sl = TJ * TP + tid;
+							if (sl < np) make_rot(rc[it][tid], Acur, kp, sl, r, tol);
+						}
+#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							const int e = tid + h * kThreads;
+							const int i = RC * kVRows + e / TP, sb = TJ * TP + e % TP;
+							if (i < kp && sb < np) {
+								const int s2 = player(sb, r, kp), t2 = player(kp - 1 - sb, r, kp);
+								x[it][2 * h] = ldA(V, (long long)i * kp + s2);
+								x[it][2 * h + 1] = ldA(V, (long long)i * kp + t2);
+							}
+						}
 					}
-					__syncthreads();
-					for (int e = threadIdx.x; e < TP * TP; e += blockDim.x) {
-						const int a = e / TP, b = e % TP;
+				}
+				__syncthreads();
+				// phase 2: apply
+#pragma unroll
+				for (int it = 0; it < kItems; it++) {
+					const int w = w0 + it;
+					if (w >= nW) break;
+					if (w < nA) {
+						const int TI = w / nt, TJ = w % nt;
+						const int a = tid / TP, b = tid % TP;
 						const int sa = TI * TP + a, sb = TJ * TP + b;
 						if (sa >= np || sb >= np) continue;
-						const Rot& R = rr[a];
-						const Rot& C = rc[b];
-						const int p = R.p, q = R.q, s = C.p, t = C.q;
+						const Rot& R = rr[it][a];
+						const Rot& C = rc[it][b];
+						const int p = player(sa, r, kp), q = player(kp - 1 - sa, r, kp);
 						if (sa == sb) {
 							Anext[(long long)p * kp + p] = make_double2(R.ap, 0.0);
 							Anext[(long long)q * kp + q] = make_double2(R.aq, 0.0);
 							if (R.rotated) {
 								Anext[(long long)p * kp + q] = make_double2(0.0, 0.0);
 								Anext[(long long)q * kp + p] = make_double2(0.0, 0.0);
-								atomicAdd(&counters[sweep], 1);
+								atomicAdd(&s_cnt, 1);
+								atomicMax(&s_tmax, (unsigned long long)__double_as_longlong(R.t));
 							} else {
-								Anext[(long long)p * kp + q] = ldA(Acur, (long long)p * kp + q);
-								Anext[(long long)q * kp + p] = ldA(Acur, (long long)q * kp + p);
+								Anext[(long long)p * kp + q] = x[it][0];
+								Anext[(long long)q * kp + p] = x[it][1];
 							}
 							continue;
 						}
-						const double2 xps = ldA(Acur, (long long)p * kp + s);
-						const double2 xpt = ldA(Acur, (long long)p * kp + t);
-						const double2 xqs = ldA(Acur, (long long)q * kp + s);
-						const double2 xqt = ldA(Acur, (long long)q * kp + t);
-						// Y = Jr^H X in the tau form y_p = x_p - s(e x_q + tau x_p),
-						// y_q = x_q + s(conj(e) x_p - tau x_q), tau = s / (1 + c)
-						double2 y1s, y1t, y2s, y2t;
-						rot_rows(R, xps, xqs, y1s, y2s);
-						rot_rows(R, xpt, xqt, y1t, y2t);
-						// X' = Y Jc: x_s' = x_s - s(conj(e) x_t + tau x_s), x_t' = x_t + s(e x_s - tau x_t)
-						double2 o;
-						rot_cols(C, y1s, y1t, o, Anext[(long long)p * kp + t]);
-						Anext[(long long)p * kp + s] = o;
-						rot_cols(C, y2s, y2t, o, Anext[(long long)q * kp + t]);
-						Anext[(long long)q * kp + s] = o;
+						const int s2 = player(sb, r, kp), t2 = player(kp - 1 - sb, r, kp);
+						double2 y1s, y1t, y2s, y2t, o1, o2;
+						rot_rows(R, x[it][0], x[it][2], y1s, y2s);
+						rot_rows(R, x[it][1], x[it][3], y1t, y2t);
+						rot_cols(C, y1s, y1t, o1, o2);
+						Anext[(long long)p * kp + s2] = o1;
+						Anext[(long long)p * kp + t2] = o2;
+						rot_cols(C, y2s, y2t, o1, o2);
+						Anext[(long long)q * kp + s2] = o1;
+						Anext[(long long)q * kp + t2] = o2;
+					} else {
+						const int v = w - nA;
+						const int RC = v / nt, TJ = v % nt;
+#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							const int e = tid + h * kThreads;
+							const int i = RC * kVRows + e / TP, b = e % TP, sb = TJ * TP + b;
+							if (i >= kp || sb >= np) continue;
+							const Rot& C = rc[it][b];
+							if (!C.rotated) continue;
+							const int s2 = player(sb, r, kp), t2 = player(kp - 1 - sb, r, kp);
+							double2 ns, nt2;
+							rot_cols(C, x[it][2 * h], x[it][2 * h + 1], ns, nt2);
+							V[(long long)i * kp + s2] = ns;
+							V[(long long)i * kp + t2] = nt2;
+						}
 					}
-					__syncthreads();
-				} else {
-					const int v = w - nA;
-					const int RC = v / nt, TJ = v % nt;
-					if (threadIdx.x < TP) {
-						const int sl = TJ * TP + threadIdx.x;
-						if (sl < np) make_rot(rc[threadIdx.x], Acur, kp, sl, r, tol);
-					}
-					__syncthreads();
-					for (int e = threadIdx.x; e < kVRows * TP; e += blockDim.x) {
-						const int ii = e / TP, b = e % TP;
-						const int i = RC * kVRows + ii, sb = TJ * TP + b;
-						if (i >= kp || sb >= np) continue;
-						const Rot& C = rc[b];
-						if (!C.rotated) continue;
-						const long long is = (long long)i * kp + C.p, it = (long long)i * kp + C.q;
-						const double2 vs = ldA(V, is), vt = ldA(V, it);
-						double2 ns, nt2;
-						rot_cols(C, vs, vt, ns, nt2);
-						V[is] = ns;
-						V[it] = nt2;
-					}
-					__syncthreads();
 				}
+				__syncthreads();
 			}
 			grid.sync();
 			double2* tmp = Acur;
 			Acur = Anext;
 			Anext = tmp;
 		}
+		// one global update per CTA and sweep, then a grid barrier so every CTA
+		// reads the final totals
+		if (tid == 0) {
+			if (s_cnt) atomicAdd(&counters[sweep], s_cnt);
+			if (s_tmax) atomicMax(&tmax[sweep], s_tmax);
+			s_cnt = 0;
+			s_tmax = 0ULL;
+		}
+		grid.sync();
+		// uniform across the grid: everything below reads values final after grid.sync
 		const int cnt = *((volatile int*)&counters[sweep]);
-		if (cnt == 0) break;
+		const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmax[sweep]));
+		if (cnt == 0 || tm < kTauFinal) converged = true;
 	}
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
-		counters[max_sweeps] = (sweep < max_sweeps) ? sweep + 1 : -1;  // sweeps used, -1: no convergence
-		counters[max_sweeps + 1] = (Acur == A0) ? 0 : 1;                // buffer holding the result
+		counters[max_sweeps] = converged ? sweep : -1;   // sweeps used, -1: no convergence
+		counters[max_sweeps + 1] = (Acur == A0) ? 0 : 1;  // buffer holding the result
 	}
 }
 
@@ -316,39 +380,50 @@ __global__ void build_w_kernel(const double2* __restrict__ V, int k, int kp, con
 
 }  // namespace
 
-size_t jacobi_counters(int max_sweeps) { return (size_t)max_sweeps + 4; }
+size_t jacobi_counters(int max_sweeps) { return jacobi_counter_ints(max_sweeps); }
 
 cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms,
 		cudaStream_t s) {
 	cudaError_t e = launch_eigh(S, k, w, st, num_sms, s, 1);
 	if (e != cudaSuccess) return e;
 	const long long n2 = (long long)k * k;
-	const int kp = (k + 1) & ~1;
+	const int kp = jacobi_kp(w, k);
 	build_w_kernel<<<(unsigned)std::min<long long>((n2 + 255) / 256, 4096), 256, 0, s>>>(w.V, k, kp, w.evals,
 			w.perm, W);
 	return cudaGetLastError();
 }
 
+int jacobi_kp(const JacobiWork& w, int k) {
+	return (w.Qbuf && k >= kBlockJacobiMinK) ? bjacobi_padded(k) : ((k + 1) & ~1);
+}
+
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check) {
-	const int kp = (k + 1) & ~1;
+	const int kp = jacobi_kp(w, k);
 	const long long n = (long long)kp * kp;
 	cudaError_t e = cudaMemsetAsync(w.counters, 0, jacobi_counters(w.max_sweeps) * sizeof(int), s);
 	if (e != cudaSuccess) return e;
 	jacobi_init_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(S, k, kp, w.A0, w.V);
-	int per_sm = 0;
-	e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_kernel, kThreads, 0);
-	if (e != cudaSuccess) return e;
-	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-	const int np = kp / 2;
-	const int nt = (np + TP - 1) / TP;
-	const int nW = nt * nt + ((kp + kVRows - 1) / kVRows) * nt;
-	int blocks = std::min(num_sms * std::min(per_sm, 2), nW);
-	if (blocks < 1) blocks = 1;
-	double tol = 1e-15;
-	int ms = w.max_sweeps;
-	void* args[] = {&w.A0, &w.A1, &w.V, (void*)&kp, &ms, &tol, &w.counters};
-	e = cudaLaunchCooperativeKernel((void*)jacobi_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
-	if (e != cudaSuccess) return e;
+	if (w.Qbuf && k >= kBlockJacobiMinK) {
+		e = launch_bjacobi(w.A0, w.A1, w.V, w.Qbuf, kp, w.max_sweeps, w.counters, num_sms, s);
+		if (e != cudaSuccess) return e;
+	} else {
+		int per_sm = 0;
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_kernel, kThreads, 0);
+		if (e != cudaSuccess) return e;
+		if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+		const int np = kp / 2;
+		const int nt = (np + TP - 1) / TP;
+		const int nW = nt * nt + ((kp + kVRows - 1) / kVRows) * nt;
+		int blocks = std::min(num_sms * std::min(per_sm, 2), (nW + kItems - 1) / kItems);
+		if (blocks < 1) blocks = 1;
+		double tol = 1e-15;
+		int ms = w.max_sweeps;
+		int kpv = kp;
+		unsigned long long* tmax = reinterpret_cast<unsigned long long*>(w.counters + jacobi_tmax_offset(ms));
+		void* args[] = {&w.A0, &w.A1, &w.V, (void*)&kpv, &ms, &tol, &w.counters, &tmax};
+		e = cudaLaunchCooperativeKernel((void*)jacobi_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
+		if (e != cudaSuccess) return e;
+	}
 	normalize_columns_kernel<<<(k + 31) / 32, 256, 0, s>>>(w.V, k, kp);
 	int P = 1;
 	while (P < k) P <<= 1;

@@ -42,7 +42,7 @@ constexpr size_t kOffVec = kOffV + kMatBytes;
 constexpr size_t kOffEval = kOffVec + kMatBytes;
 constexpr size_t kOffPerm = kOffEval + align_up(kMaxN * sizeof(double));
 constexpr size_t kOffCnt = kOffPerm + align_up(kMaxN * sizeof(int));
-constexpr size_t kOffStat = kOffCnt + align_up((kMaxSweeps + 4) * sizeof(int));
+constexpr size_t kOffStat = kOffCnt + align_up(itp2d::jacobi_counter_ints(kMaxSweeps) * sizeof(int));
 constexpr size_t kScratchBytes = kOffStat + align_up(sizeof(EigStatus));
 
 // The scratch array. In host code its name is a host-side stand-in, not a
