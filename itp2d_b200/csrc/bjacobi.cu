@@ -16,7 +16,8 @@
 // Rotations whose relative off-diagonal |A_pq| / sqrt(|A_pp A_qq|) is at the
 // rounding level of the phase-2 products (below 1e-13) do not count against
 // convergence; the iteration stops after a sweep whose largest counted
-// rotation tangent is below 1e-10 (or that counted none).
+// rotation tangent is below 3e-9 (or that counted none): quadratic convergence
+// then leaves off-diagonal elements of order k * 1e-17 relative to the gaps.
 #include <cooperative_groups.h>
 
 #include "../../include/itp2d_gpu.h"
@@ -35,7 +36,7 @@ constexpr int LD = MS + 4;    // padded row length (doubles): conflict-free DMMA
 constexpr int PL = MS * LD;   // doubles per plane
 constexpr int kThreads = 256;
 constexpr int kInnerMaxSweeps = 30;
-constexpr double kTauFinal = 1e-10;
+constexpr double kTauFinal = 3e-9;
 constexpr double kNoiseRel = 1e-13;  // relative off-diagonal treated as rounding noise
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
@@ -61,25 +62,51 @@ struct Shared {
 	unsigned long long tmax;                     // largest tangent (bits of a non-negative double)
 };
 
+// Reciprocal and reciprocal square root in double precision by Newton-Raphson
+// refinement of the single-precision hardware estimates: each step squares the
+// relative error (about 1e-7 -> 1e-14 -> below double rounding). Valid for
+// positive normal arguments inside the float exponent range, which the
+// rotation set-up below guarantees by scaling.
+__device__ __forceinline__ double rcp_nr(double x) {
+	double y = (double)__frcp_rn((float)x);
+	y = y * fma(-x, y, 2.0);
+	y = y * fma(-x, y, 2.0);
+	return y;
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+	double y = (double)rsqrtf((float)x);
+	y = y * fma(-0.5 * x * y, y, 1.5);
+	y = y * fma(-0.5 * x * y, y, 1.5);
+	return y;
+}
+
 // Rotation of the local pair (p, q) of the subproblem in planes (mr, mi).
+// With d = (b - a) / 2 and r = sqrt(d^2 + |c|^2) the tangent of the smaller
+// angle is t = |c| / (|d| + r); d and |c| are first scaled by the power of two
+// of max(|d|, |c|) so the Newton-refined estimates stay in float range.
 __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 	const double* mr = sh.pl[0];
 	const double* mi = sh.pl[1];
 	const double a = mr[p * LD + p], b = mr[q * LD + q];
 	const double cr = mr[p * LD + q], ci = mi[p * LD + q];
-	const double cabs = sqrt(cr * cr + ci * ci);
-	const double scale = sqrt(fabs(a) * fabs(b));
+	const double c2 = cr * cr + ci * ci;
+	const double scale2 = fabs(a) * fabs(b);
 	sh.rp[j] = p;
 	sh.rq[j] = q;
 	sh.rrot[j] = 0;
 	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
-	if (cabs > 0.0 && cabs > tol * scale) {
-		// tan of the smaller angle: t = |c| / (|d| + sqrt(d^2 + |c|^2)), d = (b - a) / 2
+	if (c2 > 0.0 && c2 > tol * tol * scale2) {
+		const double cabs = sqrt(c2);
 		const double d = 0.5 * (b - a);
-		const double t = cabs / (fabs(d) + sqrt(d * d + cabs * cabs));
+		// exact power-of-two scaling by the exponent of max(|d|, |c|)
+		const int ex = ilogb(fmax(fabs(d), cabs));
+		const double dn = scalbn(fabs(d), -ex), cn = scalbn(cabs, -ex);  // both in [0, 2), one >= 1
+		const double rn2 = dn * dn + cn * cn;                               // in [1, 8)
+		const double rn = rn2 * rsqrt_nr(rn2);
+		const double t = cn * rcp_nr(dn + rn);                              // dn + rn in [1, 2 + 2 sqrt 2)
 		if (t != 0.0) {
 			const double st = d < 0 ? -t : t;
-			const double c = 1.0 / sqrt(t * t + 1.0);
+			const double c = rsqrt_nr(fma(t, t, 1.0));    // t in (0, 1]
 			const double ic = 1.0 / cabs;
 			sh.rc[j] = c;
 			sh.rs[j] = st * c;
@@ -88,7 +115,7 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 			sh.rap[j] = a - st * cabs;
 			sh.raq[j] = b + st * cabs;
 			sh.rrot[j] = 1;
-			if (cabs > kNoiseRel * scale) {
+			if (c2 > kNoiseRel * kNoiseRel * scale2) {
 				atomicAdd(&sh.cnt, 1);
 				atomicMax(&sh.tmax, (unsigned long long)__double_as_longlong(t));
 			}

@@ -25,121 +25,188 @@ __device__ __forceinline__ void load_twiddles(c2<R>* tw, const LinePlan& lp) {
 	for (int i = threadIdx.x; i < lp.fft.n; i += blockDim.x) tw[i] = g[i];
 }
 
+// Asynchronous global -> shared copy of one complex element (cp.async: the
+// data does not pass through registers, so a CTA can have the next tile in
+// flight while it transforms the current one).
+template <class R> __device__ __forceinline__ void cp_elem(c2<R>* dst, const c2<R>* src);
+template <> __device__ __forceinline__ void cp_elem<double>(double2* dst, const double2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+template <> __device__ __forceinline__ void cp_elem<float>(float2* dst, const float2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Row pass, persistent and double-buffered: tile t (rows_per_tile rows of one
+// state; tiles ordered state-fastest) is transformed while tile t + grid is
+// being copied in. Shared memory: two tile buffers, one scratch buffer for the
+// FFT ping-pong, the twiddles.
 template <class R>
-__global__ void __launch_bounds__(kThreads) row_pass_kernel(RowPassArgs a) {
+__global__ void __launch_bounds__(kThreads) row_pass_kernel(RowPassArgs a, int k) {
 	using T = c2<R>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
 	const int rows = a.rows_per_tile;
-	T* buf0 = reinterpret_cast<T*>(smem_raw);
-	T* buf1 = buf0 + rows * L;
-	T* tw = buf1 + rows * L;
+	const int tsz = rows * L;
+	T* tiles = reinterpret_cast<T*>(smem_raw);
+	T* scr = tiles + 2 * tsz;
+	T* tw = scr + tsz;
 	load_twiddles<R>(tw, a.lp);
-
-	const long long state = blockIdx.x;
-	const int row0 = blockIdx.y * rows;
-	const int nrows = min(rows, a.sy - row0);
 	const int sx = a.sx;
-	const long long base = state * a.G + (long long)row0 * sx;
-	const T* in = reinterpret_cast<const T*>(a.in) + base;
+	const int ntr = (a.sy + rows - 1) / rows;
+	const long long total = (long long)k * ntr;
 	const R* mpre = reinterpret_cast<const R*>(a.mul_pre);
 	const R* mmid = reinterpret_cast<const R*>(a.mul_mid);
 	const R* mpost = reinterpret_cast<const R*>(a.mul_post);
-	const int toff = row0 * sx;  // table offset of this tile
-	const int cnt = nrows * sx;
 
-	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-		const int r = i / sx;
-		const int x = i - r * sx;
-		T v = in[i];
-		if (a.do_inv) {
-			if (mpre) v = cscale(v, mpre[toff + i]);
-		} else if (mmid) {
-			v = cscale(v, mmid[toff + i]);
+	long long t = blockIdx.x;
+	int cur = 0;
+	auto issue = [&](T* dst, long long tt) {
+		const long long state = tt % k;
+		const int row0 = (int)(tt / k) * rows;
+		const int nrows = min(rows, a.sy - row0);
+		const T* in = reinterpret_cast<const T*>(a.in) + state * a.G + (long long)row0 * sx;
+		for (int i = threadIdx.x; i < nrows * sx; i += blockDim.x) {
+			const int r = i / sx;
+			cp_elem<R>(dst + r * L + (i - r * sx), in + i);
 		}
-		buf0[r * L + x] = v;
-	}
-	__syncthreads();
+	};
+	if (t < total) issue(tiles, t);
+	cp_commit();
+	for (; t < total; t += gridDim.x) {
+		const long long tn = t + gridDim.x;
+		if (tn < total) issue(tiles + (cur ^ 1) * tsz, tn);
+		cp_commit();
+		cp_wait<1>();
+		__syncthreads();
 
-	T* cur = buf0;
-	T* oth = buf1;
-	if (a.do_inv) {
-		cur = line_transform<R, false>(buf0, buf1, a.lp, tw, nrows, 1, L, true);
-		oth = (cur == buf0) ? buf1 : buf0;
-		if (mmid) {
+		T* buf0 = tiles + cur * tsz;
+		const long long state = t % k;
+		const int row0 = (int)(t / k) * rows;
+		const int nrows = min(rows, a.sy - row0);
+		const long long base = state * a.G + (long long)row0 * sx;
+		const int toff = row0 * sx;
+		const int cnt = nrows * sx;
+		const R* m0 = a.do_inv ? mpre : mmid;
+		if (m0) {
 			for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
 				const int r = i / sx;
-				const int x = i - r * sx;
-				cur[r * L + x] = cscale(cur[r * L + x], mmid[toff + i]);
+				T& v = buf0[r * L + (i - r * sx)];
+				v = cscale(v, m0[toff + i]);
 			}
 			__syncthreads();
 		}
-	}
-	if (a.do_fwd) cur = line_transform<R, false>(cur, oth, a.lp, tw, nrows, 1, L, false);
+		T* cur_b = buf0;
+		T* oth = scr;
+		if (a.do_inv) {
+			cur_b = line_transform<R, false>(buf0, scr, a.lp, tw, nrows, 1, L, true);
+			oth = (cur_b == buf0) ? scr : buf0;
+			if (mmid) {
+				for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+					const int r = i / sx;
+					const int x = i - r * sx;
+					cur_b[r * L + x] = cscale(cur_b[r * L + x], mmid[toff + i]);
+				}
+				__syncthreads();
+			}
+		}
+		if (a.do_fwd) cur_b = line_transform<R, false>(cur_b, oth, a.lp, tw, nrows, 1, L, false);
 
-	T* out = reinterpret_cast<T*>(a.out) + base;
-	const T* acc = reinterpret_cast<const T*>(a.acc);
-	if (acc) acc += base;
-	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-		const int r = i / sx;
-		const int x = i - r * sx;
-		T v = cur[r * L + x];
-		if (a.do_fwd && mpost) v = cscale(v, mpost[toff + i]);
-		if (acc) v = cadd(v, acc[i]);
-		out[i] = v;
+		T* out = reinterpret_cast<T*>(a.out) + base;
+		const T* acc = reinterpret_cast<const T*>(a.acc);
+		if (acc) acc += base;
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / sx;
+			const int x = i - r * sx;
+			T v = cur_b[r * L + x];
+			if (a.do_fwd && mpost) v = cscale(v, mpost[toff + i]);
+			if (acc) v = cadd(v, acc[i]);
+			out[i] = v;
+		}
+		__syncthreads();  // the tile buffers are reused by the copy issued next iteration
+		cur ^= 1;
 	}
+	cp_wait<0>();
 }
 
+// Column pass, persistent and double-buffered like the row pass; tiles are
+// cols_per_tile columns x sy rows of one state, in place.
 template <class R>
-__global__ void __launch_bounds__(kThreads) col_pass_kernel(ColPassArgs a) {
+__global__ void __launch_bounds__(kThreads) col_pass_kernel(ColPassArgs a, int k) {
 	using T = c2<R>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
 	const int C = a.cols_per_tile;
-	T* buf0 = reinterpret_cast<T*>(smem_raw);
-	T* buf1 = buf0 + L * C;
-	T* tw = buf1 + L * C;
+	const int tsz = L * C;
+	T* tiles = reinterpret_cast<T*>(smem_raw);
+	T* scr = tiles + 2 * tsz;
+	T* tw = scr + tsz;
 	load_twiddles<R>(tw, a.lp);
-
-	const long long state = blockIdx.x;
-	const int col0 = blockIdx.y * C;
-	const int ncols = min(C, a.sx - col0);
 	const int sx = a.sx, sy = a.sy;
-	T* data = reinterpret_cast<T*>(a.data) + state * a.G + col0;
+	const int nct = (sx + C - 1) / C;
+	const long long total = (long long)k * nct;
+	const R* m2 = reinterpret_cast<const R*>(a.mul2d);
+	const R* m1 = reinterpret_cast<const R*>(a.mul1d);
 
-	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
-		const int y = i / C;
-		const int c = i - y * C;
-		buf0[y * C + c] = (c < ncols) ? data[(long long)y * sx + c] : mk<R>(0, 0);
-	}
-	__syncthreads();
-
-	T* cur = buf0;
-	T* oth = buf1;
-	if (a.mode == 0 || a.mode == 1) {
-		cur = line_transform<R, true>(cur, oth, a.lp, tw, C, C, 1, false);
-		oth = (cur == buf0) ? buf1 : buf0;
-	}
-	if (a.mode == 0) {
-		const R* m2 = reinterpret_cast<const R*>(a.mul2d);
-		const R* m1 = reinterpret_cast<const R*>(a.mul1d);
+	long long t = blockIdx.x;
+	int cur = 0;
+	auto issue = [&](T* dst, long long tt) {
+		const long long state = tt % k;
+		const int col0 = (int)(tt / k) * C;
+		const int ncols = min(C, sx - col0);
+		const T* src = reinterpret_cast<const T*>(a.data) + state * a.G + col0;
 		for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
 			const int y = i / C;
 			const int c = i - y * C;
-			if (c < ncols) {
-				const R f = m2 ? m2[y * sx + col0 + c] : m1[y];
-				cur[y * C + c] = cscale(cur[y * C + c], f);
+			if (c < ncols) cp_elem<R>(dst + y * C + c, src + (long long)y * sx + c);
+			else dst[y * C + c] = mk<R>(0, 0);
+		}
+	};
+	if (t < total) issue(tiles, t);
+	cp_commit();
+	for (; t < total; t += gridDim.x) {
+		const long long tn = t + gridDim.x;
+		if (tn < total) issue(tiles + (cur ^ 1) * tsz, tn);
+		cp_commit();
+		cp_wait<1>();
+		__syncthreads();
+
+		T* cur_b = tiles + cur * tsz;
+		T* oth = scr;
+		const long long state = t % k;
+		const int col0 = (int)(t / k) * C;
+		const int ncols = min(C, sx - col0);
+		if (a.mode == 0 || a.mode == 1) {
+			T* r0 = line_transform<R, true>(cur_b, oth, a.lp, tw, C, C, 1, false);
+			oth = (r0 == cur_b) ? oth : cur_b;
+			cur_b = r0;
+		}
+		if (a.mode == 0) {
+			for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+				const int y = i / C;
+				const int c = i - y * C;
+				if (c < ncols) {
+					const R f = m2 ? m2[y * sx + col0 + c] : m1[y];
+					cur_b[y * C + c] = cscale(cur_b[y * C + c], f);
+				}
 			}
+			__syncthreads();
+		}
+		if (a.mode == 0 || a.mode == 2) cur_b = line_transform<R, true>(cur_b, oth, a.lp, tw, C, C, 1, true);
+
+		T* data = reinterpret_cast<T*>(a.data) + state * a.G + col0;
+		for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
+			const int y = i / C;
+			const int c = i - y * C;
+			if (c < ncols) data[(long long)y * sx + c] = cur_b[y * C + c];
 		}
 		__syncthreads();
+		cur ^= 1;
 	}
-	if (a.mode == 0 || a.mode == 2) cur = line_transform<R, true>(cur, oth, a.lp, tw, C, C, 1, true);
-
-	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
-		const int y = i / C;
-		const int c = i - y * C;
-		if (c < ncols) data[(long long)y * sx + c] = cur[y * C + c];
-	}
+	cp_wait<0>();
 }
 
 // Deterministic block reduction of NV doubles; result valid in thread 0.
@@ -354,26 +421,45 @@ size_t row_pass_smem(int L, int rows, int n_fft, int elem_bytes) {
 	return (size_t)(2 * rows * L + n_fft) * elem_bytes + 5 * sizeof(double) * (kThreads / 32);
 }
 
+size_t pipe_smem(int L, int lines, int n_fft, int elem_bytes) {
+	return (size_t)(3 * lines * L + n_fft) * elem_bytes;
+}
+
 size_t col_pass_smem(int L, int cols, int n_fft, int elem_bytes) {
 	return (size_t)(2 * cols * L + n_fft) * elem_bytes + 5 * sizeof(double) * (kThreads / 32);
+}
+
+// Persistent grid: as many CTAs as fit on the device, at most one per tile.
+template <class K>
+int persistent_blocks(K kernel, size_t smem, long long tiles) {
+	static int sms = 0;
+	if (!sms) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	}
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+	const long long b = (long long)std::max(1, per_sm) * std::max(1, sms);
+	return (int)std::max(1LL, std::min(b, tiles));
 }
 
 template <class R>
 void launch_row_pass(const RowPassArgs& a, int k, const void*, cudaStream_t s) {
 	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
-	const dim3 grid(k, (a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
-	const size_t sm = row_pass_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	const size_t sm = pipe_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
 	set_smem_limit(row_pass_kernel<R>);
-	row_pass_kernel<R><<<grid, kThreads, sm, s>>>(a);
+	const long long tiles = (long long)k * ((a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
+	row_pass_kernel<R><<<persistent_blocks(row_pass_kernel<R>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
 template <class R>
 void launch_col_pass(const ColPassArgs& a, int k, const void*, cudaStream_t s) {
 	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
-	const dim3 grid(k, (a.sx + a.cols_per_tile - 1) / a.cols_per_tile);
-	const size_t sm = col_pass_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));
+	const size_t sm = pipe_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));
 	set_smem_limit(col_pass_kernel<R>);
-	col_pass_kernel<R><<<grid, kThreads, sm, s>>>(a);
+	const long long tiles = (long long)k * ((a.sx + a.cols_per_tile - 1) / a.cols_per_tile);
+	col_pass_kernel<R><<<persistent_blocks(col_pass_kernel<R>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
 template <class R>

@@ -94,5 +94,7 @@ int row_tile_rows(int L, int elem_bytes, int sy);
 int col_tile_cols(int L, int elem_bytes, int sx);
 size_t row_pass_smem(int L, int rows, int n_fft, int elem_bytes);
 size_t col_pass_smem(int L, int cols, int n_fft, int elem_bytes);
+// Shared memory of the persistent double-buffered row/column passes.
+size_t pipe_smem(int L, int lines, int n_fft, int elem_bytes);
 
 }  // namespace itp2d
