@@ -114,7 +114,10 @@ int itp2d_orthonormalize(itp2d_ctx* ctx, int algo, int* bad_index, double* bad_v
  * (itpsystem.cpp:116-119): E = Re<psi|H psi>, sigma = Re sqrt(<H^2> - <H>^2)
  * with <H^2> = <H psi|H psi>. sigma_residual = ||H psi - E psi|| (no
  * cancellation floor). Arrays hold num_states doubles; sigma_residual and
- * E_imag may be NULL. */
+ * E_imag may be NULL. In the FP32 form every expectation value is divided by
+ * <psi|psi> (Rayleigh quotients), so that the FP32 accuracy of the state norms
+ * does not enter E at first order; the FP64 form follows the reference
+ * (states taken as normalised). */
 int itp2d_energies(itp2d_ctx* ctx, double* E, double* sigma, double* sigma_residual, double* E_imag);
 
 /* states <- H states (Hamiltonian OperatorSum of itpsystem.cpp:116-119),
@@ -130,6 +133,23 @@ int itp2d_transform(itp2d_ctx* ctx, int kind);
  * the tables. The FP32 form switches to FP64 at its accuracy floor to refine
  * the eigenpairs; no reference counterpart (the reference is FP64 only). */
 int itp2d_set_precision(itp2d_ctx* ctx, int precision);
+
+/* Contraction engine of the orthonormalisation (overlap S = Psi^H Psi and
+ * rotation Psi W) for FP32 states. ITP2D_CONTRACT_AUTO uses the tensor cores
+ * (tcgen05, each FP32 value split into three BF16 parts, FP32 accumulation
+ * over grid chunks of at most 2048 points, chunks summed in FP64) when the
+ * grid has an even number of points, else the FP64 path.
+ * ITP2D_CONTRACT_FP64 always uses FP64 arithmetic (DMMA). FP64 states always
+ * use FP64 arithmetic. No reference counterpart (the reference is FP64 only;
+ * stateset.cpp:146-154 and 214-228 compute these products with ZHERK/ZGEMM). */
+enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1 };
+int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
+
+/* Overlap matrix of the resident states, S_ij = <psi_i|psi_j> dx^2
+ * (row-major, num_states^2 interleaved complex doubles), computed by the
+ * engine itp2d_orthonormalize would use; the states are not changed.
+ * The product of stateset.cpp:146-154. */
+int itp2d_overlap_matrix(itp2d_ctx* ctx, double* S);
 
 /* Waits for the context's stream. */
 int itp2d_synchronize(itp2d_ctx* ctx);

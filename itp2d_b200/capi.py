@@ -24,6 +24,7 @@ E_TIMEOUT, E_UNSUPPORTED = 7, 8
 PERIODIC, DIRICHLET = 0, 1
 FP64, FP32 = 0, 1
 ORTHO_DEFAULT, ORTHO_HIGHMEM = 0, 1
+CONTRACT_AUTO, CONTRACT_FP64 = 0, 1
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
 
@@ -64,6 +65,8 @@ def lib():
         L.itp2d_apply_hamiltonian.argtypes = [vp]
         L.itp2d_transform.argtypes = [vp, i]
         L.itp2d_synchronize.argtypes = [vp]
+        L.itp2d_set_contraction.argtypes = [vp, i]
+        L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
         L.itp2d_set_timing.argtypes = [vp, i]
@@ -169,6 +172,14 @@ class Context:
         st = lib().itp2d_orthonormalize(self.h, algo, C.byref(bi), C.byref(bv))
         if st != OK:
             raise ITP2DError(st, "itp2d_orthonormalize", bi.value, bv.value)
+
+    def set_contraction(self, engine=CONTRACT_AUTO):
+        _check(lib().itp2d_set_contraction(self.h, engine), "itp2d_set_contraction")
+
+    def overlap_matrix(self):
+        S = np.empty((self.k, self.k), dtype=np.complex128)
+        _check(lib().itp2d_overlap_matrix(self.h, _dp(S.view(np.float64))), "itp2d_overlap_matrix")
+        return S
 
     def energies(self):
         E, s, r, ei = (np.empty(self.k) for _ in range(4))

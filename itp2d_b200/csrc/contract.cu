@@ -279,8 +279,12 @@ void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npa
 	chunk = ((chunk + kBK - 1) / kBK) * kBK;
 	const int used = (int)((G + chunk - 1) / chunk);
 	overlap_kernel<T><<<dim3(npairs, used), 256, 0, s>>>(psi, k, G, pairs, chunk, part);
+	launch_overlap_finish(part, k, used, dx2, S, s);
+}
+
+void launch_overlap_finish(const double2* part, int k, int nsplit, double dx2, double2* S, cudaStream_t s) {
 	const long long kk = (long long)k * k;
-	overlap_finish_kernel<<<(unsigned)((kk + 255) / 256), 256, 0, s>>>(part, k, used, dx2, S);
+	overlap_finish_kernel<<<(unsigned)((kk + 255) / 256), 256, 0, s>>>(part, k, nsplit, dx2, S);
 }
 
 template <class T>

@@ -12,6 +12,21 @@ void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npa
 		double2* part, double dx2, double2* S, cudaStream_t s);
 template <class T>
 void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s);
+// Sums the nsplit partial k x k blocks of part (upper triangle i <= j used),
+// scales by dx2 and writes the full Hermitian S.
+void launch_overlap_finish(const double2* part, int k, int nsplit, double dx2, double2* S, cudaStream_t s);
+
+// Tensor-core (tcgen05, split-BF16, FP32 accumulation) contractions of FP32
+// states; *err receives ITP2D_E_TIMEOUT if a bounded wait ran out.
+bool tc_supported(int k, long long G);
+int tc_overlap_splits(int k, long long G, int num_sms);
+void launch_overlap_tc(const float2* psi, int k, long long G, int nsplit, double2* part, double dx2, double2* S,
+		int* err, cudaStream_t s);
+// wsplit: tc_wsplit_bytes(k) bytes of device scratch (W^T split into BF16 planes).
+size_t tc_wsplit_bytes(int k);
+void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit, float2* out,
+		int* err, cudaStream_t s);
+
 template <class T>
 void launch_normalize1(T* psi, long long G, double dx, double* tmp, cudaStream_t s);
 // Converts n complex values between double2 (in_fp64 = 1) and float2.

@@ -83,6 +83,11 @@ struct itp2d_ctx {
 	EigStatus* hstat = nullptr;
 	double* dnorm = nullptr;
 	int last_sweeps = 0;
+	int engine = ITP2D_CONTRACT_AUTO;
+	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
+	int* dflag = nullptr;  // tensor-core wait time-outs (device)
+	unsigned char* wsplit = nullptr;  // W^T in BF16 planes (tensor-core rotation)
+	int* hflag = nullptr;  // pinned copy
 	// energies
 	double* sums = nullptr;
 	double* dE = nullptr;
@@ -499,8 +504,8 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 		c->launches++;
 		if (want_sums) {
 			const int nt = (c->sy + a.rows_per_tile - 1) / a.rows_per_tile;
-			launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->dE, c->dsig, c->dres, c->dEi,
-					c->stream);
+			launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->precision == ITP2D_FP32, c->dE,
+					c->dsig, c->dres, c->dEi, c->stream);
 			c->launches++;
 		}
 		return ITP2D_OK;
@@ -524,8 +529,8 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 	c->launches++;
 	if (want_sums) {
 		const int nt = (c->sx + b.cols_per_tile - 1) / b.cols_per_tile;
-		launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->dE, c->dsig, c->dres, c->dEi,
-				c->stream);
+		launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->precision == ITP2D_FP32, c->dE,
+				c->dsig, c->dres, c->dEi, c->stream);
 		c->launches++;
 	}
 	return ITP2D_OK;
@@ -577,6 +582,7 @@ int itp2d_ctx_destroy(itp2d_ctx* c) {
 	for (void* p : c->table_allocs) cudaFree(p);
 	if (c->hstat) cudaFreeHost(c->hstat);
 	if (c->hbuf) cudaFreeHost(c->hbuf);
+	if (c->hflag) cudaFreeHost(c->hflag);
 	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 	delete c;
 	return ITP2D_OK;
@@ -620,7 +626,12 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	c->nsplit = std::max(1, std::min((4 * c->num_sms + c->npairs - 1) / c->npairs, (int)std::max(1LL, c->G / 512)));
 	const int kp = std::max(bjacobi_padded(k), (k + 1) & ~1);  // covers the scalar and block layouts
 	if (e == cudaSuccess) c->S = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
-	if (e == cudaSuccess) c->part = (double2*)dalloc(c, (size_t)c->nsplit * k * k * sizeof(double2), &e);
+	c->tc_nsplit = tc_overlap_splits(k, c->G, c->num_sms);
+	const int parts = std::max(c->nsplit, c->tc_nsplit);
+	if (e == cudaSuccess) c->part = (double2*)dalloc(c, (size_t)parts * k * k * sizeof(double2), &e);
+	if (e == cudaSuccess) c->dflag = (int*)dalloc(c, sizeof(int), &e);
+	if (e == cudaSuccess) e = cudaMemset(c->dflag, 0, sizeof(int));
+	if (e == cudaSuccess && tc_supported(k, c->G)) c->wsplit = (unsigned char*)dalloc(c, tc_wsplit_bytes(k), &e);
 	if (e == cudaSuccess) c->W = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
 	if (e == cudaSuccess) c->pairs = (int2*)dalloc(c, (size_t)c->npairs * sizeof(int2), &e);
 	c->jw.max_sweeps = 60;
@@ -646,6 +657,7 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 		e = cudaMemset(c->dE, 0, (size_t)5 * k * sizeof(double));
 	}
 	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hstat, sizeof(EigStatus));
+	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hflag, sizeof(int));
 	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hbuf, (size_t)4 * k * sizeof(double));
 	if (e == cudaSuccess) {
 		std::vector<int2> pr;
@@ -787,6 +799,52 @@ int itp2d_transform(itp2d_ctx* c, int kind) {
 	return cuda_status(cudaGetLastError());
 }
 
+namespace {
+
+bool use_tensor_cores(const itp2d_ctx* c) {
+	return c->precision == ITP2D_FP32 && c->engine == ITP2D_CONTRACT_AUTO && tc_supported(c->k, c->G);
+}
+
+// S = Psi^H Psi dx^2 (full Hermitian, row-major) by the selected engine.
+void launch_overlap_any(itp2d_ctx* c, bool tc) {
+	if (tc)
+		launch_overlap_tc((const float2*)c->psi, c->k, c->G, c->tc_nsplit, c->part, c->dx * c->dx, c->S, c->dflag,
+				c->stream);
+	else if (c->precision == ITP2D_FP64)
+		launch_overlap((const double2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part, c->dx * c->dx,
+				c->S, c->stream);
+	else
+		launch_overlap((const float2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part, c->dx * c->dx,
+				c->S, c->stream);
+	c->launches += 2;
+}
+
+}  // namespace
+
+int itp2d_set_contraction(itp2d_ctx* c, int engine) {
+	if (!c || (engine != ITP2D_CONTRACT_AUTO && engine != ITP2D_CONTRACT_FP64)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->engine = engine;
+	return ITP2D_OK;
+}
+
+int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
+	if (!c || !S) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	const bool tc = use_tensor_cores(c);
+	launch_overlap_any(c, tc);
+	ITP2D_TRY(cudaGetLastError());
+	ITP2D_TRY(cudaMemcpyAsync(S, c->S, (size_t)c->k * c->k * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	if (tc && *c->hflag != ITP2D_OK) {
+		const int f = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+		return f;
+	}
+	return ITP2D_OK;
+}
+
 int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_value) {
 	if (!c || (algo != ITP2D_ORTHO_DEFAULT && algo != ITP2D_ORTHO_HIGHMEM)) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
@@ -801,15 +859,10 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		ITP2D_TRY(cudaStreamSynchronize(c->stream));
 		return ITP2D_OK;
 	}
+	const bool tc = use_tensor_cores(c);
 	{
 		PhaseTimer t(c, kOverlap);
-		if (f64)
-			launch_overlap((const double2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
-					c->dx * c->dx, c->S, c->stream);
-		else
-			launch_overlap((const float2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
-					c->dx * c->dx, c->S, c->stream);
-		c->launches += 2;
+		launch_overlap_any(c, tc);
 	}
 	{
 		PhaseTimer t(c, kEigen);
@@ -818,15 +871,24 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	}
 	{
 		PhaseTimer t(c, kRotate);
-		if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
+		if (tc)
+			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
+					c->stream);
+		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
-		c->launches += 1;
+		c->launches += tc ? 2 : 1;
 	}
+	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaGetLastError());
 	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
 	const EigStatus s = *c->hstat;
 	c->last_sweeps = s.sweeps;
+	if (tc && *c->hflag != ITP2D_OK) {
+		const int f = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+		return f;
+	}
 	if (s.status != ITP2D_OK) {
 		if (bad_index) *bad_index = s.bad_index;
 		if (bad_value) *bad_value = s.bad_value;

@@ -366,7 +366,8 @@ __global__ void __launch_bounds__(kThreads) energy_col_kernel(EnergyColArgs a) {
 }
 
 __global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int ntiles, double dx2,
-		const double* __restrict__ Eshift, double* E, double* sigma, double* sigma_res, double* E_imag) {
+		const double* __restrict__ Eshift, int normalize, double* E, double* sigma, double* sigma_res,
+		double* E_imag) {
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= k) return;
@@ -376,7 +377,9 @@ __global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int
 	for (int j = 0; j < 5; j++)
 		for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
 	if (lane == 0) {
-		const double er = s[0] * dx2, ei = s[1] * dx2, m2 = s[2] * dx2;
+		// normalize: Rayleigh quotients <psi|H psi> / <psi|psi> (and <H^2> likewise)
+		const double inv = normalize ? 1.0 / (s[4] * dx2) : 1.0;
+		const double er = s[0] * dx2 * inv, ei = s[1] * dx2 * inv, m2 = s[2] * dx2 * inv;
 		// sigma = Re sqrt(<H^2> - <H>^2) with complex <H> (operators.cpp:46-49)
 		const double zr = m2 - (er * er - ei * ei);
 		const double zi = -2.0 * er * ei;
@@ -384,7 +387,7 @@ __global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int
 		const double sg = sqrt(fmax(0.0, 0.5 * (az + zr)));
 		const double es = Eshift ? Eshift[warp] : 0.0;
 		const double de = er - es;
-		const double res2 = s[3] * dx2 - de * de * (s[4] * dx2);
+		const double res2 = normalize ? s[3] * dx2 * inv - de * de : s[3] * dx2 - de * de * (s[4] * dx2);
 		E[warp] = er;
 		sigma[warp] = sg;
 		if (sigma_res) sigma_res[warp] = sqrt(fmax(0.0, res2));
@@ -480,11 +483,12 @@ void launch_energy_col(const EnergyColArgs& a, int k, const void*, cudaStream_t 
 	energy_col_kernel<R><<<grid, kThreads, sm, s>>>(a);
 }
 
-void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift,
+void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift, int normalize,
 		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s) {
 	const int threads = 128;
 	const int blocks = (k * 32 + threads - 1) / threads;
-	energy_finish_kernel<<<blocks, threads, 0, s>>>(sums, k, ntiles, dx2, Eshift, E, sigma, sigma_res, E_imag);
+	energy_finish_kernel<<<blocks, threads, 0, s>>>(sums, k, ntiles, dx2, Eshift, normalize, E, sigma, sigma_res,
+			E_imag);
 }
 
 template void launch_row_pass<double>(const RowPassArgs&, int, const void*, cudaStream_t);

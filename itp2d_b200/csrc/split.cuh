@@ -85,8 +85,10 @@ template <class R> void launch_energy_row(const EnergyRowArgs& a, int k, const v
 template <class R> void launch_energy_col(const EnergyColArgs& a, int k, const void* tw, cudaStream_t s);
 
 // Per-state reduction of the energy partial sums into E, sigma and the
-// residual deviation (deterministic order).
-void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift,
+// residual deviation (deterministic order). normalize != 0 divides by
+// <psi|psi> (Rayleigh quotients; used by the FP32 form, whose contractions
+// leave norms exact only to FP32 accuracy).
+void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift, int normalize,
 		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s);
 
 // Tile sizes (rows or columns per CTA) for a line length L (complex entries).

@@ -1,0 +1,543 @@
+// Orthonormalisation contractions of the FP32 form on the 5th-generation
+// tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulation in
+// tensor memory).
+//
+//   overlap:  S_ij = sum_g conj(psi_i[g]) psi_j[g]        (stateset.cpp:146-154)
+//   rotation: out_n[g] = sum_i W[i][n] psi_i[g]           (stateset.cpp:214-228)
+//
+// Every FP32 operand value x is split into three BF16 parts x = h + m + l
+// (24 significant bits), and each real product x*y is formed from the six
+// partial products h h, h m, m h, h l, l h, m m; the dropped terms are below
+// 2^-24 relative. A complex product takes four real products; the imaginary
+// part's "- Ai Br" term uses the instruction descriptor's negate-A bit.
+//
+// Each MMA rounds its FP32 accumulator once, with an error relative to the
+// accumulator's magnitude, so the h h products (the bulk of the sum) go to
+// their own accumulator and the five smaller products to a second one, whose
+// rounding errors are 2^-8 smaller relative to the result; the epilogue adds
+// the two in FP64. The overlap bounds the K range one accumulator sees (grid
+// chunks, summed in FP64 afterwards).
+//
+// One CTA (8 warps) owns a 128 x 128 output tile in tensor memory (512
+// columns: large-part real, imaginary, small-part real, imaginary). K
+// advances 16 per step (one MMA depth). Per step:
+//   * cp.async fetches the FP32 operand tiles of step s + 2 into a ring of
+//     three raw slots (16-byte pieces, XOR-swizzled against bank conflicts);
+//   * all threads split the raw tile of step s into six BF16 planes in the
+//     K-major canonical layout without swizzle (8 x 16-byte core matrices,
+//     LBO 128 B between the two K halves, SBO 256 B between 8-row groups),
+//     one core matrix per warp store;
+//   * one thread issues the 24 MMAs and commits them to an mbarrier; two
+//     plane buffers let the split of step s + 1 overlap the MMAs of step s.
+// The rotation's A operand W^T is split once per call by split_w_kernel into
+// global memory in exactly the shared-memory plane layout, and cp.async copies
+// it into a ring of four plane slots that the MMAs read in place.
+//
+// Waits on mbarriers are bounded: on time-out the kernel records
+// ITP2D_E_TIMEOUT, waits (bounded) for its MMAs, frees its tensor memory and
+// returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/itp2d_gpu.h"
+#include "contract.cuh"
+
+namespace itp2d {
+
+namespace {
+
+constexpr int TM = 128;                                // tile rows (M)
+constexpr int TN = 128;                                // tile cols (N)
+constexpr int KT = 16;                                 // K per step
+constexpr int kThreads = 256;
+constexpr int kPlaneBytes = TM * KT * 2;               // 4 KB: one BF16 plane of a 128 x 16 operand
+constexpr int kOperandBytes = 6 * kPlaneBytes;         // 24 KB: re/im x hi/mid/lo
+constexpr int kRawRowBytes = KT * 8;                   // 128 B: 16 complex FP32
+constexpr int kTmemCols = 512;
+constexpr long long kSpinLimit = 1LL << 24;            // ~1 s with the back-off below
+
+// Shared memory map (bytes from the 1024-aligned base).
+//   overlap:  planes[2] x (A, B) 96 KB | raw[3] x (A, B) 96 KB
+//   rotation: B planes[2] 48 KB | A plane ring[4] 96 KB | raw psi[3] 48 KB
+constexpr int kBufBytes = 192 * 1024;
+constexpr int kOvPlanes = 0;
+constexpr int kOvRaw = 2 * 2 * kOperandBytes;
+constexpr int kOvRawSlot = 2 * TM * kRawRowBytes;      // 32 KB
+constexpr int kRoB = 0;
+constexpr int kRoA = 2 * kOperandBytes;
+constexpr int kRoRaw = kRoA + 4 * kOperandBytes;
+constexpr int kRoRawSlot = KT * TN * 8;                // 16 KB: 16 rows (i) x 128 complex (g)
+static_assert(kOvRaw + 3 * kOvRawSlot <= kBufBytes, "overlap shared memory");
+static_assert(kRoRaw + 3 * kRoRawSlot <= kBufBytes, "rotation shared memory");
+static_assert(8 * 32 * 33 * 16 <= kBufBytes, "epilogue staging");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: K-major, no swizzle, version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+	const uint64_t lbo = 128, sbo = 256;
+	uint64_t d = 0;
+	d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+	d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+	d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+	d |= (uint64_t)1 << 46;
+	return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = 128, N = 128.
+__host__ __device__ constexpr uint32_t idesc(bool negate_a) {
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((negate_a ? 1u : 0u) << 13) | ((uint32_t)(TN >> 3) << 17) |
+	       ((uint32_t)(TM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+	const uint32_t z = 0;
+	asm volatile(
+			"{\n\t.reg .pred p;\n\t"
+			"setp.ne.b32 p, %4, 0;\n\t"
+			"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+			:
+			: "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+
+// Bounded wait for the phase with the given parity. Returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+	for (long long i = 0; i < kSpinLimit; i++) {
+		uint32_t done;
+		asm volatile(
+				"{\n\t.reg .pred P1;\n\t"
+				"mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+				"selp.b32 %0, 1, 0, P1;\n\t}\n"
+				: "=r"(done)
+				: "r"(mbar), "r"(parity)
+				: "memory");
+		if (done) return true;
+		if (i > 64) __nanosleep(64);
+	}
+	return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16-byte global -> shared copy; src_bytes = 0 writes zeros without reading.
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, int src_bytes) {
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+	uint32_t r[32];
+	asm volatile(
+			"tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+			"{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+			"%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+			: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+			  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+			  "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+			  "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+			: "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+	for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Three-way BF16 split of an FP32 value (x = h + m + l exactly).
+__device__ __forceinline__ void split3(float x, uint32_t& h, uint32_t& m, uint32_t& l) {
+	const __nv_bfloat16 bh = __float2bfloat16_rn(x);
+	const float r1 = x - __bfloat162float(bh);
+	const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
+	const float r2 = r1 - __bfloat162float(bm);
+	h = __bfloat16_as_ushort(bh);
+	m = __bfloat16_as_ushort(bm);
+	l = __bfloat16_as_ushort(__float2bfloat16_rn(r2));
+}
+
+// Byte offset of element (row r, k) of a K-major no-swizzle 128 x 16 plane:
+// core matrix (r / 8, k / 8) at ((r / 8) * 2 + k / 8) * 128, rows 16 B apart.
+__host__ __device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
+	return (uint32_t)((((r >> 3) << 1) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Writes two consecutive K elements (k even) of row r, split into the six
+// planes of one operand: planes 0..2 real hi/mid/lo, 3..5 imaginary.
+__device__ __forceinline__ void put2(unsigned char* op, uint32_t off, float re0, float im0, float re1, float im1) {
+	uint32_t h0, m0, l0, h1, m1, l1;
+	split3(re0, h0, m0, l0);
+	split3(re1, h1, m1, l1);
+	*reinterpret_cast<uint32_t*>(op + 0 * kPlaneBytes + off) = h0 | (h1 << 16);
+	*reinterpret_cast<uint32_t*>(op + 1 * kPlaneBytes + off) = m0 | (m1 << 16);
+	*reinterpret_cast<uint32_t*>(op + 2 * kPlaneBytes + off) = l0 | (l1 << 16);
+	split3(im0, h0, m0, l0);
+	split3(im1, h1, m1, l1);
+	*reinterpret_cast<uint32_t*>(op + 3 * kPlaneBytes + off) = h0 | (h1 << 16);
+	*reinterpret_cast<uint32_t*>(op + 4 * kPlaneBytes + off) = m0 | (m1 << 16);
+	*reinterpret_cast<uint32_t*>(op + 5 * kPlaneBytes + off) = l0 | (l1 << 16);
+}
+
+// The 24 MMAs of one step. Accumulators: h h products in columns 0..255
+// (real 0..127, imaginary 128..255), the other five in 256..511 likewise.
+// conjA selects conj(A) B (overlap) instead of A B (rotation).
+__device__ __forceinline__ void issue_step(uint32_t tmem, uint32_t abase, uint32_t bbase, bool conjA, bool first) {
+	const uint32_t id = idesc(false), idn = idesc(true);
+#pragma unroll
+	for (int t = 0; t < 6; t++) {
+		// split pairs (p, q): hh, hm, mh, hl, lh, mm
+		const int p = (t == 2 || t == 5) ? 1 : (t == 4 ? 2 : 0);
+		const int q = (t == 1 || t == 5) ? 1 : (t == 3 ? 2 : 0);
+		const uint32_t cre = tmem + (t == 0 ? 0 : 2 * TN), cim = cre + TN;
+		const uint32_t acc = (first && t <= 1) ? 0u : 1u;
+		const uint64_t ar = sdesc(abase + p * kPlaneBytes), ai = sdesc(abase + (3 + p) * kPlaneBytes);
+		const uint64_t br = sdesc(bbase + q * kPlaneBytes), bi = sdesc(bbase + (3 + q) * kPlaneBytes);
+		// (a) A B:        re = ar br - ai bi,  im = ar bi + ai br
+		// (b) conj(A) B:  re = ar br + ai bi,  im = ar bi - ai br
+		umma(cre, ar, br, id, acc);
+		umma(cre, ai, bi, conjA ? id : idn, 1u);
+		umma(cim, ar, bi, id, acc);
+		umma(cim, ai, br, conjA ? idn : id, 1u);
+	}
+}
+
+struct TcShared {
+	alignas(1024) unsigned char buf[kBufBytes];
+	alignas(8) unsigned long long mbar[2];
+	uint32_t tmem_base;
+	int abort;
+};
+
+__device__ TcShared& tc_shared() {
+	extern __shared__ __align__(1024) unsigned char smem_raw[];
+	return *reinterpret_cast<TcShared*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+}
+
+__device__ void tc_setup(TcShared& sh) {
+	if (threadIdx.x < 32) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
+				"r"(kTmemCols)
+				: "memory");
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+	}
+	if (threadIdx.x == 0) {
+		mbar_init(smem_u32(&sh.mbar[0]), 1);
+		mbar_init(smem_u32(&sh.mbar[1]), 1);
+		sh.abort = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+}
+
+__device__ void tc_teardown(TcShared& sh) {
+	tc_fence_before();
+	__syncthreads();
+	if (threadIdx.x < 32)
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh.tmem_base), "r"(kTmemCols)
+				: "memory");
+}
+
+// The step pipeline. prefetch(s) issues the cp.async copies of step s (called
+// for s < nsteps only; one group is committed per step whether or not it
+// copies, so that group counting stays uniform). convert(s) turns the raw
+// slot of step s into the plane buffer s & 1. a_addr(s) / b_addr(s) give the
+// shared-memory bases the MMAs of step s read. Returns with the accumulators
+// complete, or with sh.abort set.
+template <class Prefetch, class Convert, class AAddr, class BAddr>
+__device__ void run_pipeline(TcShared& sh, int nsteps, bool conjA, Prefetch prefetch, Convert convert, AAddr a_addr,
+		BAddr b_addr, int* err) {
+	const int tid = threadIdx.x;
+	const uint32_t mb0 = smem_u32(&sh.mbar[0]), mb1 = smem_u32(&sh.mbar[1]);
+	if (nsteps > 0) prefetch(0);
+	cp_commit();
+	if (nsteps > 1) prefetch(1);
+	cp_commit();
+	int ran = 0;
+	for (int s = 0; s < nsteps; s++) {
+		if (s >= 2) {  // the MMAs of step s - 2 read the plane buffer (and ring slot) reused now
+			const bool ok = mbar_wait((s & 1) ? mb1 : mb0, (uint32_t)(((s >> 1) - 1) & 1));
+			if (!__syncthreads_and(ok)) {
+				if (tid == 0) {
+					sh.abort = 1;
+					atomicExch(err, ITP2D_E_TIMEOUT);
+				}
+				break;
+			}
+		}
+		if (s + 2 < nsteps) prefetch(s + 2);
+		cp_commit();
+		cp_wait<2>();  // this thread's copies of step s have landed
+		__syncthreads();
+		convert(s);
+		proxy_fence();
+		__syncthreads();
+		if (tid == 0) {
+			tc_fence_after();
+			issue_step(sh.tmem_base, a_addr(s), b_addr(s), conjA, s == 0);
+			umma_commit((s & 1) ? mb1 : mb0);
+		}
+		ran = s + 1;
+	}
+	cp_wait<0>();
+	// drain: the last commit of each barrier (bounded, also after an abort)
+	for (int b = 0; b < 2; b++) {
+		const int commits = (ran - b + 1) / 2;
+		if (commits <= 0) continue;
+		const bool ok = mbar_wait(b ? mb1 : mb0, (uint32_t)((commits - 1) & 1));
+		if (!__syncthreads_and(ok) && tid == 0) {
+			sh.abort = 1;
+			atomicExch(err, ITP2D_E_TIMEOUT);
+		}
+	}
+	tc_fence_after();
+	__syncthreads();
+}
+
+// Epilogue: the tile (large and small accumulators added in FP64) leaves
+// through a per-warp 32 x 32 staging square in the idle pipeline buffers, so
+// that each global store of a warp covers 32 consecutive columns of one row.
+// Warp w reads TMEM lanes 32 (w % 4) .. + 31 and columns 64 (w / 4) .. + 63.
+// emit(r, c, re, im) stores one element.
+template <class Emit>
+__device__ void store_tile(TcShared& sh, Emit emit) {
+	const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int q = w & 3, half = w >> 2;
+	double2* buf = reinterpret_cast<double2*>(sh.buf) + w * 32 * 33;
+	const uint32_t trow = sh.tmem_base + ((uint32_t)(q * 32) << 16);
+	for (int c = half * 64; c < half * 64 + 64; c += 32) {
+		float big[32], small[32];
+		tmem_ld32(trow + c, big);
+		tmem_ld32(trow + 2 * TN + c, small);
+#pragma unroll
+		for (int j = 0; j < 32; j++) buf[lane * 33 + j].x = (double)big[j] + (double)small[j];
+		tmem_ld32(trow + TN + c, big);
+		tmem_ld32(trow + 3 * TN + c, small);
+#pragma unroll
+		for (int j = 0; j < 32; j++) buf[lane * 33 + j].y = (double)big[j] + (double)small[j];
+		__syncwarp();
+		for (int r = 0; r < 32; r++) {
+			const double2 v = buf[r * 33 + lane];
+			emit(q * 32 + r, c + lane, v.x, v.y);
+		}
+		__syncwarp();
+	}
+}
+
+// Overlap tile pair (ti <= tj) from blockIdx.x, K range [g0, g1) from
+// blockIdx.y; writes the partial S block of split blockIdx.y.
+__global__ void __launch_bounds__(kThreads, 1) overlap_tc_kernel(const float2* __restrict__ psi, int k, long long G,
+		int ntiles, long long chunk, double2* __restrict__ part, int* err) {
+	TcShared& sh = tc_shared();
+	int p = blockIdx.x, ti = 0;
+	while (p >= ntiles - ti) {
+		p -= ntiles - ti;
+		ti++;
+	}
+	const int tj = ti + p;
+	const int i0 = ti * TM, j0 = tj * TN;
+	const long long g0 = (long long)blockIdx.y * chunk;
+	const long long g1 = min(G, g0 + chunk);
+	const int nsteps = (int)((g1 - g0 + KT - 1) / KT);
+	tc_setup(sh);
+	const int tid = threadIdx.x;
+	unsigned char* const base = sh.buf;
+	// raw slot: operand o (0 = rows i0.., 1 = rows j0..), row r, 16-byte piece
+	// pc (two complex) stored at slot pc ^ 4 (r & 1)
+	auto prefetch = [&](int s) {
+		unsigned char* slot = base + kOvRaw + (s % 3) * kOvRawSlot;
+		const long long gb = g0 + (long long)s * KT;
+#pragma unroll
+		for (int it = 0; it < 8; it++) {
+			const int idx = it * kThreads + tid;  // 0..2047
+			const int o = idx >> 10, r = (idx >> 3) & 127, pc = idx & 7;
+			const int row = (o ? j0 : i0) + r;
+			const long long g = gb + 2 * pc;
+			const bool in = row < k && g < g1;  // g even, g1 even: both complex in range
+			const float2* src = in ? psi + (long long)row * G + g : psi;
+			cp16(smem_u32(slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4)), src,
+					in ? 16 : 0);
+		}
+	};
+	// convert: warp w handles core matrices m = w, w + 8, ... of the 64 (two
+	// operands x 16 row groups x 2 K halves); lane = (row in group) * 4 + pair
+	auto convert = [&](int s) {
+		const unsigned char* slot = base + kOvRaw + (s % 3) * kOvRawSlot;
+		unsigned char* planes = base + kOvPlanes + (s & 1) * 2 * kOperandBytes;
+		const int w = tid >> 5, lane = tid & 31;
+#pragma unroll
+		for (int it = 0; it < 8; it++) {
+			const int m = it * 8 + w;
+			const int o = m >> 5, rg = (m >> 1) & 15, kc = m & 1;
+			const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+			const int pc = kk >> 1;
+			const float4 v = *reinterpret_cast<const float4*>(
+					slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4));
+			put2(planes + o * kOperandBytes, kmaj_off(r, kk), v.x, v.y, v.z, v.w);
+		}
+	};
+	auto a_addr = [&](int s) { return smem_u32(base + kOvPlanes + (s & 1) * 2 * kOperandBytes); };
+	auto b_addr = [&](int s) { return smem_u32(base + kOvPlanes + (s & 1) * 2 * kOperandBytes + kOperandBytes); };
+	run_pipeline(sh, nsteps, true, prefetch, convert, a_addr, b_addr, err);
+	if (!sh.abort) {
+		double2* out = part + (size_t)blockIdx.y * k * k;
+		store_tile(sh, [&](int r, int c, double re, double im) {
+			const int i = i0 + r, j = j0 + c;
+			if (i < k && j < k) out[(size_t)i * k + j] = make_double2(re, im);
+		});
+	}
+	tc_teardown(sh);
+}
+
+// W^T split into BF16 planes, in the shared-memory layout of the rotation's A
+// operand: block (n tile nt, K step s) of kOperandBytes at
+// (nt * ksteps + s) * kOperandBytes; rows n, K index i; zero outside k x k.
+// One warp per core matrix (lane = row in group * 4 + K pair).
+__global__ void split_w_kernel(const double2* __restrict__ W, int k, int ksteps, int ntiles,
+		unsigned char* __restrict__ out) {
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	const long long total = (long long)ntiles * ksteps * 32;  // 32 core matrices per block
+	if (warp >= total) return;
+	const int m = (int)(warp & 31);
+	const long long blk = warp >> 5;
+	const int s = (int)(blk % ksteps);
+	const int nt = (int)(blk / ksteps);
+	const int rg = m >> 1, kc = m & 1;
+	const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+	const int n = nt * TM + r, i = s * KT + kk;
+	double2 w0 = make_double2(0.0, 0.0), w1 = w0;
+	if (n < k) {
+		if (i < k) w0 = W[(size_t)i * k + n];
+		if (i + 1 < k) w1 = W[(size_t)(i + 1) * k + n];
+	}
+	put2(out + blk * kOperandBytes, kmaj_off(r, kk), (float)w0.x, (float)w0.y, (float)w1.x, (float)w1.y);
+}
+
+// Rotation tile: out rows n0.. (state index n), columns gt0.. (grid points).
+// A = W^T from the pre-split planes, B[g][i] = psi_i[g].
+__global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned char* __restrict__ wsplit,
+		const float2* __restrict__ psi, int k, long long G, float2* __restrict__ out, int* err) {
+	TcShared& sh = tc_shared();
+	const int n0 = blockIdx.x * TM;
+	const long long gt0 = (long long)blockIdx.y * TN;
+	const int nsteps = (k + KT - 1) / KT;
+	tc_setup(sh);
+	const int tid = threadIdx.x;
+	unsigned char* const base = sh.buf;
+	const unsigned char* wblk = wsplit + (size_t)blockIdx.x * nsteps * kOperandBytes;
+	// raw psi slot: row r = K index within the step (16 rows of 128 complex),
+	// 16-byte piece pg (64 per row) stored at slot pg ^ 4 ((r >> 1) & 1)
+	auto prefetch = [&](int s) {
+		unsigned char* ring = base + kRoA + (s & 3) * kOperandBytes;
+		const unsigned char* src = wblk + (size_t)s * kOperandBytes;
+#pragma unroll
+		for (int it = 0; it < kOperandBytes / 16 / kThreads; it++) {
+			const int idx = it * kThreads + tid;
+			cp16(smem_u32(ring + idx * 16), src + idx * 16, 16);
+		}
+		unsigned char* slot = base + kRoRaw + (s % 3) * kRoRawSlot;
+#pragma unroll
+		for (int it = 0; it < 4; it++) {
+			const int idx = it * kThreads + tid;  // 0..1023
+			const int r = idx >> 6, pg = idx & 63;
+			const int i = s * KT + r;
+			const long long g = gt0 + 2 * pg;
+			const bool in = i < k && g < G;  // g even, G even: both complex in range
+			const float2* p = in ? psi + (long long)i * G + g : psi;
+			cp16(smem_u32(slot + r * (TN * 8) + ((pg ^ (((r >> 1) & 1) << 2)) << 4)), p, in ? 16 : 0);
+		}
+	};
+	// convert: warp w handles core matrices m = w, w + 8, w + 16, w + 24 of the
+	// 32 (16 row groups of g x 2 K halves of i)
+	auto convert = [&](int s) {
+		const unsigned char* slot = base + kRoRaw + (s % 3) * kRoRawSlot;
+		unsigned char* planes = base + kRoB + (s & 1) * kOperandBytes;
+		const int w = tid >> 5, lane = tid & 31;
+#pragma unroll
+		for (int it = 0; it < 4; it++) {
+			const int m = it * 8 + w;
+			const int rg = m >> 1, kc = m & 1;
+			const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+			const int pg = r >> 1, sub = r & 1;
+			const float2 p0 = reinterpret_cast<const float2*>(
+					slot + kk * (TN * 8) + ((pg ^ (((kk >> 1) & 1) << 2)) << 4))[sub];
+			const float2 p1 = reinterpret_cast<const float2*>(
+					slot + (kk + 1) * (TN * 8) + ((pg ^ ((((kk + 1) >> 1) & 1) << 2)) << 4))[sub];
+			put2(planes, kmaj_off(r, kk), p0.x, p0.y, p1.x, p1.y);
+		}
+	};
+	auto a_addr = [&](int s) { return smem_u32(base + kRoA + (s & 3) * kOperandBytes); };
+	auto b_addr = [&](int s) { return smem_u32(base + kRoB + (s & 1) * kOperandBytes); };
+	run_pipeline(sh, nsteps, false, prefetch, convert, a_addr, b_addr, err);
+	if (!sh.abort) {
+		store_tile(sh, [&](int r, int c, double re, double im) {
+			const int n = n0 + r;
+			const long long g = gt0 + c;
+			if (n < k && g < G) out[(long long)n * G + g] = make_float2((float)re, (float)im);
+		});
+	}
+	tc_teardown(sh);
+}
+
+size_t tc_smem() { return sizeof(TcShared) + 1024; }
+
+void set_tc_attributes() {
+	cudaFuncSetAttribute(overlap_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
+	cudaFuncSetAttribute(rotate_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
+}
+
+}  // namespace
+
+bool tc_supported(int k, long long G) { return k >= 2 && G >= KT && G % 2 == 0; }
+
+int tc_overlap_splits(int k, long long G, int num_sms) {
+	const int nt = (k + TM - 1) / TM;
+	const int npairs = nt * (nt + 1) / 2;
+	// enough CTAs to cover the SMs; chunks of at most 2048 grid points bound
+	// the FP32 accumulation in tensor memory (the splits add up in FP64)
+	const long long by_sms = (num_sms + npairs - 1) / npairs;
+	const long long by_len = (G + 2047) / 2048;
+	const long long most = std::max(1LL, G / (4 * KT));
+	return (int)std::max(1LL, std::min(std::max(by_sms, by_len), most));
+}
+
+size_t tc_wsplit_bytes(int k) {
+	const size_t nt = (k + TM - 1) / TM, ks = (k + KT - 1) / KT;
+	return nt * ks * kOperandBytes;
+}
+
+void launch_overlap_tc(const float2* psi, int k, long long G, int nsplit, double2* part, double dx2, double2* S,
+		int* err, cudaStream_t s) {
+	const int nt = (k + TM - 1) / TM;
+	const int npairs = nt * (nt + 1) / 2;
+	long long chunk = (G + nsplit - 1) / nsplit;
+	chunk = ((chunk + KT - 1) / KT) * KT;
+	const int used = (int)((G + chunk - 1) / chunk);
+	set_tc_attributes();
+	overlap_tc_kernel<<<dim3(npairs, used), kThreads, tc_smem(), s>>>(psi, k, G, nt, chunk, part, err);
+	launch_overlap_finish(part, k, used, dx2, S, s);
+}
+
+void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit, float2* out,
+		int* err, cudaStream_t s) {
+	const int nt = (k + TM - 1) / TM, ks = (k + KT - 1) / KT;
+	const long long threads = (long long)nt * ks * 32 * 32;
+	split_w_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(W, k, ks, nt, wsplit);
+	set_tc_attributes();
+	const dim3 grid(nt, (unsigned)((G + TN - 1) / TN));
+	rotate_tc_kernel<<<grid, kThreads, tc_smem(), s>>>(wsplit, psi, k, G, out, err);
+}
+
+}  // namespace itp2d

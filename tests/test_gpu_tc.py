@@ -1,0 +1,109 @@
+"""Tensor-core contractions of the FP32 form (tcgen05, split-BF16 operands,
+FP32 accumulation over bounded grid chunks) against FP64 products of the same
+FP32 states: the overlap S = Psi^H Psi dx^2 of stateset.cpp:146-154 and the
+rotation Psi W of stateset.cpp:214-228."""
+import numpy as np
+import pytest
+
+from itp2d_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+# Norm-relative error bound of the split-BF16 products with FP32 accumulation
+# over grid chunks of at most 2048 points: |S_ij - S_ij(FP64)| <= TOL_S
+# sqrt(S_ii S_jj). Each MMA rounds the FP32 accumulator once; the error grows
+# about linearly with the chunk length (about 1e-5 at 2048 points).
+TOL_S = 2e-5
+# Orthonormality of the rotated FP32 states: |<psi_i|psi_j> - delta_ij| <= TOL_ORTHO.
+TOL_ORTHO = 2e-5
+
+
+def _ctx(sx, sy, k, seed, L=10.0):
+    dx = L / sx
+    c = capi.Context(sx, sy, dx, k, precision=capi.FP32)
+    rng = np.random.default_rng(seed)
+    x = (np.arange(sx) - sx / 2) * dx
+    y = (np.arange(sy) - sy / 2) * dx
+    env = np.exp(-0.5 * (y[:, None] ** 2 + x[None, :] ** 2) / 4.0)
+    psi = (rng.standard_normal((k, sy, sx)) + 1j * rng.standard_normal((k, sy, sx))) * env
+    c.upload(psi)
+    return c, dx
+
+
+def _exact_overlap(c, dx):
+    psi = c.download().reshape(c.k, -1)  # the FP32 values, widened exactly
+    return (psi.conj() @ psi.T) * dx * dx
+
+
+def _rel(S, ref):
+    d = np.sqrt(np.abs(np.diag(ref)))
+    return np.max(np.abs(S - ref) / np.outer(d, d))
+
+
+@pytest.mark.parametrize("sx,sy,k", [(32, 32, 5), (64, 48, 130), (128, 128, 300), (256, 256, 64)])
+def test_overlap_tensor_cores(sx, sy, k):
+    c, dx = _ctx(sx, sy, k, seed=sx + k)
+    ref = _exact_overlap(c, dx)
+    S_tc = c.overlap_matrix()
+    c.set_contraction(capi.CONTRACT_FP64)
+    S_64 = c.overlap_matrix()
+    assert _rel(S_64, ref) < 1e-12
+    err = _rel(S_tc, ref)
+    print(f"overlap {sx}x{sy} k={k}: split-BF16 norm-relative error {err:.2e}")
+    assert err < TOL_S
+    assert np.array_equal(S_tc, S_tc.conj().T)
+    assert np.all(np.diag(S_tc).imag == 0)
+
+
+def test_overlap_odd_grid_uses_fp64():
+    # an odd number of grid points leaves the tensor-core path (paired loads)
+    c, dx = _ctx(35, 45, 20, seed=3)
+    assert _rel(c.overlap_matrix(), _exact_overlap(c, dx)) < 1e-12
+
+
+@pytest.mark.parametrize("sx,sy,k", [(64, 64, 40), (128, 96, 200)])
+def test_rotation_tensor_cores(sx, sy, k):
+    c, dx = _ctx(sx, sy, k, seed=7 * k)
+    psi0 = c.download().reshape(k, -1)
+    c.orthonormalize()
+    out = c.download().reshape(k, -1)
+    O = (out.conj() @ out.T) * dx * dx
+    dev = np.max(np.abs(O - np.eye(k)))
+    print(f"rotation {sx}x{sy} k={k}: orthonormality {dev:.2e}")
+    assert dev < TOL_ORTHO
+    # same span as the input states: the projection of psi0 on the new set
+    # reproduces psi0
+    coef = (out.conj() @ psi0.T) * dx * dx
+    resid = psi0 - coef.T @ out
+    rel = np.linalg.norm(resid, axis=1) / np.linalg.norm(psi0, axis=1)
+    assert np.max(rel) < 1e-4
+    # the same states as the FP64 engine (distinct overlap eigenvalues here)
+    c2, _ = _ctx(sx, sy, k, seed=7 * k)
+    c2.set_contraction(capi.CONTRACT_FP64)
+    c2.orthonormalize()
+    ref = c2.download().reshape(k, -1)
+    phase = np.sum(ref.conj() * out, axis=1)
+    phase /= np.abs(phase)
+    diff = np.linalg.norm(out - phase[:, None] * ref, axis=1) / np.linalg.norm(ref, axis=1)
+    print(f"rotation {sx}x{sy} k={k}: max state difference to FP64 engine {np.max(diff):.2e}")
+    assert np.median(diff) < 1e-4
+
+
+def test_tensor_core_solve_matches_fp64_engine():
+    """The mixed form (FP32 sweeps, FP64 refinement) reaches the same
+    energies with tensor-core contractions as with FP64 contractions."""
+    from itp2d_b200.system import ITPSystem, Parameters
+
+    kw = dict(sx=48, sy=48, length=12.0, B=1.0, halforder=2, num_states=12, wanted=6, eps=[0.1],
+              potential="harmonic(1)", timestep_test="abschange(1e-10)", final_test="abschange(1e-10)",
+              max_steps=600, seed=5, precision=capi.FP32, fp32_switch=1e-6)
+    res = {}
+    for engine in (capi.CONTRACT_AUTO, capi.CONTRACT_FP64):
+        s = ITPSystem(Parameters(**kw))
+        assert capi.lib().itp2d_set_contraction(s.context_handle(), engine) == capi.OK
+        s.run()
+        assert not s.error_flag, s.last_error
+        assert not s.in_fp32
+        print(f"engine {engine}: {s.total_steps} steps")
+        res[engine] = s.energies()[0][:6]
+    assert np.max(np.abs(res[capi.CONTRACT_AUTO] - res[capi.CONTRACT_FP64])) < 1e-9
