@@ -11,8 +11,12 @@
 //   2. every other 2BS x 2BS block of A becomes Q_r^H A_rc Q_c and every slab
 //      of 2BS rows of V becomes V Q_c, both as FP64 DMMA products staged in shared
 //      memory (three MS x MS complex operands).
-// Each round gives every subproblem one inner sweep (block Jacobi with a
-// single inner sweep); a rotation is applied when |A_pq| > tol sqrt(|A_pp A_qq|).
+// In the first round of each outer sweep every subproblem gets one full inner
+// sweep (all pairs of its 2BS indices, so every within-block pair is rotated
+// once per outer sweep); in the other rounds only the BS x BS cross pairs
+// (p in block P, q in block Q) are rotated, in BS inner rounds. Over an outer
+// sweep every index pair is thus rotated once, a block-cyclic ordering of
+// cyclic Jacobi. A rotation is applied when |A_pq| > tol sqrt(|A_pp A_qq|).
 // Rotations whose relative off-diagonal |A_pq| / sqrt(|A_pp A_qq|) is at the
 // rounding level of the phase-2 products (below 1e-13) do not count against
 // convergence; the iteration stops after a sweep whose largest counted
@@ -35,7 +39,6 @@ constexpr int NR = MS / 2;    // rotations per inner round
 constexpr int LD = MS + 4;    // padded row length (doubles): conflict-free DMMA fragments
 constexpr int PL = MS * LD;   // doubles per plane
 constexpr int kThreads = 256;
-constexpr int kInnerMaxSweeps = 30;
 constexpr double kTauFinal = 3e-9;
 constexpr double kNoiseRel = 1e-13;  // relative off-diagonal treated as rounding noise
 
@@ -55,7 +58,7 @@ __device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * B
 
 struct Shared {
 	double pl[6][PL];                            // planes: [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
-	double rc[NR], rs[NR], rer[NR], rei[NR], rap[NR], raq[NR];
+	double rc[NR], rs[NR], rtau[NR], rer[NR], rei[NR], rap[NR], raq[NR];
 	int rp[NR], rq[NR], rrot[NR];
 	int cnt;                                     // rotations in the current inner sweep
 	int total;                                   // rotations of this CTA in the current outer sweep
@@ -94,7 +97,7 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 	sh.rp[j] = p;
 	sh.rq[j] = q;
 	sh.rrot[j] = 0;
-	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
+	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rtau[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
 	if (c2 > 0.0 && c2 > tol * tol * scale2) {
 		const double cabs = sqrt(c2);
 		const double d = 0.5 * (b - a);
@@ -110,6 +113,7 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 			const double ic = 1.0 / cabs;
 			sh.rc[j] = c;
 			sh.rs[j] = st * c;
+			sh.rtau[j] = st * c / (1.0 + c);
 			sh.rer[j] = cr * ic;
 			sh.rei[j] = ci * ic;
 			sh.rap[j] = a - st * cabs;
@@ -123,10 +127,10 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 	}
 }
 
-// Rows p, q of J^H X with J = [[c, s e], [-s conj(e), c]] (correction form).
-__device__ __forceinline__ void rows2(double c, double s, double er, double ei, double& xpr, double& xpi,
+// Rows p, q of J^H X with J = [[c, s e], [-s conj(e), c]] (correction form,
+// tau = s / (1 + c)).
+__device__ __forceinline__ void rows2(double s, double tau, double er, double ei, double& xpr, double& xpi,
 		double& xqr, double& xqi) {
-	const double tau = s / (1.0 + c);
 	// yp = xp - s (e xq + tau xp)
 	const double ypr = xpr - s * (er * xqr - ei * xqi + tau * xpr);
 	const double ypi = xpi - s * (er * xqi + ei * xqr + tau * xpi);
@@ -136,10 +140,9 @@ __device__ __forceinline__ void rows2(double c, double s, double er, double ei, 
 	xpr = ypr; xpi = ypi; xqr = yqr; xqi = yqi;
 }
 
-// Columns s, t of X J (correction form).
-__device__ __forceinline__ void cols2(double c, double s, double er, double ei, double& xsr, double& xsi,
+// Columns s, t of X J (correction form, tau = s / (1 + c)).
+__device__ __forceinline__ void cols2(double s, double tau, double er, double ei, double& xsr, double& xsi,
 		double& xtr, double& xti) {
-	const double tau = s / (1.0 + c);
 	// ys = xs - s (conj(e) xt + tau xs)
 	const double ysr = xsr - s * (er * xtr + ei * xti + tau * xsr);
 	const double ysi = xsi - s * (er * xti - ei * xtr + tau * xsi);
@@ -149,19 +152,22 @@ __device__ __forceinline__ void cols2(double c, double s, double er, double ei, 
 	xsr = ysr; xsi = ysi; xtr = ytr; xti = yti;
 }
 
-// One cyclic Jacobi sweep (63 rounds of 32 rotations) on the 64 x 64
-// subproblem in planes 0/1, accumulating Q in planes 2/3. Each round updates
+// One inner sweep on the MS x MS subproblem in planes 0/1, accumulating Q in
+// planes 2/3: full (MS - 1 rounds of NR rotations over all pairs) or cross
+// (BS rounds: round r pairs p with BS + (p + r) % BS). Each round updates
 // every 2 x 2 block {p,q} x {s,t} in place as J_pq^H X J_st, so the subproblem
 // crosses shared memory once per round.
-__device__ void inner_sweep(Shared& sh, double tol) {
+__device__ void inner_sweep(Shared& sh, double tol, bool full) {
 	double* mr = sh.pl[0];
 	double* mi = sh.pl[1];
 	double* qr = sh.pl[2];
 	double* qi = sh.pl[3];
 	const int tid = threadIdx.x;
-	for (int r = 0; r < MS - 1; r++) {
+	const int rounds = full ? MS - 1 : BS;
+	for (int r = 0; r < rounds; r++) {
 		if (tid < NR) {
-			const int p = rr_player(tid, r, MS), q = rr_player(MS - 1 - tid, r, MS);
+			const int p = full ? rr_player(tid, r, MS) : tid;
+			const int q = full ? rr_player(MS - 1 - tid, r, MS) : BS + (tid + r) % BS;
 			inner_rotation(sh, tid, p, q, tol);
 		}
 		__syncthreads();
@@ -181,12 +187,12 @@ __device__ void inner_sweep(Shared& sh, double tol) {
 			double psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
 			double qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
 			if (ra) {
-				rows2(sh.rc[ja], sh.rs[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
-				rows2(sh.rc[ja], sh.rs[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
+				rows2(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
+				rows2(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
 			}
 			if (rb) {
-				cols2(sh.rc[jb], sh.rs[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
-				cols2(sh.rc[jb], sh.rs[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
+				cols2(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
+				cols2(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
 			}
 			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
 			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
@@ -197,7 +203,7 @@ __device__ void inner_sweep(Shared& sh, double tol) {
 			if (!sh.rrot[j]) continue;
 			const int p = sh.rp[j], q = sh.rq[j];
 			double ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
-			cols2(sh.rc[j], sh.rs[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
+			cols2(sh.rs[j], sh.rtau[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
 			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 		}
 		__syncthreads();
@@ -285,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, doubl
 					sh.pl[3][i * LD + l] = 0.0;
 				}
 				__syncthreads();
-				inner_sweep(sh, tol);
+				inner_sweep(sh, tol, r == 0);
 				double2* Qg = Qbuf + (size_t)j * MS * MS;
 				for (int e = tid; e < MS * MS; e += kThreads) {
 					const int i = e / MS, l = e % MS;
