@@ -133,11 +133,10 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
     s = system.ITPSystem(params(form), init_states=psi, stream=stream.cuda_stream)
     ctx = s.context_handle()
     L = capi.lib()
-    ms = np.zeros(5)
 
     def phases():
-        L.itp2d_phase_times(ctx, ms.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
-        return ms.copy()
+        st = capi.phase_stats(ctx)
+        return {(prec, ph): v for prec, d in st.items() for ph, v in d.items()}
 
     for _ in range(W):
         s.reset(psi)
@@ -145,7 +144,7 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
     torch.cuda.synchronize()
     # timed: inputs resident in HBM (the reset that uploads them is outside)
     times, steps, conv, lat = [], [], [], []
-    p0, l0 = phases(), L.itp2d_launch_count(ctx)
+    p0, l0, w0 = phases(), L.itp2d_launch_count(ctx), L.itp2d_total_sweeps(ctx)
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -159,7 +158,9 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
         steps.append(s.total_steps)
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
-    p1, l1 = phases(), L.itp2d_launch_count(ctx)
+    p1, l1, w1 = phases(), L.itp2d_launch_count(ctx), L.itp2d_total_sweeps(ctx)
+    # per solve: {(precision, phase): (ms, calls)}
+    stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
     # end to end: host inputs copied in, energies and states copied out, per solve
     e2e_times = []
@@ -173,7 +174,7 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
         L.itp2d_system_download_states(s.h, e2e_buf.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    return dict(times=times, steps=steps, conv=conv, phases_ms=(p1 - p0) / K, launches=(l1 - l0) / K,
+    return dict(times=times, steps=steps, conv=conv, stats=stats, sweeps=(w1 - w0) / K, launches=(l1 - l0) / K,
                 E=E, converged_mask=None, e2e_times=e2e_times, system=s)
 
 
@@ -232,6 +233,69 @@ def config_block(form):
                         f"solve until the {w['wanted']} lowest pass {w['test']}",
             "form": form, "global_batch": w["num_states"], "grid": [w["sx"], w["sy"]],
             "parallelism": "replicas", "l2": "inputs (524 MB of states) exceed the 126 MB L2"}
+
+
+def phase_rooflines(r, fp64_peak):
+    """Roofline of each phase of one form, per solve and per precision.
+
+    Algorithmic work per call:
+      propagate  k G b [2 m (m + 2) + (m - 1)] bytes (b = 16 FP64, 8 FP32)
+      energies   5 k G b bytes
+      overlap    FP64: 4 k^2 G flops (Hermitian half, complex MACs, DMMA)
+                 FP32 (tensor cores): BF16 MMA work issued, 24 MMAs of 128 x 128 x 16
+                 per 16 grid points per upper-triangle tile pair of 128 states
+      rotation   FP64: 8 k^2 G flops; FP32: 24 MMAs of 128 x 128 x 16 per 16 states
+                 per (128 states x 128 grid points) output tile
+      eigensolve block Jacobi: per sweep (kp/16 - 1) rounds of 32 x 32 block
+                 unitaries applied to both sides of the kp x kp matrix and to the
+                 eigenvector matrix, 3 * 8 * 32 * kp^2 flops per round (DMMA)
+    """
+    w = WORKLOAD
+    k, G, m = w["num_states"], w["sx"] * w["sy"], w["halforder"]
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm, bf16, src = peaks["hbm_gbs"], peaks["bf16_tflops_sustained"], "measured"
+    except Exception:
+        hbm, bf16, src = 6650.0, 1400.0, "fallback"
+    nt = (k + 127) // 128
+    mma = 128 * 128 * 16 * 2
+    tc_overlap = nt * (nt + 1) // 2 * 24 * mma * ((G + 15) // 16)
+    tc_rotation = nt * ((G + 127) // 128) * ((k + 15) // 16) * 24 * mma
+    kp = (k + 31) // 32 * 32
+    sweep_flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp
+    out = {}
+    for prec in ("fp64", "fp32"):
+        b = 16 if prec == "fp64" else 8
+        tc = prec == "fp32" and G % 2 == 0
+        work = {
+            "propagate": ("hbm", alg_bytes_split(w, b)),
+            "energies": ("hbm", 5 * k * G * b),
+            "overlap": ("tensor_bf16", tc_overlap) if tc else ("tensor_fp64", 4 * k * k * G),
+            "rotation": ("tensor_bf16", tc_rotation) if tc else ("tensor_fp64", 8 * k * k * G),
+        }
+        for ph, (bound, amount) in work.items():
+            ms, calls = r["stats"][(prec, ph)]
+            if calls == 0:
+                continue
+            sec = ms * 1e-3
+            if bound == "hbm":
+                ach, peak, unit, psrc = amount * calls / sec / 1e9, hbm, "GB/s", f"HBM copy ({src})"
+            elif bound == "tensor_bf16":
+                ach, peak, unit, psrc = amount * calls / sec / 1e12, bf16, "TFLOP/s", \
+                    f"cuBLAS BF16 sustained ({src})"
+            else:
+                ach, peak, unit, psrc = amount * calls / sec / 1e12, fp64_peak, "TFLOP/s", \
+                    "FP64 DMMA measured in-run"
+            out[f"{ph}_{prec}"] = {"bound": "hbm" if bound == "hbm" else "tensor", "achieved": ach, "peak": peak,
+                                   "unit": unit, "frac": ach / peak, "ms_per_solve": ms, "calls_per_solve": calls,
+                                   "peak_source": psrc}
+    ms = r["stats"][("fp64", "eigensolve")][0] + r["stats"][("fp32", "eigensolve")][0]
+    calls = r["stats"][("fp64", "eigensolve")][1] + r["stats"][("fp32", "eigensolve")][1]
+    ach = sweep_flops * r["sweeps"] / (ms * 1e-3) / 1e12
+    out["eigensolve"] = {"bound": "tensor", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": ach / fp64_peak, "ms_per_solve": ms, "calls_per_solve": calls,
+                         "sweeps_per_solve": r["sweeps"], "peak_source": "FP64 DMMA measured in-run"}
+    return out
 
 
 def main():
@@ -303,37 +367,10 @@ def main():
     rh = results[head]
     conv_h = conv_mx if head == "mixed" else r64["conv"][-1]
 
-    # roofline of the dominant phase (per-solve device times)
-    ph = rh["phases_ms"]
-    names = ["propagate", "overlap", "eigensolve", "rotation", "energies"]
-    nsteps = statistics.mean(rh["steps"])
-    hbm = None
-    try:
-        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
-        peak_src = "measured"
-    except Exception:
-        hbm, peak_src = 6650.0, "fallback"
-    b = 16  # plain FP64 bytes per complex (the mixed form's FP32 share is reported per phase)
-    roof = {}
-    alg = {
-        "propagate": ("hbm", alg_bytes_split(w, b) * nsteps / 1e9, "GB"),
-        "energies": ("hbm", 5 * k * G * b * nsteps / 1e9, "GB"),
-        "overlap": ("tensor", 4 * k * k * G * nsteps / 1e12, "TFLOP"),
-        "rotation": ("tensor", 8 * k * k * G * nsteps / 1e12, "TFLOP"),
-        "eigensolve": ("tensor", 10 * k ** 3 * nsteps / 1e12, "TFLOP"),
-    }
-    for i, n in enumerate(names):
-        bound, amount, u = alg[n]
-        sec = ph[i] * 1e-3
-        ach = amount / sec if sec > 0 else 0.0
-        peak = hbm if bound == "hbm" else fp64_peak
-        unit = "GB/s" if bound == "hbm" else "TFLOP/s"
-        roof[n] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
-                   "frac": ach / peak if peak else None, "ms_per_solve": ph[i]}
-    dom = max(names, key=lambda n: roof[n]["ms_per_solve"])
-    roofline = dict(roof[dom])
-    roofline.update({"kernel": dom, "traffic": None,
-                     "peak_source": peak_src if roof[dom]["bound"] == "hbm" else "FP64 DMMA measured in-run"})
+    roof = phase_rooflines(rh, fp64_peak)
+    dom = max(roof, key=lambda n: roof[n]["ms_per_solve"])
+    roofline = {key: roof[dom][key] for key in ("bound", "achieved", "peak", "unit", "frac")}
+    roofline.update({"traffic": None, "kernel": dom, "peak_source": roof[dom]["peak_source"]})
 
     cpu = None
     if rank == 0:
@@ -368,6 +405,7 @@ def main():
         },
         "latency_s": {"p50": statistics.median(rh["times"]), "p99": max(rh["times"])},
         "phases": roof,
+        "phases_other_form": phase_rooflines(results["fp64" if head == "mixed" else "mixed"], fp64_peak),
     }
     if rank == 0:
         print(json.dumps(out))

@@ -164,8 +164,15 @@ long long itp2d_launch_count(itp2d_ctx* ctx);
 int itp2d_set_timing(itp2d_ctx* ctx, int enable);
 int itp2d_phase_times(itp2d_ctx* ctx, double* ms5);
 
-/* Jacobi sweeps used by the last orthonormalisation. */
+/* The same phase times split by the precision the phase ran in, with the
+ * number of timed calls: ms10[p * 5 + phase] and calls10[p * 5 + phase] for
+ * p = ITP2D_FP64 (0) or ITP2D_FP32 (1), phases in the order above. */
+int itp2d_phase_stats(itp2d_ctx* ctx, double* ms10, long long* calls10);
+
+/* Jacobi sweeps used by the last orthonormalisation, and by all of them
+ * since the context was created. */
 int itp2d_last_sweeps(itp2d_ctx* ctx);
+long long itp2d_total_sweeps(itp2d_ctx* ctx);
 
 /* Eigen-decomposition of an n x n complex Hermitian matrix on the device,
  * the drop-in for EigenSolver::solve (ZHEEV("V","U"), eigensolver.hpp:80-84).

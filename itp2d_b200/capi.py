@@ -71,7 +71,10 @@ def lib():
         L.itp2d_launch_count.restype = C.c_longlong
         L.itp2d_set_timing.argtypes = [vp, i]
         L.itp2d_phase_times.argtypes = [vp, dp]
+        L.itp2d_phase_stats.argtypes = [vp, dp, C.POINTER(C.c_longlong)]
         L.itp2d_last_sweeps.argtypes = [vp]
+        L.itp2d_total_sweeps.argtypes = [vp]
+        L.itp2d_total_sweeps.restype = C.c_longlong
         L.itp2d_hermitian_eigensolve.argtypes = [i, dp, dp, dp]
         L.itp2d_device_fp64_peak.argtypes = [dp]
         L.itp2d_status_string.argtypes = [i]
@@ -106,6 +109,19 @@ def hermitian_eigensolve(A: np.ndarray):
     _check(lib().itp2d_hermitian_eigensolve(n, _dp(a.view(np.float64)), _dp(ev), _dp(vec.view(np.float64))),
            "itp2d_hermitian_eigensolve")
     return ev, vec.T.copy()
+
+
+PHASES = ["propagate", "overlap", "eigensolve", "rotation", "energies"]
+
+
+def phase_stats(handle) -> dict:
+    """Phase device times and call counts of a context handle, by precision."""
+    ms = np.zeros(10)
+    calls = np.zeros(10, dtype=np.int64)
+    _check(lib().itp2d_phase_stats(handle, _dp(ms), calls.ctypes.data_as(C.POINTER(C.c_longlong))),
+           "itp2d_phase_stats")
+    return {prec: {ph: (float(ms[p * 5 + i]), int(calls[p * 5 + i])) for i, ph in enumerate(PHASES)}
+            for p, prec in enumerate(["fp64", "fp32"])}
 
 
 class Context:
@@ -208,6 +224,10 @@ class Context:
         t = np.zeros(5)
         _check(lib().itp2d_phase_times(self.h, _dp(t)), "itp2d_phase_times")
         return dict(zip(["propagate", "overlap", "eigensolve", "rotation", "energies"], t.tolist()))
+
+    def phase_stats(self) -> dict:
+        """{precision: {phase: (ms, calls)}} with precision "fp64" / "fp32"."""
+        return phase_stats(self.h)
 
     @property
     def last_sweeps(self) -> int:

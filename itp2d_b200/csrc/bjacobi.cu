@@ -3,25 +3,34 @@
 // Same decomposition as the scalar kernel in jacobi.cu (and the same output
 // conventions), organised for fewer grid-wide rounds: the padded index range
 // is cut into blocks of BS, blocks are paired round-robin (k/BS - 1 rounds per
-// sweep), and each round has two phases separated by grid barriers:
+// sweep), and each round r has two phases:
 //   1. one CTA per block pair sweeps the 2BS x 2BS Hermitian subproblem in
 //      shared memory with cyclic Jacobi (CTA barriers only), leaving its
-//      2BS x 2BS unitary Q in global memory and the rotated subproblem in
-//      the output matrix;
-//   2. every other 2BS x 2BS block of A becomes Q_r^H A_rc Q_c and every slab
-//      of 2BS rows of V becomes V Q_c, both as FP64 DMMA products staged in shared
-//      memory (three MS x MS complex operands).
-// In the first round of each outer sweep every subproblem gets one full inner
-// sweep (all pairs of its 2BS indices, so every within-block pair is rotated
-// once per outer sweep); in the other rounds only the BS x BS cross pairs
-// (p in block P, q in block Q) are rotated, in BS inner rounds. Over an outer
-// sweep every index pair is thus rotated once, a block-cyclic ordering of
-// cyclic Jacobi. A rotation is applied when |A_pq| > tol sqrt(|A_pp A_qq|).
+//      2BS x 2BS unitary Q_r in global memory and the rotated subproblem as
+//      the diagonal pair block of A_r;
+//   2. every other 2BS x 2BS block of A_r becomes Q_r^H A_{r-1} Q_r (row and
+//      column pairs) and every slab of 2BS rows of V becomes V Q_r, both as
+//      FP64 DMMA products staged in shared memory.
+// The phases are pipelined: one grid barrier separates supersteps, and
+// superstep t runs phase 1 of round t on one set of CTAs while the others run
+// phase 2 of round t - 1. Phase 1 of round t therefore builds its subproblem
+// itself: its diagonal blocks are parts of round t - 1's rotated subproblems
+// (already in A_{t-1}), and its off-diagonal block (P', Q') is taken from
+// Q_a^H A_{t-2}(a, b) Q_b for the round t - 1 pairs a, b that held P' and Q'.
+// Three matrix buffers rotate (A_{t-2} read, A_{t-1} completed by phase 2,
+// A_t's diagonal pair blocks written by phase 1) and Q alternates between two
+// buffers.
+// In every 16th round of an outer sweep (starting with the first) every
+// subproblem gets one full inner sweep (all pairs of its 2BS indices, so every
+// within-block pair is rotated at least once per outer sweep); in the other
+// rounds only the BS x BS cross pairs (p in block P, q in block Q) are
+// rotated, in BS inner rounds. Over an outer sweep every index pair is thus
+// rotated at least once, a block-cyclic ordering of cyclic Jacobi. A rotation is applied when |A_pq| > tol sqrt(|A_pp A_qq|).
 // Rotations whose relative off-diagonal |A_pq| / sqrt(|A_pp A_qq|) is at the
 // rounding level of the phase-2 products (below 1e-13) do not count against
 // convergence; the iteration stops after a sweep whose largest counted
-// rotation tangent is below 3e-9 (or that counted none): quadratic convergence
-// then leaves off-diagonal elements of order k * 1e-17 relative to the gaps.
+// rotation tangent is below tau_final (3e-9 by default: quadratic convergence
+// then leaves off-diagonal elements of order k * 1e-17 relative to the gaps).
 #include <cooperative_groups.h>
 
 #include "../../include/itp2d_gpu.h"
@@ -40,6 +49,9 @@ constexpr int LD = MS + 4;    // padded row length (doubles): conflict-free DMMA
 constexpr int PL = MS * LD;   // doubles per plane
 constexpr int kThreads = 256;
 constexpr double kTauFinal = 3e-9;
+// Rounds between full inner sweeps (within-block pairs rotated again); every
+// 16th round measured best on k = 500 (fewer outer sweeps for little cost).
+constexpr int kFullEvery = 16;
 constexpr double kNoiseRel = 1e-13;  // relative off-diagonal treated as rounding noise
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
@@ -252,19 +264,196 @@ __device__ void load_q(double* qr, double* qi, const double2* Qg) {
 	}
 }
 
-__global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, double2* A1, double2* V, double2* Qbuf,
-		int kp, int max_sweeps, double tol, int* counters, unsigned long long* tmax) {
+// Position of player p in round r of the circle method (inverse of rr_player).
+__device__ __forceinline__ int rr_position(int p, int r, int npos) {
+	if (p == 0) return 0;
+	const int m = npos - 1;
+	return ((p - 1 - r) % m + m) % m + 1;
+}
+
+// Phase 1 for pair j of round t (within-sweep round rr): forms the subproblem
+// in planes 0/1 (Q in planes 2/3 = I), sweeps it, stores Q_t and the rotated
+// subproblem. prev: A_{t-1} (diagonal pair blocks of round t - 1), prev2:
+// A_{t-2}, Qprev: the Q buffer of round t - 1 (t >= 1). For t = 0 the
+// subproblem is read from prev = A_{-1}, the initial matrix.
+__device__ void phase1_item(Shared& sh, int j, long long t, int rounds, int nb, int np, int kp, double tol,
+		const double2* prev, const double2* prev2, const double2* Qprev, double2* Qout, double2* out) {
+	const int tid = threadIdx.x;
+	const int rr = (int)(t % rounds);
+	const int P = rr_player(j, rr, nb), Q = rr_player(nb - 1 - j, rr, nb);
+	double* mr = sh.pl[0];
+	double* mi = sh.pl[1];
+	if (t == 0) {
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const double2 v = __ldcg(prev + (long long)gidx(i, P, Q) * kp + gidx(l, P, Q));
+			mr[i * LD + l] = v.x;
+			mi[i * LD + l] = v.y;
+		}
+	} else {
+		// the round t - 1 pairs (a, b) holding P and Q, and the halves they sit in
+		const int ro = (int)((t - 1) % rounds);
+		const int posP = rr_position(P, ro, nb), posQ = rr_position(Q, ro, nb);
+		const int a = posP < np ? posP : nb - 1 - posP, hP = posP < np ? 0 : 1;
+		const int b = posQ < np ? posQ : nb - 1 - posQ, hQ = posQ < np ? 0 : 1;
+		const int Pa = rr_player(a, ro, nb), Qa = rr_player(nb - 1 - a, ro, nb);
+		const int Pb = rr_player(b, ro, nb), Qb = rr_player(nb - 1 - b, ro, nb);
+		// T = A_{t-2}(a, b) Q_b, then C = Q_a^H T
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const double2 v = __ldcg(prev2 + (long long)gidx(i, Pa, Qa) * kp + gidx(l, Pb, Qb));
+			mr[i * LD + l] = v.x;
+			mi[i * LD + l] = v.y;
+		}
+		load_q(sh.pl[2], sh.pl[3], Qprev + (size_t)a * MS * MS);
+		load_q(sh.pl[4], sh.pl[5], Qprev + (size_t)b * MS * MS);
+		__syncthreads();
+		double cr[2][2], ci[2][2];
+		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);
+		__syncthreads();
+#pragma unroll
+		for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc(bb, h, row, col);
+				mr[row * LD + col] = cr[bb][h];
+				mi[row * LD + col] = ci[bb][h];
+			}
+		__syncthreads();
+		cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
+		__syncthreads();
+		// off-diagonal blocks of the subproblem from C[hP half][hQ half]
+#pragma unroll
+		for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc(bb, h, row, col);
+				if ((row >> 4) == hP && (col >> 4) == hQ) {
+					const int i = row & (BS - 1), l = BS + (col & (BS - 1));
+					mr[i * LD + l] = cr[bb][h];
+					mi[i * LD + l] = ci[bb][h];
+					mr[l * LD + i] = cr[bb][h];
+					mi[l * LD + i] = -ci[bb][h];
+				}
+			}
+		// diagonal blocks (P, P) and (Q, Q) of A_{t-1}
+		for (int e = tid; e < 2 * BS * BS; e += kThreads) {
+			const int half = e / (BS * BS), i = (e / BS) % BS, l = e % BS;
+			const int g0 = (half ? Q : P) * BS;
+			const double2 v = __ldcg(prev + (long long)(g0 + i) * kp + g0 + l);
+			mr[(half * BS + i) * LD + half * BS + l] = v.x;
+			mi[(half * BS + i) * LD + half * BS + l] = v.y;
+		}
+	}
+	for (int e = tid; e < MS * MS; e += kThreads) {
+		const int i = e / MS, l = e % MS;
+		sh.pl[2][i * LD + l] = (i == l) ? 1.0 : 0.0;
+		sh.pl[3][i * LD + l] = 0.0;
+	}
+	__syncthreads();
+	inner_sweep(sh, tol, rr % kFullEvery == 0);
+	double2* Qg = Qout + (size_t)j * MS * MS;
+	for (int e = tid; e < MS * MS; e += kThreads) {
+		const int i = e / MS, l = e % MS;
+		Qg[e] = make_double2(sh.pl[2][i * LD + l], sh.pl[3][i * LD + l]);
+		out[(long long)gidx(i, P, Q) * kp + gidx(l, P, Q)] = make_double2(mr[i * LD + l], mi[i * LD + l]);
+	}
+	__syncthreads();
+}
+
+// Phase 2 item w of round ro: an off-diagonal pair block of A (w < nA2) or a
+// slab of V, read from src / V, written to dst / V.
+__device__ void phase2_item(Shared& sh, int w, int ro, int nb, int np, int kp, const double2* src, double2* dst,
+		double2* V, const double2* Qr) {
+	const int tid = threadIdx.x;
+	const int nA2 = np * (np - 1);
+	double cr[2][2], ci[2][2];
+	if (w < nA2) {
+		const int jr = w / (np - 1);
+		int jc = w % (np - 1);
+		if (jc >= jr) jc++;
+		const int Pr = rr_player(jr, ro, nb), Qr_ = rr_player(nb - 1 - jr, ro, nb);
+		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const double2 v = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
+			sh.pl[0][i * LD + l] = v.x;
+			sh.pl[1][i * LD + l] = v.y;
+		}
+		load_q(sh.pl[2], sh.pl[3], Qr + (size_t)jr * MS * MS);
+		load_q(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
+		__syncthreads();
+		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
+		__syncthreads();
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc(b, h, row, col);
+				sh.pl[0][row * LD + col] = cr[b][h];
+				sh.pl[1][row * LD + col] = ci[b][h];
+			}
+		__syncthreads();
+		// C = Qr^H T: A(i, m) = conj(Qr(m, i))
+		cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc(b, h, row, col);
+				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
+			}
+	} else {
+		const int v = w - nA2;
+		const int rb = v / np, jc = v % np;
+		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const double2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
+			sh.pl[0][i * LD + l] = x.x;
+			sh.pl[1][i * LD + l] = x.y;
+		}
+		load_q(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
+		__syncthreads();
+		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc(b, h, row, col);
+				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
+			}
+	}
+	__syncthreads();
+}
+
+// Buffers: A_r lives in bufs[(r + 1) % 3] (A_{-1} = the input in A0); Q_r in
+// Qbuf + (r & 1) * np * MS * MS.
+__global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, double2* A1, double2* A2, double2* V,
+		double2* Qbuf, int kp, int max_sweeps, double tol, double tau_final, int* counters,
+		unsigned long long* tmax) {
 	cg::grid_group grid = cg::this_grid();
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
 	const int tid = threadIdx.x;
 	const int nb = kp / BS;
 	const int np = nb / 2;
+	const int rounds = nb - 1;
 	const int nrb = kp / MS;
-	const int nA2 = np * (np - 1);
-	const int nW = nA2 + nrb * np;
-	double2* Acur = A0;
-	double2* Anext = A1;
+	const int nW = np * (np - 1) + nrb * np;
+	double2* const bufs[3] = {A0, A1, A2};
+	const size_t qstride = (size_t)np * MS * MS;
+	// CTAs [0, p1) take phase 1 items, the rest phase 2 items (all CTAs take
+	// both kinds when the grid is not larger than the pair count)
+	const bool split = (int)gridDim.x > np;
+	const int p1 = split ? np : (int)gridDim.x;
+	const int p2first = split ? np : 0;
+	const int p2count = split ? (int)gridDim.x - np : (int)gridDim.x;
 
 	if (tid == 0) {
 		sh.total = 0;
@@ -274,126 +463,62 @@ __global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, doubl
 	__syncthreads();
 
 	int sweep = 0;
-	bool converged = false;
-	for (; sweep < max_sweeps && !converged; sweep++) {
-		for (int r = 0; r < nb - 1; r++) {
-			// ---- phase 1: subproblems ----
-			for (int j = blockIdx.x; j < np; j += gridDim.x) {
-				const int P = rr_player(j, r, nb), Q = rr_player(nb - 1 - j, r, nb);
-				double* mr = sh.pl[0];
-				double* mi = sh.pl[1];
-				for (int e = tid; e < MS * MS; e += kThreads) {
-					const int i = e / MS, l = e % MS;
-					const double2 v = __ldcg(Acur + (long long)gidx(i, P, Q) * kp + gidx(l, P, Q));
-					mr[i * LD + l] = v.x;
-					mi[i * LD + l] = v.y;
-					sh.pl[2][i * LD + l] = (i == l) ? 1.0 : 0.0;
-					sh.pl[3][i * LD + l] = 0.0;
-				}
-				__syncthreads();
-				inner_sweep(sh, tol, r == 0);
-				double2* Qg = Qbuf + (size_t)j * MS * MS;
-				for (int e = tid; e < MS * MS; e += kThreads) {
-					const int i = e / MS, l = e % MS;
-					Qg[e] = make_double2(sh.pl[2][i * LD + l], sh.pl[3][i * LD + l]);
-					Anext[(long long)gidx(i, P, Q) * kp + gidx(l, P, Q)] = make_double2(mr[i * LD + l], mi[i * LD + l]);
-				}
-				__syncthreads();
-			}
-			grid.sync();
-			// ---- phase 2: block products ----
-			for (int w = blockIdx.x; w < nW; w += gridDim.x) {
-				double cr[2][2], ci[2][2];
-				if (w < nA2) {
-					const int jr = w / (np - 1);
-					int jc = w % (np - 1);
-					if (jc >= jr) jc++;
-					const int Pr = rr_player(jr, r, nb), Qr = rr_player(nb - 1 - jr, r, nb);
-					const int Pc = rr_player(jc, r, nb), Qc = rr_player(nb - 1 - jc, r, nb);
-					for (int e = tid; e < MS * MS; e += kThreads) {
-						const int i = e / MS, l = e % MS;
-						const double2 v = __ldcg(Acur + (long long)gidx(i, Pr, Qr) * kp + gidx(l, Pc, Qc));
-						sh.pl[0][i * LD + l] = v.x;
-						sh.pl[1][i * LD + l] = v.y;
-					}
-					load_q(sh.pl[2], sh.pl[3], Qbuf + (size_t)jr * MS * MS);
-					load_q(sh.pl[4], sh.pl[5], Qbuf + (size_t)jc * MS * MS);
-					__syncthreads();
-					cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
-					__syncthreads();
-#pragma unroll
-					for (int b = 0; b < 2; b++)
-#pragma unroll
-						for (int h = 0; h < 2; h++) {
-							int row, col;
-							acc_rc(b, h, row, col);
-							sh.pl[0][row * LD + col] = cr[b][h];
-							sh.pl[1][row * LD + col] = ci[b][h];
-						}
-					__syncthreads();
-					// C = Qr^H T: A(i, m) = conj(Qr(m, i))
-					cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
-#pragma unroll
-					for (int b = 0; b < 2; b++)
-#pragma unroll
-						for (int h = 0; h < 2; h++) {
-							int row, col;
-							acc_rc(b, h, row, col);
-							Anext[(long long)gidx(row, Pr, Qr) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
-						}
-				} else {
-					const int v = w - nA2;
-					const int rb = v / np, jc = v % np;
-					const int Pc = rr_player(jc, r, nb), Qc = rr_player(nb - 1 - jc, r, nb);
-					for (int e = tid; e < MS * MS; e += kThreads) {
-						const int i = e / MS, l = e % MS;
-						const double2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
-						sh.pl[0][i * LD + l] = x.x;
-						sh.pl[1][i * LD + l] = x.y;
-					}
-					load_q(sh.pl[4], sh.pl[5], Qbuf + (size_t)jc * MS * MS);
-					__syncthreads();
-					cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
-#pragma unroll
-					for (int b = 0; b < 2; b++)
-#pragma unroll
-						for (int h = 0; h < 2; h++) {
-							int row, col;
-							acc_rc(b, h, row, col);
-							V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
-						}
-				}
-				__syncthreads();
-			}
-			grid.sync();
-			double2* t = Acur;
-			Acur = Anext;
-			Anext = t;
+	bool stop = false, converged = false;
+	long long t = 0;
+	for (;;) {
+		const bool do_p1 = !stop;  // phase 1 of round t
+		const bool do_p2 = t >= 1;  // phase 2 of round t - 1
+		if (do_p1 && (int)blockIdx.x < p1) {
+			const double2* prev = bufs[t % 3];
+			const double2* prev2 = bufs[(t + 2) % 3];
+			double2* out = bufs[(t + 1) % 3];
+			for (int j = blockIdx.x; j < np; j += p1)
+				phase1_item(sh, j, t, rounds, nb, np, kp, tol, prev, prev2, Qbuf + ((t + 1) & 1) * qstride,
+						Qbuf + (t & 1) * qstride, out);
 		}
-		if (tid == 0) {
+		if (do_p2 && (int)blockIdx.x >= p2first) {
+			const int ro = (int)((t - 1) % rounds);
+			const double2* src = bufs[(t + 2) % 3];
+			double2* dst = bufs[t % 3];
+			for (int w = (int)blockIdx.x - p2first; w < nW; w += p2count)
+				phase2_item(sh, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+		}
+		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
+		if (sweep_end && tid == 0) {
 			if (sh.cnt) atomicAdd(&counters[sweep], sh.cnt);
 			if (sh.tmax) atomicMax(&tmax[sweep], sh.tmax);
 			sh.cnt = 0;
 			sh.tmax = 0ULL;
 		}
 		grid.sync();
-		const int cnt = *((volatile int*)&counters[sweep]);
-		const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmax[sweep]));
-		if (cnt == 0 || tm < kTauFinal) converged = true;
+		if (!do_p1) break;  // that was the last phase 2
+		if (sweep_end) {
+			// uniform across the grid: the counters are final after grid.sync
+			const int cnt = *((volatile int*)&counters[sweep]);
+			const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmax[sweep]));
+			if (cnt == 0 || tm < tau_final) {
+				converged = true;
+				stop = true;
+			}
+			sweep++;
+			if (sweep >= max_sweeps) stop = true;
+		}
+		t++;
 	}
+	// the last round completed is t - 1; A_{t-1} lives in bufs[t % 3]
 	if (blockIdx.x == 0 && tid == 0) {
 		counters[max_sweeps] = converged ? sweep : -1;
-		counters[max_sweeps + 1] = (Acur == A0) ? 0 : 1;
+		counters[max_sweeps + 1] = (int)(t % 3);
 	}
 }
 
 }  // namespace
 
 int bjacobi_padded(int k) { return ((k + MS - 1) / MS) * MS; }
-size_t bjacobi_qbuf_elems(int k) { return (size_t)(bjacobi_padded(k) / MS) * MS * MS; }
+size_t bjacobi_qbuf_elems(int k) { return 2 * (size_t)(bjacobi_padded(k) / MS) * MS * MS; }
 
-cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* V, double2* Qbuf, int kp, int max_sweeps, int* counters,
-		int num_sms, cudaStream_t s) {
+cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* A2, double2* V, double2* Qbuf, int kp,
+		int max_sweeps, double tau_final, int* counters, int num_sms, cudaStream_t s) {
 	const size_t smem = sizeof(Shared);
 	cudaError_t e = cudaFuncSetAttribute(bjacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	if (e != cudaSuccess) return e;
@@ -403,8 +528,9 @@ cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* V, double2* Qbuf, 
 	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
 	const int blocks = num_sms * per_sm;
 	double tol = 1e-15;
+	if (!(tau_final > 0.0)) tau_final = kTauFinal;
 	unsigned long long* tmax = reinterpret_cast<unsigned long long*>(counters + jacobi_tmax_offset(max_sweeps));
-	void* args[] = {&A0, &A1, &V, &Qbuf, &kp, &max_sweeps, &tol, &counters, &tmax};
+	void* args[] = {&A0, &A1, &A2, &V, &Qbuf, &kp, &max_sweeps, &tol, &tau_final, &counters, &tmax};
 	return cudaLaunchCooperativeKernel((void*)bjacobi_kernel, dim3(blocks), dim3(kThreads), args, smem, s);
 }
 

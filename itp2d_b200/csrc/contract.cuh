@@ -50,17 +50,23 @@ struct JacobiWork {
 	int* counters;    // jacobi_counter_ints(max_sweeps) ints
 	int max_sweeps;
 	double2* Qbuf = nullptr;  // block Jacobi unitaries (bjacobi_qbuf_elems); null: scalar Jacobi only
+	double2* A2 = nullptr;    // third kp x kp buffer of the block path (required with Qbuf)
+	// Stop after a sweep whose largest rotation tangent is below tau_final;
+	// 0 selects the FP64 default of the kernel. The remaining off-diagonal
+	// elements are then of order tau_final^2 relative to the eigenvalue gaps.
+	double tau_final = 0.0;
 };
 
 // Smallest k solved by block Jacobi (when JacobiWork::Qbuf is set).
 constexpr int kBlockJacobiMinK = 256;
-// Padded dimension of the block path (multiple of 64) and its Q buffer size.
+// Padded dimension of the block path (multiple of 32) and its Q buffer size
+// (the unitaries of two rounds).
 int bjacobi_padded(int k);
 size_t bjacobi_qbuf_elems(int k);
 // Padded dimension the eigensolver uses for (w, k); A0/A1/V are kp x kp.
 int jacobi_kp(const JacobiWork& w, int k);
-cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* V, double2* Qbuf, int kp, int max_sweeps, int* counters,
-		int num_sms, cudaStream_t s);
+cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* A2, double2* V, double2* Qbuf, int kp,
+		int max_sweeps, double tau_final, int* counters, int num_sms, cudaStream_t s);
 
 // Eigen-decomposition of the Hermitian S (k x k, row-major, full storage) by
 // parallel cyclic Jacobi, then W[:, n] = V[:, p(n)] / sqrt(l_n) with l

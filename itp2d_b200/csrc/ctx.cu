@@ -83,6 +83,7 @@ struct itp2d_ctx {
 	EigStatus* hstat = nullptr;
 	double* dnorm = nullptr;
 	int last_sweeps = 0;
+	long long sweeps_total = 0;
 	int engine = ITP2D_CONTRACT_AUTO;
 	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
 	int* dflag = nullptr;  // tensor-core wait time-outs (device)
@@ -99,6 +100,8 @@ struct itp2d_ctx {
 	long long launches = 0;
 	bool timing = false;
 	double phase_ms[5] = {0, 0, 0, 0, 0};
+	double phase_ms_p[10] = {};     // [precision * 5 + phase]
+	long long phase_calls_p[10] = {};
 	std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 	std::vector<void*> allocs;
 };
@@ -375,7 +378,7 @@ struct PhaseTimer {
 	itp2d_ctx* c;
 	int phase;
 	cudaEvent_t a = nullptr, b = nullptr;
-	PhaseTimer(itp2d_ctx* c_, int ph) : c(c_), phase(ph) {
+	PhaseTimer(itp2d_ctx* c_, int ph) : c(c_), phase(ph + 5 * c_->precision) {
 		if (c->timing) {
 			cudaEventCreate(&a);
 			cudaEventCreate(&b);
@@ -395,7 +398,9 @@ void flush_timers(itp2d_ctx* c) {
 		cudaEventSynchronize(p.second.second);
 		float ms = 0.f;
 		cudaEventElapsedTime(&ms, p.second.first, p.second.second);
-		c->phase_ms[p.first] += ms;
+		c->phase_ms[p.first % 5] += ms;
+		c->phase_ms_p[p.first] += ms;
+		c->phase_calls_p[p.first]++;
 		cudaEventDestroy(p.second.first);
 		cudaEventDestroy(p.second.second);
 	}
@@ -640,6 +645,8 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	if (e == cudaSuccess) c->jw.V = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
 	if (e == cudaSuccess && k >= kBlockJacobiMinK)
 		c->jw.Qbuf = (double2*)dalloc(c, bjacobi_qbuf_elems(k) * sizeof(double2), &e);
+	if (e == cudaSuccess && k >= kBlockJacobiMinK)
+		c->jw.A2 = (double2*)dalloc(c, (size_t)kp * kp * sizeof(double2), &e);
 	if (e == cudaSuccess) c->jw.evals = (double*)dalloc(c, (size_t)k * sizeof(double), &e);
 	if (e == cudaSuccess) c->jw.perm = (int*)dalloc(c, (size_t)k * sizeof(int), &e);
 	if (e == cudaSuccess) c->jw.counters = (int*)dalloc(c, jacobi_counters(c->jw.max_sweeps) * sizeof(int), &e);
@@ -866,6 +873,9 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	}
 	{
 		PhaseTimer t(c, kEigen);
+		// FP32 states: an overlap accurate to about 1e-5 needs eigenvectors to
+		// about 1e-8, which a final tangent of 1e-4 gives
+		c->jw.tau_final = f64 ? 0.0 : 1e-4;
 		ITP2D_TRY(launch_eigensolve(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
 		c->launches += 6;
 	}
@@ -884,6 +894,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
 	const EigStatus s = *c->hstat;
 	c->last_sweeps = s.sweeps;
+	if (s.sweeps > 0) c->sweeps_total += s.sweeps;
 	if (tc && *c->hflag != ITP2D_OK) {
 		const int f = *c->hflag;
 		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
@@ -972,7 +983,20 @@ int itp2d_phase_times(itp2d_ctx* c, double* ms5) {
 	return ITP2D_OK;
 }
 
+int itp2d_phase_stats(itp2d_ctx* c, double* ms10, long long* calls10) {
+	if (!c || !ms10 || !calls10) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	flush_timers(c);
+	for (int i = 0; i < 10; i++) {
+		ms10[i] = c->phase_ms_p[i];
+		calls10[i] = c->phase_calls_p[i];
+	}
+	return ITP2D_OK;
+}
+
 int itp2d_last_sweeps(itp2d_ctx* c) { return c ? c->last_sweeps : -1; }
+
+long long itp2d_total_sweeps(itp2d_ctx* c) { return c ? c->sweeps_total : -1; }
 
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs) {
 	if (n < 1 || !A || !evals || !evecs) return ITP2D_E_INVALID;
@@ -1001,13 +1025,14 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
 	w.A1 = (double2*)al((size_t)kp * kp * sizeof(double2));
 	w.V = (double2*)al((size_t)kp * kp * sizeof(double2));
 	if (n >= kBlockJacobiMinK) w.Qbuf = (double2*)al(bjacobi_qbuf_elems(n) * sizeof(double2));
+	if (n >= kBlockJacobiMinK) w.A2 = (double2*)al((size_t)kp * kp * sizeof(double2));
 	w.evals = (double*)al((size_t)n * sizeof(double));
 	w.perm = (int*)al((size_t)n * sizeof(int));
 	w.counters = (int*)al(jacobi_counters(w.max_sweeps) * sizeof(int));
 	EigStatus* dst = (EigStatus*)al(sizeof(EigStatus));
 	int status = ITP2D_OK;
 	if (!dS || !w.A0 || !w.A1 || !w.V || !w.evals || !w.perm || !w.counters || !dst ||
-			(n >= kBlockJacobiMinK && !w.Qbuf))
+			(n >= kBlockJacobiMinK && (!w.Qbuf || !w.A2)))
 		status = ITP2D_E_OOM;
 	std::vector<double2> V;
 	std::vector<int> perm(n);

@@ -99,7 +99,7 @@ constexpr double kTauFinal = 1e-10;
 // loads of the rotation inputs, then applies the rotations after one CTA
 // barrier; the round ends with one grid barrier.
 __global__ void __launch_bounds__(kThreads) jacobi_kernel(double2* A0, double2* A1, double2* V, int kp,
-		int max_sweeps, double tol, int* counters, unsigned long long* tmax) {
+		int max_sweeps, double tol, double tau_final, int* counters, unsigned long long* tmax) {
 	cg::grid_group grid = cg::this_grid();
 	__shared__ Rot rr[kItems][TP];
 	__shared__ Rot rc[kItems][TP];
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) jacobi_kernel(double2* A0, double2* 
 		// uniform across the grid: everything below reads values final after grid.sync
 		const int cnt = *((volatile int*)&counters[sweep]);
 		const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmax[sweep]));
-		if (cnt == 0 || tm < kTauFinal) converged = true;
+		if (cnt == 0 || tm < tau_final) converged = true;
 	}
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		counters[max_sweeps] = converged ? sweep : -1;   // sweeps used, -1: no convergence
@@ -296,14 +296,16 @@ __global__ void __launch_bounds__(256) normalize_columns_kernel(double2* V, int 
 
 // Sort the k eigenvalues ascending (bitonic, one CTA) and run the checks of
 // stateset.cpp:158-173 in that order.
-__global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* __restrict__ A1, int k, int kp,
-		const int* counters, int max_sweeps, double* evals, int* perm, EigStatus* st, int check) {
+__global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* __restrict__ A1,
+		const double2* __restrict__ A2, int k, int kp, const int* counters, int max_sweeps, double* evals, int* perm,
+		EigStatus* st, int check) {
 	extern __shared__ unsigned char sm[];
 	int P = 1;
 	while (P < k) P <<= 1;
 	double* key = reinterpret_cast<double*>(sm);
 	int* idx = reinterpret_cast<int*>(key + P);
-	const double2* A = counters[max_sweeps + 1] == 0 ? A0 : A1;
+	const int which = counters[max_sweeps + 1];
+	const double2* A = which == 0 ? A0 : (which == 1 ? A1 : A2);
 	for (int i = threadIdx.x; i < P; i += blockDim.x) {
 		if (i < k) {
 			double v = __ldcg(A + (long long)i * kp + i).x;
@@ -394,7 +396,7 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 }
 
 int jacobi_kp(const JacobiWork& w, int k) {
-	return (w.Qbuf && k >= kBlockJacobiMinK) ? bjacobi_padded(k) : ((k + 1) & ~1);
+	return (w.Qbuf && w.A2 && k >= kBlockJacobiMinK) ? bjacobi_padded(k) : ((k + 1) & ~1);
 }
 
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check) {
@@ -403,8 +405,8 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 	cudaError_t e = cudaMemsetAsync(w.counters, 0, jacobi_counters(w.max_sweeps) * sizeof(int), s);
 	if (e != cudaSuccess) return e;
 	jacobi_init_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(S, k, kp, w.A0, w.V);
-	if (w.Qbuf && k >= kBlockJacobiMinK) {
-		e = launch_bjacobi(w.A0, w.A1, w.V, w.Qbuf, kp, w.max_sweeps, w.counters, num_sms, s);
+	if (w.Qbuf && w.A2 && k >= kBlockJacobiMinK) {
+		e = launch_bjacobi(w.A0, w.A1, w.A2, w.V, w.Qbuf, kp, w.max_sweeps, w.tau_final, w.counters, num_sms, s);
 		if (e != cudaSuccess) return e;
 	} else {
 		int per_sm = 0;
@@ -417,10 +419,11 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 		int blocks = std::min(num_sms * std::min(per_sm, 2), (nW + kItems - 1) / kItems);
 		if (blocks < 1) blocks = 1;
 		double tol = 1e-15;
+		double tau_final = w.tau_final > 0.0 ? w.tau_final : kTauFinal;
 		int ms = w.max_sweeps;
 		int kpv = kp;
 		unsigned long long* tmax = reinterpret_cast<unsigned long long*>(w.counters + jacobi_tmax_offset(ms));
-		void* args[] = {&w.A0, &w.A1, &w.V, (void*)&kpv, &ms, &tol, &w.counters, &tmax};
+		void* args[] = {&w.A0, &w.A1, &w.V, (void*)&kpv, &ms, &tol, &tau_final, &w.counters, &tmax};
 		e = cudaLaunchCooperativeKernel((void*)jacobi_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
 		if (e != cudaSuccess) return e;
 	}
@@ -429,8 +432,8 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 	while (P < k) P <<= 1;
 	const size_t smem = (size_t)P * (sizeof(double) + sizeof(int));
 	if (smem > 48 * 1024) cudaFuncSetAttribute(eig_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	eig_sort_kernel<<<1, 1024, smem, s>>>(w.A0, w.A1, k, kp, w.counters, w.max_sweeps, w.evals, w.perm, st,
-			check);
+	eig_sort_kernel<<<1, 1024, smem, s>>>(w.A0, w.A1, w.A2, k, kp, w.counters, w.max_sweeps, w.evals, w.perm,
+			st, check);
 	return cudaGetLastError();
 }
 
