@@ -1,0 +1,350 @@
+// Row and column passes of the split operator for periodic lines of
+// N = A * B points (N = 32 ... 1024, powers of two), with the line FFTs held
+// in registers.
+//
+// One line is owned by B threads of one warp; thread t holds the A elements at
+// positions t + B a (a = 0..A-1). A forward or backward DFT of the line is the
+// two-stage (four-step) factorisation
+//   Y[b][k1]      = sum_a x[B a + b] w_A^(a k1)                 (registers)
+//   Y[b][k1]     *= w_N^(b k1)
+//   X[k1 + A k2]  = sum_b Y[b][k1] w_B^(b k2)                   (registers)
+// with one exchange of Y through shared memory between the stages (warp
+// barriers only). Thread t then holds X at k1 = t + B i, all k2, that is at
+// positions t + B (i + (A/B) k2): the same position set it started with, so an
+// inverse transform, a pointwise table and a forward transform chain without
+// any further data movement. The exchange index of Y[b][k1] is
+// k1 B + (b xor (k1 mod B)), which makes both the writes (fixed k1) and the
+// reads (fixed b) free of shared-memory bank conflicts for 8- and 16-byte
+// elements. The in-register DFTs are radix-2 decimation in time with
+// compile-time twiddle factors.
+//
+// Same arithmetic contract as the shared-memory Stockham passes in split.cu:
+// unnormalised transforms with FFTW's sign convention (forward exp(-2 pi i jk/N)),
+// tables applied as in RowPassArgs / ColPassArgs.
+#include "split.cuh"
+
+#include <algorithm>
+#include <mutex>
+#include <set>
+#include <type_traits>
+#include <utility>
+
+namespace itp2d {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// cos(2 pi j / 32) and sin(2 pi j / 32), j = 0..31.
+__host__ __device__ constexpr double cos32(int j) {
+	constexpr double c[32] = {
+			1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+			0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173, 0.19509032201612826785,
+			0.0, -0.19509032201612826785, -0.38268343236508977173, -0.55557023301960222474,
+			-0.70710678118654752440, -0.83146961230254523708, -0.92387953251128675613, -0.98078528040323044913,
+			-1.0, -0.98078528040323044913, -0.92387953251128675613, -0.83146961230254523708,
+			-0.70710678118654752440, -0.55557023301960222474, -0.38268343236508977173, -0.19509032201612826785,
+			0.0, 0.19509032201612826785, 0.38268343236508977173, 0.55557023301960222474,
+			0.70710678118654752440, 0.83146961230254523708, 0.92387953251128675613, 0.98078528040323044913};
+	return c[j & 31];
+}
+__host__ __device__ constexpr double sin32(int j) { return cos32(j - 8); }
+
+__host__ __device__ constexpr int bitrev(int i, int n) {
+	int r = 0;
+	for (int m = n >> 1; m > 0; m >>= 1, i >>= 1) r = (r << 1) | (i & 1);
+	return r;
+}
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I = 0 .. N-1, so
+// that register-array indices inside f are constants.
+template <class F, int... I>
+__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, I...>) {
+	(f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void sfor(F&& f) {
+	sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// In-register DFT of length M (power of two, <= 32) of v[0..M), in place,
+// natural order in and out: v[k] = sum_j v[j] exp(SIGN 2 pi i jk / M).
+template <class R, int M, int SIGN>
+__device__ __forceinline__ void dft_reg(c2<R>* v) {
+	sfor<M>([&](auto I) {
+		constexpr int i = I;
+		constexpr int r = bitrev(i, M);
+		if constexpr (r > i) {
+			const c2<R> x = v[i];
+			v[i] = v[r];
+			v[r] = x;
+		}
+	});
+	sfor<ilog2(M)>([&](auto S) {
+		constexpr int m = 2 << S;
+		constexpr int h = m >> 1;
+		sfor<M / m>([&](auto G) {
+			constexpr int base = G * m;
+			sfor<h>([&](auto J) {
+				constexpr int j = J;
+				c2<R> x = v[base + j + h];
+				if constexpr (j == 0) {
+				} else if constexpr (4 * j == m) {
+					x = cmul_i(x, SIGN);  // exp(SIGN i pi / 2)
+				} else {
+					constexpr double cr = cos32(j * (32 / m));
+					constexpr double ci = SIGN * sin32(j * (32 / m));
+					x = cmul(x, mk<R>((R)cr, (R)ci));
+				}
+				const c2<R> u = v[base + j];
+				v[base + j] = cadd(u, x);
+				v[base + j + h] = csub(u, x);
+			});
+		});
+	});
+}
+
+// Transform of one line held as v[a] = x[t + B a]. xb: the line's exchange
+// area (N elements, element stride es); xtw: w_N^(b k1) at [k1 * B + b]
+// (forward sign). On return v[a] = X[t + B a].
+template <class R, int A, int B, int SIGN>
+__device__ __forceinline__ void line_fft(c2<R>* v, int t, c2<R>* xb, int es, const c2<R>* xtw) {
+	constexpr int S2 = A / B;
+	dft_reg<R, A, SIGN>(v);
+	sfor<A - 1>([&](auto K) {
+		constexpr int k1 = K + 1;
+		c2<R> w = xtw[k1 * B + t];
+		if (SIGN > 0) w.y = -w.y;
+		v[k1] = cmul(v[k1], w);
+	});
+	__syncwarp();  // earlier readers of xb are done
+	sfor<A>([&](auto K) {
+		constexpr int k1 = K;
+		xb[(k1 * B + (t ^ (k1 & (B - 1)))) * es] = v[k1];
+	});
+	__syncwarp();
+	c2<R> u[A];
+	sfor<S2>([&](auto I) {
+		constexpr int i = I;
+		const int k1 = t + B * i;
+		sfor<B>([&](auto Bi) {
+			constexpr int b = Bi;
+			u[i * B + b] = xb[(k1 * B + (b ^ t)) * es];
+		});
+		dft_reg<R, B, SIGN>(u + i * B);
+	});
+	sfor<S2>([&](auto I) {
+		sfor<B>([&](auto K2) { v[I + S2 * K2] = u[I * B + K2]; });
+	});
+}
+
+template <class R, int A, int B>
+__device__ __forceinline__ void load_xtw(c2<R>* xtw, const c2<R>* tw) {
+	constexpr int N = A * B;
+	for (int i = threadIdx.x; i < N; i += blockDim.x) {
+		const int k1 = i / B, b = i - k1 * B;
+		xtw[i] = tw[(b * k1) & (N - 1)];
+	}
+}
+
+// Row pass: 256 / B rows of one state per tile, tiles ordered state-fastest.
+template <class R, int A, int B>
+__global__ void __launch_bounds__(kThreads) row_reg_kernel(RowPassArgs a, int k) {
+	using T = c2<R>;
+	constexpr int N = A * B, LPI = kThreads / B;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T* xtw = reinterpret_cast<T*>(smem_raw);
+	T* xb = xtw + N;
+	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
+	__syncthreads();
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
+	T* lxb = xb + line * N;
+	const int sx = a.sx;
+	const int ntr = (a.sy + LPI - 1) / LPI;
+	const long long total = (long long)k * ntr;
+	const R* mpre = reinterpret_cast<const R*>(a.mul_pre);
+	const R* mmid = reinterpret_cast<const R*>(a.mul_mid);
+	const R* mpost = reinterpret_cast<const R*>(a.mul_post);
+	const T* in = reinterpret_cast<const T*>(a.in);
+	T* out = reinterpret_cast<T*>(a.out);
+	const T* acc = reinterpret_cast<const T*>(a.acc);
+	for (long long tile = blockIdx.x; tile < total; tile += gridDim.x) {
+		const long long state = tile % k;
+		const int y = (int)(tile / k) * LPI + line;
+		const bool valid = y < a.sy;  // the whole warp runs the transforms
+		const long long base = state * a.G + (long long)y * sx + t;
+		const int toff = y * sx + t;
+		T v[A];
+#pragma unroll
+		for (int i = 0; i < A; i++) v[i] = valid ? in[base + B * i] : mk<R>(0, 0);
+		const R* m0 = a.do_inv ? mpre : mmid;
+		if (m0 && valid) {
+#pragma unroll
+			for (int i = 0; i < A; i++) v[i] = cscale(v[i], m0[toff + B * i]);
+		}
+		if (a.do_inv) {
+			line_fft<R, A, B, 1>(v, t, lxb, 1, xtw);
+			if (mmid && valid) {
+#pragma unroll
+				for (int i = 0; i < A; i++) v[i] = cscale(v[i], mmid[toff + B * i]);
+			}
+		}
+		if (a.do_fwd) {
+			line_fft<R, A, B, -1>(v, t, lxb, 1, xtw);
+			if (mpost && valid) {
+#pragma unroll
+				for (int i = 0; i < A; i++) v[i] = cscale(v[i], mpost[toff + B * i]);
+			}
+		}
+		if (valid) {
+			if (acc) {
+#pragma unroll
+				for (int i = 0; i < A; i++) v[i] = cadd(v[i], acc[base + B * i]);
+			}
+#pragma unroll
+			for (int i = 0; i < A; i++) out[base + B * i] = v[i];
+		}
+	}
+}
+
+// Column pass, in place: tiles of W = 256 / B columns x N rows of one state
+// staged in shared memory ([y][c], row stride W + 1); each column line is
+// transformed by B threads of one warp, using the line's own column of the
+// tile as its exchange area.
+template <class R, int A, int B>
+__global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k) {
+	using T = c2<R>;
+	constexpr int N = A * B, W = kThreads / B, LD = W + 1;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T* xtw = reinterpret_cast<T*>(smem_raw);
+	T* tile = xtw + N;
+	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
+	const int sx = a.sx;
+	const int nct = (sx + W - 1) / W;
+	const long long total = (long long)k * nct;
+	const R* m2 = reinterpret_cast<const R*>(a.mul2d);
+	const R* m1 = reinterpret_cast<const R*>(a.mul1d);
+	T* data = reinterpret_cast<T*>(a.data);
+	for (long long tl = blockIdx.x; tl < total; tl += gridDim.x) {
+		const long long state = tl % k;
+		const int col0 = (int)(tl / k) * W;
+		const int ncols = min(W, sx - col0);
+		T* src = data + state * a.G + col0;
+		__syncthreads();  // the previous tile has left shared memory
+#pragma unroll
+		for (int it = 0; it < N * W / kThreads; it++) {
+			const int i = it * kThreads + threadIdx.x;
+			const int y = i / W, c = i - y * W;
+			tile[y * LD + c] = c < ncols ? src[(long long)y * sx + c] : mk<R>(0, 0);
+		}
+		__syncthreads();
+		T v[A];
+#pragma unroll
+		for (int i = 0; i < A; i++) v[i] = tile[(t + B * i) * LD + line];
+		T* lxb = tile + line;
+		if (a.mode == 0 || a.mode == 1) line_fft<R, A, B, -1>(v, t, lxb, LD, xtw);
+		if (a.mode == 0) {
+			const bool valid = line < ncols;
+#pragma unroll
+			for (int i = 0; i < A; i++) {
+				const int y = t + B * i;
+				const R f = !valid ? (R)0 : (m2 ? m2[y * sx + col0 + line] : m1[y]);
+				v[i] = cscale(v[i], f);
+			}
+		}
+		if (a.mode == 0 || a.mode == 2) line_fft<R, A, B, 1>(v, t, lxb, LD, xtw);
+		__syncwarp();
+#pragma unroll
+		for (int i = 0; i < A; i++) tile[(t + B * i) * LD + line] = v[i];
+		__syncthreads();
+#pragma unroll
+		for (int it = 0; it < N * W / kThreads; it++) {
+			const int i = it * kThreads + threadIdx.x;
+			const int y = i / W, c = i - y * W;
+			if (c < ncols) src[(long long)y * sx + c] = tile[y * LD + c];
+		}
+	}
+}
+
+template <class K>
+void opt_in_smem(K kernel, size_t bytes) {
+	static std::mutex mu;
+	static std::set<const void*> done;
+	std::lock_guard<std::mutex> g(mu);
+	if (bytes > 48 * 1024 && done.insert((const void*)kernel).second)
+		cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+template <class K>
+int grid_for(K kernel, size_t smem, long long tiles) {
+	static int sms = 0;
+	if (!sms) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	}
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem);
+	const long long b = (long long)std::max(1, per_sm) * std::max(1, sms);
+	return (int)std::max(1LL, std::min(b, tiles));
+}
+
+template <class R, int A, int B>
+void row_reg(const RowPassArgs& a, int k, cudaStream_t s) {
+	constexpr int N = A * B;
+	const size_t sm = (size_t)(N + (kThreads / B) * N) * sizeof(c2<R>);
+	opt_in_smem(row_reg_kernel<R, A, B>, sm);
+	const long long tiles = (long long)k * ((a.sy + kThreads / B - 1) / (kThreads / B));
+	row_reg_kernel<R, A, B><<<grid_for(row_reg_kernel<R, A, B>, sm, tiles), kThreads, sm, s>>>(a, k);
+}
+
+template <class R, int A, int B>
+void col_reg(const ColPassArgs& a, int k, cudaStream_t s) {
+	constexpr int N = A * B, W = kThreads / B;
+	const size_t sm = (size_t)(N + N * (W + 1)) * sizeof(c2<R>);
+	opt_in_smem(col_reg_kernel<R, A, B>, sm);
+	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
+	col_reg_kernel<R, A, B><<<grid_for(col_reg_kernel<R, A, B>, sm, tiles), kThreads, sm, s>>>(a, k);
+}
+
+}  // namespace
+
+bool reg_fft_supported(int N) { return N >= 32 && N <= 1024 && (N & (N - 1)) == 0; }
+
+template <class R>
+bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s) {
+	if (a.lp.kind != 0) return false;
+	switch (a.sx) {
+		case 32: row_reg<R, 8, 4>(a, k, s); return true;
+		case 64: row_reg<R, 8, 8>(a, k, s); return true;
+		case 128: row_reg<R, 16, 8>(a, k, s); return true;
+		case 256: row_reg<R, 16, 16>(a, k, s); return true;
+		case 512: row_reg<R, 32, 16>(a, k, s); return true;
+		case 1024: row_reg<R, 32, 32>(a, k, s); return true;
+		default: return false;
+	}
+}
+
+template <class R>
+bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s) {
+	if (a.lp.kind != 0) return false;
+	switch (a.sy) {
+		case 32: col_reg<R, 8, 4>(a, k, s); return true;
+		case 64: col_reg<R, 8, 8>(a, k, s); return true;
+		case 128: col_reg<R, 16, 8>(a, k, s); return true;
+		case 256: col_reg<R, 16, 16>(a, k, s); return true;
+		case 512: col_reg<R, 32, 16>(a, k, s); return true;
+		case 1024: col_reg<R, 32, 32>(a, k, s); return true;
+		default: return false;
+	}
+}
+
+template bool launch_row_pass_reg<double>(const RowPassArgs&, int, cudaStream_t);
+template bool launch_row_pass_reg<float>(const RowPassArgs&, int, cudaStream_t);
+template bool launch_col_pass_reg<double>(const ColPassArgs&, int, cudaStream_t);
+template bool launch_col_pass_reg<float>(const ColPassArgs&, int, cudaStream_t);
+
+}  // namespace itp2d

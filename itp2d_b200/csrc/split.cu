@@ -449,6 +449,7 @@ int persistent_blocks(K kernel, size_t smem, long long tiles) {
 
 template <class R>
 void launch_row_pass(const RowPassArgs& a, int k, const void*, cudaStream_t s) {
+	if (launch_row_pass_reg<R>(a, k, s)) return;
 	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
 	const size_t sm = pipe_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
 	set_smem_limit(row_pass_kernel<R>);
@@ -458,6 +459,7 @@ void launch_row_pass(const RowPassArgs& a, int k, const void*, cudaStream_t s) {
 
 template <class R>
 void launch_col_pass(const ColPassArgs& a, int k, const void*, cudaStream_t s) {
+	if (launch_col_pass_reg<R>(a, k, s)) return;
 	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
 	const size_t sm = pipe_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));
 	set_smem_limit(col_pass_kernel<R>);

@@ -80,6 +80,10 @@ struct EnergyColArgs {
 };
 
 template <class R> void launch_row_pass(const RowPassArgs& a, int k, const void* tw, cudaStream_t s);
+// Register-FFT passes (rfft.cu) for periodic lines of 32..1024 points (powers
+// of two); return false, launching nothing, for other lines.
+template <class R> bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s);
+template <class R> bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s);
 template <class R> void launch_col_pass(const ColPassArgs& a, int k, const void* tw, cudaStream_t s);
 template <class R> void launch_energy_row(const EnergyRowArgs& a, int k, const void* tw, cudaStream_t s);
 template <class R> void launch_energy_col(const EnergyColArgs& a, int k, const void* tw, cudaStream_t s);
