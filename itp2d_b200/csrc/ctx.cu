@@ -489,6 +489,17 @@ int propagate_fused(itp2d_ctx* c) {
 	return ITP2D_OK;
 }
 
+// Row / column tile of the energy passes: the register-FFT tile where that
+// path applies, else the shared-memory tile.
+int energy_rows(const LinePlan& lp, int elem, int sy) {
+	const int r = energy_row_tile_reg(lp, sy);
+	return r ? r : row_tile_rows(line_len(lp), elem, sy);
+}
+int energy_cols(const LinePlan& lp, int elem, int sx) {
+	const int c = energy_col_tile_reg(lp, sx);
+	return c ? c : col_tile_cols(line_len(lp), elem, sx);
+}
+
 template <class R>
 int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
@@ -503,7 +514,7 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 		a.src_t = c->acc; a.psi = c->psi; a.tmul = nullptr; a.V = V;
 		a.h_out = h_out; a.sums = want_sums ? c->sums : nullptr; a.Eshift = c->dEshift;
 		a.do_fwd = 0; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
-		a.rows_per_tile = row_tile_rows(line_len(lx), sizeof(c2<R>), c->sy);
+		a.rows_per_tile = energy_rows(lx, sizeof(c2<R>), c->sy);
 		a.lp = lx;
 		launch_energy_row<R>(a, c->k, nullptr, c->stream);
 		c->launches++;
@@ -520,7 +531,7 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 	a.src_t = c->psi; a.psi = c->psi; a.tmul = c->eTx; a.V = V;
 	a.h_out = c->acc; a.sums = nullptr; a.Eshift = nullptr;
 	a.do_fwd = 1; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
-	a.rows_per_tile = row_tile_rows(line_len(lx), sizeof(c2<R>), c->sy);
+	a.rows_per_tile = energy_rows(lx, sizeof(c2<R>), c->sy);
 	a.lp = lx;
 	launch_energy_row<R>(a, c->k, nullptr, c->stream);
 	c->launches++;
@@ -528,7 +539,7 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 	b.psi = c->psi; b.add_in = c->acc; b.ty = c->eTy;
 	b.h_out = h_out; b.sums = want_sums ? c->sums : nullptr; b.Eshift = c->dEshift;
 	b.sx = c->sx; b.sy = c->sy; b.G = c->G;
-	b.cols_per_tile = col_tile_cols(line_len(ly), sizeof(c2<R>), c->sx);
+	b.cols_per_tile = energy_cols(ly, sizeof(c2<R>), c->sx);
 	b.lp = ly;
 	launch_energy_col<R>(b, c->k, nullptr, c->stream);
 	c->launches++;

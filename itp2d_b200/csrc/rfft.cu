@@ -269,6 +269,146 @@ __global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k)
 	}
 }
 
+// Energy sums of one element: Re, Im <psi|h>, <h|h>, |h - es psi|^2, <psi|psi>.
+template <class T>
+__device__ __forceinline__ void esums(double* s, T p, T h, double es) {
+	const double pr = p.x, pi = p.y, hr = h.x, hi = h.y;
+	s[0] += pr * hr + pi * hi;
+	s[1] += pr * hi - pi * hr;
+	s[2] += hr * hr + hi * hi;
+	const double dr = hr - es * pr, di = hi - es * pi;
+	s[3] += dr * dr + di * di;
+	s[4] += pr * pr + pi * pi;
+}
+
+// Deterministic CTA reduction of the five sums into out[0..5) (thread 0).
+__device__ __forceinline__ void reduce5(double* s, double* red, double* out) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int j = 0; j < 5; j++)
+		for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+	__syncthreads();
+	if (lane == 0)
+		for (int j = 0; j < 5; j++) red[warp * 5 + j] = s[j];
+	__syncthreads();
+	if (threadIdx.x == 0)
+		for (int j = 0; j < 5; j++) {
+			double v = 0.0;
+			for (int w = 0; w < kThreads / 32; w++) v += red[w * 5 + j];
+			out[j] = v;
+		}
+}
+
+// Energy row pass (grid: states x row tiles of 256 / B rows):
+//   t = Tinv_x(tmul .* Tfwd_x(src_t)) (do_fwd) or Tinv_x(src_t);
+//   h = t + V .* psi; h -> h_out; per-tile sums.
+template <class R, int A, int B>
+__global__ void __launch_bounds__(kThreads) energy_row_reg_kernel(EnergyRowArgs a) {
+	using T = c2<R>;
+	constexpr int N = A * B, LPI = kThreads / B;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T* xtw = reinterpret_cast<T*>(smem_raw);
+	T* xb = xtw + N;
+	double* red = reinterpret_cast<double*>(xb + LPI * N);
+	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
+	__syncthreads();
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
+	const long long state = blockIdx.x;
+	const int y = blockIdx.y * LPI + line;
+	const bool valid = y < a.sy;
+	const long long base = state * a.G + (long long)y * a.sx + t;
+	const int toff = y * a.sx + t;
+	const T* src = reinterpret_cast<const T*>(a.src_t);
+	T v[A];
+#pragma unroll
+	for (int i = 0; i < A; i++) v[i] = valid ? src[base + B * i] : mk<R>(0, 0);
+	if (a.do_fwd) {
+		line_fft<R, A, B, -1>(v, t, xb + line * N, 1, xtw);
+		const R* tm = reinterpret_cast<const R*>(a.tmul);
+		if (valid) {
+#pragma unroll
+			for (int i = 0; i < A; i++) v[i] = cscale(v[i], tm[toff + B * i]);
+		}
+	}
+	line_fft<R, A, B, 1>(v, t, xb + line * N, 1, xtw);
+	double s[5] = {0, 0, 0, 0, 0};
+	if (valid) {
+		const T* psi = reinterpret_cast<const T*>(a.psi);
+		const R* V = reinterpret_cast<const R*>(a.V);
+		T* hout = reinterpret_cast<T*>(a.h_out);
+		const double es = a.Eshift ? a.Eshift[state] : 0.0;
+#pragma unroll
+		for (int i = 0; i < A; i++) {
+			T h = v[i];
+			const T p = psi[base + B * i];
+			if (V) {
+				const R w = V[toff + B * i];
+				h.x += w * p.x;
+				h.y += w * p.y;
+			}
+			if (hout) hout[base + B * i] = h;
+			if (a.sums) esums(s, p, h, es);
+		}
+	}
+	if (a.sums) reduce5(s, red, a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5);
+}
+
+// Energy column pass (periodic magnetic field; grid: states x column tiles of
+// 256 / B columns): t = Tinv_y(ty .* Tfwd_y(psi)), h = t + add_in; h -> h_out;
+// per-tile sums.
+template <class R, int A, int B>
+__global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs a) {
+	using T = c2<R>;
+	constexpr int N = A * B, W = kThreads / B, LD = W + 1;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T* xtw = reinterpret_cast<T*>(smem_raw);
+	T* tile = xtw + N;
+	double* red = reinterpret_cast<double*>(tile + N * LD);
+	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
+	const long long state = blockIdx.x;
+	const int col0 = blockIdx.y * W;
+	const int ncols = min(W, a.sx - col0);
+	const int sx = a.sx;
+	const long long base = state * a.G + col0;
+	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
+#pragma unroll
+	for (int it = 0; it < N * W / kThreads; it++) {
+		const int i = it * kThreads + threadIdx.x;
+		const int y = i / W, c = i - y * W;
+		tile[y * LD + c] = c < ncols ? psi[(long long)y * sx + c] : mk<R>(0, 0);
+	}
+	__syncthreads();
+	T v[A];
+#pragma unroll
+	for (int i = 0; i < A; i++) v[i] = tile[(t + B * i) * LD + line];
+	line_fft<R, A, B, -1>(v, t, tile + line, LD, xtw);
+	const R* ty = reinterpret_cast<const R*>(a.ty);
+#pragma unroll
+	for (int i = 0; i < A; i++) v[i] = cscale(v[i], ty[t + B * i]);
+	line_fft<R, A, B, 1>(v, t, tile + line, LD, xtw);
+	__syncwarp();
+#pragma unroll
+	for (int i = 0; i < A; i++) tile[(t + B * i) * LD + line] = v[i];
+	__syncthreads();
+	const T* add = reinterpret_cast<const T*>(a.add_in) + base;
+	T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
+	const double es = a.Eshift ? a.Eshift[state] : 0.0;
+	double s[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+	for (int it = 0; it < N * W / kThreads; it++) {
+		const int i = it * kThreads + threadIdx.x;
+		const int y = i / W, c = i - y * W;
+		if (c < ncols) {
+			const long long off = (long long)y * sx + c;
+			const T h = cadd(tile[y * LD + c], add[off]);
+			if (hout) hout[off] = h;
+			if (a.sums) esums(s, psi[off], h, es);
+		}
+	}
+	if (a.sums) reduce5(s, red, a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5);
+}
+
 template <class K>
 void opt_in_smem(K kernel, size_t bytes) {
 	static std::mutex mu;
@@ -310,9 +450,74 @@ void col_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	col_reg_kernel<R, A, B><<<grid_for(col_reg_kernel<R, A, B>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
+template <class R, int A, int B>
+void energy_row_reg(const EnergyRowArgs& a, int k, cudaStream_t s) {
+	constexpr int N = A * B, LPI = kThreads / B;
+	const size_t sm = (size_t)(N + LPI * N) * sizeof(c2<R>) + 5 * (kThreads / 32) * sizeof(double);
+	opt_in_smem(energy_row_reg_kernel<R, A, B>, sm);
+	energy_row_reg_kernel<R, A, B><<<dim3(k, (a.sy + LPI - 1) / LPI), kThreads, sm, s>>>(a);
+}
+
+template <class R, int A, int B>
+void energy_col_reg(const EnergyColArgs& a, int k, cudaStream_t s) {
+	constexpr int N = A * B, W = kThreads / B;
+	const size_t sm = (size_t)(N + N * (W + 1)) * sizeof(c2<R>) + 5 * (kThreads / 32) * sizeof(double);
+	opt_in_smem(energy_col_reg_kernel<R, A, B>, sm);
+	energy_col_reg_kernel<R, A, B><<<dim3(k, (a.sx + W - 1) / W), kThreads, sm, s>>>(a);
+}
+
+// Threads per line (B) of the register path for line length N, 0 if none.
+int reg_threads(int N) {
+	switch (N) {
+		case 32: return 4;
+		case 64: return 8;
+		case 128: return 8;
+		case 256: return 16;
+		case 512: return 16;
+		case 1024: return 32;
+		default: return 0;
+	}
+}
+
 }  // namespace
 
-bool reg_fft_supported(int N) { return N >= 32 && N <= 1024 && (N & (N - 1)) == 0; }
+int energy_row_tile_reg(const LinePlan& lp, int) {
+	const int B = lp.kind == 0 ? reg_threads(lp.N) : 0;
+	return B ? kThreads / B : 0;
+}
+
+int energy_col_tile_reg(const LinePlan& lp, int) {
+	const int B = lp.kind == 0 ? reg_threads(lp.N) : 0;
+	return B ? kThreads / B : 0;
+}
+
+template <class R>
+bool launch_energy_row_reg(const EnergyRowArgs& a, int k, cudaStream_t s) {
+	if (a.lp.kind != 0 || a.rows_per_tile == 0 || a.rows_per_tile != energy_row_tile_reg(a.lp, a.sy)) return false;
+	switch (a.sx) {
+		case 32: energy_row_reg<R, 8, 4>(a, k, s); return true;
+		case 64: energy_row_reg<R, 8, 8>(a, k, s); return true;
+		case 128: energy_row_reg<R, 16, 8>(a, k, s); return true;
+		case 256: energy_row_reg<R, 16, 16>(a, k, s); return true;
+		case 512: energy_row_reg<R, 32, 16>(a, k, s); return true;
+		case 1024: energy_row_reg<R, 32, 32>(a, k, s); return true;
+		default: return false;
+	}
+}
+
+template <class R>
+bool launch_energy_col_reg(const EnergyColArgs& a, int k, cudaStream_t s) {
+	if (a.lp.kind != 0 || a.cols_per_tile == 0 || a.cols_per_tile != energy_col_tile_reg(a.lp, a.sx)) return false;
+	switch (a.sy) {
+		case 32: energy_col_reg<R, 8, 4>(a, k, s); return true;
+		case 64: energy_col_reg<R, 8, 8>(a, k, s); return true;
+		case 128: energy_col_reg<R, 16, 8>(a, k, s); return true;
+		case 256: energy_col_reg<R, 16, 16>(a, k, s); return true;
+		case 512: energy_col_reg<R, 32, 16>(a, k, s); return true;
+		case 1024: energy_col_reg<R, 32, 32>(a, k, s); return true;
+		default: return false;
+	}
+}
 
 template <class R>
 bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s) {
@@ -346,5 +551,9 @@ template bool launch_row_pass_reg<double>(const RowPassArgs&, int, cudaStream_t)
 template bool launch_row_pass_reg<float>(const RowPassArgs&, int, cudaStream_t);
 template bool launch_col_pass_reg<double>(const ColPassArgs&, int, cudaStream_t);
 template bool launch_col_pass_reg<float>(const ColPassArgs&, int, cudaStream_t);
+template bool launch_energy_row_reg<double>(const EnergyRowArgs&, int, cudaStream_t);
+template bool launch_energy_row_reg<float>(const EnergyRowArgs&, int, cudaStream_t);
+template bool launch_energy_col_reg<double>(const EnergyColArgs&, int, cudaStream_t);
+template bool launch_energy_col_reg<float>(const EnergyColArgs&, int, cudaStream_t);
 
 }  // namespace itp2d

@@ -469,6 +469,7 @@ void launch_col_pass(const ColPassArgs& a, int k, const void*, cudaStream_t s) {
 
 template <class R>
 void launch_energy_row(const EnergyRowArgs& a, int k, const void*, cudaStream_t s) {
+	if (launch_energy_row_reg<R>(a, k, s)) return;
 	const int L = a.lp.kind == 0 ? a.sx : 2 * a.sx;
 	const dim3 grid(k, (a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
 	const size_t sm = row_pass_smem(L, a.rows_per_tile, a.lp.fft.n, sizeof(c2<R>));
@@ -478,6 +479,7 @@ void launch_energy_row(const EnergyRowArgs& a, int k, const void*, cudaStream_t 
 
 template <class R>
 void launch_energy_col(const EnergyColArgs& a, int k, const void*, cudaStream_t s) {
+	if (launch_energy_col_reg<R>(a, k, s)) return;
 	const int L = a.lp.kind == 0 ? a.sy : 2 * a.sy;
 	const dim3 grid(k, (a.sx + a.cols_per_tile - 1) / a.cols_per_tile);
 	const size_t sm = col_pass_smem(L, a.cols_per_tile, a.lp.fft.n, sizeof(c2<R>));

@@ -84,6 +84,12 @@ template <class R> void launch_row_pass(const RowPassArgs& a, int k, const void*
 // of two); return false, launching nothing, for other lines.
 template <class R> bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s);
 template <class R> bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s);
+// Register-FFT energy passes; they run when the tile size equals
+// energy_row_tile_reg / energy_col_tile_reg (non-zero for supported lines).
+int energy_row_tile_reg(const LinePlan& lp, int sy);
+int energy_col_tile_reg(const LinePlan& lp, int sx);
+template <class R> bool launch_energy_row_reg(const EnergyRowArgs& a, int k, cudaStream_t s);
+template <class R> bool launch_energy_col_reg(const EnergyColArgs& a, int k, cudaStream_t s);
 template <class R> void launch_col_pass(const ColPassArgs& a, int k, const void* tw, cudaStream_t s);
 template <class R> void launch_energy_row(const EnergyRowArgs& a, int k, const void* tw, cudaStream_t s);
 template <class R> void launch_energy_col(const EnergyColArgs& a, int k, const void* tw, cudaStream_t s);
