@@ -66,7 +66,7 @@ struct itp2d_ctx {
 	bool null_pot = true;
 	bool eps_set = false;
 	PlanStore planstore[2][2][3];  // [precision][axis x=0/y=1][kind]
-	std::vector<void*> table_allocs;  // tables in the working precision (freed on a precision switch)
+	std::vector<void*> table_allocs;  // tables (room for doubles; refilled in the working precision)
 	std::vector<MemberTables> members;
 	void* eV = nullptr;     // potential in working precision (energies)
 	void* eT2 = nullptr;    // B = 0: 0.5 k^2 norm
@@ -202,11 +202,12 @@ int build_plans(itp2d_ctx* c, int axis, int kind) {
 
 const LinePlan& plan(const itp2d_ctx* c, int axis, int kind) { return c->planstore[c->precision][axis][kind].lp; }
 
-// Uploads a double host table in the working precision into dst (allocating on first use).
+// Uploads a double host table in the working precision into dst (allocating on
+// first use, with room for doubles so that a precision switch reuses it).
 int upload_table(itp2d_ctx* c, void** dst, const std::vector<double>& h) {
 	const size_t n = h.size();
 	if (!*dst) {
-		const cudaError_t e = cudaMalloc(dst, n * c->es / 2);
+		const cudaError_t e = cudaMalloc(dst, n * sizeof(double));
 		if (e != cudaSuccess) {
 			*dst = nullptr;
 			return cuda_status(e);
@@ -631,7 +632,9 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 		if (e != cudaSuccess) { delete c; return cuda_status(e); }
 		c->own_stream = true;
 	}
-	const size_t sbytes = (size_t)c->G * c->k * c->es;
+	// state buffers sized for FP64 whatever the starting precision, so that a
+	// precision switch converts into the spare buffer without allocating
+	const size_t sbytes = (size_t)c->G * c->k * 16;
 	const int k = c->k;
 	c->psi = dalloc(c, sbytes, &e);
 	if (e == cudaSuccess) c->acc = dalloc(c, sbytes, &e);
@@ -731,11 +734,13 @@ int itp2d_upload_states(itp2d_ctx* c, const double* h) {
 	if (c->precision == ITP2D_FP64) {
 		ITP2D_TRY(cudaMemcpyAsync(c->psi, h, n * 16, cudaMemcpyHostToDevice, c->stream));
 	} else {
-		std::vector<float> f(2 * n);
-		for (size_t i = 0; i < 2 * n; i++) f[i] = (float)h[i];
-		ITP2D_TRY(cudaMemcpyAsync(c->psi, f.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
-		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		// FP64 values into the spare state buffer, converted on the device
+		ITP2D_TRY(cudaMemcpyAsync(c->acc, h, n * 16, cudaMemcpyHostToDevice, c->stream));
+		launch_convert(c->acc, 1, c->psi, (long long)n, c->stream);
+		c->launches++;
+		ITP2D_TRY(cudaGetLastError());
 	}
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
 	return ITP2D_OK;
 }
 
@@ -747,10 +752,12 @@ int itp2d_download_states(itp2d_ctx* c, double* h) {
 		ITP2D_TRY(cudaMemcpyAsync(h, c->psi, n * 16, cudaMemcpyDeviceToHost, c->stream));
 		ITP2D_TRY(cudaStreamSynchronize(c->stream));
 	} else {
-		std::vector<float> f(2 * n);
-		ITP2D_TRY(cudaMemcpyAsync(f.data(), c->psi, n * 8, cudaMemcpyDeviceToHost, c->stream));
+		// widened on the device into the spare state buffer
+		launch_convert(c->psi, 0, c->acc, (long long)n, c->stream);
+		c->launches++;
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaMemcpyAsync(h, c->acc, n * 16, cudaMemcpyDeviceToHost, c->stream));
 		ITP2D_TRY(cudaStreamSynchronize(c->stream));
-		for (size_t i = 0; i < 2 * n; i++) h[i] = f[i];
 	}
 	return ITP2D_OK;
 }
@@ -928,40 +935,15 @@ int itp2d_set_precision(itp2d_ctx* c, int precision) {
 	if (precision == c->precision) return ITP2D_OK;
 	const size_t n = (size_t)c->G * c->k;
 	const size_t es_new = precision == ITP2D_FP64 ? 16 : 8;
-	void* np = nullptr;
-	ITP2D_TRY(cudaMalloc(&np, n * es_new));
-	launch_convert(c->psi, c->precision == ITP2D_FP64 ? 1 : 0, np, (long long)n, c->stream);
+	// the state buffers hold FP64 states: convert into the spare one and swap
+	launch_convert(c->psi, c->precision == ITP2D_FP64 ? 1 : 0, c->acc, (long long)n, c->stream);
 	c->launches++;
-	cudaError_t e = cudaStreamSynchronize(c->stream);
-	if (e != cudaSuccess) {
-		cudaFree(np);
-		return cuda_status(e);
-	}
-	// replace the state buffers
-	auto drop = [&](void* p) {
-		if (!p) return;
-		for (auto& a : c->allocs)
-			if (a == p) a = nullptr;
-		cudaFree(p);
-	};
-	drop(c->psi);
-	drop(c->acc);
-	drop(c->work);
-	c->psi = np;
-	c->allocs.push_back(np);
-	c->acc = c->work = nullptr;
-	e = cudaMalloc(&c->acc, n * es_new);
-	if (e == cudaSuccess) c->allocs.push_back(c->acc);
-	if (e == cudaSuccess && c->halforder >= 3) {
-		e = cudaMalloc(&c->work, n * es_new);
-		if (e == cudaSuccess) c->allocs.push_back(c->work);
-	}
-	if (e != cudaSuccess) return cuda_status(e);
-	// tables in the new precision
-	for (void* p : c->table_allocs) cudaFree(p);
-	c->table_allocs.clear();
-	for (auto& m : c->members) m = MemberTables();
-	c->eV = c->eT2 = c->eTx = c->eTy = nullptr;
+	ITP2D_TRY(cudaGetLastError());
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	void* t = c->psi;
+	c->psi = c->acc;
+	c->acc = t;
+	// tables in the new precision, uploaded into the existing allocations
 	c->precision = precision;
 	c->es = es_new;
 	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;

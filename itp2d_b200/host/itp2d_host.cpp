@@ -520,7 +520,11 @@ void ITPSystem::reset(const double* init) {
 		precision = p.precision;
 	}
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
-	if (init) initial_states.assign(init, init + 2 * dl.N * (size_t)p.num_states);
+	if (init) {
+		initial_states.clear();  // a later recovery re-randomises like the reference
+		check(itp2d_upload_states(ctx, init), "itp2d_upload_states");
+		return;
+	}
 	init_states();
 }
 
