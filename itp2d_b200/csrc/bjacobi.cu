@@ -95,11 +95,23 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 	return y;
 }
 
+// Exponent of a positive normal double, and 2^e for -1022 <= e <= 1023, by
+// bit manipulation (exact).
+__device__ __forceinline__ int exp2i(double x) { return (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023; }
+__device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
 // Rotation of the local pair (p, q) of the subproblem in planes (mr, mi).
-// With d = (b - a) / 2 and r = sqrt(d^2 + |c|^2) the tangent of the smaller
-// angle is t = |c| / (|d| + r); d and |c| are first scaled by the power of two
-// of max(|d|, |c|) so the Newton-refined estimates stay in float range.
-__device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
+// With d = (b - a) / 2, r = sqrt(d^2 + |c|^2), u = |d| + r and w = 2 r u, the
+// rotation of the smaller angle has tan = |c| / u, cos = u / sqrt(w) and
+// |sin| = |c| / sqrt(w) (cos^2 + sin^2 = (u^2 + |c|^2) / w = 1), and
+// tau = sin / (1 + cos) = |c| / (sqrt(w) + u): three dependent Newton-refined
+// reciprocal (square root) steps. d and c are scaled by the power of two of
+// max(|d|, |c|), and c alone by its own for e = c / |c|, so that every refined
+// estimate starts inside float range; exponents beyond +-1000 take the same
+// formulas through scalbn.
+// Counted rotations and the largest counted tangent accumulate in the caller's
+// registers (cnt, tmax) and are reduced once per inner sweep.
+__device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol, int& cnt, double& tmax) {
 	const double* mr = sh.pl[0];
 	const double* mi = sh.pl[1];
 	const double a = mr[p * LD + p], b = mr[q * LD + q];
@@ -110,32 +122,47 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol) {
 	sh.rq[j] = q;
 	sh.rrot[j] = 0;
 	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rtau[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
-	if (c2 > 0.0 && c2 > tol * tol * scale2) {
-		const double cabs = sqrt(c2);
-		const double d = 0.5 * (b - a);
-		// exact power-of-two scaling by the exponent of max(|d|, |c|)
-		const int ex = ilogb(fmax(fabs(d), cabs));
-		const double dn = scalbn(fabs(d), -ex), cn = scalbn(cabs, -ex);  // both in [0, 2), one >= 1
-		const double rn2 = dn * dn + cn * cn;                               // in [1, 8)
-		const double rn = rn2 * rsqrt_nr(rn2);
-		const double t = cn * rcp_nr(dn + rn);                              // dn + rn in [1, 2 + 2 sqrt 2)
-		if (t != 0.0) {
-			const double st = d < 0 ? -t : t;
-			const double c = rsqrt_nr(fma(t, t, 1.0));    // t in (0, 1]
-			const double ic = 1.0 / cabs;
-			sh.rc[j] = c;
-			sh.rs[j] = st * c;
-			sh.rtau[j] = st * c / (1.0 + c);
-			sh.rer[j] = cr * ic;
-			sh.rei[j] = ci * ic;
-			sh.rap[j] = a - st * cabs;
-			sh.raq[j] = b + st * cabs;
-			sh.rrot[j] = 1;
-			if (c2 > kNoiseRel * kNoiseRel * scale2) {
-				atomicAdd(&sh.cnt, 1);
-				atomicMax(&sh.tmax, (unsigned long long)__double_as_longlong(t));
-			}
-		}
+	if (!(c2 > 0.0 && c2 > tol * tol * scale2)) return;
+	const double d = 0.5 * (b - a);
+	const double ad = fabs(d);
+	const double mc = fmax(fabs(cr), fabs(ci));
+	const double m = fmax(ad, mc);
+	int ex = exp2i(m), exc = exp2i(mc);
+	const bool fast = ex > -1000 && ex < 1000 && exc > -1000 && exc < 1000;
+	if (!fast) {
+		ex = ilogb(m);
+		exc = ilogb(mc);
+	}
+	const double sc = fast ? pow2i(-ex) : scalbn(1.0, -ex);
+	const double scc = fast ? pow2i(-exc) : scalbn(1.0, -exc);
+	// ratios in units of 2^ex: max(dn, |crn|, |cin|) in [1, 2)
+	const double dn = ad * sc, crn = cr * sc, cin = ci * sc;
+	const double cn2 = crn * crn + cin * cin;
+	const double rn2 = dn * dn + cn2;         // [1, 12)
+	const double rn = rn2 * rsqrt_nr(rn2);
+	const double un = dn + rn;                // [1, 5.5)
+	const double wn = 2.0 * rn * un;          // [2, 38)
+	const double qn = rsqrt_nr(wn);
+	const double cn = sqrt(cn2);
+	const double t = cn * rcp_nr(un);
+	if (t == 0.0) return;
+	// e = c / |c| from c scaled by its own exponent: crs^2 + cis^2 in [1, 8)
+	const double crs = cr * scc, cis = ci * scc;
+	const double ec = rsqrt_nr(crs * crs + cis * cis);
+	const double sg = d < 0 ? -1.0 : 1.0;
+	const double sw = wn * qn;                 // sqrt(w)
+	const double cabs = fast ? cn * pow2i(ex) : scalbn(cn, ex);
+	sh.rc[j] = un * qn;
+	sh.rs[j] = sg * cn * qn;
+	sh.rtau[j] = sg * cn * rcp_nr(sw + un);    // sw + un in [2.4, 12)
+	sh.rer[j] = crs * ec;
+	sh.rei[j] = cis * ec;
+	sh.rap[j] = a - sg * t * cabs;
+	sh.raq[j] = b + sg * t * cabs;
+	sh.rrot[j] = 1;
+	if (c2 > kNoiseRel * kNoiseRel * scale2) {
+		cnt++;
+		tmax = fmax(tmax, t);
 	}
 }
 
@@ -176,11 +203,13 @@ __device__ void inner_sweep(Shared& sh, double tol, bool full) {
 	double* qi = sh.pl[3];
 	const int tid = threadIdx.x;
 	const int rounds = full ? MS - 1 : BS;
+	int cnt = 0;
+	double tmax = 0.0;
 	for (int r = 0; r < rounds; r++) {
 		if (tid < NR) {
 			const int p = full ? rr_player(tid, r, MS) : tid;
 			const int q = full ? rr_player(MS - 1 - tid, r, MS) : BS + (tid + r) % BS;
-			inner_rotation(sh, tid, p, q, tol);
+			inner_rotation(sh, tid, p, q, tol, cnt, tmax);
 		}
 		__syncthreads();
 		// NR x NR blocks of M
@@ -219,6 +248,18 @@ __device__ void inner_sweep(Shared& sh, double tol, bool full) {
 			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 		}
 		__syncthreads();
+	}
+	// warp 0 holds the NR rotation threads: fold their counts into the CTA's
+	if (tid < 32) {
+		for (int o = 16; o > 0; o >>= 1) {
+			cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+			tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+		}
+		if (tid == 0) {
+			sh.cnt += cnt;
+			const unsigned long long tb = (unsigned long long)__double_as_longlong(tmax);
+			if (tb > sh.tmax) sh.tmax = tb;
+		}
 	}
 }
 
