@@ -116,7 +116,7 @@ def params(form: str):
                              timestep_test=w["test"], final_test=w["test"], max_steps=5000,
                              potential=w["potential"],
                              precision=capi.FP32 if form == "mixed" else capi.FP64,
-                             fp32_switch=1e-6 if form == "mixed" else 0.0)
+                             fp32_switch=1e-7 if form == "mixed" else 0.0)
 
 
 def alg_bytes_split(w, b):

@@ -67,6 +67,7 @@ def lib():
         L.itp2d_synchronize.argtypes = [vp]
         L.itp2d_set_contraction.argtypes = [vp, i]
         L.itp2d_set_precision.argtypes = [vp, i]
+        L.itp2d_set_precision.argtypes = [vp, i]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
@@ -189,6 +190,10 @@ class Context:
         st = lib().itp2d_orthonormalize(self.h, algo, C.byref(bi), C.byref(bv))
         if st != OK:
             raise ITP2DError(st, "itp2d_orthonormalize", bi.value, bv.value)
+
+    def set_precision(self, precision):
+        _check(lib().itp2d_set_precision(self.h, precision), "itp2d_set_precision")
+        self.precision = precision
 
     def set_precision(self, precision):
         _check(lib().itp2d_set_precision(self.h, precision), "itp2d_set_precision")

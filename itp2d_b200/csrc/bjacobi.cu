@@ -339,15 +339,36 @@ __device__ void phase1_item(Shared& sh, int j, long long t, int rounds, int nb, 
 		const int b = posQ < np ? posQ : nb - 1 - posQ, hQ = posQ < np ? 0 : 1;
 		const int Pa = rr_player(a, ro, nb), Qa = rr_player(nb - 1 - a, ro, nb);
 		const int Pb = rr_player(b, ro, nb), Qb = rr_player(nb - 1 - b, ro, nb);
-		// T = A_{t-2}(a, b) Q_b, then C = Q_a^H T
-		for (int e = tid; e < MS * MS; e += kThreads) {
-			const int i = e / MS, l = e % MS;
-			const double2 v = __ldcg(prev2 + (long long)gidx(i, Pa, Qa) * kp + gidx(l, Pb, Qb));
-			mr[i * LD + l] = v.x;
-			mi[i * LD + l] = v.y;
+		// all global loads of the formation at once: A_{t-2}(a, b), Q_a, Q_b
+		// and the diagonal blocks (P, P), (Q, Q) of A_{t-1} (kept in registers);
+		// then T = A_{t-2}(a, b) Q_b and C = Q_a^H T
+		static_assert(MS * MS % kThreads == 0 && 2 * BS * BS % kThreads == 0, "formation tiling");
+		constexpr int NL = MS * MS / kThreads, ND = 2 * BS * BS / kThreads;
+		double2 la[NL], lqa[NL], lqb[NL], ld[ND];
+#pragma unroll
+		for (int it = 0; it < NL; it++) {
+			const int e = it * kThreads + tid, i = e / MS, l = e % MS;
+			la[it] = __ldcg(prev2 + (long long)gidx(i, Pa, Qa) * kp + gidx(l, Pb, Qb));
+			lqa[it] = __ldcg(Qprev + (size_t)a * MS * MS + e);
+			lqb[it] = __ldcg(Qprev + (size_t)b * MS * MS + e);
 		}
-		load_q(sh.pl[2], sh.pl[3], Qprev + (size_t)a * MS * MS);
-		load_q(sh.pl[4], sh.pl[5], Qprev + (size_t)b * MS * MS);
+#pragma unroll
+		for (int it = 0; it < ND; it++) {
+			const int e = it * kThreads + tid;
+			const int half = e / (BS * BS), i = (e / BS) % BS, l = e % BS;
+			const int g0 = (half ? Q : P) * BS;
+			ld[it] = __ldcg(prev + (long long)(g0 + i) * kp + g0 + l);
+		}
+#pragma unroll
+		for (int it = 0; it < NL; it++) {
+			const int e = it * kThreads + tid, i = e / MS, l = e % MS;
+			mr[i * LD + l] = la[it].x;
+			mi[i * LD + l] = la[it].y;
+			sh.pl[2][i * LD + l] = lqa[it].x;
+			sh.pl[3][i * LD + l] = lqa[it].y;
+			sh.pl[4][i * LD + l] = lqb[it].x;
+			sh.pl[5][i * LD + l] = lqb[it].y;
+		}
 		__syncthreads();
 		double cr[2][2], ci[2][2];
 		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);
@@ -380,12 +401,12 @@ __device__ void phase1_item(Shared& sh, int j, long long t, int rounds, int nb, 
 				}
 			}
 		// diagonal blocks (P, P) and (Q, Q) of A_{t-1}
-		for (int e = tid; e < 2 * BS * BS; e += kThreads) {
+#pragma unroll
+		for (int it = 0; it < ND; it++) {
+			const int e = it * kThreads + tid;
 			const int half = e / (BS * BS), i = (e / BS) % BS, l = e % BS;
-			const int g0 = (half ? Q : P) * BS;
-			const double2 v = __ldcg(prev + (long long)(g0 + i) * kp + g0 + l);
-			mr[(half * BS + i) * LD + half * BS + l] = v.x;
-			mi[(half * BS + i) * LD + half * BS + l] = v.y;
+			mr[(half * BS + i) * LD + half * BS + l] = ld[it].x;
+			mi[(half * BS + i) * LD + half * BS + l] = ld[it].y;
 		}
 	}
 	for (int e = tid; e < MS * MS; e += kThreads) {

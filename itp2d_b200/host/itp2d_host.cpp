@@ -443,12 +443,27 @@ void ITPSystem::change_time_step() {
 // FP32 form: once every wanted state's energy changes by less than the switch
 // threshold per step (the FP32 sweep floor), continue in FP64, which refines
 // the eigenpairs to the FP64 fixed point.
+// The FP32 form switches to FP64 once every wanted energy changes by less than
+// fp32_switch per step, or once the largest change has not decreased for
+// kFp32Stall steps (the FP32 noise floor lies above fp32_switch).
 void ITPSystem::maybe_switch_precision() {
 	if (precision != ITP2D_FP32 || !(p.fp32_switch > 0) || energies.size() < 2) return;
+	constexpr int kFp32Stall = 3;
 	const auto& a = energies[energies.size() - 1];
 	const auto& b = energies[energies.size() - 2];
-	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
-		if (!(std::fabs(a[n] - b[n]) < p.fp32_switch)) return;
+	double worst = 0.0;
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) {
+		const double d = std::fabs(a[n] - b[n]);
+		worst = (d >= 0.0) ? std::max(worst, d) : INFINITY;  // NaN never counts as converged
+	}
+	if (!(worst < p.fp32_switch)) {
+		if (worst < fp32_best) {
+			fp32_best = worst;
+			fp32_stall = 0;
+			return;
+		}
+		if (++fp32_stall < kFp32Stall) return;
+	}
 	check(itp2d_set_precision(ctx, ITP2D_FP64), "itp2d_set_precision");
 	precision = ITP2D_FP64;
 	step_counter = 0;
@@ -499,6 +514,8 @@ void ITPSystem::reset(const double* init) {
 	all_timestep_converged = all_finally_converged = false;
 	exhausting = p.exhaust_eps != 0;
 	total_step_counter = step_counter = 0;
+	fp32_best = INFINITY;
+	fp32_stall = 0;
 	t_total = t_prop = t_ortho = t_conv = 0;
 	energies.clear();
 	deviations.clear();

@@ -5,6 +5,7 @@
 // exactly as in itpsystem.cpp:202-511 and convergence.cpp:28-199.
 #pragma once
 
+#include <cmath>
 #include <list>
 #include <memory>
 #include <stdexcept>
@@ -208,6 +209,8 @@ class ITPSystem {
 	bool all_timestep_converged = false, all_finally_converged = false;
 	bool exhausting;
 	int total_step_counter = 0, step_counter = 0;
+	double fp32_best = INFINITY;  // smallest per-step energy change seen in the FP32 form
+	int fp32_stall = 0;           // FP32 steps since that change last decreased
 	double eps = 0;
 	std::list<double> eps_values;
 	std::vector<Esn> sorted;
