@@ -37,7 +37,8 @@ struct MemberTables {
 	void* vp = nullptr;    // c_t exp(-eps_t V / 2)
 	void* vsq = nullptr;   // exp(-eps_t V)
 	void* kmul = nullptr;  // B = 0: 2-D kinetic multiplier
-	void* kx = nullptr;    // B != 0: X(k_x, y)
+	void* kx = nullptr;    // B != 0: X(k_x, y) (Dirichlet: the cosh part)
+	void* kx2 = nullptr;   // Dirichlet, B != 0: the sinh part of X
 	void* ky = nullptr;    // B != 0: Y(k_y)
 };
 
@@ -72,6 +73,7 @@ struct itp2d_ctx {
 	void* eT2 = nullptr;    // B = 0: 0.5 k^2 norm
 	void* eTx = nullptr;    // B != 0: 0.5 (k_x - B y)^2 / sx
 	void* eTy = nullptr;    // B != 0: 0.5 k_y^2 / sy
+	void* eTx2 = nullptr;   // Dirichlet, B != 0: B y k_x normalisation (first-derivative part)
 	// orthonormalisation
 	double2* S = nullptr;
 	double2* part = nullptr;
@@ -91,6 +93,7 @@ struct itp2d_ctx {
 	int* hflag = nullptr;  // pinned copy
 	// energies
 	double* sums = nullptr;
+	double* sums2 = nullptr;  // Dirichlet, B != 0: tile sums of <psi|H H psi>
 	double* dE = nullptr;
 	double* dsig = nullptr;
 	double* dres = nullptr;
@@ -197,7 +200,11 @@ int build_plan(itp2d_ctx* c, int axis, int kind) {
 }
 
 int build_plans(itp2d_ctx* c, int axis, int kind) {
-	return c->precision == ITP2D_FP64 ? build_plan<double>(c, axis, kind) : build_plan<float>(c, axis, kind);
+	int st = c->precision == ITP2D_FP64 ? build_plan<double>(c, axis, kind) : build_plan<float>(c, axis, kind);
+	// Dirichlet with a magnetic field also needs the x-axis cosine lines
+	if (!st && axis == 0 && kind == 1 && c->B != 0)
+		st = c->precision == ITP2D_FP64 ? build_plan<double>(c, 0, 2) : build_plan<float>(c, 0, 2);
+	return st;
 }
 
 const LinePlan& plan(const itp2d_ctx* c, int axis, int kind) { return c->planstore[c->precision][axis][kind].lp; }
@@ -283,7 +290,10 @@ int kinetic_exp_tables(itp2d_ctx* c, MemberTables& mt, double e, double coeff, d
 				mul[(size_t)y * sx + x] = p * std::exp(A * (kt.kx[x] * kt.kx[x] + kt.ky[y] * kt.ky[y]));
 		return upload_table(c, &mt.kmul, mul);
 	}
-	const double normfacx = std::sqrt(kt.normx);  // periodic: applied twice
+	// periodic: X is applied twice around one FFTx/iFFTx pair; Dirichlet: once
+	// per DSTx / (iDSTx, iDCTx) round trip (expkinetic.cpp:83-85)
+	const bool per = c->boundary == ITP2D_PERIODIC;
+	const double normfacx = per ? std::sqrt(kt.normx) : kt.normx;
 	const double z = c->B * e;
 	const double Cy = (std::fabs(z) < 1e-6) ? 1 + std::pow(z, 2) / 6 + std::pow(z, 4) / 120 : std::sinh(z) / z;
 	const double Cx = (std::fabs(z) < 1e-6) ? 0.5 - std::pow(z, 2) / 24 + std::pow(z, 4) / 240 : std::tanh(z / 2) / z;
@@ -291,17 +301,32 @@ int kinetic_exp_tables(itp2d_ctx* c, MemberTables& mt, double e, double coeff, d
 	const double Ay = coeff * e * 0.5 * Cy;
 	const double px = normfacx;
 	const double py = prefactor * kt.normy;
-	std::vector<double> X((size_t)sx * sy), Y(sy);
+	std::vector<double> X((size_t)sx * sy), Y(sy), X2;
+	if (!per) X2.resize((size_t)sx * sy);
 	for (int y = 0; y < sy; y++) {
 		const double dy = kt.posy[y];
 		Y[y] = py * std::exp(Ay * kt.ky[y] * kt.ky[y]);
 		for (int x = 0; x < sx; x++) {
-			const double q = kt.kx[x] - c->B * dy;
-			X[(size_t)y * sx + x] = px * std::exp(Ax * q * q);
+			if (per) {
+				const double q = kt.kx[x] - c->B * dy;
+				X[(size_t)y * sx + x] = px * std::exp(Ax * q * q);
+			} else {
+				// sine and cosine parts of exp(c P^2) on a sine series
+				// (expkinetic.cpp:108-133)
+				const double By = c->B * dy;
+				const double common = px * std::exp(Ax * (kt.kx[x] * kt.kx[x] + By * By));
+				const double arg = 2 * Ax * kt.kx[x] * By;
+				X[(size_t)y * sx + x] = common * std::cosh(arg);
+				X2[(size_t)y * sx + x] = common * std::sinh(arg);
+			}
 		}
 	}
 	int st = upload_table(c, &mt.kx, X);
 	if (st) return st;
+	if (!per) {
+		st = upload_table(c, &mt.kx2, X2);
+		if (st) return st;
+	}
 	return upload_table(c, &mt.ky, Y);
 }
 
@@ -355,16 +380,29 @@ int rebuild_energy_tables(itp2d_ctx* c) {
 		st = upload_table(c, &c->eT2, t2);
 		if (st) return st;
 	} else {
-		std::vector<double> tx((size_t)sx * sy), ty(sy);
+		const bool per = c->boundary == ITP2D_PERIODIC;
+		std::vector<double> tx((size_t)sx * sy), ty(sy), tx2;
+		if (!per) tx2.resize((size_t)sx * sy);
 		for (int y = 0; y < sy; y++) {
 			ty[y] = 0.5 * kt.ky[y] * kt.ky[y] * kt.normy;
+			const double By = c->B * kt.posy[y];
 			for (int x = 0; x < sx; x++) {
-				const double q = kt.kx[x] - c->B * kt.posy[y];
-				tx[(size_t)y * sx + x] = 0.5 * q * q * kt.normx;
+				if (per) {
+					const double q = kt.kx[x] - By;
+					tx[(size_t)y * sx + x] = 0.5 * q * q * kt.normx;
+				} else {
+					// kinetic.cpp:66-80: the first derivative gives a cosine series
+					tx[(size_t)y * sx + x] = 0.5 * (kt.kx[x] * kt.kx[x] + By * By) * kt.normx;
+					tx2[(size_t)y * sx + x] = By * kt.kx[x] * kt.normx;
+				}
 			}
 		}
 		st = upload_table(c, &c->eTx, tx);
 		if (st) return st;
+		if (!per) {
+			st = upload_table(c, &c->eTx2, tx2);
+			if (st) return st;
+		}
 		st = upload_table(c, &c->eTy, ty);
 		if (st) return st;
 	}
@@ -441,20 +479,45 @@ void col_pass(itp2d_ctx* c, const LinePlan& lp, void* data, const void* mul2d, c
 // pair with the kinetic multiplier, each interior row pass the inverse x
 // transform, V and the forward x transform, and the last row pass the inverse
 // x transform and c_t V/2.
+bool dirichlet_magnetic(const itp2d_ctx* c) { return c->boundary == ITP2D_DIRICHLET && c->B != 0; }
+
+// Row pass of a kinetic factor: do_inv ends the previous factor (X table and
+// inverse x-transform), mid multiplies, do_fwd starts the next one (forward
+// x-transform and X table). With Dirichlet boundaries and a magnetic field the
+// x-part acts through the sine/cosine split of the Dirichlet magnetic row pass.
+template <class R>
+void kinetic_row(itp2d_ctx* c, const MemberTables& mt, const void* in, void* out, const void* acc,
+		const void* mid, int do_inv, int do_fwd) {
+	if (dirichlet_magnetic(c)) {
+		DmRowArgs a;
+		a.in = in; a.out = out; a.acc = acc;
+		a.x1 = mt.kx; a.x2 = mt.kx2; a.mul_mid = mid; a.vadd = nullptr;
+		a.lead_fwd = 0; a.do_inv = do_inv; a.do_fwd = do_fwd;
+		a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+		a.rows_per_tile = dm_row_tile_rows(c->sx, sizeof(c2<R>), c->sy);
+		a.lp_dst = plan(c, 0, 1);
+		a.lp_dct = plan(c, 0, 2);
+		launch_dm_row_pass<R>(a, c->k, c->stream);
+		c->launches++;
+		return;
+	}
+	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
+	row_pass<R>(c, plan(c, 0, kind), in, out, acc, do_inv ? mt.kx : nullptr, mid, do_fwd ? mt.kx : nullptr, do_inv,
+			do_fwd);
+}
+
 template <class R>
 void apply_member(itp2d_ctx* c, const MemberTables& mt, const void* src, void* dst, const void* acc) {
 	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
-	const LinePlan& lx = plan(c, 0, kind);
 	const LinePlan& ly = plan(c, 1, kind);
-	const void* X = mt.kx;  // null for B = 0
 	const void* vfirst = c->null_pot ? nullptr : mt.vh;
 	const void* vlast = c->null_pot ? nullptr : mt.vp;
-	row_pass<R>(c, lx, src, dst, nullptr, nullptr, vfirst, X, 0, 1);
+	kinetic_row<R>(c, mt, src, dst, nullptr, vfirst, 0, 1);
 	for (int r = 1; r <= mt.t; r++) {
 		col_pass<R>(c, ly, dst, c->B == 0 ? mt.kmul : nullptr, c->B == 0 ? nullptr : mt.ky, 0);
-		if (r < mt.t) row_pass<R>(c, lx, dst, dst, nullptr, X, mt.vsq, X, 1, 1);
+		if (r < mt.t) kinetic_row<R>(c, mt, dst, dst, nullptr, mt.vsq, 1, 1);
 	}
-	row_pass<R>(c, lx, dst, dst, acc, X, vlast, nullptr, 1, 0);
+	kinetic_row<R>(c, mt, dst, dst, acc, vlast, 1, 0);
 }
 
 // Multi-product propagation (MultiProductSplit over OperatorSum,
@@ -465,7 +528,6 @@ void apply_member(itp2d_ctx* c, const MemberTables& mt, const void* src, void* d
 template <class R>
 int propagate_fused(itp2d_ctx* c) {
 	const int kind = c->boundary == ITP2D_PERIODIC ? 0 : 1;
-	const LinePlan& lx = plan(c, 0, kind);
 	const LinePlan& ly = plan(c, 1, kind);
 	if (c->m == 1) {
 		apply_member<R>(c, c->members[0], c->psi, c->psi, nullptr);
@@ -475,14 +537,13 @@ int propagate_fused(itp2d_ctx* c) {
 	for (int t = 2; t <= c->m; t++) {
 		const MemberTables& mt = c->members[t - 1];
 		void* buf = (t == c->m) ? c->psi : c->work;
-		const void* X = mt.kx;
-		row_pass<R>(c, lx, c->psi, buf, nullptr, nullptr, mt.vh, X, 0, 1);
+		kinetic_row<R>(c, mt, c->psi, buf, nullptr, mt.vh, 0, 1);
 		for (int r = 1; r <= mt.t; r++) {
 			col_pass<R>(c, ly, buf, c->B == 0 ? mt.kmul : nullptr, c->B == 0 ? nullptr : mt.ky, 0);
-			if (r < mt.t) row_pass<R>(c, lx, buf, buf, nullptr, X, mt.vsq, X, 1, 1);
+			if (r < mt.t) kinetic_row<R>(c, mt, buf, buf, nullptr, mt.vsq, 1, 1);
 		}
 		// acc = member_t + acc
-		row_pass<R>(c, lx, buf, c->acc, c->acc, X, mt.vp, nullptr, 1, 0);
+		kinetic_row<R>(c, mt, buf, c->acc, c->acc, mt.vp, 1, 0);
 	}
 	void* t = c->psi;
 	c->psi = c->acc;
@@ -521,33 +582,55 @@ int energies_impl(itp2d_ctx* c, void* h_out, bool want_sums) {
 		c->launches++;
 		if (want_sums) {
 			const int nt = (c->sy + a.rows_per_tile - 1) / a.rows_per_tile;
-			launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->precision == ITP2D_FP32, c->dE,
-					c->dsig, c->dres, c->dEi, c->stream);
+			launch_energy_finish(c->sums, nullptr, c->k, nt, c->dx * c->dx, c->dEshift, c->precision == ITP2D_FP32,
+					c->dE, c->dsig, c->dres, c->dEi, c->stream);
 			c->launches++;
 		}
 		return ITP2D_OK;
 	}
-	// periodic, B != 0: acc = T_x psi + V psi; h = T_y psi + acc
-	EnergyRowArgs a;
-	a.src_t = c->psi; a.psi = c->psi; a.tmul = c->eTx; a.V = V;
-	a.h_out = c->acc; a.sums = nullptr; a.Eshift = nullptr;
-	a.do_fwd = 1; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
-	a.rows_per_tile = energy_rows(lx, sizeof(c2<R>), c->sy);
-	a.lp = lx;
-	launch_energy_row<R>(a, c->k, nullptr, c->stream);
-	c->launches++;
-	EnergyColArgs b;
-	b.psi = c->psi; b.add_in = c->acc; b.ty = c->eTy;
-	b.h_out = h_out; b.sums = want_sums ? c->sums : nullptr; b.Eshift = c->dEshift;
-	b.sx = c->sx; b.sy = c->sy; b.G = c->G;
-	b.cols_per_tile = energy_cols(ly, sizeof(c2<R>), c->sx);
-	b.lp = ly;
-	launch_energy_col<R>(b, c->k, nullptr, c->stream);
-	c->launches++;
+	// magnetic field: acc = T_x src + V src (row pass), h = T_y src + acc
+	// (column pass, sums against psi)
+	auto hpass = [&](const void* src, void* hout, double* sums) -> int {
+		if (dirichlet_magnetic(c)) {
+			// the x-part through the sine/cosine split (kinetic.cpp:126-138)
+			DmRowArgs d;
+			d.in = src; d.out = c->acc; d.acc = nullptr;
+			d.x1 = c->eTx; d.x2 = c->eTx2; d.mul_mid = nullptr; d.vadd = V;
+			d.lead_fwd = 1; d.do_inv = 1; d.do_fwd = 0;
+			d.sx = c->sx; d.sy = c->sy; d.G = c->G;
+			d.rows_per_tile = dm_row_tile_rows(c->sx, sizeof(c2<R>), c->sy);
+			d.lp_dst = plan(c, 0, 1);
+			d.lp_dct = plan(c, 0, 2);
+			launch_dm_row_pass<R>(d, c->k, c->stream);
+		} else {
+			EnergyRowArgs a;
+			a.src_t = src; a.psi = src; a.tmul = c->eTx; a.V = V;
+			a.h_out = c->acc; a.sums = nullptr; a.Eshift = nullptr;
+			a.do_fwd = 1; a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+			a.rows_per_tile = energy_rows(lx, sizeof(c2<R>), c->sy);
+			a.lp = lx;
+			launch_energy_row<R>(a, c->k, nullptr, c->stream);
+		}
+		c->launches++;
+		EnergyColArgs b;
+		b.src = src; b.psi = c->psi; b.add_in = c->acc; b.ty = c->eTy;
+		b.h_out = hout; b.sums = sums; b.Eshift = c->dEshift;
+		b.sx = c->sx; b.sy = c->sy; b.G = c->G;
+		b.cols_per_tile = energy_cols(ly, sizeof(c2<R>), c->sx);
+		b.lp = ly;
+		launch_energy_col<R>(b, c->k, nullptr, c->stream);
+		c->launches++;
+		return (c->sx + b.cols_per_tile - 1) / b.cols_per_tile;
+	};
+	// The Dirichlet magnetic H is not Hermitian in its discrete form, so
+	// <H^2> = <psi|H (H psi)> needs the second application the reference makes
+	// (operators.cpp:40-50); elsewhere |H psi|^2 equals it.
+	const bool second = want_sums && dirichlet_magnetic(c);
+	const int nt = hpass(c->psi, second ? c->work : h_out, want_sums ? c->sums : nullptr);
+	if (second) hpass(c->work, nullptr, c->sums2);
 	if (want_sums) {
-		const int nt = (c->sx + b.cols_per_tile - 1) / b.cols_per_tile;
-		launch_energy_finish(c->sums, c->k, nt, c->dx * c->dx, c->dEshift, c->precision == ITP2D_FP32, c->dE,
-				c->dsig, c->dres, c->dEi, c->stream);
+		launch_energy_finish(c->sums, second ? c->sums2 : nullptr, c->k, nt, c->dx * c->dx, c->dEshift,
+				c->precision == ITP2D_FP32, c->dE, c->dsig, c->dres, c->dEi, c->stream);
 		c->launches++;
 	}
 	return ITP2D_OK;
@@ -612,7 +695,6 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	if (boundary != ITP2D_PERIODIC && boundary != ITP2D_DIRICHLET) return ITP2D_E_INVALID;
 	if (precision != ITP2D_FP64 && precision != ITP2D_FP32) return ITP2D_E_INVALID;
 	if (!smooth7(sx) || !smooth7(sy) || sx > 4096 || sy > 4096) return ITP2D_E_UNSUPPORTED;
-	if (boundary == ITP2D_DIRICHLET && B != 0) return ITP2D_E_UNSUPPORTED;
 	*out = nullptr;
 	itp2d_ctx* c = new (std::nothrow) itp2d_ctx();
 	if (!c) return ITP2D_E_OOM;
@@ -638,7 +720,10 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	const int k = c->k;
 	c->psi = dalloc(c, sbytes, &e);
 	if (e == cudaSuccess) c->acc = dalloc(c, sbytes, &e);
-	if (e == cudaSuccess && halforder >= 3) c->work = dalloc(c, sbytes, &e);
+	// work: third member buffer (halforder >= 3) or H psi for the second H
+	// application of the Dirichlet magnetic energies
+	if (e == cudaSuccess && (halforder >= 3 || (boundary == ITP2D_DIRICHLET && B != 0)))
+		c->work = dalloc(c, sbytes, &e);
 	// overlap / eigensolver buffers
 	const int nt = overlap_tiles(k);
 	c->npairs = nt * (nt + 1) / 2;
@@ -669,6 +754,8 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	// energies
 	const int ntiles = std::max(sx, sy);  // upper bound of row or column tiles
 	if (e == cudaSuccess) c->sums = (double*)dalloc(c, (size_t)k * ntiles * 5 * sizeof(double), &e);
+	if (e == cudaSuccess && boundary == ITP2D_DIRICHLET && B != 0)
+		c->sums2 = (double*)dalloc(c, (size_t)k * ntiles * 5 * sizeof(double), &e);
 	if (e == cudaSuccess) c->dE = (double*)dalloc(c, (size_t)5 * k * sizeof(double), &e);
 	if (e == cudaSuccess) {
 		c->dsig = c->dE + k;

@@ -372,11 +372,12 @@ __global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs 
 	const int sx = a.sx;
 	const long long base = state * a.G + col0;
 	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
+	const T* src = a.src ? reinterpret_cast<const T*>(a.src) + base : psi;
 #pragma unroll
 	for (int it = 0; it < N * W / kThreads; it++) {
 		const int i = it * kThreads + threadIdx.x;
 		const int y = i / W, c = i - y * W;
-		tile[y * LD + c] = c < ncols ? psi[(long long)y * sx + c] : mk<R>(0, 0);
+		tile[y * LD + c] = c < ncols ? src[(long long)y * sx + c] : mk<R>(0, 0);
 	}
 	__syncthreads();
 	T v[A];

@@ -209,6 +209,95 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(ColPassArgs a, int k
 	cp_wait<0>();
 }
 
+// Dirichlet magnetic row pass (DmRowArgs). One CTA per (state, tile of rows);
+// four line buffers of 2 sx elements per row: P0/P1 carry the main (sine)
+// branch and its FFT scratch, Q0/Q1 the shifted (cosine) branch.
+template <class R>
+__global__ void __launch_bounds__(kThreads) dm_row_kernel(DmRowArgs a) {
+	using T = c2<R>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int N = a.sx, L = 2 * N, rows = a.rows_per_tile, tsz = rows * L;
+	T* P0 = reinterpret_cast<T*>(smem_raw);
+	T* P1 = P0 + tsz;
+	T* Q0 = P1 + tsz;
+	T* Q1 = Q0 + tsz;
+	T* tw = Q1 + tsz;
+	load_twiddles<R>(tw, a.lp_dst);  // the 2 sx-point FFT of both line kinds
+	const long long state = blockIdx.x;
+	const int row0 = blockIdx.y * rows;
+	const int nrows = min(rows, a.sy - row0);
+	const long long base = state * a.G + (long long)row0 * N;
+	const int toff = row0 * N;
+	const int cnt = nrows * N;
+	const T* in = reinterpret_cast<const T*>(a.in) + base;
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / N;
+		P0[r * L + (i - r * N)] = in[i];
+	}
+	__syncthreads();
+	const R* x1 = reinterpret_cast<const R*>(a.x1);
+	const R* x2 = reinterpret_cast<const R*>(a.x2);
+	auto other = [&](T* b) { return b == P0 ? P1 : P0; };
+	auto fwd = [&](T* b) { return line_transform<R, false>(b, other(b), a.lp_dst, tw, nrows, 1, L, false); };
+	auto xop = [&](T* b) -> T* {
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / N, x = i - r * N;
+			T u = mk<R>(0, 0);
+			if (x >= 1) {
+				const T v = b[r * L + x - 1];
+				const R w = x2[toff + i - 1];
+				u = mk<R>(-w * v.y, w * v.x);  // i w v
+			}
+			Q0[r * L + x] = u;
+		}
+		__syncthreads();
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / N, x = i - r * N;
+			b[r * L + x] = cscale(b[r * L + x], x1[toff + i]);
+		}
+		__syncthreads();
+		T* ra = line_transform<R, false>(b, other(b), a.lp_dst, tw, nrows, 1, L, true);
+		T* rb = line_transform<R, false>(Q0, Q1, a.lp_dct, tw, nrows, 1, L, true);
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / N, x = i - r * N;
+			ra[r * L + x] = cadd(ra[r * L + x], rb[r * L + x]);
+		}
+		__syncthreads();
+		return ra;
+	};
+	T* cur = P0;
+	if (a.lead_fwd) cur = fwd(cur);
+	if (a.do_inv) cur = xop(cur);
+	const R* mid = reinterpret_cast<const R*>(a.mul_mid);
+	if (mid) {
+		for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+			const int r = i / N, x = i - r * N;
+			cur[r * L + x] = cscale(cur[r * L + x], mid[toff + i]);
+		}
+		__syncthreads();
+	}
+	if (a.do_fwd) {
+		cur = fwd(cur);
+		cur = xop(cur);
+		cur = fwd(cur);
+	}
+	T* out = reinterpret_cast<T*>(a.out) + base;
+	const T* acc = a.acc ? reinterpret_cast<const T*>(a.acc) + base : nullptr;
+	const R* vadd = reinterpret_cast<const R*>(a.vadd);
+	for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+		const int r = i / N, x = i - r * N;
+		T v = cur[r * L + x];
+		if (vadd) {
+			const T p = in[i];
+			const R w = vadd[toff + i];
+			v.x += w * p.x;
+			v.y += w * p.y;
+		}
+		if (acc) v = cadd(v, acc[i]);
+		out[i] = v;
+	}
+}
+
 // Deterministic block reduction of NV doubles; result valid in thread 0.
 template <int NV>
 __device__ __forceinline__ void block_reduce(double* v, double* red) {
@@ -326,10 +415,11 @@ __global__ void __launch_bounds__(kThreads) energy_col_kernel(EnergyColArgs a) {
 	const int sx = a.sx, sy = a.sy;
 	const long long base = state * a.G + col0;
 	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
+	const T* src = a.src ? reinterpret_cast<const T*>(a.src) + base : psi;
 	for (int i = threadIdx.x; i < sy * C; i += blockDim.x) {
 		const int y = i / C;
 		const int c = i - y * C;
-		buf0[y * C + c] = (c < ncols) ? psi[(long long)y * sx + c] : mk<R>(0, 0);
+		buf0[y * C + c] = (c < ncols) ? src[(long long)y * sx + c] : mk<R>(0, 0);
 	}
 	__syncthreads();
 	T* cur = line_transform<R, true>(buf0, buf1, a.lp, tw, C, C, 1, false);
@@ -365,24 +455,33 @@ __global__ void __launch_bounds__(kThreads) energy_col_kernel(EnergyColArgs a) {
 	}
 }
 
-__global__ void energy_finish_kernel(const double* __restrict__ sums, int k, int ntiles, double dx2,
-		const double* __restrict__ Eshift, int normalize, double* E, double* sigma, double* sigma_res,
-		double* E_imag) {
+__global__ void energy_finish_kernel(const double* __restrict__ sums, const double* __restrict__ sums2, int k,
+		int ntiles, double dx2, const double* __restrict__ Eshift, int normalize, double* E, double* sigma,
+		double* sigma_res, double* E_imag) {
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
 	if (warp >= k) return;
 	double s[5] = {0, 0, 0, 0, 0};
 	for (int t = lane; t < ntiles; t += 32)
 		for (int j = 0; j < 5; j++) s[j] += sums[((size_t)warp * ntiles + t) * 5 + j];
+	double q[2] = {0, 0};
+	if (sums2)
+		for (int t = lane; t < ntiles; t += 32)
+			for (int j = 0; j < 2; j++) q[j] += sums2[((size_t)warp * ntiles + t) * 5 + j];
 	for (int j = 0; j < 5; j++)
 		for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+	for (int j = 0; j < 2; j++)
+		for (int o = 16; o > 0; o >>= 1) q[j] += __shfl_xor_sync(0xffffffffu, q[j], o);
 	if (lane == 0) {
 		// normalize: Rayleigh quotients <psi|H psi> / <psi|psi> (and <H^2> likewise)
 		const double inv = normalize ? 1.0 / (s[4] * dx2) : 1.0;
-		const double er = s[0] * dx2 * inv, ei = s[1] * dx2 * inv, m2 = s[2] * dx2 * inv;
+		const double er = s[0] * dx2 * inv, ei = s[1] * dx2 * inv;
+		// <H^2>: <psi|H H psi> from the second pass, else |H psi|^2 (H Hermitian)
+		const double m2r = (sums2 ? q[0] : s[2]) * dx2 * inv;
+		const double m2i = sums2 ? q[1] * dx2 * inv : 0.0;
 		// sigma = Re sqrt(<H^2> - <H>^2) with complex <H> (operators.cpp:46-49)
-		const double zr = m2 - (er * er - ei * ei);
-		const double zi = -2.0 * er * ei;
+		const double zr = m2r - (er * er - ei * ei);
+		const double zi = m2i - 2.0 * er * ei;
 		const double az = hypot(zr, zi);
 		const double sg = sqrt(fmax(0.0, 0.5 * (az + zr)));
 		const double es = Eshift ? Eshift[warp] : 0.0;
@@ -447,6 +546,22 @@ int persistent_blocks(K kernel, size_t smem, long long tiles) {
 	return (int)std::max(1LL, std::min(b, tiles));
 }
 
+int dm_row_tile_rows(int sx, int elem_bytes, int sy) {
+	const size_t row_bytes = (size_t)4 * 2 * sx * elem_bytes;
+	const size_t room = 200 * 1024 - (size_t)2 * sx * elem_bytes;
+	const int r = (int)std::max<size_t>(1, room / row_bytes);
+	return std::min(std::min(r, 32), sy);
+}
+
+template <class R>
+void launch_dm_row_pass(const DmRowArgs& a, int k, cudaStream_t s) {
+	const size_t es = sizeof(c2<R>);
+	const size_t sm = (size_t)4 * a.rows_per_tile * 2 * a.sx * es + (size_t)a.lp_dst.fft.n * es;
+	set_smem_limit(dm_row_kernel<R>);
+	const dim3 grid(k, (a.sy + a.rows_per_tile - 1) / a.rows_per_tile);
+	dm_row_kernel<R><<<grid, kThreads, sm, s>>>(a);
+}
+
 template <class R>
 void launch_row_pass(const RowPassArgs& a, int k, const void*, cudaStream_t s) {
 	if (launch_row_pass_reg<R>(a, k, s)) return;
@@ -487,14 +602,17 @@ void launch_energy_col(const EnergyColArgs& a, int k, const void*, cudaStream_t 
 	energy_col_kernel<R><<<grid, kThreads, sm, s>>>(a);
 }
 
-void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift, int normalize,
-		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s) {
+void launch_energy_finish(const double* sums, const double* sums2, int k, int ntiles, double dx2,
+		const double* Eshift, int normalize, double* E, double* sigma, double* sigma_res, double* E_imag,
+		cudaStream_t s) {
 	const int threads = 128;
 	const int blocks = (k * 32 + threads - 1) / threads;
-	energy_finish_kernel<<<blocks, threads, 0, s>>>(sums, k, ntiles, dx2, Eshift, normalize, E, sigma, sigma_res,
-			E_imag);
+	energy_finish_kernel<<<blocks, threads, 0, s>>>(sums, sums2, k, ntiles, dx2, Eshift, normalize, E, sigma,
+			sigma_res, E_imag);
 }
 
+template void launch_dm_row_pass<double>(const DmRowArgs&, int, cudaStream_t);
+template void launch_dm_row_pass<float>(const DmRowArgs&, int, cudaStream_t);
 template void launch_row_pass<double>(const RowPassArgs&, int, const void*, cudaStream_t);
 template void launch_row_pass<float>(const RowPassArgs&, int, const void*, cudaStream_t);
 template void launch_col_pass<double>(const ColPassArgs&, int, const void*, cudaStream_t);

@@ -64,9 +64,10 @@ struct EnergyRowArgs {
 	LinePlan lp;
 };
 
-// Energy pass over columns (periodic magnetic field): t = Tinv_y(ty .* Tfwd_y(psi)),
-// h = t + add_in; sums as above.
+// Energy pass over columns (magnetic field): t = Tinv_y(ty .* Tfwd_y(src)),
+// h = t + add_in; sums as above against psi. src null: src = psi.
 struct EnergyColArgs {
+	const void* src = nullptr;
 	const void* psi;
 	const void* add_in;
 	const void* ty;
@@ -78,6 +79,39 @@ struct EnergyColArgs {
 	int cols_per_tile;
 	LinePlan lp;
 };
+
+// Row pass of the Dirichlet kinetic factor with a magnetic field, whose
+// x-part maps a sine series to sines and cosines (expkinetic.cpp:108-133,
+// 173-194; kinetic.cpp:66-80,126-138):
+//   Xop(s) = iDSTx(x1 .* s) + iDCTx(shift(i x2 .* s)),
+//   shift(u)[x] = u[x - 1] for x >= 1, shift(u)[0] = 0 (state.hpp:192-201).
+//   v = in[row]
+//   if lead_fwd: v = DSTx(v)
+//   if do_inv:   v = Xop(v)                 (v arrives as a DSTx series)
+//   v = mul_mid .* v                        (when non-null)
+//   if do_fwd:   v = DSTx(Xop(DSTx(v)))     (start of the next kinetic factor)
+//   out[row] = v (+ vadd .* in[row]) (+ acc[row])
+// Tables are [sy][sx] in the working precision.
+struct DmRowArgs {
+	const void* in;
+	void* out;
+	const void* acc;
+	const void* x1;
+	const void* x2;
+	const void* mul_mid;
+	const void* vadd;
+	int lead_fwd;
+	int do_inv;
+	int do_fwd;
+	int sx, sy;
+	long long G;
+	int rows_per_tile;
+	LinePlan lp_dst;  // x-lines, DST-II / DST-III
+	LinePlan lp_dct;  // x-lines, DCT-II / DCT-III
+};
+
+template <class R> void launch_dm_row_pass(const DmRowArgs& a, int k, cudaStream_t s);
+int dm_row_tile_rows(int sx, int elem_bytes, int sy);
 
 template <class R> void launch_row_pass(const RowPassArgs& a, int k, const void* tw, cudaStream_t s);
 // Register-FFT passes (rfft.cu) for periodic lines of 32..1024 points (powers
@@ -98,7 +132,11 @@ template <class R> void launch_energy_col(const EnergyColArgs& a, int k, const v
 // residual deviation (deterministic order). normalize != 0 divides by
 // <psi|psi> (Rayleigh quotients; used by the FP32 form, whose contractions
 // leave norms exact only to FP32 accuracy).
-void launch_energy_finish(const double* sums, int k, int ntiles, double dx2, const double* Eshift, int normalize,
+// sums2 (may be null): tile sums of a second energy pass whose h is H(H psi);
+// then <H^2> = <psi|H H psi> (complex) as operators.cpp:40-50 computes it,
+// instead of |H psi|^2.
+void launch_energy_finish(const double* sums, const double* sums2, int k, int ntiles, double dx2,
+		const double* Eshift, int normalize,
 		double* E, double* sigma, double* sigma_res, double* E_imag, cudaStream_t s);
 
 // Tile sizes (rows or columns per CTA) for a line length L (complex entries).

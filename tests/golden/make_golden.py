@@ -28,6 +28,7 @@ SEAMS = {
     "periodic_b1_m2": (16, 12, 14.0, O.PERIODIC, 1.0, 2, 0.05, "harmonic(1)"),
     "periodic_b05_m3": (16, 16, 16.0, O.PERIODIC, 0.5, 3, 0.05, "harmonic(1)"),
     "periodic_b0_null": (16, 12, 6.0, O.PERIODIC, 0.0, 2, 0.1, "zero"),
+    "dirichlet_b07_m2": (20, 16, 12.0, O.DIRICHLET, 0.7, 2, 0.1, "harmonic(1)"),
 }
 K = 3
 

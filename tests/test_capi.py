@@ -28,5 +28,5 @@ def test_invalid_arguments_rejected_before_device_use():
     assert L.itp2d_ctx_create(1, 16, 0.1, 4, 0, 0.0, 1, 0, None, ctypes.byref(out)) == capi.E_INVALID
     assert L.itp2d_ctx_create(16, 16, 0.1, 4, 7, 0.0, 1, 0, None, ctypes.byref(out)) == capi.E_INVALID
     assert L.itp2d_ctx_create(22, 16, 0.1, 4, 0, 0.0, 1, 0, None, ctypes.byref(out)) == capi.E_UNSUPPORTED
-    assert L.itp2d_ctx_create(16, 16, 0.1, 4, 1, 1.0, 1, 0, None, ctypes.byref(out)) == capi.E_UNSUPPORTED
+    assert L.itp2d_ctx_create(8192, 16, 0.1, 4, 1, 1.0, 1, 0, None, ctypes.byref(out)) == capi.E_UNSUPPORTED
     assert L.itp2d_propagate(None) == capi.E_INVALID

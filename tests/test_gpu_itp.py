@@ -108,6 +108,44 @@ def test_hamiltonian_ground_state_stable(itp, case):
         assert math.sqrt(np.mean(np.abs(t - gs) ** 2)) < 5e-3
 
 
+def test_particle_in_a_box_magnetic(itp):
+    """test_itp.cpp:412-443: Dirichlet box 64x64, L = pi, B = 1, no potential;
+    the lowest 8 converged energies equal the reference's known-good values
+    (tests/golden/magnetic_box_energies.json) within twice the test tolerance."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "magnetic_box_energies.json")) as f:
+        ref = json.load(f)
+    s = _solve(itp, sx=64, sy=64, length=math.pi, boundary=1, B=1.0, num_states=16, wanted=8,
+               eps=[0.3], potential="zero", timestep_test="abschange(1e-3)", final_test="onestep",
+               max_steps=2000)
+    E = s.energies()[0]
+    assert np.max(np.abs(E[:8] - np.array(ref["energies"]))) < 2e-3
+
+
+def test_dirichlet_magnetic_whole_solve_matches_reference(itp):
+    """Dirichlet boundaries with a magnetic field through the reference
+    ITPSystem (compiled oracle) and the GPU driver, same initial states."""
+    if not R.available():
+        pytest.skip("oracle/_ref not built")
+    g = O.Grid.from_length(32, 32, 10.0)
+    psi = O.gaussian_states(g, 8, 17)
+    kw = dict(num_states=8, wanted=5, eps_values=[0.1], eps_divisor=2.0, timestep_test="abschange(1e-11)",
+              final_test="abschange(1e-11)", max_steps=600)
+    ref = R.RefSystem(32, 32, 10.0, 1, 1.0, 2, potential="harmonic(1)", init_states=psi, threads=4, **kw)
+    while not ref.finished:
+        ref.step()
+    assert not ref.error_flag
+    Er, _ = ref.energies()
+    s = itp.ITPSystem(itp.Parameters(sx=32, sy=32, length=10.0, boundary=1, B=1.0, halforder=2, num_states=8,
+                                     wanted=5, eps=[0.1], eps_divisor=2.0, timestep_test="abschange(1e-11)",
+                                     final_test="abschange(1e-11)", max_steps=600, potential="harmonic(1)"),
+                      init_states=psi)
+    s.run()
+    assert not s.error_flag, s.last_error
+    assert np.max(np.abs(s.energies()[0][:5] - Er[:5])) < 1e-9
+
+
 def test_whole_solve_matches_reference(itp):
     """Same parameters and initial states through the reference ITPSystem
     (compiled oracle) and the GPU driver: sorted converged energies agree."""

@@ -153,6 +153,8 @@ CONFIGS = [
     (64, 64, 16.0, O.PERIODIC, 0.5, 3, 0.05),
     (96, 40, 12.0, O.PERIODIC, 0.3, 2, 0.05),
     (42, 42, 12.0, O.DIRICHLET, 0.0, 3, 0.1),
+    (64, 48, 12.0, O.DIRICHLET, 0.7, 2, 0.05),
+    (40, 40, 10.0, O.DIRICHLET, 1.5, 3, 0.05),
 ]
 
 

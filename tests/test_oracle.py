@@ -1,7 +1,9 @@
 """CPU tests of the oracle: the numpy restatement against the reference's own
 known-answer tests, and against the reference sources compiled into
 oracle/_ref (when built). No GPU needed."""
+import glob
 import math
+import os
 
 import numpy as np
 import pytest
@@ -241,3 +243,31 @@ def test_reference_harmonic_oscillator_spectrum(refkit_available):
     E, _ = sysm.energies()
     ref = [1, 2, 2, 3, 3, 3, 4, 4]
     assert np.max(np.abs(E[:8] - ref)) < tol
+
+
+# ---- the restatement against the golden fixtures (outputs of the compiled reference) ----
+
+GOLDEN_SEAMS = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "seam_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN_SEAMS, ids=[p.rsplit("seam_", 1)[1][:-4] for p in GOLDEN_SEAMS])
+def test_restatement_matches_golden_fixtures(path):
+    """tests/golden/seam_*.npz hold the compiled reference's propagation step,
+    H psi, energies and orthonormalised states on seeded inputs
+    (tests/golden/make_golden.py); the numpy restatement reproduces them."""
+    z = np.load(path)
+    sx, sy, L, bt, B, m, eps = z["cfg"]
+    g = O.Grid.from_length(int(sx), int(sy), float(L))
+    V = None if bool(z["potential_null"]) else z["V"]
+    bt, B, m, eps = int(bt), float(B), int(m), float(eps)
+    psi = z["psi"]
+    prop = O.MultiProductSplit(g, V, bt, B, m, eps).apply(psi)
+    rel = np.max(np.abs(prop - z["prop"]), axis=(1, 2)) / np.max(np.abs(z["prop"]), axis=(1, 2))
+    assert rel.max() < 1e-13
+    H = O.Hamiltonian(g, V, bt, B)
+    hpsi = H.apply(psi)
+    assert np.max(np.abs(hpsi - z["hpsi"])) < 1e-13 * np.max(np.abs(z["hpsi"]))
+    mean, _ = O.energies(H, z["prop"])
+    assert np.max(np.abs(mean.real - z["E"]) / np.abs(z["E"])) < 1e-13
+    ortho, _ = O.orthonormalize(g, z["prop"])
+    assert 1 - O.subspace_cosines(g, ortho, z["ortho"]).min() < 1e-12
