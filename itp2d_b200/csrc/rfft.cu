@@ -209,17 +209,33 @@ __global__ void __launch_bounds__(kThreads) row_reg_kernel(RowPassArgs a, int k)
 	}
 }
 
+// Asynchronous global -> shared copy of one complex element.
+template <class T> __device__ __forceinline__ void cp_async_elem(T* dst, const T* src);
+template <> __device__ __forceinline__ void cp_async_elem<double2>(double2* dst, const double2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+template <> __device__ __forceinline__ void cp_async_elem<float2>(float2* dst, const float2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Column pass, in place: tiles of W = 256 / B columns x N rows of one state
 // staged in shared memory ([y][c], row stride W + 1); each column line is
 // transformed by B threads of one warp, using the line's own column of the
-// tile as its exchange area.
-template <class R, int A, int B>
+// tile as its exchange area. Persistent; with NBUF = 2 the next tile is copied
+// in by cp.async while the current one is transformed (NBUF = 1 where two
+// tiles do not fit in shared memory).
+template <class R, int A, int B, int NBUF>
 __global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k) {
 	using T = c2<R>;
-	constexpr int N = A * B, W = kThreads / B, LD = W + 1;
+	constexpr int N = A * B, W = kThreads / B, LD = W + 1, TS = N * LD;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	T* xtw = reinterpret_cast<T*>(smem_raw);
-	T* tile = xtw + N;
+	T* tiles = xtw + N;
 	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
 	const int line = threadIdx.x / B, t = threadIdx.x % B;
 	const int sx = a.sx;
@@ -228,19 +244,42 @@ __global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k)
 	const R* m2 = reinterpret_cast<const R*>(a.mul2d);
 	const R* m1 = reinterpret_cast<const R*>(a.mul1d);
 	T* data = reinterpret_cast<T*>(a.data);
-	for (long long tl = blockIdx.x; tl < total; tl += gridDim.x) {
+	// copies tile tl into dst (asynchronously when NBUF = 2); columns beyond sx read as zero
+	auto fetch = [&](T* dst, long long tl) {
 		const long long state = tl % k;
 		const int col0 = (int)(tl / k) * W;
 		const int ncols = min(W, sx - col0);
-		T* src = data + state * a.G + col0;
-		__syncthreads();  // the previous tile has left shared memory
+		const T* src = data + state * a.G + col0;
 #pragma unroll
 		for (int it = 0; it < N * W / kThreads; it++) {
 			const int i = it * kThreads + threadIdx.x;
 			const int y = i / W, c = i - y * W;
-			tile[y * LD + c] = c < ncols ? src[(long long)y * sx + c] : mk<R>(0, 0);
+			if (c >= ncols) dst[y * LD + c] = mk<R>(0, 0);
+			else if (NBUF == 2) cp_async_elem<T>(dst + y * LD + c, src + (long long)y * sx + c);
+			else dst[y * LD + c] = src[(long long)y * sx + c];
 		}
-		__syncthreads();
+	};
+	long long tl = blockIdx.x;
+	int cur = 0;
+	if (NBUF == 2) {
+		if (tl < total) fetch(tiles, tl);
+		cp_async_commit();
+	}
+	for (; tl < total; tl += gridDim.x) {
+		T* tile = tiles + cur * TS;
+		if (NBUF == 2) {
+			const long long nx = tl + gridDim.x;
+			if (nx < total) fetch(tiles + (cur ^ 1) * TS, nx);
+			cp_async_commit();
+			cp_async_wait<1>();  // this thread's copies of the current tile have landed
+			__syncthreads();
+		} else {
+			fetch(tile, tl);
+			__syncthreads();
+		}
+		const long long state = tl % k;
+		const int col0 = (int)(tl / k) * W;
+		const int ncols = min(W, sx - col0);
 		T v[A];
 #pragma unroll
 		for (int i = 0; i < A; i++) v[i] = tile[(t + B * i) * LD + line];
@@ -260,13 +299,17 @@ __global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k)
 #pragma unroll
 		for (int i = 0; i < A; i++) tile[(t + B * i) * LD + line] = v[i];
 		__syncthreads();
+		T* dst = data + state * a.G + col0;
 #pragma unroll
 		for (int it = 0; it < N * W / kThreads; it++) {
 			const int i = it * kThreads + threadIdx.x;
 			const int y = i / W, c = i - y * W;
-			if (c < ncols) src[(long long)y * sx + c] = tile[y * LD + c];
+			if (c < ncols) dst[(long long)y * sx + c] = tile[y * LD + c];
 		}
+		__syncthreads();  // the tile buffer is refilled by a later fetch
+		if (NBUF == 2) cur ^= 1;
 	}
+	if (NBUF == 2) cp_async_wait<0>();
 }
 
 // Energy sums of one element: Re, Im <psi|h>, <h|h>, |h - es psi|^2, <psi|psi>.
@@ -445,10 +488,12 @@ void row_reg(const RowPassArgs& a, int k, cudaStream_t s) {
 template <class R, int A, int B>
 void col_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	constexpr int N = A * B, W = kThreads / B;
-	const size_t sm = (size_t)(N + N * (W + 1)) * sizeof(c2<R>);
-	opt_in_smem(col_reg_kernel<R, A, B>, sm);
+	constexpr size_t tile_bytes = (size_t)N * (W + 1) * sizeof(c2<R>);
+	constexpr int NBUF = (2 * tile_bytes + N * sizeof(c2<R>) <= 220 * 1024) ? 2 : 1;
+	const size_t sm = N * sizeof(c2<R>) + NBUF * tile_bytes;
+	opt_in_smem(col_reg_kernel<R, A, B, NBUF>, sm);
 	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
-	col_reg_kernel<R, A, B><<<grid_for(col_reg_kernel<R, A, B>, sm, tiles), kThreads, sm, s>>>(a, k);
+	col_reg_kernel<R, A, B, NBUF><<<grid_for(col_reg_kernel<R, A, B, NBUF>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
 template <class R, int A, int B>
