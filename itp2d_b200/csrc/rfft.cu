@@ -396,61 +396,96 @@ __global__ void __launch_bounds__(kThreads) energy_row_reg_kernel(EnergyRowArgs 
 	if (a.sums) reduce5(s, red, a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5);
 }
 
-// Energy column pass (periodic magnetic field; grid: states x column tiles of
-// 256 / B columns): t = Tinv_y(ty .* Tfwd_y(psi)), h = t + add_in; h -> h_out;
-// per-tile sums.
-template <class R, int A, int B>
-__global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs a) {
+// Energy column pass (magnetic field): t = Tinv_y(ty .* Tfwd_y(src)),
+// h = t + add_in; h -> h_out; per-tile sums against psi at
+// sums[(state * ntiles + tile) * 5]. Persistent over tiles of 256 / B columns
+// of one state, with the next tile's src copied in by cp.async while the
+// current one is transformed (NBUF = 2; NBUF = 1 where two tiles do not fit).
+template <class R, int A, int B, int NBUF>
+__global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs a, int k) {
 	using T = c2<R>;
-	constexpr int N = A * B, W = kThreads / B, LD = W + 1;
+	constexpr int N = A * B, W = kThreads / B, LD = W + 1, TS = N * LD;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	T* xtw = reinterpret_cast<T*>(smem_raw);
-	T* tile = xtw + N;
-	double* red = reinterpret_cast<double*>(tile + N * LD);
+	T* tiles = xtw + N;
+	double* red = reinterpret_cast<double*>(tiles + NBUF * TS);
 	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
 	const int line = threadIdx.x / B, t = threadIdx.x % B;
-	const long long state = blockIdx.x;
-	const int col0 = blockIdx.y * W;
-	const int ncols = min(W, a.sx - col0);
 	const int sx = a.sx;
-	const long long base = state * a.G + col0;
-	const T* psi = reinterpret_cast<const T*>(a.psi) + base;
-	const T* src = a.src ? reinterpret_cast<const T*>(a.src) + base : psi;
+	const int nct = (sx + W - 1) / W;
+	const long long total = (long long)k * nct;
+	const T* psi_all = reinterpret_cast<const T*>(a.psi);
+	const T* src_all = a.src ? reinterpret_cast<const T*>(a.src) : psi_all;
+	auto fetch = [&](T* dst, long long tl) {
+		const long long state = tl % k;
+		const int col0 = (int)(tl / k) * W;
+		const int ncols = min(W, sx - col0);
+		const T* src = src_all + state * a.G + col0;
 #pragma unroll
-	for (int it = 0; it < N * W / kThreads; it++) {
-		const int i = it * kThreads + threadIdx.x;
-		const int y = i / W, c = i - y * W;
-		tile[y * LD + c] = c < ncols ? src[(long long)y * sx + c] : mk<R>(0, 0);
-	}
-	__syncthreads();
-	T v[A];
-#pragma unroll
-	for (int i = 0; i < A; i++) v[i] = tile[(t + B * i) * LD + line];
-	line_fft<R, A, B, -1>(v, t, tile + line, LD, xtw);
-	const R* ty = reinterpret_cast<const R*>(a.ty);
-#pragma unroll
-	for (int i = 0; i < A; i++) v[i] = cscale(v[i], ty[t + B * i]);
-	line_fft<R, A, B, 1>(v, t, tile + line, LD, xtw);
-	__syncwarp();
-#pragma unroll
-	for (int i = 0; i < A; i++) tile[(t + B * i) * LD + line] = v[i];
-	__syncthreads();
-	const T* add = reinterpret_cast<const T*>(a.add_in) + base;
-	T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
-	const double es = a.Eshift ? a.Eshift[state] : 0.0;
-	double s[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-	for (int it = 0; it < N * W / kThreads; it++) {
-		const int i = it * kThreads + threadIdx.x;
-		const int y = i / W, c = i - y * W;
-		if (c < ncols) {
-			const long long off = (long long)y * sx + c;
-			const T h = cadd(tile[y * LD + c], add[off]);
-			if (hout) hout[off] = h;
-			if (a.sums) esums(s, psi[off], h, es);
+		for (int it = 0; it < N * W / kThreads; it++) {
+			const int i = it * kThreads + threadIdx.x;
+			const int y = i / W, c = i - y * W;
+			if (c >= ncols) dst[y * LD + c] = mk<R>(0, 0);
+			else if (NBUF == 2) cp_async_elem<T>(dst + y * LD + c, src + (long long)y * sx + c);
+			else dst[y * LD + c] = src[(long long)y * sx + c];
 		}
+	};
+	const R* ty = reinterpret_cast<const R*>(a.ty);
+	long long tl = blockIdx.x;
+	int cur = 0;
+	if (NBUF == 2) {
+		if (tl < total) fetch(tiles, tl);
+		cp_async_commit();
 	}
-	if (a.sums) reduce5(s, red, a.sums + ((size_t)state * gridDim.y + blockIdx.y) * 5);
+	for (; tl < total; tl += gridDim.x) {
+		T* tile = tiles + cur * TS;
+		if (NBUF == 2) {
+			const long long nx = tl + gridDim.x;
+			if (nx < total) fetch(tiles + (cur ^ 1) * TS, nx);
+			cp_async_commit();
+			cp_async_wait<1>();
+			__syncthreads();
+		} else {
+			fetch(tile, tl);
+			__syncthreads();
+		}
+		const long long state = tl % k;
+		const int ct = (int)(tl / k);
+		const int col0 = ct * W;
+		const int ncols = min(W, sx - col0);
+		const long long base = state * a.G + col0;
+		T v[A];
+#pragma unroll
+		for (int i = 0; i < A; i++) v[i] = tile[(t + B * i) * LD + line];
+		line_fft<R, A, B, -1>(v, t, tile + line, LD, xtw);
+#pragma unroll
+		for (int i = 0; i < A; i++) v[i] = cscale(v[i], ty[t + B * i]);
+		line_fft<R, A, B, 1>(v, t, tile + line, LD, xtw);
+		__syncwarp();
+#pragma unroll
+		for (int i = 0; i < A; i++) tile[(t + B * i) * LD + line] = v[i];
+		__syncthreads();
+		const T* add = reinterpret_cast<const T*>(a.add_in) + base;
+		const T* psi = psi_all + base;
+		T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
+		const double es = a.Eshift ? a.Eshift[state] : 0.0;
+		double s[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+		for (int it = 0; it < N * W / kThreads; it++) {
+			const int i = it * kThreads + threadIdx.x;
+			const int y = i / W, c = i - y * W;
+			if (c < ncols) {
+				const long long off = (long long)y * sx + c;
+				const T h = cadd(tile[y * LD + c], add[off]);
+				if (hout) hout[off] = h;
+				if (a.sums) esums(s, psi[off], h, es);
+			}
+		}
+		if (a.sums) reduce5(s, red, a.sums + ((size_t)state * nct + ct) * 5);
+		__syncthreads();  // the tile buffer is refilled by a later fetch
+		if (NBUF == 2) cur ^= 1;
+	}
+	if (NBUF == 2) cp_async_wait<0>();
 }
 
 template <class K>
@@ -507,9 +542,13 @@ void energy_row_reg(const EnergyRowArgs& a, int k, cudaStream_t s) {
 template <class R, int A, int B>
 void energy_col_reg(const EnergyColArgs& a, int k, cudaStream_t s) {
 	constexpr int N = A * B, W = kThreads / B;
-	const size_t sm = (size_t)(N + N * (W + 1)) * sizeof(c2<R>) + 5 * (kThreads / 32) * sizeof(double);
-	opt_in_smem(energy_col_reg_kernel<R, A, B>, sm);
-	energy_col_reg_kernel<R, A, B><<<dim3(k, (a.sx + W - 1) / W), kThreads, sm, s>>>(a);
+	constexpr size_t tile_bytes = (size_t)N * (W + 1) * sizeof(c2<R>);
+	constexpr int NBUF = (2 * tile_bytes + N * sizeof(c2<R>) <= 220 * 1024) ? 2 : 1;
+	const size_t sm = N * sizeof(c2<R>) + NBUF * tile_bytes + 5 * (kThreads / 32) * sizeof(double);
+	opt_in_smem(energy_col_reg_kernel<R, A, B, NBUF>, sm);
+	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
+	energy_col_reg_kernel<R, A, B, NBUF>
+			<<<grid_for(energy_col_reg_kernel<R, A, B, NBUF>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
 // Threads per line (B) of the register path for line length N, 0 if none.
