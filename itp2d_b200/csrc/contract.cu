@@ -36,11 +36,30 @@ struct Stage {
 	double bi[kBN * kPad];
 };
 
+// Asynchronous global -> shared copy of one complex element.
+template <class T> __device__ __forceinline__ void cp_async_elem(T* dst, const T* src);
+template <> __device__ __forceinline__ void cp_async_elem<double2>(double2* dst, const double2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+template <> __device__ __forceinline__ void cp_async_elem<float2>(float2* dst, const float2* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Overlap: A rows i (conjugated side) and B rows j, both rows of psi (k x G).
+// The g range of the split advances kBK per step through two shared-memory
+// stages of complex-interleaved rows (pitch kPad elements: conflict-free
+// fragment loads): cp.async fetches step s + 1 while the DMMAs of step s run.
 template <class T>
 __global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi, int k, long long G,
 		const int2* __restrict__ pairs, long long chunk, double2* __restrict__ part) {
-	__shared__ __align__(16) Stage st;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T* stage = reinterpret_cast<T*>(smem_raw);  // [2][A rows kBM | B rows kBN][kPad]
+	constexpr int SS = (kBM + kBN) * kPad;
 	const int2 tp = pairs[blockIdx.x];
 	const int i0 = tp.x * kBM, j0 = tp.y * kBN;
 	const long long g0 = (long long)blockIdx.y * chunk;
@@ -56,40 +75,45 @@ __global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi,
 			accr[a][b][0] = accr[a][b][1] = 0.0;
 			acci[a][b][0] = acci[a][b][1] = 0.0;
 		}
-	// loader mapping: row = tid / 4, 4 consecutive complex at seg*4
+	// loader mapping: row = tid / 4, 4 consecutive complex at seg*4, for A and B
 	const int lrow = tid >> 2, lseg = (tid & 3) * 4;
-	for (long long g = g0; g < g1; g += kBK) {
-		{
-			const int ia = i0 + lrow, jb = j0 + lrow;
+	auto fetch = [&](T* st, long long g) {
+		const int ia = i0 + lrow, jb = j0 + lrow;
 #pragma unroll
-			for (int q = 0; q < 4; q++) {
-				const long long gg = g + lseg + q;
-				double2 va = make_double2(0, 0), vb = make_double2(0, 0);
-				if (gg < g1) {
-					if (ia < k) { const T t = psi[(long long)ia * G + gg]; va = make_double2(t.x, t.y); }
-					if (jb < k) { const T t = psi[(long long)jb * G + gg]; vb = make_double2(t.x, t.y); }
-				}
-				st.ar[lrow * kPad + lseg + q] = va.x;
-				st.ai[lrow * kPad + lseg + q] = va.y;
-				st.br[lrow * kPad + lseg + q] = vb.x;
-				st.bi[lrow * kPad + lseg + q] = vb.y;
-			}
+		for (int q = 0; q < 4; q++) {
+			const long long gg = g + lseg + q;
+			T* da = st + lrow * kPad + lseg + q;
+			T* db = st + (kBM + lrow) * kPad + lseg + q;
+			if (gg < g1 && ia < k) cp_async_elem<T>(da, psi + (long long)ia * G + gg);
+			else *da = T{0, 0};
+			if (gg < g1 && jb < k) cp_async_elem<T>(db, psi + (long long)jb * G + gg);
+			else *db = T{0, 0};
 		}
+	};
+	int cur = 0;
+	if (g0 < g1) fetch(stage, g0);
+	cp_async_commit();
+	for (long long g = g0; g < g1; g += kBK) {
+		if (g + kBK < g1) fetch(stage + (cur ^ 1) * SS, g + kBK);
+		cp_async_commit();
+		cp_async_wait<1>();
 		__syncthreads();
+		const T* sa = stage + cur * SS;
+		const T* sb = sa + kBM * kPad;
 #pragma unroll
 		for (int kk = 0; kk < kBK; kk += 4) {
 			double far[4], fai[4], fbr[2], fbi[2];
 #pragma unroll
 			for (int a = 0; a < 4; a++) {
-				const int r = wi * 32 + a * 8 + (lane >> 2);
-				far[a] = st.ar[r * kPad + kk + (lane & 3)];
-				fai[a] = st.ai[r * kPad + kk + (lane & 3)];
+				const T v = sa[(wi * 32 + a * 8 + (lane >> 2)) * kPad + kk + (lane & 3)];
+				far[a] = v.x;
+				fai[a] = v.y;
 			}
 #pragma unroll
 			for (int b = 0; b < 2; b++) {
-				const int c = wj * 16 + b * 8 + (lane >> 2);
-				fbr[b] = st.br[c * kPad + kk + (lane & 3)];
-				fbi[b] = st.bi[c * kPad + kk + (lane & 3)];
+				const T v = sb[(wj * 16 + b * 8 + (lane >> 2)) * kPad + kk + (lane & 3)];
+				fbr[b] = v.x;
+				fbi[b] = v.y;
 			}
 #pragma unroll
 			for (int a = 0; a < 4; a++)
@@ -102,8 +126,10 @@ __global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi,
 					dmma(acci[a][b][0], acci[a][b][1], -fai[a], fbr[b]);
 				}
 		}
-		__syncthreads();
+		__syncthreads();  // this stage is refilled by the fetch of the next step
+		cur ^= 1;
 	}
+	cp_async_wait<0>();
 	// write the partial tile: part[split][i][j]
 	double2* out = part + (size_t)blockIdx.y * k * k;
 #pragma unroll
@@ -278,7 +304,9 @@ void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npa
 	long long chunk = (G + nsplit - 1) / nsplit;
 	chunk = ((chunk + kBK - 1) / kBK) * kBK;
 	const int used = (int)((G + chunk - 1) / chunk);
-	overlap_kernel<T><<<dim3(npairs, used), 256, 0, s>>>(psi, k, G, pairs, chunk, part);
+	const size_t sm = (size_t)2 * (kBM + kBN) * kPad * sizeof(T);
+	cudaFuncSetAttribute(overlap_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+	overlap_kernel<T><<<dim3(npairs, used), 256, sm, s>>>(psi, k, G, pairs, chunk, part);
 	launch_overlap_finish(part, k, used, dx2, S, s);
 }
 

@@ -727,7 +727,9 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	// overlap / eigensolver buffers
 	const int nt = overlap_tiles(k);
 	c->npairs = nt * (nt + 1) / 2;
-	c->nsplit = std::max(1, std::min((4 * c->num_sms + c->npairs - 1) / c->npairs, (int)std::max(1LL, c->G / 512)));
+	// split-K count: the largest that keeps the grid within two waves of two
+	// CTAs per SM (a third, nearly empty wave costs a third of the kernel)
+	c->nsplit = std::max(1, std::min((4 * c->num_sms) / c->npairs, (int)std::max(1LL, c->G / 512)));
 	const int kp = std::max(bjacobi_padded(k), (k + 1) & ~1);  // covers the scalar and block layouts
 	if (e == cudaSuccess) c->S = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
 	c->tc_nsplit = tc_overlap_splits(k, c->G, c->num_sms);
