@@ -28,13 +28,6 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 			: "d"(a), "d"(b));
 }
 
-// Shared-memory planes: [64][kPad] doubles each.
-struct Stage {
-	double ar[kBM * kPad];
-	double ai[kBM * kPad];
-	double br[kBN * kPad];
-	double bi[kBN * kPad];
-};
 
 // Asynchronous global -> shared copy of one complex element.
 template <class T> __device__ __forceinline__ void cp_async_elem(T* dst, const T* src);
@@ -169,11 +162,17 @@ __global__ void overlap_finish_kernel(const double2* __restrict__ part, int k, i
 	}
 }
 
-// Rotation: out[n][g] = sum_i W[i][n] psi[i][g]; tile 64 n x 64 g.
+// Rotation: out[n][g] = sum_i W[i][n] psi[i][g]; tile 64 n x 64 g. The i range
+// advances kBK per step through two shared-memory stages holding the W rows
+// [i][n] and the psi rows [i][g] as in global memory (cp.async fetches step
+// s + 1 while the DMMAs of step s run); row pitches of 66 (16-byte elements)
+// and 68 (8-byte elements) make the transposed fragment reads conflict-free.
 template <class T>
 __global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__ W, const T* __restrict__ psi,
 		int k, long long G, T* __restrict__ out) {
-	__shared__ __align__(16) Stage st;  // a*: [n][i], b*: [g][i]
+	constexpr int PW = 66, PP = sizeof(T) == 16 ? 66 : 68;
+	constexpr int SW = kBK * PW * (int)sizeof(double2), SP = kBK * PP * (int)sizeof(T);
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int n0 = blockIdx.x * kBM;
 	const long long g0 = (long long)blockIdx.y * kBN;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -186,45 +185,49 @@ __global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__
 			accr[a][b][0] = accr[a][b][1] = 0.0;
 			acci[a][b][0] = acci[a][b][1] = 0.0;
 		}
+	auto sw = [&](int buf) { return reinterpret_cast<double2*>(smem_raw + buf * (SW + SP)); };
+	auto sp = [&](int buf) { return reinterpret_cast<T*>(smem_raw + buf * (SW + SP) + SW); };
+	// W tile 16 i x 64 n and psi tile 16 i x 64 g: 4 elements each per thread
+	auto fetch = [&](int buf, int i0) {
+		double2* dw = sw(buf);
+		T* dp = sp(buf);
+#pragma unroll
+		for (int q = 0; q < 4; q++) {
+			const int e = tid + q * 256;
+			const int ii = e >> 6, cc = e & 63;
+			const int i = i0 + ii, n = n0 + cc;
+			const long long g = g0 + cc;
+			if (i < k && n < k) cp_async_elem<double2>(dw + ii * PW + cc, W + (size_t)i * k + n);
+			else dw[ii * PW + cc] = make_double2(0, 0);
+			if (i < k && g < G) cp_async_elem<T>(dp + ii * PP + cc, psi + (long long)i * G + g);
+			else dp[ii * PP + cc] = T{0, 0};
+		}
+	};
+	int cur = 0;
+	fetch(0, 0);
+	cp_async_commit();
 	for (int i0 = 0; i0 < k; i0 += kBK) {
-		// W tile: 16 i x 64 n, contiguous in n. 1024 elements, 4 per thread.
-#pragma unroll
-		for (int q = 0; q < 4; q++) {
-			const int e = tid + q * 256;
-			const int ii = e >> 6, nn = e & 63;
-			const int i = i0 + ii, n = n0 + nn;
-			double2 v = make_double2(0, 0);
-			if (i < k && n < k) v = W[(size_t)i * k + n];
-			st.ar[nn * kPad + ii] = v.x;
-			st.ai[nn * kPad + ii] = v.y;
-		}
-		// psi tile: 16 i x 64 g, contiguous in g.
-#pragma unroll
-		for (int q = 0; q < 4; q++) {
-			const int e = tid + q * 256;
-			const int ii = e >> 6, gg = e & 63;
-			const int i = i0 + ii;
-			const long long g = g0 + gg;
-			double2 v = make_double2(0, 0);
-			if (i < k && g < G) { const T t = psi[(long long)i * G + g]; v = make_double2(t.x, t.y); }
-			st.br[gg * kPad + ii] = v.x;
-			st.bi[gg * kPad + ii] = v.y;
-		}
+		if (i0 + kBK < k) fetch(cur ^ 1, i0 + kBK);
+		cp_async_commit();
+		cp_async_wait<1>();
 		__syncthreads();
+		const double2* a_s = sw(cur);
+		const T* b_s = sp(cur);
 #pragma unroll
 		for (int kk = 0; kk < kBK; kk += 4) {
 			double far[4], fai[4], fbr[2], fbi[2];
+			const int ii = kk + (lane & 3);
 #pragma unroll
 			for (int a = 0; a < 4; a++) {
-				const int r = wn * 32 + a * 8 + (lane >> 2);
-				far[a] = st.ar[r * kPad + kk + (lane & 3)];
-				fai[a] = st.ai[r * kPad + kk + (lane & 3)];
+				const double2 v = a_s[ii * PW + wn * 32 + a * 8 + (lane >> 2)];
+				far[a] = v.x;
+				fai[a] = v.y;
 			}
 #pragma unroll
 			for (int b = 0; b < 2; b++) {
-				const int c = wg * 16 + b * 8 + (lane >> 2);
-				fbr[b] = st.br[c * kPad + kk + (lane & 3)];
-				fbi[b] = st.bi[c * kPad + kk + (lane & 3)];
+				const T v = b_s[ii * PP + wg * 16 + b * 8 + (lane >> 2)];
+				fbr[b] = v.x;
+				fbi[b] = v.y;
 			}
 #pragma unroll
 			for (int a = 0; a < 4; a++)
@@ -237,8 +240,10 @@ __global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__
 					dmma(acci[a][b][0], acci[a][b][1], fai[a], fbr[b]);
 				}
 		}
-		__syncthreads();
+		__syncthreads();  // this stage is refilled by the fetch of the next step
+		cur ^= 1;
 	}
+	cp_async_wait<0>();
 #pragma unroll
 	for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -318,7 +323,9 @@ void launch_overlap_finish(const double2* part, int k, int nsplit, double dx2, d
 template <class T>
 void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s) {
 	const dim3 grid((k + kBM - 1) / kBM, (unsigned)((G + kBN - 1) / kBN));
-	rotate_kernel<T><<<grid, 256, 0, s>>>(W, psi, k, G, out);
+	const size_t sm = (size_t)2 * kBK * (66 * sizeof(double2) + (sizeof(T) == 16 ? 66 : 68) * sizeof(T));
+	cudaFuncSetAttribute(rotate_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+	rotate_kernel<T><<<grid, 256, sm, s>>>(W, psi, k, G, out);
 }
 
 template <class T>
