@@ -506,11 +506,26 @@ int tc_overlap_splits(int k, long long G, int num_sms) {
 	const int nt = (k + TM - 1) / TM;
 	const int npairs = nt * (nt + 1) / 2;
 	// enough CTAs to cover the SMs; chunks of at most 2048 grid points bound
-	// the FP32 accumulation in tensor memory (the splits add up in FP64)
+	// the FP32 accumulation in tensor memory (the splits add up in FP64); then
+	// the first count (up to twice that) whose grid fills its last wave of one
+	// CTA per SM to 90% or more, else the best-filled one
 	const long long by_sms = (num_sms + npairs - 1) / npairs;
 	const long long by_len = (G + 2047) / 2048;
 	const long long most = std::max(1LL, G / (4 * KT));
-	return (int)std::max(1LL, std::min(std::max(by_sms, by_len), most));
+	const long long lo = std::max(1LL, std::min(std::max(by_sms, by_len), most));
+	long long best = lo;
+	double best_fill = 0.0;
+	for (long long ns = lo; ns <= std::min(2 * lo, most); ns++) {
+		const long long ctas = npairs * ns;
+		const long long waves = (ctas + num_sms - 1) / num_sms;
+		const double fill = (double)ctas / (double)(waves * num_sms);
+		if (fill > best_fill + 1e-9) {
+			best = ns;
+			best_fill = fill;
+		}
+		if (fill >= 0.9) break;
+	}
+	return (int)best;
 }
 
 size_t tc_wsplit_bytes(int k) {
