@@ -438,7 +438,8 @@ __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned c
 	unsigned char* const base = sh.buf;
 	const unsigned char* wblk = wsplit + (size_t)blockIdx.x * nsteps * kOperandBytes;
 	// raw psi slot: row r = K index within the step (16 rows of 128 complex),
-	// 16-byte piece pg (64 per row) stored at slot pg ^ 4 ((r >> 1) & 1)
+	// 16-byte piece pg (64 per row) stored at slot pg ^ 2 ((r >> 1) & 3): the
+	// four rows a half-warp of the split reads land in distinct 32-byte banks
 	auto prefetch = [&](int s) {
 		unsigned char* ring = base + kRoA + (s & 3) * kOperandBytes;
 		const unsigned char* src = wblk + (size_t)s * kOperandBytes;
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned c
 			const long long g = gt0 + 2 * pg;
 			const bool in = i < k && g < G;  // g even, G even: both complex in range
 			const float2* p = in ? psi + (long long)i * G + g : psi;
-			cp16(smem_u32(slot + r * (TN * 8) + ((pg ^ (((r >> 1) & 1) << 2)) << 4)), p, in ? 16 : 0);
+			cp16(smem_u32(slot + r * (TN * 8) + ((pg ^ (((r >> 1) & 3) << 1)) << 4)), p, in ? 16 : 0);
 		}
 	};
 	// convert: warp w handles core matrices m = w, w + 8, w + 16, w + 24 of the
@@ -472,9 +473,9 @@ __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned c
 			const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
 			const int pg = r >> 1, sub = r & 1;
 			const float2 p0 = reinterpret_cast<const float2*>(
-					slot + kk * (TN * 8) + ((pg ^ (((kk >> 1) & 1) << 2)) << 4))[sub];
+					slot + kk * (TN * 8) + ((pg ^ (((kk >> 1) & 3) << 1)) << 4))[sub];
 			const float2 p1 = reinterpret_cast<const float2*>(
-					slot + (kk + 1) * (TN * 8) + ((pg ^ ((((kk + 1) >> 1) & 1) << 2)) << 4))[sub];
+					slot + (kk + 1) * (TN * 8) + ((pg ^ ((((kk + 1) >> 1) & 3) << 1)) << 4))[sub];
 			put2(planes, kmaj_off(r, kk), p0.x, p0.y, p1.x, p1.y);
 		}
 	};
