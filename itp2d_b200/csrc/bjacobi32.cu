@@ -1,0 +1,523 @@
+// Single-precision block Jacobi for the overlap matrix of the FP32 form.
+//
+// The FP32 form's overlap is accurate to about 1e-5 (split-BF16 tensor-core
+// contraction) and its eigensolve stops at a largest rotation tangent of 1e-3,
+// so FP64 arithmetic buys nothing there. This is the schedule of bjacobi.cu —
+// round-robin pairs of 16-index blocks, 32 x 32 subproblems swept on 16 CTAs
+// (cross pairs only except every 16th round), phase 1 of round t pipelined
+// against phase 2 of round t - 1, one grid barrier per round — in single
+// precision: the rotation set-up uses the hardware square root and reciprocal
+// square root directly (no Newton refinement), and the block products are
+// FFMA. Its latency chains are the short ones of FP32, which is what the
+// latency-bound subproblem sweeps need.
+//
+// Accuracy: rotations are unitary to a few FP32 units, so the eigenvector
+// matrix is orthonormal to about 1e-6; normalize_columns_kernel (jacobi.cu)
+// renormalises its columns in FP64 afterwards. Rotations whose relative
+// off-diagonal element is below 1e-7 are not applied, those below 1e-6 do not
+// count toward convergence.
+#include <cooperative_groups.h>
+
+#include "../../include/itp2d_gpu.h"
+#include "contract.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace itp2d {
+
+namespace {
+
+constexpr int BS = 16;        // block size
+constexpr int MS = 32;        // subproblem size: two blocks
+constexpr int NR = MS / 2;    // rotations per inner round
+constexpr int LD = MS + 1;    // padded row length (floats)
+constexpr int PL = MS * LD;   // floats per plane
+constexpr int kThreads = 256;
+constexpr int kFullEvery = 16;
+constexpr float kSkipRel = 1e-7f;
+constexpr float kNoiseRel = 1e-6f;
+
+__device__ __forceinline__ int rr_player(int pos, int r, int npos) {
+	return pos == 0 ? 0 : ((pos - 1 + r) % (npos - 1)) + 1;
+}
+
+__device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * BS + i : Q * BS + (i - BS); }
+
+struct Shared32 {
+	float pl[6][PL];  // [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
+	float rs[NR], rtau[NR], rer[NR], rei[NR], rap[NR], raq[NR];
+	int rp[NR], rq[NR], rrot[NR];
+	int cnt;
+	unsigned long long tmax;  // bits of a non-negative double
+};
+
+// Rotation of the local pair (p, q): with d = (b - a) / 2, r = sqrt(d^2 + |c|^2),
+// u = |d| + r and w = 2 r u: cos = u / sqrt(w), |sin| = |c| / sqrt(w),
+// tau = |sin| / (1 + cos), tan = |c| / u (the formulas of bjacobi.cu).
+__device__ void inner_rotation32(Shared32& sh, int j, int p, int q, int& cnt, float& tmax) {
+	const float* mr = sh.pl[0];
+	const float* mi = sh.pl[1];
+	const float a = mr[p * LD + p], b = mr[q * LD + q];
+	const float cr = mr[p * LD + q], ci = mi[p * LD + q];
+	const float c2 = cr * cr + ci * ci;
+	const float scale2 = fabsf(a) * fabsf(b);
+	sh.rp[j] = p;
+	sh.rq[j] = q;
+	sh.rrot[j] = 0;
+	sh.rs[j] = 0.f; sh.rtau[j] = 0.f; sh.rer[j] = 1.f; sh.rei[j] = 0.f; sh.rap[j] = a; sh.raq[j] = b;
+	if (!(c2 > 0.f && c2 > kSkipRel * kSkipRel * scale2)) return;
+	const float d = 0.5f * (b - a);
+	const float ad = fabsf(d);
+	const float rn = sqrtf(fmaf(d, d, c2));
+	const float un = ad + rn;
+	const float wn = 2.f * rn * un;
+	const float qn = rsqrtf(wn);
+	const float cabs = sqrtf(c2);
+	const float t = __fdividef(cabs, un);
+	const float ic = rsqrtf(c2);
+	const float sg = d < 0.f ? -1.f : 1.f;
+	sh.rs[j] = sg * cabs * qn;
+	sh.rtau[j] = sg * __fdividef(cabs, wn * qn + un);
+	sh.rer[j] = cr * ic;
+	sh.rei[j] = ci * ic;
+	sh.rap[j] = a - sg * t * cabs;
+	sh.raq[j] = b + sg * t * cabs;
+	sh.rrot[j] = 1;
+	if (c2 > kNoiseRel * kNoiseRel * scale2) {
+		cnt++;
+		tmax = fmaxf(tmax, t);
+	}
+}
+
+__device__ __forceinline__ void rows2f(float s, float tau, float er, float ei, float& xpr, float& xpi, float& xqr,
+		float& xqi) {
+	const float ypr = xpr - s * (er * xqr - ei * xqi + tau * xpr);
+	const float ypi = xpi - s * (er * xqi + ei * xqr + tau * xpi);
+	const float yqr = xqr + s * (er * xpr + ei * xpi - tau * xqr);
+	const float yqi = xqi + s * (er * xpi - ei * xpr - tau * xqi);
+	xpr = ypr; xpi = ypi; xqr = yqr; xqi = yqi;
+}
+
+__device__ __forceinline__ void cols2f(float s, float tau, float er, float ei, float& xsr, float& xsi, float& xtr,
+		float& xti) {
+	const float ysr = xsr - s * (er * xtr + ei * xti + tau * xsr);
+	const float ysi = xsi - s * (er * xti - ei * xtr + tau * xsi);
+	const float ytr = xtr + s * (er * xsr - ei * xsi - tau * xtr);
+	const float yti = xti + s * (er * xsi + ei * xsr - tau * xti);
+	xsr = ysr; xsi = ysi; xtr = ytr; xti = yti;
+}
+
+// One inner sweep (full: MS - 1 rounds over all pairs; cross: BS rounds of the
+// BS x BS cross pairs) on the subproblem in planes 0/1, Q in planes 2/3.
+__device__ void inner_sweep32(Shared32& sh, bool full) {
+	float* mr = sh.pl[0];
+	float* mi = sh.pl[1];
+	float* qr = sh.pl[2];
+	float* qi = sh.pl[3];
+	const int tid = threadIdx.x;
+	const int rounds = full ? MS - 1 : BS;
+	int cnt = 0;
+	float tmax = 0.f;
+	for (int r = 0; r < rounds; r++) {
+		if (tid < NR) {
+			const int p = full ? rr_player(tid, r, MS) : tid;
+			const int q = full ? rr_player(MS - 1 - tid, r, MS) : BS + (tid + r) % BS;
+			inner_rotation32(sh, tid, p, q, cnt, tmax);
+		}
+		__syncthreads();
+		for (int e = tid; e < NR * NR; e += kThreads) {
+			const int ja = e / NR, jb = e % NR;
+			const bool ra = sh.rrot[ja], rb = sh.rrot[jb];
+			if (!ra && !rb) continue;
+			const int p = sh.rp[ja], q = sh.rq[ja], s2 = sh.rp[jb], t2 = sh.rq[jb];
+			if (ja == jb) {
+				mr[p * LD + p] = sh.rap[ja]; mi[p * LD + p] = 0.f;
+				mr[q * LD + q] = sh.raq[ja]; mi[q * LD + q] = 0.f;
+				mr[p * LD + q] = 0.f; mi[p * LD + q] = 0.f;
+				mr[q * LD + p] = 0.f; mi[q * LD + p] = 0.f;
+				continue;
+			}
+			float psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
+			float qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
+			if (ra) {
+				rows2f(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
+				rows2f(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
+			}
+			if (rb) {
+				cols2f(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
+				cols2f(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
+			}
+			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
+			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
+		}
+		for (int e = tid; e < MS * NR; e += kThreads) {
+			const int i = e / NR, j = e % NR;
+			if (!sh.rrot[j]) continue;
+			const int p = sh.rp[j], q = sh.rq[j];
+			float ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
+			cols2f(sh.rs[j], sh.rtau[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
+			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
+		}
+		__syncthreads();
+	}
+	if (tid < 32) {
+		for (int o = 16; o > 0; o >>= 1) {
+			cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+			tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+		}
+		if (tid == 0) {
+			sh.cnt += cnt;
+			const unsigned long long tb = (unsigned long long)__double_as_longlong((double)tmax);
+			if (tb > sh.tmax) sh.tmax = tb;
+		}
+	}
+}
+
+// acc = A B for 32 x 32 complex operands given as plane pairs, FFMA. Thread
+// outputs: row (warp >> 1) * 8 + (lane >> 2), columns (warp & 1) * 16 + b * 8 +
+// 2 * (lane & 3) + h. A element (i, m) at a_re[i * as_i + m * as_m], B element
+// (m, l) at b_re[m * LD + l]; conjA conjugates A.
+__device__ __forceinline__ void acc_rc32(int b, int h, int& row, int& col) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	row = (warp >> 1) * 8 + (lane >> 2);
+	col = (warp & 1) * 16 + b * 8 + 2 * (lane & 3) + h;
+}
+
+__device__ __forceinline__ void cgemm32(const float* ar, const float* ai, int as_i, int as_m, bool conjA,
+		const float* br, const float* bi, float (&cr)[2][2], float (&ci)[2][2]) {
+	int row, col0;
+	acc_rc32(0, 0, row, col0);
+#pragma unroll
+	for (int b = 0; b < 2; b++) cr[b][0] = cr[b][1] = ci[b][0] = ci[b][1] = 0.f;
+#pragma unroll 8
+	for (int m = 0; m < MS; m++) {
+		const float xr = ar[row * as_i + m * as_m];
+		const float xi = conjA ? -ai[row * as_i + m * as_m] : ai[row * as_i + m * as_m];
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int l = col0 + b * 8 + h;
+				const float yr = br[m * LD + l], yi = bi[m * LD + l];
+				cr[b][h] = fmaf(xr, yr, fmaf(-xi, yi, cr[b][h]));
+				ci[b][h] = fmaf(xr, yi, fmaf(xi, yr, ci[b][h]));
+			}
+	}
+}
+
+__device__ void load_q32(float* qr, float* qi, const float2* Qg) {
+	for (int e = threadIdx.x; e < MS * MS; e += kThreads) {
+		const float2 v = __ldcg(Qg + e);
+		qr[(e / MS) * LD + (e % MS)] = v.x;
+		qi[(e / MS) * LD + (e % MS)] = v.y;
+	}
+}
+
+__device__ __forceinline__ int rr_position(int p, int r, int npos) {
+	if (p == 0) return 0;
+	const int m = npos - 1;
+	return ((p - 1 - r) % m + m) % m + 1;
+}
+
+// Phase 1 for pair j of round t (bjacobi.cu phase1_item in FP32).
+__device__ void phase1_item32(Shared32& sh, int j, long long t, int rounds, int nb, int np, int kp,
+		const float2* prev, const float2* prev2, const float2* Qprev, float2* Qout, float2* out) {
+	const int tid = threadIdx.x;
+	const int rr = (int)(t % rounds);
+	const int P = rr_player(j, rr, nb), Q = rr_player(nb - 1 - j, rr, nb);
+	float* mr = sh.pl[0];
+	float* mi = sh.pl[1];
+	if (t == 0) {
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const float2 v = __ldcg(prev + (long long)gidx(i, P, Q) * kp + gidx(l, P, Q));
+			mr[i * LD + l] = v.x;
+			mi[i * LD + l] = v.y;
+		}
+	} else {
+		const int ro = (int)((t - 1) % rounds);
+		const int posP = rr_position(P, ro, nb), posQ = rr_position(Q, ro, nb);
+		const int a = posP < np ? posP : nb - 1 - posP, hP = posP < np ? 0 : 1;
+		const int b = posQ < np ? posQ : nb - 1 - posQ, hQ = posQ < np ? 0 : 1;
+		const int Pa = rr_player(a, ro, nb), Qa = rr_player(nb - 1 - a, ro, nb);
+		const int Pb = rr_player(b, ro, nb), Qb = rr_player(nb - 1 - b, ro, nb);
+		constexpr int NL = MS * MS / kThreads, ND = 2 * BS * BS / kThreads;
+		float2 la[NL], lqa[NL], lqb[NL], ldg[ND];
+#pragma unroll
+		for (int it = 0; it < NL; it++) {
+			const int e = it * kThreads + tid, i = e / MS, l = e % MS;
+			la[it] = __ldcg(prev2 + (long long)gidx(i, Pa, Qa) * kp + gidx(l, Pb, Qb));
+			lqa[it] = __ldcg(Qprev + (size_t)a * MS * MS + e);
+			lqb[it] = __ldcg(Qprev + (size_t)b * MS * MS + e);
+		}
+#pragma unroll
+		for (int it = 0; it < ND; it++) {
+			const int e = it * kThreads + tid;
+			const int half = e / (BS * BS), i = (e / BS) % BS, l = e % BS;
+			const int g0 = (half ? Q : P) * BS;
+			ldg[it] = __ldcg(prev + (long long)(g0 + i) * kp + g0 + l);
+		}
+#pragma unroll
+		for (int it = 0; it < NL; it++) {
+			const int e = it * kThreads + tid, i = e / MS, l = e % MS;
+			mr[i * LD + l] = la[it].x;
+			mi[i * LD + l] = la[it].y;
+			sh.pl[2][i * LD + l] = lqa[it].x;
+			sh.pl[3][i * LD + l] = lqa[it].y;
+			sh.pl[4][i * LD + l] = lqb[it].x;
+			sh.pl[5][i * LD + l] = lqb[it].y;
+		}
+		__syncthreads();
+		float cr[2][2], ci[2][2];
+		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);
+		__syncthreads();
+#pragma unroll
+		for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc32(bb, h, row, col);
+				mr[row * LD + col] = cr[bb][h];
+				mi[row * LD + col] = ci[bb][h];
+			}
+		__syncthreads();
+		cgemm32(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
+		__syncthreads();
+#pragma unroll
+		for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc32(bb, h, row, col);
+				if ((row >> 4) == hP && (col >> 4) == hQ) {
+					const int i = row & (BS - 1), l = BS + (col & (BS - 1));
+					mr[i * LD + l] = cr[bb][h];
+					mi[i * LD + l] = ci[bb][h];
+					mr[l * LD + i] = cr[bb][h];
+					mi[l * LD + i] = -ci[bb][h];
+				}
+			}
+#pragma unroll
+		for (int it = 0; it < ND; it++) {
+			const int e = it * kThreads + tid;
+			const int half = e / (BS * BS), i = (e / BS) % BS, l = e % BS;
+			mr[(half * BS + i) * LD + half * BS + l] = ldg[it].x;
+			mi[(half * BS + i) * LD + half * BS + l] = ldg[it].y;
+		}
+	}
+	for (int e = tid; e < MS * MS; e += kThreads) {
+		const int i = e / MS, l = e % MS;
+		sh.pl[2][i * LD + l] = (i == l) ? 1.f : 0.f;
+		sh.pl[3][i * LD + l] = 0.f;
+	}
+	__syncthreads();
+	inner_sweep32(sh, rr % kFullEvery == 0);
+	float2* Qg = Qout + (size_t)j * MS * MS;
+	for (int e = tid; e < MS * MS; e += kThreads) {
+		const int i = e / MS, l = e % MS;
+		Qg[e] = make_float2(sh.pl[2][i * LD + l], sh.pl[3][i * LD + l]);
+		out[(long long)gidx(i, P, Q) * kp + gidx(l, P, Q)] = make_float2(mr[i * LD + l], mi[i * LD + l]);
+	}
+	__syncthreads();
+}
+
+// Phase 2 item w of round ro (bjacobi.cu phase2_item in FP32).
+__device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int kp, const float2* src, float2* dst,
+		float2* V, const float2* Qr) {
+	const int tid = threadIdx.x;
+	const int nA2 = np * (np - 1);
+	float cr[2][2], ci[2][2];
+	if (w < nA2) {
+		const int jr = w / (np - 1);
+		int jc = w % (np - 1);
+		if (jc >= jr) jc++;
+		const int Pr = rr_player(jr, ro, nb), Qr_ = rr_player(nb - 1 - jr, ro, nb);
+		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const float2 v = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
+			sh.pl[0][i * LD + l] = v.x;
+			sh.pl[1][i * LD + l] = v.y;
+		}
+		load_q32(sh.pl[2], sh.pl[3], Qr + (size_t)jr * MS * MS);
+		load_q32(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
+		__syncthreads();
+		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
+		__syncthreads();
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc32(b, h, row, col);
+				sh.pl[0][row * LD + col] = cr[b][h];
+				sh.pl[1][row * LD + col] = ci[b][h];
+			}
+		__syncthreads();
+		cgemm32(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);  // Qr^H T
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc32(b, h, row, col);
+				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
+			}
+	} else {
+		const int v = w - nA2;
+		const int rb = v / np, jc = v % np;
+		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
+		for (int e = tid; e < MS * MS; e += kThreads) {
+			const int i = e / MS, l = e % MS;
+			const float2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
+			sh.pl[0][i * LD + l] = x.x;
+			sh.pl[1][i * LD + l] = x.y;
+		}
+		load_q32(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
+		__syncthreads();
+		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
+#pragma unroll
+		for (int b = 0; b < 2; b++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				int row, col;
+				acc_rc32(b, h, row, col);
+				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
+			}
+	}
+	__syncthreads();
+}
+
+// The cooperative solve: bjacobi_kernel of bjacobi.cu in FP32. A_r lives in
+// bufs[(r + 1) % 3] (A_{-1} = the input in A0); Q_r in Qbuf + (r & 1) * np * MS^2.
+__global__ void __launch_bounds__(kThreads, 2) bjacobi32_kernel(float2* A0, float2* A1, float2* A2, float2* V,
+		float2* Qbuf, int kp, int max_sweeps, double tau_final, int* counters, unsigned long long* tmaxg) {
+	cg::grid_group grid = cg::this_grid();
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	Shared32& sh = *reinterpret_cast<Shared32*>(smem_raw);
+	const int tid = threadIdx.x;
+	const int nb = kp / BS;
+	const int np = nb / 2;
+	const int rounds = nb - 1;
+	const int nrb = kp / MS;
+	const int nW = np * (np - 1) + nrb * np;
+	float2* const bufs[3] = {A0, A1, A2};
+	const size_t qstride = (size_t)np * MS * MS;
+	const bool split = (int)gridDim.x > np;
+	const int p1 = split ? np : (int)gridDim.x;
+	const int p2first = split ? np : 0;
+	const int p2count = split ? (int)gridDim.x - np : (int)gridDim.x;
+	if (tid == 0) {
+		sh.cnt = 0;
+		sh.tmax = 0ULL;
+	}
+	__syncthreads();
+	int sweep = 0;
+	bool stop = false, converged = false;
+	long long t = 0;
+	for (;;) {
+		const bool do_p1 = !stop;
+		const bool do_p2 = t >= 1;
+		if (do_p1 && (int)blockIdx.x < p1) {
+			const float2* prev = bufs[t % 3];
+			const float2* prev2 = bufs[(t + 2) % 3];
+			float2* out = bufs[(t + 1) % 3];
+			for (int j = blockIdx.x; j < np; j += p1)
+				phase1_item32(sh, j, t, rounds, nb, np, kp, prev, prev2, Qbuf + ((t + 1) & 1) * qstride,
+						Qbuf + (t & 1) * qstride, out);
+		}
+		if (do_p2 && (int)blockIdx.x >= p2first) {
+			const int ro = (int)((t - 1) % rounds);
+			const float2* src = bufs[(t + 2) % 3];
+			float2* dst = bufs[t % 3];
+			for (int w = (int)blockIdx.x - p2first; w < nW; w += p2count)
+				phase2_item32(sh, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+		}
+		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
+		if (sweep_end && tid == 0) {
+			if (sh.cnt) atomicAdd(&counters[sweep], sh.cnt);
+			if (sh.tmax) atomicMax(&tmaxg[sweep], sh.tmax);
+			sh.cnt = 0;
+			sh.tmax = 0ULL;
+		}
+		grid.sync();
+		if (!do_p1) break;
+		if (sweep_end) {
+			const int cnt = *((volatile int*)&counters[sweep]);
+			const double tm = __longlong_as_double((long long)*((volatile unsigned long long*)&tmaxg[sweep]));
+			if (cnt == 0 || tm < tau_final) {
+				converged = true;
+				stop = true;
+			}
+			sweep++;
+			if (sweep >= max_sweeps) stop = true;
+		}
+		t++;
+	}
+	if (blockIdx.x == 0 && tid == 0) {
+		counters[max_sweeps] = converged ? sweep : -1;
+		counters[max_sweeps + 1] = (int)(t % 3);
+	}
+}
+
+// S (k x k, FP64) into the FP32 work matrix A (kp x kp, zero padded) and V = I.
+__global__ void narrow_init_kernel(const double2* __restrict__ S, int k, int kp, float2* A, float2* V) {
+	const long long n = (long long)kp * kp;
+	for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+			idx += (long long)gridDim.x * blockDim.x) {
+		const int i = (int)(idx / kp), j = (int)(idx % kp);
+		const double2 s = (i < k && j < k) ? S[(long long)i * k + j] : make_double2(0.0, 0.0);
+		A[idx] = make_float2((float)s.x, (float)s.y);
+		V[idx] = make_float2(i == j ? 1.f : 0.f, 0.f);
+	}
+}
+
+// The FP32 result widened into the FP64 work matrices the sort and the W build
+// read: the diagonal of the final A into A0 (whose result index becomes 0) and
+// V into the FP64 V.
+__global__ void widen_result_kernel(const float2* A0f, const float2* A1f, const float2* A2f, const float2* Vf,
+		int kp, int* counters, int max_sweeps, double2* A0, double2* V) {
+	const int which = counters[max_sweeps + 1];
+	const float2* A = which == 0 ? A0f : (which == 1 ? A1f : A2f);
+	const long long n = (long long)kp * kp;
+	for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+			idx += (long long)gridDim.x * blockDim.x) {
+		const float2 v = Vf[idx];
+		V[idx] = make_double2(v.x, v.y);
+		const int i = (int)(idx / kp), j = (int)(idx % kp);
+		if (i == j) A0[idx] = make_double2(A[idx].x, 0.0);
+	}
+}
+
+__global__ void set_result_index_kernel(int* counters, int max_sweeps) { counters[max_sweeps + 1] = 0; }
+
+}  // namespace
+
+cudaError_t launch_bjacobi32(const double2* S, int k, JacobiWork& w, int num_sms, cudaStream_t s) {
+	const int kp = bjacobi_padded(k);
+	const long long n = (long long)kp * kp;
+	const unsigned gblocks = (unsigned)std::min<long long>((n + 255) / 256, 4096);
+	narrow_init_kernel<<<gblocks, 256, 0, s>>>(S, k, kp, w.f32.A0, w.f32.V);
+	const size_t smem = sizeof(Shared32);
+	cudaError_t e = cudaFuncSetAttribute(bjacobi32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	if (e != cudaSuccess) return e;
+	int per_sm = 0;
+	e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bjacobi32_kernel, kThreads, smem);
+	if (e != cudaSuccess) return e;
+	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+	const int blocks = num_sms * std::min(per_sm, 2);
+	int kpv = kp, ms = w.max_sweeps;
+	double tau = w.tau_final > 0.0 ? w.tau_final : 1e-3;
+	int* counters = w.counters;
+	unsigned long long* tmax = reinterpret_cast<unsigned long long*>(counters + jacobi_tmax_offset(ms));
+	float2 *a0 = w.f32.A0, *a1 = w.f32.A1, *a2 = w.f32.A2, *v = w.f32.V, *q = w.f32.Qbuf;
+	void* args[] = {&a0, &a1, &a2, &v, &q, &kpv, &ms, &tau, &counters, &tmax};
+	e = cudaLaunchCooperativeKernel((void*)bjacobi32_kernel, dim3(blocks), dim3(kThreads), args, smem, s);
+	if (e != cudaSuccess) return e;
+	widen_result_kernel<<<gblocks, 256, 0, s>>>(w.f32.A0, w.f32.A1, w.f32.A2, w.f32.V, kp, w.counters, ms, w.A0,
+			w.V);
+	set_result_index_kernel<<<1, 1, 0, s>>>(w.counters, ms);
+	return cudaGetLastError();
+}
+
+}  // namespace itp2d

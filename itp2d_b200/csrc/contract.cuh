@@ -55,6 +55,17 @@ struct JacobiWork {
 	// 0 selects the FP64 default of the kernel. The remaining off-diagonal
 	// elements are then of order tau_final^2 relative to the eigenvalue gaps.
 	double tau_final = 0.0;
+	// FP32 block path (launch_bjacobi32): set, with k >= kBlockJacobiMinK, the
+	// solve runs in single precision on these kp x kp buffers and widens its
+	// result into A0 (diagonal) and V. They may alias A1, A2 and Qbuf, which
+	// that path does not use otherwise; none may alias A0 or V.
+	struct F32 {
+		float2* A0 = nullptr;
+		float2* A1 = nullptr;
+		float2* A2 = nullptr;
+		float2* V = nullptr;
+		float2* Qbuf = nullptr;  // bjacobi_qbuf_elems(k) elements
+	} f32;
 };
 
 // Smallest k solved by block Jacobi (when JacobiWork::Qbuf is set).
@@ -67,6 +78,10 @@ size_t bjacobi_qbuf_elems(int k);
 int jacobi_kp(const JacobiWork& w, int k);
 cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* A2, double2* V, double2* Qbuf, int kp,
 		int max_sweeps, double tau_final, int* counters, int num_sms, cudaStream_t s);
+// Single-precision block Jacobi of S (k x k, FP64) on w.f32; leaves the
+// eigenvalues on the diagonal of w.A0, the eigenvectors in w.V and the result
+// fields of w.counters as the FP64 path does (result index 0).
+cudaError_t launch_bjacobi32(const double2* S, int k, JacobiWork& w, int num_sms, cudaStream_t s);
 
 // Eigen-decomposition of the Hermitian S (k x k, row-major, full storage) by
 // parallel cyclic Jacobi, then W[:, n] = V[:, p(n)] / sqrt(l_n) with l

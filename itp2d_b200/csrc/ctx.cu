@@ -984,6 +984,17 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		// 1e-3 leaves off-diagonal elements of about 1e-6, below that (measured
 		// on the magnetic dot: one more FP32 iteration, 3% less solve time)
 		c->jw.tau_final = f64 ? 0.0 : 1e-3;
+		// FP32 states also solve in FP32, on views of the FP64 buffers the block
+		// path leaves free (A1 holds two FP32 matrices, A2 two more)
+		c->jw.f32 = {};
+		if (!f64 && c->jw.Qbuf && c->jw.A2) {
+			const size_t kp2 = (size_t)bjacobi_padded(c->k) * bjacobi_padded(c->k);
+			c->jw.f32.A0 = (float2*)c->jw.A1;
+			c->jw.f32.A1 = c->jw.f32.A0 + kp2;
+			c->jw.f32.A2 = (float2*)c->jw.A2;
+			c->jw.f32.V = c->jw.f32.A2 + kp2;
+			c->jw.f32.Qbuf = (float2*)c->jw.Qbuf;
+		}
 		ITP2D_TRY(launch_eigensolve(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
 		c->launches += 6;
 	}

@@ -404,11 +404,17 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 	const long long n = (long long)kp * kp;
 	cudaError_t e = cudaMemsetAsync(w.counters, 0, jacobi_counters(w.max_sweeps) * sizeof(int), s);
 	if (e != cudaSuccess) return e;
-	jacobi_init_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(S, k, kp, w.A0, w.V);
-	if (w.Qbuf && w.A2 && k >= kBlockJacobiMinK) {
+	if (w.f32.A0 && w.Qbuf && w.A2 && k >= kBlockJacobiMinK) {
+		e = launch_bjacobi32(S, k, w, num_sms, s);
+		if (e != cudaSuccess) return e;
+	} else if (w.Qbuf && w.A2 && k >= kBlockJacobiMinK) {
+		jacobi_init_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(S, k, kp, w.A0,
+				w.V);
 		e = launch_bjacobi(w.A0, w.A1, w.A2, w.V, w.Qbuf, kp, w.max_sweeps, w.tau_final, w.counters, num_sms, s);
 		if (e != cudaSuccess) return e;
 	} else {
+		jacobi_init_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, s>>>(S, k, kp, w.A0,
+				w.V);
 		int per_sm = 0;
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi_kernel, kThreads, 0);
 		if (e != cudaSuccess) return e;
