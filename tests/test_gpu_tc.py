@@ -89,35 +89,35 @@ def test_rotation_tensor_cores(sx, sy, k):
     assert np.median(diff) < 1e-4
 
 
-def test_fp32_block_jacobi_matches_fp64_precision():
+def test_fp32_block_jacobi_canonical():
     """k >= 256: the FP32 form solves the overlap eigenproblem by block Jacobi
-    in single precision (stopping at a rotation tangent of 1e-3); the states
-    it produces match the FP64 form's orthonormalisation of the same states."""
+    in single precision (stopping at a rotation tangent of 1e-3). The result is
+    the canonical orthonormalisation Psi' = Psi V L^{-1/2} of stateset.cpp:136-232
+    up to the FP32 accuracy: with M = Psi'^H Psi dx^2 = L^{1/2} V^H, M M^H is
+    diagonal and its diagonal holds the eigenvalues of S. These checks do not
+    depend on the gaps between eigenvalues (the eigenvectors themselves do)."""
     sx = sy = 128
     k = 320
     c, dx = _ctx(sx, sy, k, seed=11)
-    psi0 = c.download()
+    psi0 = c.download().reshape(k, -1)
+    S = (psi0.conj() @ psi0.T) * dx * dx
+    S0 = np.abs(S - np.diag(np.diag(S))) / np.sqrt(np.outer(np.diag(S).real, np.diag(S).real))
     c.orthonormalize()
     out = c.download().reshape(k, -1)
     O = (out.conj() @ out.T) * dx * dx
     dev = np.max(np.abs(O - np.eye(k)))
-    print(f"FP32 block Jacobi k={k}: orthonormality {dev:.2e}")
+    M = (out.conj() @ psi0.T) * dx * dx
+    MM = M @ M.conj().T
+    lam = np.diag(MM).real
+    off = np.max(np.abs(MM - np.diag(lam)) / np.sqrt(np.outer(lam, lam)))
+    ev = np.linalg.eigvalsh(S)
+    lam_err = np.max(np.abs(lam - ev) / ev)
+    print(f"FP32 block Jacobi k={k}: orthonormality {dev:.2e}, off-diagonal {np.max(S0):.1e} -> {off:.2e}, "
+          f"eigenvalues {lam_err:.2e}")
     assert dev < TOL_ORTHO
-    c64 = capi.Context(sx, sy, dx, k, precision=capi.FP64)
-    c64.upload(psi0.reshape(k, sy, sx))
-    c64.orthonormalize()
-    ref = c64.download().reshape(k, -1)
-    phase = np.sum(ref.conj() * out, axis=1)
-    phase /= np.abs(phase)
-    diff = np.linalg.norm(out - phase[:, None] * ref, axis=1) / np.linalg.norm(ref, axis=1)
-    print(f"FP32 block Jacobi k={k}: median / max state difference to FP64 {np.median(diff):.2e} / "
-          f"{np.max(diff):.2e}")
-    assert np.median(diff) < 1e-4
-    # the span is the same whatever the eigenvector errors of close overlap
-    # eigenvalues: the FP64 states project onto the FP32 set
-    coef = (out.conj() @ ref.T) * dx * dx
-    resid = ref - coef.T @ out
-    assert np.max(np.linalg.norm(resid, axis=1) / np.linalg.norm(ref, axis=1)) < 1e-4
+    assert np.all(np.diff(lam) > -1e-4 * lam[1:])  # ascending, as the sort leaves them
+    assert off < 1e-4
+    assert lam_err < 1e-4
 
 
 def test_tensor_core_solve_matches_fp64_engine():
