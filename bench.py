@@ -144,7 +144,10 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
     torch.cuda.synchronize()
     # timed: inputs resident in HBM (the reset that uploads them is outside)
     times, steps, conv, lat = [], [], [], []
-    p0, l0, w0 = phases(), L.itp2d_launch_count(ctx), L.itp2d_total_sweeps(ctx)
+    def sweeps():
+        return {prec: L.itp2d_precision_sweeps(ctx, code) for prec, code in (("fp64", capi.FP64), ("fp32", capi.FP32))}
+
+    p0, l0, w0 = phases(), L.itp2d_launch_count(ctx), sweeps()
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -158,7 +161,7 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
         steps.append(s.total_steps)
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
-    p1, l1, w1 = phases(), L.itp2d_launch_count(ctx), L.itp2d_total_sweeps(ctx)
+    p1, l1, w1 = phases(), L.itp2d_launch_count(ctx), sweeps()
     # per solve: {(precision, phase): (ms, calls)}
     stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
@@ -174,7 +177,8 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
         L.itp2d_system_download_states(s.h, e2e_buf.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    return dict(times=times, steps=steps, conv=conv, stats=stats, sweeps=(w1 - w0) / K, launches=(l1 - l0) / K,
+    return dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
+                launches=(l1 - l0) / K,
                 E=E, converged_mask=None, e2e_times=e2e_times, system=s)
 
 
@@ -238,7 +242,7 @@ def config_block(form):
 # DRAM bytes (read + write) per launch of the phase's dominant kernel, from one ncu
 # capture of `python bench.py --steps 1 --warmup 1 --form mixed` (profiles/
 # bjacobi_regfft_tc_magnetic_dot_256_k500.md): block Jacobi 8.44 + 2.80 MB.
-PROFILED_TRAFFIC = {"eigensolve": 11.24e6}
+PROFILED_TRAFFIC = {"eigensolve_fp64": 11.24e6}
 
 
 def max_over_ranks(x, dist, device):
@@ -260,7 +264,7 @@ def replica_rate(conv, tsum, n, world, dist, device):
     return conv * world / per_solve, per_solve
 
 
-def phase_rooflines(r, fp64_peak):
+def phase_rooflines(r, fp64_peak, fp32_peak):
     """Roofline of each phase of one form, per solve and per precision.
 
     Algorithmic work per call:
@@ -273,7 +277,8 @@ def phase_rooflines(r, fp64_peak):
                  per (128 states x 128 grid points) output tile
       eigensolve block Jacobi: per sweep (kp/16 - 1) rounds of 32 x 32 block
                  unitaries applied to both sides of the kp x kp matrix and to the
-                 eigenvector matrix, 3 * 8 * 32 * kp^2 flops per round (DMMA)
+                 eigenvector matrix, 3 * 8 * 32 * kp^2 flops per round (DMMA for
+                 FP64 states, FFMA for FP32 states)
     """
     w = WORKLOAD
     k, G, m = w["num_states"], w["sx"] * w["sy"], w["halforder"]
@@ -314,12 +319,15 @@ def phase_rooflines(r, fp64_peak):
             out[f"{ph}_{prec}"] = {"bound": "hbm" if bound == "hbm" else "tensor", "achieved": ach, "peak": peak,
                                    "unit": unit, "frac": ach / peak, "ms_per_solve": ms, "calls_per_solve": calls,
                                    "peak_source": psrc}
-    ms = r["stats"][("fp64", "eigensolve")][0] + r["stats"][("fp32", "eigensolve")][0]
-    calls = r["stats"][("fp64", "eigensolve")][1] + r["stats"][("fp32", "eigensolve")][1]
-    ach = sweep_flops * r["sweeps"] / (ms * 1e-3) / 1e12
-    out["eigensolve"] = {"bound": "tensor", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": ach / fp64_peak, "ms_per_solve": ms, "calls_per_solve": calls,
-                         "sweeps_per_solve": r["sweeps"], "peak_source": "FP64 DMMA measured in-run"}
+    for prec, peak, bound, psrc in (("fp64", fp64_peak, "tensor", "FP64 DMMA measured in-run"),
+                                    ("fp32", fp32_peak, "fp32", "FP32 FFMA measured in-run")):
+        ms, calls = r["stats"][(prec, "eigensolve")]
+        if calls == 0:
+            continue
+        ach = sweep_flops * r["sweeps"][prec] / (ms * 1e-3) / 1e12
+        out[f"eigensolve_{prec}"] = {"bound": bound, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                                     "frac": ach / peak, "ms_per_solve": ms, "calls_per_solve": calls,
+                                     "sweeps_per_solve": r["sweeps"][prec], "peak_source": psrc}
     return out
 
 
@@ -358,6 +366,7 @@ def main():
     e2e_pin = _t.empty(2 * k * G, dtype=_t.float64, pin_memory=True)
     e2e_buf = e2e_pin.numpy()
     fp64_peak = capi.device_fp64_peak()
+    fp32_peak = capi.device_fp32_peak()
 
     results = {}
     with torch.cuda.stream(stream):
@@ -397,7 +406,7 @@ def main():
             forms["mixed"]["max_abs_dE_vs_fp64_wanted"] = float(
                 np.max(np.abs(rmx["E"][:w["wanted"]] - r64["E"][:w["wanted"]])))
 
-    roof = phase_rooflines(rh, fp64_peak)
+    roof = phase_rooflines(rh, fp64_peak, fp32_peak)
     dom = max(roof, key=lambda n: roof[n]["ms_per_solve"])
     roofline = {key: roof[dom][key] for key in ("bound", "achieved", "peak", "unit", "frac")}
     roofline.update({"traffic": PROFILED_TRAFFIC.get(dom), "kernel": dom, "peak_source": roof[dom]["peak_source"]})
@@ -432,7 +441,8 @@ def main():
         "phases": roof,
     }
     if r64 and rmx:
-        out["phases_other_form"] = phase_rooflines(results["fp64" if head == "mixed" else "mixed"], fp64_peak)
+        out["phases_other_form"] = phase_rooflines(results["fp64" if head == "mixed" else "mixed"], fp64_peak,
+                                                  fp32_peak)
     if rank == 0:
         print(json.dumps(out))
     if dist:

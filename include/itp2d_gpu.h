@@ -173,6 +173,9 @@ int itp2d_phase_stats(itp2d_ctx* ctx, double* ms10, long long* calls10);
  * since the context was created. */
 int itp2d_last_sweeps(itp2d_ctx* ctx);
 long long itp2d_total_sweeps(itp2d_ctx* ctx);
+/* Jacobi sweeps of the orthonormalisations run on states of one precision
+ * (ITP2D_FP64 or ITP2D_FP32); -1 for another value. */
+long long itp2d_precision_sweeps(itp2d_ctx* ctx, int precision);
 
 /* Eigen-decomposition of an n x n complex Hermitian matrix on the device,
  * the drop-in for EigenSolver::solve (ZHEEV("V","U"), eigensolver.hpp:80-84).
@@ -204,6 +207,9 @@ int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double* evals, do
  * TFLOP/s with a register-only kernel: the roofline denominator of the FP64
  * contractions. Diagnostic; no reference counterpart. */
 int itp2d_device_fp64_peak(double* tflops);
+/* The same for FP32 FFMA throughput (CUDA cores): the roofline denominator of
+ * the single-precision eigensolver. Diagnostic; no reference counterpart. */
+int itp2d_device_fp32_peak(double* tflops);
 
 /* Short description of a status code. */
 const char* itp2d_status_string(int status);

@@ -77,6 +77,9 @@ def lib():
         L.itp2d_last_sweeps.argtypes = [vp]
         L.itp2d_total_sweeps.argtypes = [vp]
         L.itp2d_total_sweeps.restype = C.c_longlong
+        L.itp2d_precision_sweeps.argtypes = [vp, i]
+        L.itp2d_precision_sweeps.restype = C.c_longlong
+        L.itp2d_device_fp32_peak.argtypes = [dp]
         L.itp2d_hermitian_eigensolve.argtypes = [i, dp, dp, dp]
         L.itp2d_device_fp64_peak.argtypes = [dp]
         L.itp2d_status_string.argtypes = [i]
@@ -92,6 +95,13 @@ def _dp(a):
 def _check(st, what):
     if st != OK:
         raise ITP2DError(st, what)
+
+
+def device_fp32_peak() -> float:
+    """Measured FP32 FFMA TFLOP/s of the current device."""
+    t = C.c_double(0.0)
+    _check(lib().itp2d_device_fp32_peak(C.byref(t)), "itp2d_device_fp32_peak")
+    return t.value
 
 
 def device_fp64_peak() -> float:

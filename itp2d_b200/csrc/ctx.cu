@@ -86,6 +86,7 @@ struct itp2d_ctx {
 	double* dnorm = nullptr;
 	int last_sweeps = 0;
 	long long sweeps_total = 0;
+	long long sweeps_p[2] = {0, 0};  // by precision: FP64, FP32
 	int engine = ITP2D_CONTRACT_AUTO;
 	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
 	int* dflag = nullptr;  // tensor-core wait time-outs (device)
@@ -1013,7 +1014,10 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
 	const EigStatus s = *c->hstat;
 	c->last_sweeps = s.sweeps;
-	if (s.sweeps > 0) c->sweeps_total += s.sweeps;
+	if (s.sweeps > 0) {
+		c->sweeps_total += s.sweeps;
+		c->sweeps_p[f64 ? 0 : 1] += s.sweeps;
+	}
 	if (tc && *c->hflag != ITP2D_OK) {
 		const int f = *c->hflag;
 		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
@@ -1091,6 +1095,10 @@ int itp2d_phase_stats(itp2d_ctx* c, double* ms10, long long* calls10) {
 int itp2d_last_sweeps(itp2d_ctx* c) { return c ? c->last_sweeps : -1; }
 
 long long itp2d_total_sweeps(itp2d_ctx* c) { return c ? c->sweeps_total : -1; }
+long long itp2d_precision_sweeps(itp2d_ctx* c, int precision) {
+	if (!c || (precision != ITP2D_FP64 && precision != ITP2D_FP32)) return -1;
+	return c->sweeps_p[precision == ITP2D_FP64 ? 0 : 1];
+}
 
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs) {
 	if (n < 1 || !A || !evals || !evecs) return ITP2D_E_INVALID;
