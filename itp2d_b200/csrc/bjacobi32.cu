@@ -30,7 +30,10 @@ namespace {
 constexpr int BS = 16;        // block size
 constexpr int MS = 32;        // subproblem size: two blocks
 constexpr int NR = MS / 2;    // rotations per inner round
-constexpr int LD = MS + 1;    // padded row length (floats)
+// Row pitch 48 floats: rows p and p + 1 fall 16 banks apart, so the half-warps
+// of the cross-pair updates (consecutive p, 16 consecutive columns) and of the
+// block products (two consecutive rows per warp) never share a bank.
+constexpr int LD = 48;
 constexpr int PL = MS * LD;   // floats per plane
 constexpr int kThreads = 256;
 constexpr int kFullEvery = 16;
@@ -45,8 +48,9 @@ __device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * B
 
 struct Shared32 {
 	float pl[6][PL];  // [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
-	float rs[NR], rtau[NR], rer[NR], rei[NR], rap[NR], raq[NR];
-	int rp[NR], rq[NR], rrot[NR];
+	float4 rot[NR];   // rotation j: (sin, tau, Re e, Im e)
+	float rap[NR], raq[NR];
+	int rpq[NR];      // p | q << 8 | applied << 16
 	int cnt;
 	unsigned long long tmax;  // bits of a non-negative double
 };
@@ -61,10 +65,7 @@ __device__ void inner_rotation32(Shared32& sh, int j, int p, int q, int& cnt, fl
 	const float cr = mr[p * LD + q], ci = mi[p * LD + q];
 	const float c2 = cr * cr + ci * ci;
 	const float scale2 = fabsf(a) * fabsf(b);
-	sh.rp[j] = p;
-	sh.rq[j] = q;
-	sh.rrot[j] = 0;
-	sh.rs[j] = 0.f; sh.rtau[j] = 0.f; sh.rer[j] = 1.f; sh.rei[j] = 0.f; sh.rap[j] = a; sh.raq[j] = b;
+	sh.rpq[j] = p | q << 8;
 	if (!(c2 > 0.f && c2 > kSkipRel * kSkipRel * scale2)) return;
 	const float d = 0.5f * (b - a);
 	const float ad = fabsf(d);
@@ -76,13 +77,10 @@ __device__ void inner_rotation32(Shared32& sh, int j, int p, int q, int& cnt, fl
 	const float t = __fdividef(cabs, un);
 	const float ic = rsqrtf(c2);
 	const float sg = d < 0.f ? -1.f : 1.f;
-	sh.rs[j] = sg * cabs * qn;
-	sh.rtau[j] = sg * __fdividef(cabs, wn * qn + un);
-	sh.rer[j] = cr * ic;
-	sh.rei[j] = ci * ic;
+	sh.rot[j] = make_float4(sg * cabs * qn, sg * __fdividef(cabs, wn * qn + un), cr * ic, ci * ic);
 	sh.rap[j] = a - sg * t * cabs;
 	sh.raq[j] = b + sg * t * cabs;
-	sh.rrot[j] = 1;
+	sh.rpq[j] = p | q << 8 | 1 << 16;
 	if (c2 > kNoiseRel * kNoiseRel * scale2) {
 		cnt++;
 		tmax = fmaxf(tmax, t);
@@ -127,9 +125,10 @@ __device__ void inner_sweep32(Shared32& sh, bool full) {
 		__syncthreads();
 		for (int e = tid; e < NR * NR; e += kThreads) {
 			const int ja = e / NR, jb = e % NR;
-			const bool ra = sh.rrot[ja], rb = sh.rrot[jb];
+			const int pa = sh.rpq[ja], pb = sh.rpq[jb];
+			const bool ra = pa >> 16, rb = pb >> 16;
 			if (!ra && !rb) continue;
-			const int p = sh.rp[ja], q = sh.rq[ja], s2 = sh.rp[jb], t2 = sh.rq[jb];
+			const int p = pa & 255, q = (pa >> 8) & 255, s2 = pb & 255, t2 = (pb >> 8) & 255;
 			if (ja == jb) {
 				mr[p * LD + p] = sh.rap[ja]; mi[p * LD + p] = 0.f;
 				mr[q * LD + q] = sh.raq[ja]; mi[q * LD + q] = 0.f;
@@ -140,22 +139,26 @@ __device__ void inner_sweep32(Shared32& sh, bool full) {
 			float psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
 			float qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
 			if (ra) {
-				rows2f(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
-				rows2f(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
+				const float4 R = sh.rot[ja];
+				rows2f(R.x, R.y, R.z, R.w, psr, psi, qsr, qsi);
+				rows2f(R.x, R.y, R.z, R.w, ptr, pti, qtr, qti);
 			}
 			if (rb) {
-				cols2f(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
-				cols2f(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
+				const float4 R = sh.rot[jb];
+				cols2f(R.x, R.y, R.z, R.w, psr, psi, ptr, pti);
+				cols2f(R.x, R.y, R.z, R.w, qsr, qsi, qtr, qti);
 			}
 			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
 			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
 		}
 		for (int e = tid; e < MS * NR; e += kThreads) {
 			const int i = e / NR, j = e % NR;
-			if (!sh.rrot[j]) continue;
-			const int p = sh.rp[j], q = sh.rq[j];
+			const int pj = sh.rpq[j];
+			if (!(pj >> 16)) continue;
+			const int p = pj & 255, q = (pj >> 8) & 255;
 			float ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
-			cols2f(sh.rs[j], sh.rtau[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
+			const float4 R = sh.rot[j];
+			cols2f(R.x, R.y, R.z, R.w, ysr, ysi, ytr, yti);
 			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 		}
 		__syncthreads();
@@ -173,36 +176,56 @@ __device__ void inner_sweep32(Shared32& sh, bool full) {
 	}
 }
 
-// acc = A B for 32 x 32 complex operands given as plane pairs, FFMA. Thread
-// outputs: row (warp >> 1) * 8 + (lane >> 2), columns (warp & 1) * 16 + b * 8 +
-// 2 * (lane & 3) + h. A element (i, m) at a_re[i * as_i + m * as_m], B element
-// (m, l) at b_re[m * LD + l]; conjA conjugates A.
-__device__ __forceinline__ void acc_rc32(int b, int h, int& row, int& col) {
+// Complex products of 32-deep operands given as plane pairs, FFMA: the thread
+// accumulates rows row0 + r * rstep (r < NRW) by columns col0 + c * cstep
+// (c < NCL). A element (i, m) at a_re[i * as_i + m * as_m], B element (m, l)
+// at b_re[m * LD + l]; conjA conjugates A.
+template <int NRW, int NCL>
+__device__ __forceinline__ void cmm32(const float* ar, const float* ai, int as_i, int as_m, bool conjA,
+		const float* br, const float* bi, int row0, int rstep, int col0, int cstep, float (&cr)[NRW][NCL],
+		float (&ci)[NRW][NCL]) {
+#pragma unroll
+	for (int r = 0; r < NRW; r++)
+#pragma unroll
+		for (int c = 0; c < NCL; c++) cr[r][c] = ci[r][c] = 0.f;
+#pragma unroll 4
+	for (int m = 0; m < MS; m++) {
+		float xr[NRW], xi[NRW], yr[NCL], yi[NCL];
+#pragma unroll
+		for (int r = 0; r < NRW; r++) {
+			const int o = (row0 + r * rstep) * as_i + m * as_m;
+			xr[r] = ar[o];
+			xi[r] = conjA ? -ai[o] : ai[o];
+		}
+#pragma unroll
+		for (int c = 0; c < NCL; c++) {
+			yr[c] = br[m * LD + col0 + c * cstep];
+			yi[c] = bi[m * LD + col0 + c * cstep];
+		}
+#pragma unroll
+		for (int r = 0; r < NRW; r++)
+#pragma unroll
+			for (int c = 0; c < NCL; c++) {
+				cr[r][c] = fmaf(xr[r], yr[c], fmaf(-xi[r], yi[c], cr[r][c]));
+				ci[r][c] = fmaf(xr[r], yi[c], fmaf(xi[r], yr[c], ci[r][c]));
+			}
+	}
+}
+
+// Output (r, c) of a thread in the full 32 x 32 product: warp w owns rows
+// 4w .. 4w + 3; lane (h, l) = (lane >> 4, lane & 15) computes rows 4w + h and
+// 4w + 2 + h at columns l and l + 16.
+__device__ __forceinline__ void full_rc(int r, int c, int& row, int& col) {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	row = (warp >> 1) * 8 + (lane >> 2);
-	col = (warp & 1) * 16 + b * 8 + 2 * (lane & 3) + h;
+	row = 4 * warp + (lane >> 4) + 2 * r;
+	col = (lane & 15) + 16 * c;
 }
 
 __device__ __forceinline__ void cgemm32(const float* ar, const float* ai, int as_i, int as_m, bool conjA,
 		const float* br, const float* bi, float (&cr)[2][2], float (&ci)[2][2]) {
-	int row, col0;
-	acc_rc32(0, 0, row, col0);
-#pragma unroll
-	for (int b = 0; b < 2; b++) cr[b][0] = cr[b][1] = ci[b][0] = ci[b][1] = 0.f;
-#pragma unroll 8
-	for (int m = 0; m < MS; m++) {
-		const float xr = ar[row * as_i + m * as_m];
-		const float xi = conjA ? -ai[row * as_i + m * as_m] : ai[row * as_i + m * as_m];
-#pragma unroll
-		for (int b = 0; b < 2; b++)
-#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				const int l = col0 + b * 8 + h;
-				const float yr = br[m * LD + l], yi = bi[m * LD + l];
-				cr[b][h] = fmaf(xr, yr, fmaf(-xi, yi, cr[b][h]));
-				ci[b][h] = fmaf(xr, yi, fmaf(xi, yr, ci[b][h]));
-			}
-	}
+	int row0, col0;
+	full_rc(0, 0, row0, col0);
+	cmm32<2, 2>(ar, ai, as_i, as_m, conjA, br, bi, row0, 2, col0, 16, cr, ci);
 }
 
 __device__ void load_q32(float* qr, float* qi, const float2* Qg) {
@@ -268,35 +291,30 @@ __device__ void phase1_item32(Shared32& sh, int j, long long t, int rounds, int 
 			sh.pl[5][i * LD + l] = lqb[it].y;
 		}
 		__syncthreads();
-		float cr[2][2], ci[2][2];
-		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);
-		__syncthreads();
+		// only the (hP, hQ) quadrant of Q_a^H A_{t-2}(a, b) Q_b enters the
+		// subproblem: T = A_{t-2}(a, b) Q_b[:, hQ half] (32 x 16, two elements per
+		// thread), then C = Q_a[:, hP half]^H T (16 x 16, one per thread)
+		{
+			const int lane = tid & 31, warp = tid >> 5;
+			const int trow = 4 * warp + (lane >> 4), tcol = lane & 15;
+			float tr[2][1], ti[2][1];
+			cmm32<2, 1>(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], trow, 2, hQ * BS + tcol, 0, tr, ti);
+			__syncthreads();
 #pragma unroll
-		for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				int row, col;
-				acc_rc32(bb, h, row, col);
-				mr[row * LD + col] = cr[bb][h];
-				mi[row * LD + col] = ci[bb][h];
+			for (int r = 0; r < 2; r++) {
+				mr[(trow + 2 * r) * LD + tcol] = tr[r][0];
+				mi[(trow + 2 * r) * LD + tcol] = ti[r][0];
 			}
-		__syncthreads();
-		cgemm32(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
-		__syncthreads();
-#pragma unroll
-		for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				int row, col;
-				acc_rc32(bb, h, row, col);
-				if ((row >> 4) == hP && (col >> 4) == hQ) {
-					const int i = row & (BS - 1), l = BS + (col & (BS - 1));
-					mr[i * LD + l] = cr[bb][h];
-					mi[i * LD + l] = ci[bb][h];
-					mr[l * LD + i] = cr[bb][h];
-					mi[l * LD + i] = -ci[bb][h];
-				}
-			}
+			__syncthreads();
+			float cr[1][1], ci[1][1];
+			const int i = tid >> 4, l = tid & 15;
+			cmm32<1, 1>(sh.pl[2] + hP * BS, sh.pl[3] + hP * BS, 1, LD, true, sh.pl[0], sh.pl[1], i, 0, l, 0, cr, ci);
+			__syncthreads();
+			mr[i * LD + BS + l] = cr[0][0];
+			mi[i * LD + BS + l] = ci[0][0];
+			mr[(BS + l) * LD + i] = cr[0][0];
+			mi[(BS + l) * LD + i] = -ci[0][0];
+		}
 #pragma unroll
 		for (int it = 0; it < ND; it++) {
 			const int e = it * kThreads + tid;
@@ -349,7 +367,7 @@ __device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int k
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc32(b, h, row, col);
+				full_rc(b, h, row, col);
 				sh.pl[0][row * LD + col] = cr[b][h];
 				sh.pl[1][row * LD + col] = ci[b][h];
 			}
@@ -360,7 +378,7 @@ __device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int k
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc32(b, h, row, col);
+				full_rc(b, h, row, col);
 				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
 			}
 	} else {
@@ -381,7 +399,7 @@ __device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int k
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc32(b, h, row, col);
+				full_rc(b, h, row, col);
 				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
 			}
 	}
