@@ -229,8 +229,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // tile as its exchange area. Persistent; with NBUF = 2 the next tile is copied
 // in by cp.async while the current one is transformed (NBUF = 1 where two
 // tiles do not fit in shared memory).
+// FP32 lines of up to 256 points fit in 80 registers without spills: three
+// CTAs per SM (the shared-memory tiles allow three as well).
 template <class R, int A, int B, int NBUF>
-__global__ void __launch_bounds__(kThreads) col_reg_kernel(ColPassArgs a, int k) {
+__global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : 0)
+		col_reg_kernel(ColPassArgs a, int k) {
 	using T = c2<R>;
 	constexpr int N = A * B, W = kThreads / B, LD = W + 1, TS = N * LD;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -402,7 +405,8 @@ __global__ void __launch_bounds__(kThreads) energy_row_reg_kernel(EnergyRowArgs 
 // of one state, with the next tile's src copied in by cp.async while the
 // current one is transformed (NBUF = 2; NBUF = 1 where two tiles do not fit).
 template <class R, int A, int B, int NBUF>
-__global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs a, int k) {
+__global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : 0)
+		energy_col_reg_kernel(EnergyColArgs a, int k) {
 	using T = c2<R>;
 	constexpr int N = A * B, W = kThreads / B, LD = W + 1, TS = N * LD;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -470,15 +474,31 @@ __global__ void __launch_bounds__(kThreads) energy_col_reg_kernel(EnergyColArgs 
 		T* hout = a.h_out ? reinterpret_cast<T*>(a.h_out) + base : nullptr;
 		const double es = a.Eshift ? a.Eshift[state] : 0.0;
 		double s[5] = {0, 0, 0, 0, 0};
+		// the global loads of EB rows at once (the compiler cannot move them
+		// across the hout stores): one latency per EB rows instead of per row
+		constexpr int NE = N * W / kThreads, EB = NE < 8 ? NE : 8;
+		static_assert(NE % EB == 0, "epilogue batches");
 #pragma unroll
-		for (int it = 0; it < N * W / kThreads; it++) {
-			const int i = it * kThreads + threadIdx.x;
-			const int y = i / W, c = i - y * W;
-			if (c < ncols) {
+		for (int b0 = 0; b0 < NE; b0 += EB) {
+			T av[EB], pv[EB];
+#pragma unroll
+			for (int e = 0; e < EB; e++) {
+				const int i = (b0 + e) * kThreads + threadIdx.x;
+				const int y = i / W, c = i - y * W;
 				const long long off = (long long)y * sx + c;
-				const T h = cadd(tile[y * LD + c], add[off]);
-				if (hout) hout[off] = h;
-				if (a.sums) esums(s, psi[off], h, es);
+				av[e] = c < ncols ? add[off] : mk<R>(0, 0);
+				pv[e] = c < ncols ? psi[off] : mk<R>(0, 0);
+			}
+#pragma unroll
+			for (int e = 0; e < EB; e++) {
+				const int i = (b0 + e) * kThreads + threadIdx.x;
+				const int y = i / W, c = i - y * W;
+				if (c < ncols) {
+					const long long off = (long long)y * sx + c;
+					const T h = cadd(tile[y * LD + c], av[e]);
+					if (hout) hout[off] = h;
+					if (a.sums) esums(s, pv[e], h, es);
+				}
 			}
 		}
 		if (a.sums) reduce5(s, red, a.sums + ((size_t)state * nct + ct) * 5);
