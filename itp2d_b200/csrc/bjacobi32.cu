@@ -35,7 +35,10 @@ constexpr int NR = MS / 2;    // rotations per inner round
 // block products (two consecutive rows per warp) never share a bank.
 constexpr int LD = 48;
 constexpr int PL = MS * LD;   // floats per plane
-constexpr int kThreads = 256;
+// 512 threads, one CTA per SM: in an inner round, threads [0, 256) update the
+// 256 2 x 2 blocks of M while threads [256, 512) rotate the columns of Q.
+constexpr int kThreads = 512;
+constexpr int kMThreads = NR * NR;
 constexpr int kFullEvery = 16;
 constexpr float kSkipRel = 1e-7f;
 constexpr float kNoiseRel = 1e-6f;
@@ -47,26 +50,32 @@ __device__ __forceinline__ int rr_player(int pos, int r, int npos) {
 __device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * BS + i : Q * BS + (i - BS); }
 
 struct Shared32 {
-	float pl[6][PL];  // [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
-	float4 rot[NR];   // rotation j: (sin, tau, Re e, Im e)
-	float rap[NR], raq[NR];
-	int rpq[NR];      // p | q << 8 | applied << 16
+	// phase 1: [0,1] M, [2,3] Q, [4,5] formation operands; phase 2: half h of
+	// the CTA uses [6h, 6h + 6): X/T, Q_r, Q_c
+	float pl[12][PL];
+	// rotations of two consecutive inner rounds (round r in buffer r & 1)
+	float4 rot[2][NR];  // rotation j: (sin, tau, Re e, Im e)
+	float rap[2][NR], raq[2][NR];  // M(p, p), M(q, q) after the round
+	int rpq[2][NR];     // p | q << 8 | applied << 16
 	int cnt;
 	unsigned long long tmax;  // bits of a non-negative double
 };
 
-// Rotation of the local pair (p, q): with d = (b - a) / 2, r = sqrt(d^2 + |c|^2),
-// u = |d| + r and w = 2 r u: cos = u / sqrt(w), |sin| = |c| / sqrt(w),
-// tau = |sin| / (1 + cos), tan = |c| / u (the formulas of bjacobi.cu).
-__device__ void inner_rotation32(Shared32& sh, int j, int p, int q, int& cnt, float& tmax) {
-	const float* mr = sh.pl[0];
-	const float* mi = sh.pl[1];
-	const float a = mr[p * LD + p], b = mr[q * LD + q];
-	const float cr = mr[p * LD + q], ci = mi[p * LD + q];
+// Rotation j of an inner round (into rotation buffer buf) of the local pair
+// (p, q) with M(p, p) = a, M(q, q) = b, M(p, q) = (cr, ci): with
+// d = (b - a) / 2, r = sqrt(d^2 + |c|^2), u = |d| + r and w = 2 r u:
+// cos = u / sqrt(w), |sin| = |c| / sqrt(w), tau = |sin| / (1 + cos),
+// tan = |c| / u (the formulas of bjacobi.cu).
+__device__ __forceinline__ void inner_rotation32(Shared32& sh, int buf, int j, int p, int q, float a, float b,
+		float cr, float ci, int& cnt, float& tmax) {
 	const float c2 = cr * cr + ci * ci;
 	const float scale2 = fabsf(a) * fabsf(b);
-	sh.rpq[j] = p | q << 8;
-	if (!(c2 > 0.f && c2 > kSkipRel * kSkipRel * scale2)) return;
+	if (!(c2 > 0.f && c2 > kSkipRel * kSkipRel * scale2)) {
+		sh.rap[buf][j] = a;
+		sh.raq[buf][j] = b;
+		sh.rpq[buf][j] = p | q << 8;
+		return;
+	}
 	const float d = 0.5f * (b - a);
 	const float ad = fabsf(d);
 	const float rn = sqrtf(fmaf(d, d, c2));
@@ -77,14 +86,22 @@ __device__ void inner_rotation32(Shared32& sh, int j, int p, int q, int& cnt, fl
 	const float t = __fdividef(cabs, un);
 	const float ic = rsqrtf(c2);
 	const float sg = d < 0.f ? -1.f : 1.f;
-	sh.rot[j] = make_float4(sg * cabs * qn, sg * __fdividef(cabs, wn * qn + un), cr * ic, ci * ic);
-	sh.rap[j] = a - sg * t * cabs;
-	sh.raq[j] = b + sg * t * cabs;
-	sh.rpq[j] = p | q << 8 | 1 << 16;
+	sh.rot[buf][j] = make_float4(sg * cabs * qn, sg * __fdividef(cabs, wn * qn + un), cr * ic, ci * ic);
+	sh.rap[buf][j] = a - sg * t * cabs;
+	sh.raq[buf][j] = b + sg * t * cabs;
+	sh.rpq[buf][j] = p | q << 8 | 1 << 16;
 	if (c2 > kNoiseRel * kNoiseRel * scale2) {
 		cnt++;
 		tmax = fmaxf(tmax, t);
 	}
+}
+
+// Rotation j of an inner round from the subproblem in shared memory.
+__device__ __forceinline__ void inner_rotation32_sm(Shared32& sh, int buf, int j, int p, int q, int& cnt,
+		float& tmax) {
+	const float* mr = sh.pl[0];
+	const float* mi = sh.pl[1];
+	inner_rotation32(sh, buf, j, p, q, mr[p * LD + p], mr[q * LD + q], mr[p * LD + q], mi[p * LD + q], cnt, tmax);
 }
 
 __device__ __forceinline__ void rows2f(float s, float tau, float er, float ei, float& xpr, float& xpi, float& xqr,
@@ -106,7 +123,14 @@ __device__ __forceinline__ void cols2f(float s, float tau, float er, float ei, f
 }
 
 // One inner sweep (full: MS - 1 rounds over all pairs; cross: BS rounds of the
-// BS x BS cross pairs) on the subproblem in planes 0/1, Q in planes 2/3.
+// BS x BS cross pairs, round r pairing p < BS with BS + (p + r) % BS) on the
+// subproblem in planes 0/1, Q in planes 2/3. In each round the M blocks and
+// the Q columns are rotated by separate threads at the same time.
+// In a cross sweep, round r + 1 pairs p with q' = BS + (p + r + 1) % BS, the
+// second index of pair p + 1 in round r; so the thread updating the block
+// (pair p, pair p + 1) of round r holds M(p, q') and finds M(p, p) and
+// M(q', q') among round r's results, and sets up rotation p of round r + 1
+// right away: one barrier per inner round.
 __device__ void inner_sweep32(Shared32& sh, bool full) {
 	float* mr = sh.pl[0];
 	float* mi = sh.pl[1];
@@ -116,63 +140,74 @@ __device__ void inner_sweep32(Shared32& sh, bool full) {
 	const int rounds = full ? MS - 1 : BS;
 	int cnt = 0;
 	float tmax = 0.f;
+	if (tid < NR) {
+		const int p = full ? rr_player(tid, 0, MS) : tid;
+		const int q = full ? rr_player(MS - 1 - tid, 0, MS) : BS + tid;
+		inner_rotation32_sm(sh, 0, tid, p, q, cnt, tmax);
+	}
+	__syncthreads();
 	for (int r = 0; r < rounds; r++) {
-		if (tid < NR) {
-			const int p = full ? rr_player(tid, r, MS) : tid;
-			const int q = full ? rr_player(MS - 1 - tid, r, MS) : BS + (tid + r) % BS;
-			inner_rotation32(sh, tid, p, q, cnt, tmax);
+		const int cur = r & 1;
+		if (full && r > 0) {
+			if (tid < NR) inner_rotation32_sm(sh, cur, tid, rr_player(tid, r, MS), rr_player(MS - 1 - tid, r, MS), cnt,
+					tmax);
+			__syncthreads();
 		}
-		__syncthreads();
-		for (int e = tid; e < NR * NR; e += kThreads) {
-			const int ja = e / NR, jb = e % NR;
-			const int pa = sh.rpq[ja], pb = sh.rpq[jb];
+		if (tid < kMThreads) {
+			const int ja = tid / NR, jb = tid % NR;
+			const int pa = sh.rpq[cur][ja], pb = sh.rpq[cur][jb];
 			const bool ra = pa >> 16, rb = pb >> 16;
-			if (!ra && !rb) continue;
+			const bool nx = !full && r + 1 < rounds && jb == ((ja + 1) & (NR - 1));
 			const int p = pa & 255, q = (pa >> 8) & 255, s2 = pb & 255, t2 = (pb >> 8) & 255;
 			if (ja == jb) {
-				mr[p * LD + p] = sh.rap[ja]; mi[p * LD + p] = 0.f;
-				mr[q * LD + q] = sh.raq[ja]; mi[q * LD + q] = 0.f;
-				mr[p * LD + q] = 0.f; mi[p * LD + q] = 0.f;
-				mr[q * LD + p] = 0.f; mi[q * LD + p] = 0.f;
-				continue;
+				if (ra) {
+					mr[p * LD + p] = sh.rap[cur][ja]; mi[p * LD + p] = 0.f;
+					mr[q * LD + q] = sh.raq[cur][ja]; mi[q * LD + q] = 0.f;
+					mr[p * LD + q] = 0.f; mi[p * LD + q] = 0.f;
+					mr[q * LD + p] = 0.f; mi[q * LD + p] = 0.f;
+				}
+			} else if (ra || rb || nx) {
+				float psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
+				float qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
+				if (ra) {
+					const float4 R = sh.rot[cur][ja];
+					rows2f(R.x, R.y, R.z, R.w, psr, psi, qsr, qsi);
+					rows2f(R.x, R.y, R.z, R.w, ptr, pti, qtr, qti);
+				}
+				if (rb) {
+					const float4 R = sh.rot[cur][jb];
+					cols2f(R.x, R.y, R.z, R.w, psr, psi, ptr, pti);
+					cols2f(R.x, R.y, R.z, R.w, qsr, qsi, qtr, qti);
+				}
+				if (ra || rb) {
+					mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
+					mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
+				}
+				if (nx)
+					inner_rotation32(sh, cur ^ 1, ja, p, t2, sh.rap[cur][ja], sh.raq[cur][jb], ptr, pti, cnt, tmax);
 			}
-			float psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
-			float qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
-			if (ra) {
-				const float4 R = sh.rot[ja];
-				rows2f(R.x, R.y, R.z, R.w, psr, psi, qsr, qsi);
-				rows2f(R.x, R.y, R.z, R.w, ptr, pti, qtr, qti);
+		} else {
+			for (int e = tid - kMThreads; e < MS * NR; e += kThreads - kMThreads) {
+				const int i = e / NR, j = e % NR;
+				const int pj = sh.rpq[cur][j];
+				if (!(pj >> 16)) continue;
+				const int p = pj & 255, q = (pj >> 8) & 255;
+				float ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
+				const float4 R = sh.rot[cur][j];
+				cols2f(R.x, R.y, R.z, R.w, ysr, ysi, ytr, yti);
+				qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 			}
-			if (rb) {
-				const float4 R = sh.rot[jb];
-				cols2f(R.x, R.y, R.z, R.w, psr, psi, ptr, pti);
-				cols2f(R.x, R.y, R.z, R.w, qsr, qsi, qtr, qti);
-			}
-			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
-			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
-		}
-		for (int e = tid; e < MS * NR; e += kThreads) {
-			const int i = e / NR, j = e % NR;
-			const int pj = sh.rpq[j];
-			if (!(pj >> 16)) continue;
-			const int p = pj & 255, q = (pj >> 8) & 255;
-			float ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
-			const float4 R = sh.rot[j];
-			cols2f(R.x, R.y, R.z, R.w, ysr, ysi, ytr, yti);
-			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 		}
 		__syncthreads();
 	}
-	if (tid < 32) {
-		for (int o = 16; o > 0; o >>= 1) {
-			cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-			tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-		}
-		if (tid == 0) {
-			sh.cnt += cnt;
-			const unsigned long long tb = (unsigned long long)__double_as_longlong((double)tmax);
-			if (tb > sh.tmax) sh.tmax = tb;
-		}
+	// counts and tangents of every thread that set up rotations
+	for (int o = 16; o > 0; o >>= 1) {
+		cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+		tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+	}
+	if ((tid & 31) == 0 && cnt) {
+		atomicAdd(&sh.cnt, cnt);
+		atomicMax(&sh.tmax, (unsigned long long)__double_as_longlong((double)tmax));
 	}
 }
 
@@ -212,24 +247,28 @@ __device__ __forceinline__ void cmm32(const float* ar, const float* ai, int as_i
 	}
 }
 
-// Output (r, c) of a thread in the full 32 x 32 product: warp w owns rows
-// 4w .. 4w + 3; lane (h, l) = (lane >> 4, lane & 15) computes rows 4w + h and
-// 4w + 2 + h at columns l and l + 16.
-__device__ __forceinline__ void full_rc(int r, int c, int& row, int& col) {
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	row = 4 * warp + (lane >> 4) + 2 * r;
+// Half-CTA products of phase 2: thread lt of 256, warp lw = lt >> 5 owns rows
+// 4 lw .. 4 lw + 3; lane (h, l) computes rows 4 lw + h + 2r at columns l + 16c.
+__device__ __forceinline__ void half_rc(int lt, int r, int c, int& row, int& col) {
+	const int lane = lt & 31, lw = lt >> 5;
+	row = 4 * lw + (lane >> 4) + 2 * r;
 	col = (lane & 15) + 16 * c;
 }
 
-__device__ __forceinline__ void cgemm32(const float* ar, const float* ai, int as_i, int as_m, bool conjA,
+__device__ __forceinline__ void half_gemm(int lt, const float* ar, const float* ai, int as_i, int as_m, bool conjA,
 		const float* br, const float* bi, float (&cr)[2][2], float (&ci)[2][2]) {
 	int row0, col0;
-	full_rc(0, 0, row0, col0);
+	half_rc(lt, 0, 0, row0, col0);
 	cmm32<2, 2>(ar, ai, as_i, as_m, conjA, br, bi, row0, 2, col0, 16, cr, ci);
 }
 
-__device__ void load_q32(float* qr, float* qi, const float2* Qg) {
-	for (int e = threadIdx.x; e < MS * MS; e += kThreads) {
+// Barrier of one half of the CTA (named barrier 1 + half, 256 threads).
+__device__ __forceinline__ void half_sync(int half) {
+	asm volatile("bar.sync %0, %1;\n" ::"r"(1 + half), "r"(kThreads / 2) : "memory");
+}
+
+__device__ void load_q32_half(int lt, float* qr, float* qi, const float2* Qg) {
+	for (int e = lt; e < MS * MS; e += kThreads / 2) {
 		const float2 v = __ldcg(Qg + e);
 		qr[(e / MS) * LD + (e % MS)] = v.x;
 		qi[(e / MS) * LD + (e % MS)] = v.y;
@@ -292,28 +331,29 @@ __device__ void phase1_item32(Shared32& sh, int j, long long t, int rounds, int 
 		}
 		__syncthreads();
 		// only the (hP, hQ) quadrant of Q_a^H A_{t-2}(a, b) Q_b enters the
-		// subproblem: T = A_{t-2}(a, b) Q_b[:, hQ half] (32 x 16, two elements per
-		// thread), then C = Q_a[:, hP half]^H T (16 x 16, one per thread)
+		// subproblem: T = A_{t-2}(a, b) Q_b[:, hQ half] (32 x 16, one element per
+		// thread), then C = Q_a[:, hP half]^H T (16 x 16, threads [0, 256))
 		{
 			const int lane = tid & 31, warp = tid >> 5;
-			const int trow = 4 * warp + (lane >> 4), tcol = lane & 15;
-			float tr[2][1], ti[2][1];
-			cmm32<2, 1>(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], trow, 2, hQ * BS + tcol, 0, tr, ti);
+			const int trow = 2 * warp + (lane >> 4), tcol = lane & 15;
+			float tr[1][1], ti[1][1];
+			cmm32<1, 1>(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], trow, 0, hQ * BS + tcol, 0, tr, ti);
 			__syncthreads();
-#pragma unroll
-			for (int r = 0; r < 2; r++) {
-				mr[(trow + 2 * r) * LD + tcol] = tr[r][0];
-				mi[(trow + 2 * r) * LD + tcol] = ti[r][0];
-			}
+			mr[trow * LD + tcol] = tr[0][0];
+			mi[trow * LD + tcol] = ti[0][0];
 			__syncthreads();
 			float cr[1][1], ci[1][1];
-			const int i = tid >> 4, l = tid & 15;
-			cmm32<1, 1>(sh.pl[2] + hP * BS, sh.pl[3] + hP * BS, 1, LD, true, sh.pl[0], sh.pl[1], i, 0, l, 0, cr, ci);
+			const int i = (tid >> 4) & (BS - 1), l = tid & 15;
+			if (tid < BS * BS)
+				cmm32<1, 1>(sh.pl[2] + hP * BS, sh.pl[3] + hP * BS, 1, LD, true, sh.pl[0], sh.pl[1], i, 0, l, 0, cr,
+						ci);
 			__syncthreads();
-			mr[i * LD + BS + l] = cr[0][0];
-			mi[i * LD + BS + l] = ci[0][0];
-			mr[(BS + l) * LD + i] = cr[0][0];
-			mi[(BS + l) * LD + i] = -ci[0][0];
+			if (tid < BS * BS) {
+				mr[i * LD + BS + l] = cr[0][0];
+				mi[i * LD + BS + l] = ci[0][0];
+				mr[(BS + l) * LD + i] = cr[0][0];
+				mi[(BS + l) * LD + i] = -ci[0][0];
+			}
 		}
 #pragma unroll
 		for (int it = 0; it < ND; it++) {
@@ -339,10 +379,18 @@ __device__ void phase1_item32(Shared32& sh, int j, long long t, int rounds, int 
 	__syncthreads();
 }
 
-// Phase 2 item w of round ro (bjacobi.cu phase2_item in FP32).
-__device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int kp, const float2* src, float2* dst,
-		float2* V, const float2* Qr) {
-	const int tid = threadIdx.x;
+// Phase 2 item w of round ro (bjacobi.cu phase2_item in FP32), on one half of
+// the CTA: the two halves take alternate items, each with its own planes and
+// named barrier.
+__device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int np, int kp, const float2* src,
+		float2* dst, float2* V, const float2* Qr) {
+	const int lt = threadIdx.x & (kThreads / 2 - 1);
+	float* xr = sh.pl[6 * half + 0];
+	float* xi = sh.pl[6 * half + 1];
+	float* ar = sh.pl[6 * half + 2];
+	float* ai = sh.pl[6 * half + 3];
+	float* br = sh.pl[6 * half + 4];
+	float* bi = sh.pl[6 * half + 5];
 	const int nA2 = np * (np - 1);
 	float cr[2][2], ci[2][2];
 	if (w < nA2) {
@@ -351,64 +399,64 @@ __device__ void phase2_item32(Shared32& sh, int w, int ro, int nb, int np, int k
 		if (jc >= jr) jc++;
 		const int Pr = rr_player(jr, ro, nb), Qr_ = rr_player(nb - 1 - jr, ro, nb);
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = tid; e < MS * MS; e += kThreads) {
+		for (int e = lt; e < MS * MS; e += kThreads / 2) {
 			const int i = e / MS, l = e % MS;
 			const float2 v = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
-			sh.pl[0][i * LD + l] = v.x;
-			sh.pl[1][i * LD + l] = v.y;
+			xr[i * LD + l] = v.x;
+			xi[i * LD + l] = v.y;
 		}
-		load_q32(sh.pl[2], sh.pl[3], Qr + (size_t)jr * MS * MS);
-		load_q32(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
-		__syncthreads();
-		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
-		__syncthreads();
+		load_q32_half(lt, ar, ai, Qr + (size_t)jr * MS * MS);
+		load_q32_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+		half_sync(half);
+		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // T = X Qc
+		half_sync(half);
 #pragma unroll
-		for (int b = 0; b < 2; b++)
+		for (int r = 0; r < 2; r++)
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
+			for (int c = 0; c < 2; c++) {
 				int row, col;
-				full_rc(b, h, row, col);
-				sh.pl[0][row * LD + col] = cr[b][h];
-				sh.pl[1][row * LD + col] = ci[b][h];
+				half_rc(lt, r, c, row, col);
+				xr[row * LD + col] = cr[r][c];
+				xi[row * LD + col] = ci[r][c];
 			}
-		__syncthreads();
-		cgemm32(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);  // Qr^H T
+		half_sync(half);
+		half_gemm(lt, ar, ai, 1, LD, true, xr, xi, cr, ci);  // Qr^H T
 #pragma unroll
-		for (int b = 0; b < 2; b++)
+		for (int r = 0; r < 2; r++)
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
+			for (int c = 0; c < 2; c++) {
 				int row, col;
-				full_rc(b, h, row, col);
-				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
+				half_rc(lt, r, c, row, col);
+				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_float2(cr[r][c], ci[r][c]);
 			}
 	} else {
 		const int v = w - nA2;
 		const int rb = v / np, jc = v % np;
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = tid; e < MS * MS; e += kThreads) {
+		for (int e = lt; e < MS * MS; e += kThreads / 2) {
 			const int i = e / MS, l = e % MS;
 			const float2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
-			sh.pl[0][i * LD + l] = x.x;
-			sh.pl[1][i * LD + l] = x.y;
+			xr[i * LD + l] = x.x;
+			xi[i * LD + l] = x.y;
 		}
-		load_q32(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
-		__syncthreads();
-		cgemm32(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
+		load_q32_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+		half_sync(half);
+		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // V Qc
 #pragma unroll
-		for (int b = 0; b < 2; b++)
+		for (int r = 0; r < 2; r++)
 #pragma unroll
-			for (int h = 0; h < 2; h++) {
+			for (int c = 0; c < 2; c++) {
 				int row, col;
-				full_rc(b, h, row, col);
-				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_float2(cr[b][h], ci[b][h]);
+				half_rc(lt, r, c, row, col);
+				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_float2(cr[r][c], ci[r][c]);
 			}
 	}
-	__syncthreads();
+	half_sync(half);
 }
 
-// The cooperative solve: bjacobi_kernel of bjacobi.cu in FP32. A_r lives in
+// The cooperative solve: bjacobi_kernel of bjacobi.cu in FP32 (one CTA per SM). A_r lives in
 // bufs[(r + 1) % 3] (A_{-1} = the input in A0); Q_r in Qbuf + (r & 1) * np * MS^2.
-__global__ void __launch_bounds__(kThreads, 2) bjacobi32_kernel(float2* A0, float2* A1, float2* A2, float2* V,
+__global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, float2* A1, float2* A2, float2* V,
 		float2* Qbuf, int kp, int max_sweeps, double tau_final, int* counters, unsigned long long* tmaxg) {
 	cg::grid_group grid = cg::this_grid();
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -448,8 +496,9 @@ __global__ void __launch_bounds__(kThreads, 2) bjacobi32_kernel(float2* A0, floa
 			const int ro = (int)((t - 1) % rounds);
 			const float2* src = bufs[(t + 2) % 3];
 			float2* dst = bufs[t % 3];
-			for (int w = (int)blockIdx.x - p2first; w < nW; w += p2count)
-				phase2_item32(sh, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+			const int half = tid / (kThreads / 2);
+			for (int w = 2 * ((int)blockIdx.x - p2first) + half; w < nW; w += 2 * p2count)
+				phase2_item32(sh, half, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
 		}
 		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
 		if (sweep_end && tid == 0) {
@@ -523,7 +572,7 @@ cudaError_t launch_bjacobi32(const double2* S, int k, JacobiWork& w, int num_sms
 	e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bjacobi32_kernel, kThreads, smem);
 	if (e != cudaSuccess) return e;
 	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-	const int blocks = num_sms * std::min(per_sm, 2);
+	const int blocks = num_sms * std::min(per_sm, 1);
 	int kpv = kp, ms = w.max_sweeps;
 	double tau = w.tau_final > 0.0 ? w.tau_final : 1e-3;
 	int* counters = w.counters;
