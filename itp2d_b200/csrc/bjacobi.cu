@@ -47,7 +47,11 @@ constexpr int MS = 32;        // subproblem size: two blocks
 constexpr int NR = MS / 2;    // rotations per inner round
 constexpr int LD = MS + 4;    // padded row length (doubles): conflict-free DMMA fragments
 constexpr int PL = MS * LD;   // doubles per plane
-constexpr int kThreads = 256;
+// 512 threads, one CTA per SM: in an inner round, threads [0, 256) update the
+// 256 2 x 2 blocks of M while threads [256, 512) rotate the columns of Q; the
+// two halves of a phase-2 CTA work on separate products.
+constexpr int kThreads = 512;
+constexpr int kMThreads = NR * NR;
 constexpr double kTauFinal = 3e-9;
 // Rounds between full inner sweeps (within-block pairs rotated again); every
 // 16th round measured best on k = 500 (fewer outer sweeps for little cost).
@@ -69,11 +73,15 @@ __device__ __forceinline__ int rr_player(int pos, int r, int npos) {
 __device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * BS + i : Q * BS + (i - BS); }
 
 struct Shared {
-	double pl[6][PL];                            // planes: [0,1] M or X/T, [2,3] Q or Q_r, [4,5] Q_c
-	double rc[NR], rs[NR], rtau[NR], rer[NR], rei[NR], rap[NR], raq[NR];
-	int rp[NR], rq[NR], rrot[NR];
-	int cnt;                                     // rotations in the current inner sweep
-	int total;                                   // rotations of this CTA in the current outer sweep
+	// phase 1: [0,1] M, [2,3] Q, [4,5] formation operands; phase 2: half h of
+	// the CTA uses [6h, 6h + 6): X/T, Q_r, Q_c
+	double pl[12][PL];
+	// rotations of two consecutive inner rounds (round r in buffer r & 1)
+	double2 rst[2][NR];                          // (sin, tau)
+	double2 re[2][NR];                           // e = c / |c|
+	double rap[2][NR], raq[2][NR];               // M(p, p), M(q, q) after the round
+	int rpq[2][NR];                              // p | q << 8 | applied << 16
+	int cnt;                                     // counted rotations of the current outer sweep
 	unsigned long long tmax;                     // largest tangent (bits of a non-negative double)
 };
 
@@ -109,19 +117,17 @@ __device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((lo
 // max(|d|, |c|), and c alone by its own for e = c / |c|, so that every refined
 // estimate starts inside float range; exponents beyond +-1000 take the same
 // formulas through scalbn.
-// Counted rotations and the largest counted tangent accumulate in the caller's
-// registers (cnt, tmax) and are reduced once per inner sweep.
-__device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol, int& cnt, double& tmax) {
-	const double* mr = sh.pl[0];
-	const double* mi = sh.pl[1];
-	const double a = mr[p * LD + p], b = mr[q * LD + q];
-	const double cr = mr[p * LD + q], ci = mi[p * LD + q];
+// The pair has M(p, p) = a, M(q, q) = b, M(p, q) = (cr, ci); the rotation
+// goes to rotation buffer buf, slot j. Counted rotations and the largest
+// counted tangent accumulate in the caller's registers (cnt, tmax) and are
+// reduced once per inner sweep.
+__device__ __forceinline__ void inner_rotation(Shared& sh, int buf, int j, int p, int q, double a, double b,
+		double cr, double ci, double tol, int& cnt, double& tmax) {
 	const double c2 = cr * cr + ci * ci;
 	const double scale2 = fabs(a) * fabs(b);
-	sh.rp[j] = p;
-	sh.rq[j] = q;
-	sh.rrot[j] = 0;
-	sh.rc[j] = 1.0; sh.rs[j] = 0.0; sh.rtau[j] = 0.0; sh.rer[j] = 1.0; sh.rei[j] = 0.0; sh.rap[j] = a; sh.raq[j] = b;
+	sh.rap[buf][j] = a;
+	sh.raq[buf][j] = b;
+	sh.rpq[buf][j] = p | q << 8;
 	if (!(c2 > 0.0 && c2 > tol * tol * scale2)) return;
 	const double d = 0.5 * (b - a);
 	const double ad = fabs(d);
@@ -152,18 +158,24 @@ __device__ void inner_rotation(Shared& sh, int j, int p, int q, double tol, int&
 	const double sg = d < 0 ? -1.0 : 1.0;
 	const double sw = wn * qn;                 // sqrt(w)
 	const double cabs = fast ? cn * pow2i(ex) : scalbn(cn, ex);
-	sh.rc[j] = un * qn;
-	sh.rs[j] = sg * cn * qn;
-	sh.rtau[j] = sg * cn * rcp_nr(sw + un);    // sw + un in [2.4, 12)
-	sh.rer[j] = crs * ec;
-	sh.rei[j] = cis * ec;
-	sh.rap[j] = a - sg * t * cabs;
-	sh.raq[j] = b + sg * t * cabs;
-	sh.rrot[j] = 1;
+	sh.rst[buf][j] = make_double2(sg * cn * qn, sg * cn * rcp_nr(sw + un));  // sw + un in [2.4, 12)
+	sh.re[buf][j] = make_double2(crs * ec, cis * ec);
+	sh.rap[buf][j] = a - sg * t * cabs;
+	sh.raq[buf][j] = b + sg * t * cabs;
+	sh.rpq[buf][j] = p | q << 8 | 1 << 16;
 	if (c2 > kNoiseRel * kNoiseRel * scale2) {
 		cnt++;
 		tmax = fmax(tmax, t);
 	}
+}
+
+// Rotation j of an inner round from the subproblem in shared memory.
+__device__ __forceinline__ void inner_rotation_sm(Shared& sh, int buf, int j, int p, int q, double tol, int& cnt,
+		double& tmax) {
+	const double* mr = sh.pl[0];
+	const double* mi = sh.pl[1];
+	inner_rotation(sh, buf, j, p, q, mr[p * LD + p], mr[q * LD + q], mr[p * LD + q], mi[p * LD + q], tol, cnt,
+			tmax);
 }
 
 // Rows p, q of J^H X with J = [[c, s e], [-s conj(e), c]] (correction form,
@@ -194,8 +206,14 @@ __device__ __forceinline__ void cols2(double s, double tau, double er, double ei
 // One inner sweep on the MS x MS subproblem in planes 0/1, accumulating Q in
 // planes 2/3: full (MS - 1 rounds of NR rotations over all pairs) or cross
 // (BS rounds: round r pairs p with BS + (p + r) % BS). Each round updates
-// every 2 x 2 block {p,q} x {s,t} in place as J_pq^H X J_st, so the subproblem
-// crosses shared memory once per round.
+// every 2 x 2 block {p,q} x {s,t} in place as J_pq^H X J_st (threads
+// [0, 256)) while threads [256, 512) rotate the columns of Q, so the
+// subproblem crosses shared memory once per round.
+// In a cross sweep, round r + 1 pairs p with q' = BS + (p + r + 1) % BS, the
+// second index of pair p + 1 in round r; so the thread updating the block
+// (pair p, pair p + 1) of round r holds M(p, q') and finds M(p, p) and
+// M(q', q') among round r's results, and sets up rotation p of round r + 1
+// right away: one barrier per inner round.
 __device__ void inner_sweep(Shared& sh, double tol, bool full) {
 	double* mr = sh.pl[0];
 	double* mi = sh.pl[1];
@@ -205,100 +223,124 @@ __device__ void inner_sweep(Shared& sh, double tol, bool full) {
 	const int rounds = full ? MS - 1 : BS;
 	int cnt = 0;
 	double tmax = 0.0;
+	if (tid < NR) {
+		const int p = full ? rr_player(tid, 0, MS) : tid;
+		const int q = full ? rr_player(MS - 1 - tid, 0, MS) : BS + tid;
+		inner_rotation_sm(sh, 0, tid, p, q, tol, cnt, tmax);
+	}
+	__syncthreads();
 	for (int r = 0; r < rounds; r++) {
-		if (tid < NR) {
-			const int p = full ? rr_player(tid, r, MS) : tid;
-			const int q = full ? rr_player(MS - 1 - tid, r, MS) : BS + (tid + r) % BS;
-			inner_rotation(sh, tid, p, q, tol, cnt, tmax);
+		const int cur = r & 1;
+		if (full && r > 0) {
+			if (tid < NR)
+				inner_rotation_sm(sh, cur, tid, rr_player(tid, r, MS), rr_player(MS - 1 - tid, r, MS), tol, cnt, tmax);
+			__syncthreads();
 		}
-		__syncthreads();
-		// NR x NR blocks of M
-		for (int e = tid; e < NR * NR; e += kThreads) {
-			const int ja = e / NR, jb = e % NR;
-			const bool ra = sh.rrot[ja], rb = sh.rrot[jb];
-			if (!ra && !rb) continue;
-			const int p = sh.rp[ja], q = sh.rq[ja], s2 = sh.rp[jb], t2 = sh.rq[jb];
+		if (tid < kMThreads) {
+			const int ja = tid / NR, jb = tid % NR;
+			const int pa = sh.rpq[cur][ja], pb = sh.rpq[cur][jb];
+			const bool ra = pa >> 16, rb = pb >> 16;
+			const bool nx = !full && r + 1 < rounds && jb == ((ja + 1) & (NR - 1));
+			const int p = pa & 255, q = (pa >> 8) & 255, s2 = pb & 255, t2 = (pb >> 8) & 255;
 			if (ja == jb) {
-				mr[p * LD + p] = sh.rap[ja]; mi[p * LD + p] = 0.0;
-				mr[q * LD + q] = sh.raq[ja]; mi[q * LD + q] = 0.0;
-				mr[p * LD + q] = 0.0; mi[p * LD + q] = 0.0;
-				mr[q * LD + p] = 0.0; mi[q * LD + p] = 0.0;
-				continue;
+				if (ra) {
+					mr[p * LD + p] = sh.rap[cur][ja]; mi[p * LD + p] = 0.0;
+					mr[q * LD + q] = sh.raq[cur][ja]; mi[q * LD + q] = 0.0;
+					mr[p * LD + q] = 0.0; mi[p * LD + q] = 0.0;
+					mr[q * LD + p] = 0.0; mi[q * LD + p] = 0.0;
+				}
+			} else if (ra || rb || nx) {
+				double psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
+				double qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
+				if (ra) {
+					const double2 st = sh.rst[cur][ja], e = sh.re[cur][ja];
+					rows2(st.x, st.y, e.x, e.y, psr, psi, qsr, qsi);
+					rows2(st.x, st.y, e.x, e.y, ptr, pti, qtr, qti);
+				}
+				if (rb) {
+					const double2 st = sh.rst[cur][jb], e = sh.re[cur][jb];
+					cols2(st.x, st.y, e.x, e.y, psr, psi, ptr, pti);
+					cols2(st.x, st.y, e.x, e.y, qsr, qsi, qtr, qti);
+				}
+				if (ra || rb) {
+					mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
+					mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
+				}
+				if (nx)
+					inner_rotation(sh, cur ^ 1, ja, p, t2, sh.rap[cur][ja], sh.raq[cur][jb], ptr, pti, tol, cnt, tmax);
 			}
-			double psr = mr[p * LD + s2], psi = mi[p * LD + s2], ptr = mr[p * LD + t2], pti = mi[p * LD + t2];
-			double qsr = mr[q * LD + s2], qsi = mi[q * LD + s2], qtr = mr[q * LD + t2], qti = mi[q * LD + t2];
-			if (ra) {
-				rows2(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], psr, psi, qsr, qsi);
-				rows2(sh.rs[ja], sh.rtau[ja], sh.rer[ja], sh.rei[ja], ptr, pti, qtr, qti);
+		} else {
+			for (int e = tid - kMThreads; e < MS * NR; e += kThreads - kMThreads) {
+				const int i = e / NR, j = e % NR;
+				const int pj = sh.rpq[cur][j];
+				if (!(pj >> 16)) continue;
+				const int p = pj & 255, q = (pj >> 8) & 255;
+				double ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
+				const double2 st = sh.rst[cur][j], ev = sh.re[cur][j];
+				cols2(st.x, st.y, ev.x, ev.y, ysr, ysi, ytr, yti);
+				qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 			}
-			if (rb) {
-				cols2(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], psr, psi, ptr, pti);
-				cols2(sh.rs[jb], sh.rtau[jb], sh.rer[jb], sh.rei[jb], qsr, qsi, qtr, qti);
-			}
-			mr[p * LD + s2] = psr; mi[p * LD + s2] = psi; mr[p * LD + t2] = ptr; mi[p * LD + t2] = pti;
-			mr[q * LD + s2] = qsr; mi[q * LD + s2] = qsi; mr[q * LD + t2] = qtr; mi[q * LD + t2] = qti;
-		}
-		// Q columns
-		for (int e = tid; e < MS * NR; e += kThreads) {
-			const int i = e / NR, j = e % NR;
-			if (!sh.rrot[j]) continue;
-			const int p = sh.rp[j], q = sh.rq[j];
-			double ysr = qr[i * LD + p], ysi = qi[i * LD + p], ytr = qr[i * LD + q], yti = qi[i * LD + q];
-			cols2(sh.rs[j], sh.rtau[j], sh.rer[j], sh.rei[j], ysr, ysi, ytr, yti);
-			qr[i * LD + p] = ysr; qi[i * LD + p] = ysi; qr[i * LD + q] = ytr; qi[i * LD + q] = yti;
 		}
 		__syncthreads();
 	}
-	// warp 0 holds the NR rotation threads: fold their counts into the CTA's
-	if (tid < 32) {
-		for (int o = 16; o > 0; o >>= 1) {
-			cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-			tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-		}
-		if (tid == 0) {
-			sh.cnt += cnt;
-			const unsigned long long tb = (unsigned long long)__double_as_longlong(tmax);
-			if (tb > sh.tmax) sh.tmax = tb;
-		}
+	// counts and tangents of every thread that set up rotations
+	for (int o = 16; o > 0; o >>= 1) {
+		cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+		tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+	}
+	if ((tid & 31) == 0 && cnt) {
+		atomicAdd(&sh.cnt, cnt);
+		atomicMax(&sh.tmax, (unsigned long long)__double_as_longlong(tmax));
 	}
 }
 
-// acc = A B for 32 x 32 complex operands given as plane pairs, FP64 DMMA.
-// Warp w owns output rows (w >> 1) * 8 .. +8 and columns (w & 1) * 16 .. +16
-// (two 8 x 8 tiles). A element (i, m) at a_re[i*as_i + m*as_m], B element
-// (m, l) at b_re[m*LD + l]; conjA conjugates A.
-__device__ __forceinline__ void cgemm(const double* ar, const double* ai, int as_i, int as_m, bool conjA,
-		const double* br, const double* bi, double (&cr)[2][2], double (&ci)[2][2]) {
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int i = (warp >> 1) * 8 + (lane >> 2);
-#pragma unroll
-	for (int b = 0; b < 2; b++) cr[b][0] = cr[b][1] = ci[b][0] = ci[b][1] = 0.0;
+// One 8 x 8 tile of the complex product A B (32-deep operands given as plane
+// pairs) by one warp with FP64 DMMA: acc (h) of lane holds output row
+// row0 + (lane >> 2), column col0 + 2 (lane & 3) + h. A element (i, m) at
+// a_re[i * as_i + m * as_m], B element (m, l) at b_re[m * LD + l]; conjA
+// conjugates A.
+__device__ __forceinline__ void ctile(int lane, const double* ar, const double* ai, int as_i, int as_m, bool conjA,
+		const double* br, const double* bi, int row0, int col0, double (&cr)[2], double (&ci)[2]) {
+	const int i = row0 + (lane >> 2);
+	const int l = col0 + (lane >> 2);
+	cr[0] = cr[1] = ci[0] = ci[1] = 0.0;
 #pragma unroll
 	for (int kk = 0; kk < MS; kk += 4) {
 		const int m = kk + (lane & 3);
 		const double far = ar[i * as_i + m * as_m];
 		const double fai = conjA ? -ai[i * as_i + m * as_m] : ai[i * as_i + m * as_m];
-#pragma unroll
-		for (int b = 0; b < 2; b++) {
-			const int l = (warp & 1) * 16 + b * 8 + (lane >> 2);
-			const double fbr = br[m * LD + l], fbi = bi[m * LD + l];
-			dmma(cr[b][0], cr[b][1], far, fbr);
-			dmma(cr[b][0], cr[b][1], -fai, fbi);
-			dmma(ci[b][0], ci[b][1], far, fbi);
-			dmma(ci[b][0], ci[b][1], fai, fbr);
-		}
+		const double fbr = br[m * LD + l], fbi = bi[m * LD + l];
+		dmma(cr[0], cr[1], far, fbr);
+		dmma(cr[0], cr[1], -fai, fbi);
+		dmma(ci[0], ci[1], far, fbi);
+		dmma(ci[0], ci[1], fai, fbr);
 	}
 }
 
-// Output element coordinates of accumulator (b, h) of this thread.
-__device__ __forceinline__ void acc_rc(int b, int h, int& row, int& col) {
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	row = (warp >> 1) * 8 + (lane >> 2);
-	col = (warp & 1) * 16 + b * 8 + 2 * (lane & 3) + h;
+// Full 32 x 32 product on one half of the CTA (local warp lw of 8): warp lw
+// owns rows (lw >> 1) * 8 .. + 8 and columns (lw & 1) * 16 .. + 16 (tiles b).
+__device__ __forceinline__ void half_gemm(int lt, const double* ar, const double* ai, int as_i, int as_m,
+		bool conjA, const double* br, const double* bi, double (&cr)[2][2], double (&ci)[2][2]) {
+	const int lane = lt & 31, lw = lt >> 5;
+#pragma unroll
+	for (int b = 0; b < 2; b++)
+		ctile(lane, ar, ai, as_i, as_m, conjA, br, bi, (lw >> 1) * 8, (lw & 1) * 16 + b * 8, cr[b], ci[b]);
 }
 
-__device__ void load_q(double* qr, double* qi, const double2* Qg) {
-	for (int e = threadIdx.x; e < MS * MS; e += kThreads) {
+// Output coordinates of accumulator (b, h) of half_gemm for local thread lt.
+__device__ __forceinline__ void half_rc(int lt, int b, int h, int& row, int& col) {
+	const int lane = lt & 31, lw = lt >> 5;
+	row = (lw >> 1) * 8 + (lane >> 2);
+	col = (lw & 1) * 16 + b * 8 + 2 * (lane & 3) + h;
+}
+
+// Barrier of one half of the CTA (named barrier 1 + half, 256 threads).
+__device__ __forceinline__ void half_sync(int half) {
+	asm volatile("bar.sync %0, %1;\n" ::"r"(1 + half), "r"(kThreads / 2) : "memory");
+}
+
+__device__ void load_q_half(int lt, double* qr, double* qi, const double2* Qg) {
+	for (int e = lt; e < MS * MS; e += kThreads / 2) {
 		const double2 v = __ldcg(Qg + e);
 		qr[(e / MS) * LD + (e % MS)] = v.x;
 		qi[(e / MS) * LD + (e % MS)] = v.y;
@@ -370,36 +412,39 @@ __device__ void phase1_item(Shared& sh, int j, long long t, int rounds, int nb, 
 			sh.pl[5][i * LD + l] = lqb[it].y;
 		}
 		__syncthreads();
-		double cr[2][2], ci[2][2];
-		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);
-		__syncthreads();
+		// only the (hP, hQ) quadrant of Q_a^H A_{t-2}(a, b) Q_b enters the
+		// subproblem: T = A_{t-2}(a, b) Q_b[:, hQ half] (32 x 16: eight 8 x 8
+		// tiles, warps 0-7), then C = Q_a[:, hP half]^H T (16 x 16: four tiles,
+		// warps 0-3)
+		{
+			const int lane = tid & 31, warp = tid >> 5;
+			double cr[2], ci[2];
+			if (warp < 8)
+				ctile(lane, sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4] + hQ * BS, sh.pl[5] + hQ * BS, (warp >> 1) * 8,
+						(warp & 1) * 8, cr, ci);
+			__syncthreads();
+			if (warp < 8)
 #pragma unroll
-		for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				int row, col;
-				acc_rc(bb, h, row, col);
-				mr[row * LD + col] = cr[bb][h];
-				mi[row * LD + col] = ci[bb][h];
-			}
-		__syncthreads();
-		cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
-		__syncthreads();
-		// off-diagonal blocks of the subproblem from C[hP half][hQ half]
-#pragma unroll
-		for (int bb = 0; bb < 2; bb++)
-#pragma unroll
-			for (int h = 0; h < 2; h++) {
-				int row, col;
-				acc_rc(bb, h, row, col);
-				if ((row >> 4) == hP && (col >> 4) == hQ) {
-					const int i = row & (BS - 1), l = BS + (col & (BS - 1));
-					mr[i * LD + l] = cr[bb][h];
-					mi[i * LD + l] = ci[bb][h];
-					mr[l * LD + i] = cr[bb][h];
-					mi[l * LD + i] = -ci[bb][h];
+				for (int h = 0; h < 2; h++) {
+					const int row = (warp >> 1) * 8 + (lane >> 2), col = (warp & 1) * 8 + 2 * (lane & 3) + h;
+					mr[row * LD + col] = cr[h];
+					mi[row * LD + col] = ci[h];
 				}
-			}
+			__syncthreads();
+			if (warp < 4)
+				ctile(lane, sh.pl[2] + hP * BS, sh.pl[3] + hP * BS, 1, LD, true, sh.pl[0], sh.pl[1], (warp >> 1) * 8,
+						(warp & 1) * 8, cr, ci);
+			__syncthreads();
+			if (warp < 4)
+#pragma unroll
+				for (int h = 0; h < 2; h++) {
+					const int i = (warp >> 1) * 8 + (lane >> 2), l = BS + (warp & 1) * 8 + 2 * (lane & 3) + h;
+					mr[i * LD + l] = cr[h];
+					mi[i * LD + l] = ci[h];
+					mr[l * LD + i] = cr[h];
+					mi[l * LD + i] = -ci[h];
+				}
+		}
 		// diagonal blocks (P, P) and (Q, Q) of A_{t-1}
 #pragma unroll
 		for (int it = 0; it < ND; it++) {
@@ -426,10 +471,18 @@ __device__ void phase1_item(Shared& sh, int j, long long t, int rounds, int nb, 
 }
 
 // Phase 2 item w of round ro: an off-diagonal pair block of A (w < nA2) or a
-// slab of V, read from src / V, written to dst / V.
-__device__ void phase2_item(Shared& sh, int w, int ro, int nb, int np, int kp, const double2* src, double2* dst,
-		double2* V, const double2* Qr) {
-	const int tid = threadIdx.x;
+// slab of V, read from src / V, written to dst / V; on one half of the CTA
+// (the two halves take alternate items, each with its own planes and named
+// barrier).
+__device__ void phase2_item(Shared& sh, int half, int w, int ro, int nb, int np, int kp, const double2* src,
+		double2* dst, double2* V, const double2* Qr) {
+	const int lt = threadIdx.x & (kThreads / 2 - 1);
+	double* xr = sh.pl[6 * half + 0];
+	double* xi = sh.pl[6 * half + 1];
+	double* ar = sh.pl[6 * half + 2];
+	double* ai = sh.pl[6 * half + 3];
+	double* br = sh.pl[6 * half + 4];
+	double* bi = sh.pl[6 * half + 5];
 	const int nA2 = np * (np - 1);
 	double cr[2][2], ci[2][2];
 	if (w < nA2) {
@@ -438,65 +491,65 @@ __device__ void phase2_item(Shared& sh, int w, int ro, int nb, int np, int kp, c
 		if (jc >= jr) jc++;
 		const int Pr = rr_player(jr, ro, nb), Qr_ = rr_player(nb - 1 - jr, ro, nb);
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = tid; e < MS * MS; e += kThreads) {
+		for (int e = lt; e < MS * MS; e += kThreads / 2) {
 			const int i = e / MS, l = e % MS;
 			const double2 v = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
-			sh.pl[0][i * LD + l] = v.x;
-			sh.pl[1][i * LD + l] = v.y;
+			xr[i * LD + l] = v.x;
+			xi[i * LD + l] = v.y;
 		}
-		load_q(sh.pl[2], sh.pl[3], Qr + (size_t)jr * MS * MS);
-		load_q(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
-		__syncthreads();
-		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // T = X Qc
-		__syncthreads();
+		load_q_half(lt, ar, ai, Qr + (size_t)jr * MS * MS);
+		load_q_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+		half_sync(half);
+		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // T = X Qc
+		half_sync(half);
 #pragma unroll
 		for (int b = 0; b < 2; b++)
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc(b, h, row, col);
-				sh.pl[0][row * LD + col] = cr[b][h];
-				sh.pl[1][row * LD + col] = ci[b][h];
+				half_rc(lt, b, h, row, col);
+				xr[row * LD + col] = cr[b][h];
+				xi[row * LD + col] = ci[b][h];
 			}
-		__syncthreads();
+		half_sync(half);
 		// C = Qr^H T: A(i, m) = conj(Qr(m, i))
-		cgemm(sh.pl[2], sh.pl[3], 1, LD, true, sh.pl[0], sh.pl[1], cr, ci);
+		half_gemm(lt, ar, ai, 1, LD, true, xr, xi, cr, ci);
 #pragma unroll
 		for (int b = 0; b < 2; b++)
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc(b, h, row, col);
+				half_rc(lt, b, h, row, col);
 				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
 			}
 	} else {
 		const int v = w - nA2;
 		const int rb = v / np, jc = v % np;
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = tid; e < MS * MS; e += kThreads) {
+		for (int e = lt; e < MS * MS; e += kThreads / 2) {
 			const int i = e / MS, l = e % MS;
 			const double2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
-			sh.pl[0][i * LD + l] = x.x;
-			sh.pl[1][i * LD + l] = x.y;
+			xr[i * LD + l] = x.x;
+			xi[i * LD + l] = x.y;
 		}
-		load_q(sh.pl[4], sh.pl[5], Qr + (size_t)jc * MS * MS);
-		__syncthreads();
-		cgemm(sh.pl[0], sh.pl[1], LD, 1, false, sh.pl[4], sh.pl[5], cr, ci);  // V Qc
+		load_q_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+		half_sync(half);
+		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // V Qc
 #pragma unroll
 		for (int b = 0; b < 2; b++)
 #pragma unroll
 			for (int h = 0; h < 2; h++) {
 				int row, col;
-				acc_rc(b, h, row, col);
+				half_rc(lt, b, h, row, col);
 				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_double2(cr[b][h], ci[b][h]);
 			}
 	}
-	__syncthreads();
+	half_sync(half);
 }
 
 // Buffers: A_r lives in bufs[(r + 1) % 3] (A_{-1} = the input in A0); Q_r in
 // Qbuf + (r & 1) * np * MS * MS.
-__global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, double2* A1, double2* A2, double2* V,
+__global__ void __launch_bounds__(kThreads, 1) bjacobi_kernel(double2* A0, double2* A1, double2* A2, double2* V,
 		double2* Qbuf, int kp, int max_sweeps, double tol, double tau_final, int* counters,
 		unsigned long long* tmax) {
 	cg::grid_group grid = cg::this_grid();
@@ -518,7 +571,6 @@ __global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, doubl
 	const int p2count = split ? (int)gridDim.x - np : (int)gridDim.x;
 
 	if (tid == 0) {
-		sh.total = 0;
 		sh.cnt = 0;
 		sh.tmax = 0ULL;
 	}
@@ -542,8 +594,9 @@ __global__ void __launch_bounds__(kThreads, 2) bjacobi_kernel(double2* A0, doubl
 			const int ro = (int)((t - 1) % rounds);
 			const double2* src = bufs[(t + 2) % 3];
 			double2* dst = bufs[t % 3];
-			for (int w = (int)blockIdx.x - p2first; w < nW; w += p2count)
-				phase2_item(sh, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+			const int half = tid / (kThreads / 2);
+			for (int w = 2 * ((int)blockIdx.x - p2first) + half; w < nW; w += 2 * p2count)
+				phase2_item(sh, half, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
 		}
 		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
 		if (sweep_end && tid == 0) {
@@ -588,7 +641,7 @@ cudaError_t launch_bjacobi(double2* A0, double2* A1, double2* A2, double2* V, do
 	e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bjacobi_kernel, kThreads, smem);
 	if (e != cudaSuccess) return e;
 	if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-	const int blocks = num_sms * per_sm;
+	const int blocks = num_sms * std::min(per_sm, 1);
 	double tol = 1e-15;
 	if (!(tau_final > 0.0)) tau_final = kTauFinal;
 	unsigned long long* tmax = reinterpret_cast<unsigned long long*>(counters + jacobi_tmax_offset(max_sweeps));
