@@ -267,31 +267,37 @@ __global__ void jacobi_init_kernel(const double2* __restrict__ S, int k, int kp,
 
 // Normalises the first k columns of V in place (removes the norm drift that
 // the accumulated rotations leave). 32 columns per CTA, 8 row groups.
-__global__ void __launch_bounds__(256) normalize_columns_kernel(double2* V, int k, int kp) {
-	__shared__ double part[8][32];
+// Columns j of V scaled to unit norm: 32 columns per CTA, 32 row groups; the
+// row loops are unrolled by 4 so that several loads are in flight per thread.
+__global__ void __launch_bounds__(1024) normalize_columns_kernel(double2* V, int k, int kp) {
+	__shared__ double part[32][33];
 	const int cl = threadIdx.x & 31, rg = threadIdx.x >> 5;
 	const int j = blockIdx.x * 32 + cl;
 	double sum = 0.0;
-	if (j < k)
-		for (int i = rg; i < kp; i += 8) {
+	if (j < k) {
+#pragma unroll 4
+		for (int i = rg; i < kp; i += 32) {
 			const double2 v = __ldcg(V + (long long)i * kp + j);
 			sum += v.x * v.x + v.y * v.y;
 		}
+	}
 	part[rg][cl] = sum;
 	__syncthreads();
 	if (rg == 0) {
 		double t = 0.0;
-		for (int r = 0; r < 8; r++) t += part[r][cl];
+		for (int r = 0; r < 32; r++) t += part[r][cl];
 		part[0][cl] = t > 0.0 ? 1.0 / sqrt(t) : 1.0;
 	}
 	__syncthreads();
 	const double f = part[0][cl];
-	if (j < k)
-		for (int i = rg; i < kp; i += 8) {
+	if (j < k) {
+#pragma unroll 4
+		for (int i = rg; i < kp; i += 32) {
 			const long long o = (long long)i * kp + j;
 			const double2 v = __ldcg(V + o);
 			V[o] = make_double2(v.x * f, v.y * f);
 		}
+	}
 }
 
 // Sort the k eigenvalues ascending (bitonic, one CTA) and run the checks of
@@ -338,9 +344,15 @@ __global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* _
 			__syncthreads();
 		}
 	}
+	// the checks in eigenvalue order: the first failing n, found in parallel
+	__shared__ int first_bad;
+	if (threadIdx.x == 0) first_bad = k;
+	__syncthreads();
 	for (int i = threadIdx.x; i < k; i += blockDim.x) {
 		perm[i] = idx[i];
-		evals[i] = __ldcg(A + (long long)idx[i] * kp + idx[i]).x;
+		const double v = __ldcg(A + (long long)idx[i] * kp + idx[i]).x;
+		evals[i] = v;
+		if (check && (v <= 0.0 || !(v >= 2.2250738585072014e-308) || isinf(v) || v != v)) atomicMin(&first_bad, i);
 	}
 	__syncthreads();
 	if (threadIdx.x == 0) {
@@ -350,18 +362,14 @@ __global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* _
 		s.bad_value = 0.0;
 		s.pad = 0;
 		s.sweeps = counters[max_sweeps];
-		if (s.sweeps < 0) s.status = ITP2D_E_EIGENSOLVER;
-		for (int n = 0; n < k && s.status == ITP2D_OK && check; n++) {
-			const double v = evals[n];
-			if (v <= 0.0) {
-				s.status = ITP2D_E_NONPOSITIVE_EIGENVALUE;
-				s.bad_index = n;
-				s.bad_value = v;
-			} else if (!(v >= 2.2250738585072014e-308) || isinf(v) || v != v) {
-				s.status = ITP2D_E_NONNORMAL_EIGENVALUE;
-				s.bad_index = n;
-				s.bad_value = v;
-			}
+		if (s.sweeps < 0) {
+			s.status = ITP2D_E_EIGENSOLVER;
+		} else if (first_bad < k) {
+			const int n = first_bad;
+			const double v = __ldcg(A + (long long)idx[n] * kp + idx[n]).x;
+			s.status = v <= 0.0 ? ITP2D_E_NONPOSITIVE_EIGENVALUE : ITP2D_E_NONNORMAL_EIGENVALUE;
+			s.bad_index = n;
+			s.bad_value = v;
 		}
 		*st = s;
 	}
@@ -433,7 +441,7 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 		e = cudaLaunchCooperativeKernel((void*)jacobi_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
 		if (e != cudaSuccess) return e;
 	}
-	normalize_columns_kernel<<<(k + 31) / 32, 256, 0, s>>>(w.V, k, kp);
+	normalize_columns_kernel<<<(k + 31) / 32, 1024, 0, s>>>(w.V, k, kp);
 	int P = 1;
 	while (P < k) P <<= 1;
 	const size_t smem = (size_t)P * (sizeof(double) + sizeof(int));
