@@ -155,37 +155,40 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 	for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Three-way BF16 split of an FP32 value (x = h + m + l exactly).
-__device__ __forceinline__ void split3(float x, uint32_t& h, uint32_t& m, uint32_t& l) {
-	const __nv_bfloat16 bh = __float2bfloat16_rn(x);
-	const float r1 = x - __bfloat162float(bh);
-	const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
-	const float r2 = r1 - __bfloat162float(bm);
-	h = __bfloat16_as_ushort(bh);
-	m = __bfloat16_as_ushort(bm);
-	l = __bfloat16_as_ushort(__float2bfloat16_rn(r2));
-}
-
 // Byte offset of element (row r, k) of a K-major no-swizzle 128 x 16 plane:
 // core matrix (r / 8, k / 8) at ((r / 8) * 2 + k / 8) * 128, rows 16 B apart.
 __host__ __device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
 	return (uint32_t)((((r >> 3) << 1) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// Three-way BF16 split of two FP32 values at once (x = h + m + l exactly:
+// each remainder is exact in FP32), with packed round-to-nearest
+// conversions; returns the h, m and l parts as bf16x2 words, x0 in the low
+// half.
+__device__ __forceinline__ void split3x2(float x0, float x1, uint32_t& h, uint32_t& m, uint32_t& l) {
+	const __nv_bfloat162 bh = __floats2bfloat162_rn(x0, x1);
+	const float2 fh = __bfloat1622float2(bh);
+	const float r0 = x0 - fh.x, r1 = x1 - fh.y;
+	const __nv_bfloat162 bm = __floats2bfloat162_rn(r0, r1);
+	const float2 fm = __bfloat1622float2(bm);
+	const __nv_bfloat162 bl = __floats2bfloat162_rn(r0 - fm.x, r1 - fm.y);
+	h = *reinterpret_cast<const uint32_t*>(&bh);
+	m = *reinterpret_cast<const uint32_t*>(&bm);
+	l = *reinterpret_cast<const uint32_t*>(&bl);
+}
+
 // Writes two consecutive K elements (k even) of row r, split into the six
 // planes of one operand: planes 0..2 real hi/mid/lo, 3..5 imaginary.
 __device__ __forceinline__ void put2(unsigned char* op, uint32_t off, float re0, float im0, float re1, float im1) {
-	uint32_t h0, m0, l0, h1, m1, l1;
-	split3(re0, h0, m0, l0);
-	split3(re1, h1, m1, l1);
-	*reinterpret_cast<uint32_t*>(op + 0 * kPlaneBytes + off) = h0 | (h1 << 16);
-	*reinterpret_cast<uint32_t*>(op + 1 * kPlaneBytes + off) = m0 | (m1 << 16);
-	*reinterpret_cast<uint32_t*>(op + 2 * kPlaneBytes + off) = l0 | (l1 << 16);
-	split3(im0, h0, m0, l0);
-	split3(im1, h1, m1, l1);
-	*reinterpret_cast<uint32_t*>(op + 3 * kPlaneBytes + off) = h0 | (h1 << 16);
-	*reinterpret_cast<uint32_t*>(op + 4 * kPlaneBytes + off) = m0 | (m1 << 16);
-	*reinterpret_cast<uint32_t*>(op + 5 * kPlaneBytes + off) = l0 | (l1 << 16);
+	uint32_t h, m, l;
+	split3x2(re0, re1, h, m, l);
+	*reinterpret_cast<uint32_t*>(op + 0 * kPlaneBytes + off) = h;
+	*reinterpret_cast<uint32_t*>(op + 1 * kPlaneBytes + off) = m;
+	*reinterpret_cast<uint32_t*>(op + 2 * kPlaneBytes + off) = l;
+	split3x2(im0, im1, h, m, l);
+	*reinterpret_cast<uint32_t*>(op + 3 * kPlaneBytes + off) = h;
+	*reinterpret_cast<uint32_t*>(op + 4 * kPlaneBytes + off) = m;
+	*reinterpret_cast<uint32_t*>(op + 5 * kPlaneBytes + off) = l;
 }
 
 // The 24 MMAs of one step. Accumulators: h h products in columns 0..255
