@@ -356,42 +356,56 @@ __global__ void __launch_bounds__(kThreads, 1) overlap_tc_kernel(const float2* _
 	tc_setup(sh);
 	const int tid = threadIdx.x;
 	unsigned char* const base = sh.buf;
+	// a diagonal tile pair (ti == tj) has one operand: B reads A's planes
+	const bool diag = ti == tj;
 	// raw slot: operand o (0 = rows i0.., 1 = rows j0..), row r, 16-byte piece
 	// pc (two complex) stored at slot pc ^ 4 (r & 1)
+	auto fetch = [&](unsigned char* slot, long long gb, int it) {
+		const int idx = it * kThreads + tid;  // 0..2047
+		const int o = idx >> 10, r = (idx >> 3) & 127, pc = idx & 7;
+		const int row = (o ? j0 : i0) + r;
+		const long long g = gb + 2 * pc;
+		const bool in = row < k && g < g1;  // g even, g1 even: both complex in range
+		const float2* src = in ? psi + (long long)row * G + g : psi;
+		cp16(smem_u32(slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4)), src,
+				in ? 16 : 0);
+	};
 	auto prefetch = [&](int s) {
 		unsigned char* slot = base + kOvRaw + (s % 3) * kOvRawSlot;
 		const long long gb = g0 + (long long)s * KT;
 #pragma unroll
-		for (int it = 0; it < 8; it++) {
-			const int idx = it * kThreads + tid;  // 0..2047
-			const int o = idx >> 10, r = (idx >> 3) & 127, pc = idx & 7;
-			const int row = (o ? j0 : i0) + r;
-			const long long g = gb + 2 * pc;
-			const bool in = row < k && g < g1;  // g even, g1 even: both complex in range
-			const float2* src = in ? psi + (long long)row * G + g : psi;
-			cp16(smem_u32(slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4)), src,
-					in ? 16 : 0);
+		for (int it = 0; it < 4; it++) fetch(slot, gb, it);
+		if (!diag) {
+#pragma unroll
+			for (int it = 4; it < 8; it++) fetch(slot, gb, it);
 		}
 	};
 	// convert: warp w handles core matrices m = w, w + 8, ... of the 64 (two
 	// operands x 16 row groups x 2 K halves); lane = (row in group) * 4 + pair
+	auto convert_one = [&](const unsigned char* slot, unsigned char* planes, int it) {
+		const int w = tid >> 5, lane = tid & 31;
+		const int m = it * 8 + w;
+		const int o = m >> 5, rg = (m >> 1) & 15, kc = m & 1;
+		const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+		const int pc = kk >> 1;
+		const float4 v = *reinterpret_cast<const float4*>(
+				slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4));
+		put2(planes + o * kOperandBytes, kmaj_off(r, kk), v.x, v.y, v.z, v.w);
+	};
 	auto convert = [&](int s) {
 		const unsigned char* slot = base + kOvRaw + (s % 3) * kOvRawSlot;
 		unsigned char* planes = base + kOvPlanes + (s & 1) * 2 * kOperandBytes;
-		const int w = tid >> 5, lane = tid & 31;
 #pragma unroll
-		for (int it = 0; it < 8; it++) {
-			const int m = it * 8 + w;
-			const int o = m >> 5, rg = (m >> 1) & 15, kc = m & 1;
-			const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
-			const int pc = kk >> 1;
-			const float4 v = *reinterpret_cast<const float4*>(
-					slot + o * (TM * kRawRowBytes) + r * kRawRowBytes + ((pc ^ ((r & 1) << 2)) << 4));
-			put2(planes + o * kOperandBytes, kmaj_off(r, kk), v.x, v.y, v.z, v.w);
+		for (int it = 0; it < 4; it++) convert_one(slot, planes, it);
+		if (!diag) {
+#pragma unroll
+			for (int it = 4; it < 8; it++) convert_one(slot, planes, it);
 		}
 	};
 	auto a_addr = [&](int s) { return smem_u32(base + kOvPlanes + (s & 1) * 2 * kOperandBytes); };
-	auto b_addr = [&](int s) { return smem_u32(base + kOvPlanes + (s & 1) * 2 * kOperandBytes + kOperandBytes); };
+	auto b_addr = [&](int s) {
+		return smem_u32(base + kOvPlanes + (s & 1) * 2 * kOperandBytes + (diag ? 0 : kOperandBytes));
+	};
 	run_pipeline(sh, nsteps, true, prefetch, convert, a_addr, b_addr, err);
 	if (!sh.abort) {
 		double2* out = part + (size_t)blockIdx.y * k * k;
