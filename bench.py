@@ -2,8 +2,9 @@
 B200, mixed (FP32 sweeps + FP64 refinement) and plain FP64 forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dot|bumpy]
 
-Workload (the magnetic quantum dot): V = r^2/2, B = 1 (linear gauge), periodic
+Workload "dot" (the default, the magnetic quantum dot): V = r^2/2, B = 1 (linear gauge), periodic
 256 x 256 grid of side 14, k = 500 states from seeded complex Gaussian noise,
 4th-order multi-product split (halforder 2) at eps = 0.05, canonical
 orthonormalisation every step. A solve runs ITP iterations until the 250
@@ -12,6 +13,12 @@ lowest states change their energy by less than 1e-9 between iterations
 step is one such solve from the same initial states; "converged states" are
 the states passing the final test (for the mixed form, only those whose
 energy also agrees with the plain FP64 solve within 1e-9).
+
+Workload "bumpy" (the bumpy dot): V = r^2/2 plus 400 Gaussian bumps (amplitude
+uniform in [0.8, 1.2], width 0.1, centres uniform in |x|, |y| < 6, seeded),
+B = 0.5, periodic 512 x 512 grid of side 16, k = 2000 states, 6th-order split
+(halforder 3) at eps = 0.05, until the 1000 lowest pass abschange(1e-9). The
+reference CPU arm is not timed for it (one reference iteration takes minutes).
 
 Multi-GPU (torchrun): independent replicas, one solve per rank (weak scaling).
 """
@@ -33,13 +40,38 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Converged states/s at |ΔE|≤1e-9, mixed vs plain FP64 (1 B200); p50/p99 solve latency"
 UNIT = "converged states/s"
-WORKLOAD = dict(sx=256, sy=256, length=14.0, B=1.0, halforder=2, num_states=500, wanted=250, eps=0.05,
-                potential="harmonic(1)", test="abschange(1e-9)", seed=20240601)
+WORKLOADS = {
+    "dot": dict(name="magnetic dot", sx=256, sy=256, length=14.0, B=1.0, halforder=2, num_states=500, wanted=250,
+                eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240601),
+    "bumpy": dict(name="bumpy dot", sx=512, sy=512, length=16.0, B=0.5, halforder=3, num_states=2000, wanted=1000,
+                  eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240602,
+                  bumps=dict(n=400, amp=(0.8, 1.2), width=0.1, box=6.0, seed=20240603)),
+}
+WORKLOAD = WORKLOADS["dot"]
 # Solve length and converged count of the plain FP64 form on the initial states above
 # (measured by this benchmark's own FP64 solve and re-checked every run); used only to
 # extrapolate the reference CPU arm, which times a bounded sample of iterations.
 FP64_SOLVE_STEPS = 33
 FP64_CONVERGED = 285
+
+
+def extra_potential():
+    """The workload's seeded Gaussian bumps on the cell-centred grid (added to
+    the parsed potential like the reference's user noise), or None."""
+    w = WORKLOAD
+    b = w.get("bumps")
+    if not b:
+        return None
+    rng = np.random.default_rng(b["seed"])
+    amp = rng.uniform(b["amp"][0], b["amp"][1], size=b["n"])
+    cen = rng.uniform(-b["box"], b["box"], size=(b["n"], 2))
+    dx = w["length"] / w["sx"]
+    x = (2 * np.arange(w["sx"]) + 1 - w["sx"]) * dx / 2
+    y = (2 * np.arange(w["sy"]) + 1 - w["sy"]) * dx / 2
+    V = np.zeros((w["sy"], w["sx"]))
+    for a, (cx, cy) in zip(amp, cen):
+        V += a * np.exp(-((x[None, :] - cx) ** 2 + (y[:, None] - cy) ** 2) / (2 * b["width"] ** 2))
+    return V
 
 
 def initial_states(pinned=True):
@@ -130,7 +162,8 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
     from itp2d_b200 import capi, system
     w = WORKLOAD
     k = w["num_states"]
-    s = system.ITPSystem(params(form), init_states=psi, stream=stream.cuda_stream)
+    s = system.ITPSystem(params(form), extra_potential=extra_potential(), init_states=psi,
+                         stream=stream.cuda_stream)
     ctx = s.context_handle()
     L = capi.lib()
 
@@ -206,6 +239,11 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if WORKLOAD is not WORKLOADS["dot"]:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU arm is timed on the dot workload "
+                                                              "only (one reference iteration of this one takes "
+                                                              "minutes)"}))
+        return
     psi, _ = initial_states(pinned=False)
     from oracle import refkit as R
     if not R.available():
@@ -232,16 +270,18 @@ def reference_arm(args):
 
 def config_block(form):
     w = WORKLOAD
-    return {"workload": f"magnetic dot: V=r^2/2, B={w['B']}, periodic {w['sx']}x{w['sy']}, L={w['length']}, "
-                        f"k={w['num_states']} states, 4th-order multi-product split, eps={w['eps']}, "
-                        f"solve until the {w['wanted']} lowest pass {w['test']}",
+    bumps = (f" + {w['bumps']['n']} Gaussian bumps (width {w['bumps']['width']})" if w.get("bumps") else "")
+    state_mb = w["num_states"] * w["sx"] * w["sy"] * 16 / 1e6
+    return {"workload": f"{w['name']}: V=r^2/2{bumps}, B={w['B']}, periodic {w['sx']}x{w['sy']}, L={w['length']}, "
+                        f"k={w['num_states']} states, {2 * w['halforder']}th-order multi-product split, "
+                        f"eps={w['eps']}, solve until the {w['wanted']} lowest pass {w['test']}",
             "form": form, "global_batch": w["num_states"], "grid": [w["sx"], w["sy"]],
-            "parallelism": "replicas", "l2": "inputs (524 MB of states) exceed the 126 MB L2"}
+            "parallelism": "replicas", "l2": f"inputs ({state_mb:.0f} MB of states) exceed the 126 MB L2"}
 
 
-# DRAM bytes (read + write) per launch of the phase's dominant kernel, from one ncu
-# capture of `python bench.py --steps 1 --warmup 1 --form mixed` (profiles/
-# bjacobi_regfft_tc_magnetic_dot_256_k500.md): block Jacobi 8.44 + 2.80 MB.
+# DRAM bytes (read + write) per launch of the phase's dominant kernel, from ncu
+# captures of `python bench.py --steps 1 --warmup 1 --form mixed` on the dot
+# workload (the block Jacobi matrices stay in L2, so the figure is small).
 PROFILED_TRAFFIC = {"eigensolve_fp64": 11.24e6}
 
 
@@ -340,7 +380,10 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed"],
                     help="run one form only (profiling); the headline needs both")
+    ap.add_argument("--workload", default="dot", choices=sorted(WORKLOADS))
     args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -412,7 +455,7 @@ def main():
     roofline.update({"traffic": PROFILED_TRAFFIC.get(dom), "kernel": dom, "peak_source": roof[dom]["peak_source"]})
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and args.workload == "dot":
         cs = cpu_reference_sample(np.ascontiguousarray(psi), args.cpu_iters)
         if cs:
             cpu = {"value": FP64_CONVERGED / (FP64_SOLVE_STEPS * cs["sec_per_iter"]), "unit": UNIT,
