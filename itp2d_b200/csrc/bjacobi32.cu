@@ -57,6 +57,7 @@ struct Shared32 {
 	float4 rot[2][NR];  // rotation j: (sin, tau, Re e, Im e)
 	float rap[2][NR], raq[2][NR];  // M(p, p), M(q, q) after the round
 	int rpq[2][NR];     // p | q << 8 | applied << 16
+	int next[2];  // phase-2 item of each CTA half
 	int cnt;
 	unsigned long long tmax;  // bits of a non-negative double
 };
@@ -267,14 +268,6 @@ __device__ __forceinline__ void half_sync(int half) {
 	asm volatile("bar.sync %0, %1;\n" ::"r"(1 + half), "r"(kThreads / 2) : "memory");
 }
 
-__device__ void load_q32_half(int lt, float* qr, float* qi, const float2* Qg) {
-	for (int e = lt; e < MS * MS; e += kThreads / 2) {
-		const float2 v = __ldcg(Qg + e);
-		qr[(e / MS) * LD + (e % MS)] = v.x;
-		qi[(e / MS) * LD + (e % MS)] = v.y;
-	}
-}
-
 __device__ __forceinline__ int rr_position(int p, int r, int npos) {
 	if (p == 0) return 0;
 	const int m = npos - 1;
@@ -392,6 +385,7 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 	float* br = sh.pl[6 * half + 4];
 	float* bi = sh.pl[6 * half + 5];
 	const int nA2 = np * (np - 1);
+	constexpr int NH = MS * MS / (kThreads / 2);  // elements per thread and operand
 	float cr[2][2], ci[2][2];
 	if (w < nA2) {
 		const int jr = w / (np - 1);
@@ -399,14 +393,25 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 		if (jc >= jr) jc++;
 		const int Pr = rr_player(jr, ro, nb), Qr_ = rr_player(nb - 1 - jr, ro, nb);
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = lt; e < MS * MS; e += kThreads / 2) {
-			const int i = e / MS, l = e % MS;
-			const float2 v = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
-			xr[i * LD + l] = v.x;
-			xi[i * LD + l] = v.y;
+		// all global loads of the item at once, then the shared-memory stores
+		float2 lx[NH], la[NH], lb[NH];
+#pragma unroll
+		for (int it = 0; it < NH; it++) {
+			const int e = it * (kThreads / 2) + lt, i = e / MS, l = e % MS;
+			lx[it] = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
+			la[it] = __ldcg(Qr + (size_t)jr * MS * MS + e);
+			lb[it] = __ldcg(Qr + (size_t)jc * MS * MS + e);
 		}
-		load_q32_half(lt, ar, ai, Qr + (size_t)jr * MS * MS);
-		load_q32_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+#pragma unroll
+		for (int it = 0; it < NH; it++) {
+			const int e = it * (kThreads / 2) + lt, o = (e / MS) * LD + e % MS;
+			xr[o] = lx[it].x;
+			xi[o] = lx[it].y;
+			ar[o] = la[it].x;
+			ai[o] = la[it].y;
+			br[o] = lb[it].x;
+			bi[o] = lb[it].y;
+		}
 		half_sync(half);
 		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // T = X Qc
 		half_sync(half);
@@ -433,13 +438,21 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 		const int v = w - nA2;
 		const int rb = v / np, jc = v % np;
 		const int Pc = rr_player(jc, ro, nb), Qc = rr_player(nb - 1 - jc, ro, nb);
-		for (int e = lt; e < MS * MS; e += kThreads / 2) {
-			const int i = e / MS, l = e % MS;
-			const float2 x = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
-			xr[i * LD + l] = x.x;
-			xi[i * LD + l] = x.y;
+		float2 lx[NH], lb[NH];
+#pragma unroll
+		for (int it = 0; it < NH; it++) {
+			const int e = it * (kThreads / 2) + lt, i = e / MS, l = e % MS;
+			lx[it] = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
+			lb[it] = __ldcg(Qr + (size_t)jc * MS * MS + e);
 		}
-		load_q32_half(lt, br, bi, Qr + (size_t)jc * MS * MS);
+#pragma unroll
+		for (int it = 0; it < NH; it++) {
+			const int e = it * (kThreads / 2) + lt, o = (e / MS) * LD + e % MS;
+			xr[o] = lx[it].x;
+			xi[o] = lx[it].y;
+			br[o] = lb[it].x;
+			bi[o] = lb[it].y;
+		}
 		half_sync(half);
 		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // V Qc
 #pragma unroll
@@ -457,7 +470,8 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 // The cooperative solve: bjacobi_kernel of bjacobi.cu in FP32 (one CTA per SM). A_r lives in
 // bufs[(r + 1) % 3] (A_{-1} = the input in A0); Q_r in Qbuf + (r & 1) * np * MS^2.
 __global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, float2* A1, float2* A2, float2* V,
-		float2* Qbuf, int kp, int max_sweeps, double tau_final, int* counters, unsigned long long* tmaxg) {
+		float2* Qbuf, int kp, int max_sweeps, double tau_final, int* counters, unsigned long long* tmaxg,
+		int* p2ctr) {
 	cg::grid_group grid = cg::this_grid();
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	Shared32& sh = *reinterpret_cast<Shared32*>(smem_raw);
@@ -473,6 +487,9 @@ __global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, floa
 	const int p1 = split ? np : (int)gridDim.x;
 	const int p2first = split ? np : 0;
 	const int p2count = split ? (int)gridDim.x - np : (int)gridDim.x;
+	// with many phase-2 items the phase-1 CTAs take items too once their own
+	// subproblems are done (phase 2 is then the longer phase)
+	const bool join = split && nW > 8 * p2count;
 	if (tid == 0) {
 		sh.cnt = 0;
 		sh.tmax = 0ULL;
@@ -483,6 +500,8 @@ __global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, floa
 	long long t = 0;
 	for (;;) {
 		const bool do_p1 = !stop;
+		// round t + 1's item counter (its last use, round t - 3, is complete)
+		if (blockIdx.x == 0 && tid == 0) p2ctr[(t + 1) & 3] = 0;
 		const bool do_p2 = t >= 1;
 		if (do_p1 && (int)blockIdx.x < p1) {
 			const float2* prev = bufs[t % 3];
@@ -492,13 +511,25 @@ __global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, floa
 				phase1_item32(sh, j, t, rounds, nb, np, kp, prev, prev2, Qbuf + ((t + 1) & 1) * qstride,
 						Qbuf + (t & 1) * qstride, out);
 		}
-		if (do_p2 && (int)blockIdx.x >= p2first) {
+		if (do_p2 && ((int)blockIdx.x >= p2first || join)) {
 			const int ro = (int)((t - 1) % rounds);
 			const float2* src = bufs[(t + 2) % 3];
 			float2* dst = bufs[t % 3];
-			const int half = tid / (kThreads / 2);
-			for (int w = 2 * ((int)blockIdx.x - p2first) + half; w < nW; w += 2 * p2count)
+			// items handed out by the round's counter; the next index is fetched
+			// while the current item is processed
+			const int half = tid / (kThreads / 2), lt = tid & (kThreads / 2 - 1);
+			int* ctr = p2ctr + ((t - 1) & 3);
+			if (lt == 0) sh.next[half] = atomicAdd(ctr, 1);
+			half_sync(half);
+			int w = sh.next[half];
+			while (w < nW) {
+				int wn = 0;
+				if (lt == 0) wn = atomicAdd(ctr, 1);
 				phase2_item32(sh, half, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+				if (lt == 0) sh.next[half] = wn;
+				half_sync(half);
+				w = sh.next[half];
+			}
 		}
 		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
 		if (sweep_end && tid == 0) {
@@ -578,7 +609,8 @@ cudaError_t launch_bjacobi32(const double2* S, int k, JacobiWork& w, int num_sms
 	int* counters = w.counters;
 	unsigned long long* tmax = reinterpret_cast<unsigned long long*>(counters + jacobi_tmax_offset(ms));
 	float2 *a0 = w.f32.A0, *a1 = w.f32.A1, *a2 = w.f32.A2, *v = w.f32.V, *q = w.f32.Qbuf;
-	void* args[] = {&a0, &a1, &a2, &v, &q, &kpv, &ms, &tau, &counters, &tmax};
+	int* p2ctr = counters + jacobi_p2ctr_offset(ms);
+	void* args[] = {&a0, &a1, &a2, &v, &q, &kpv, &ms, &tau, &counters, &tmax, &p2ctr};
 	e = cudaLaunchCooperativeKernel((void*)bjacobi32_kernel, dim3(blocks), dim3(kThreads), args, smem, s);
 	if (e != cudaSuccess) return e;
 	widen_result_kernel<<<gblocks, 256, 0, s>>>(w.f32.A0, w.f32.A1, w.f32.A2, w.f32.V, kp, w.counters, ms, w.A0,

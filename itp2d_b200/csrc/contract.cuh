@@ -95,9 +95,11 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
 // Counter block of the Jacobi kernel, in ints: per-sweep rotation counts, the
 // result fields at [max_sweeps] and [max_sweeps + 1], then per-sweep maxima of
-// the rotation tangents as 64-bit words starting at jacobi_tmax_offset().
+// the rotation tangents as 64-bit words starting at jacobi_tmax_offset(), then
+// the four phase-2 item counters of the block path (round r in slot r & 3).
 constexpr size_t jacobi_tmax_offset(int max_sweeps) { return ((size_t)max_sweeps + 4 + 1) & ~(size_t)1; }
-constexpr size_t jacobi_counter_ints(int max_sweeps) { return jacobi_tmax_offset(max_sweeps) + 2 * (size_t)max_sweeps + 2; }
+constexpr size_t jacobi_p2ctr_offset(int max_sweeps) { return jacobi_tmax_offset(max_sweeps) + 2 * (size_t)max_sweeps + 2; }
+constexpr size_t jacobi_counter_ints(int max_sweeps) { return jacobi_p2ctr_offset(max_sweeps) + 4; }
 size_t jacobi_counters(int max_sweeps);
 
 }  // namespace itp2d
