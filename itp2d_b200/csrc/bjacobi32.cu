@@ -39,6 +39,10 @@ constexpr int PL = MS * LD;   // floats per plane
 // 256 2 x 2 blocks of M while threads [256, 512) rotate the columns of Q.
 constexpr int kThreads = 512;
 constexpr int kMThreads = NR * NR;
+// Phase 2 runs on four groups of 128 threads, each on its own block product:
+// four DRAM-latency-bound products in flight per SM.
+constexpr int kGroups = 4;
+constexpr int kGT = kThreads / kGroups;
 constexpr int kFullEvery = 16;
 constexpr float kSkipRel = 1e-7f;
 constexpr float kNoiseRel = 1e-6f;
@@ -50,14 +54,14 @@ __device__ __forceinline__ int rr_player(int pos, int r, int npos) {
 __device__ __forceinline__ int gidx(int i, int P, int Q) { return i < BS ? P * BS + i : Q * BS + (i - BS); }
 
 struct Shared32 {
-	// phase 1: [0,1] M, [2,3] Q, [4,5] formation operands; phase 2: half h of
-	// the CTA uses [6h, 6h + 6): X/T, Q_r, Q_c
-	float pl[12][PL];
+	// phase 1: [0,1] M, [2,3] Q, [4,5] formation operands; phase 2: group g
+	// of the CTA uses [6g, 6g + 6): X/T, Q_r, Q_c
+	float pl[6 * kGroups][PL];
 	// rotations of two consecutive inner rounds (round r in buffer r & 1)
 	float4 rot[2][NR];  // rotation j: (sin, tau, Re e, Im e)
 	float rap[2][NR], raq[2][NR];  // M(p, p), M(q, q) after the round
 	int rpq[2][NR];     // p | q << 8 | applied << 16
-	int next[2];  // phase-2 item of each CTA half
+	int next[kGroups];  // phase-2 item of each thread group
 	int cnt;
 	unsigned long long tmax;  // bits of a non-negative double
 };
@@ -248,24 +252,24 @@ __device__ __forceinline__ void cmm32(const float* ar, const float* ai, int as_i
 	}
 }
 
-// Half-CTA products of phase 2: thread lt of 256, warp lw = lt >> 5 owns rows
-// 4 lw .. 4 lw + 3; lane (h, l) computes rows 4 lw + h + 2r at columns l + 16c.
-__device__ __forceinline__ void half_rc(int lt, int r, int c, int& row, int& col) {
+// Group products of phase 2: thread lt of 128, warp lw = lt >> 5 owns rows
+// 8 lw .. 8 lw + 7; lane (h, l) computes rows 8 lw + h + 2r at columns l + 16c.
+__device__ __forceinline__ void group_rc(int lt, int r, int c, int& row, int& col) {
 	const int lane = lt & 31, lw = lt >> 5;
-	row = 4 * lw + (lane >> 4) + 2 * r;
+	row = 8 * lw + (lane >> 4) + 2 * r;
 	col = (lane & 15) + 16 * c;
 }
 
-__device__ __forceinline__ void half_gemm(int lt, const float* ar, const float* ai, int as_i, int as_m, bool conjA,
-		const float* br, const float* bi, float (&cr)[2][2], float (&ci)[2][2]) {
+__device__ __forceinline__ void group_gemm(int lt, const float* ar, const float* ai, int as_i, int as_m, bool conjA,
+		const float* br, const float* bi, float (&cr)[4][2], float (&ci)[4][2]) {
 	int row0, col0;
-	half_rc(lt, 0, 0, row0, col0);
-	cmm32<2, 2>(ar, ai, as_i, as_m, conjA, br, bi, row0, 2, col0, 16, cr, ci);
+	group_rc(lt, 0, 0, row0, col0);
+	cmm32<4, 2>(ar, ai, as_i, as_m, conjA, br, bi, row0, 2, col0, 16, cr, ci);
 }
 
-// Barrier of one half of the CTA (named barrier 1 + half, 256 threads).
-__device__ __forceinline__ void half_sync(int half) {
-	asm volatile("bar.sync %0, %1;\n" ::"r"(1 + half), "r"(kThreads / 2) : "memory");
+// Barrier of one thread group (named barrier 1 + g, 128 threads).
+__device__ __forceinline__ void group_sync(int g) {
+	asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "r"(kGT) : "memory");
 }
 
 __device__ __forceinline__ int rr_position(int p, int r, int npos) {
@@ -372,21 +376,20 @@ __device__ void phase1_item32(Shared32& sh, int j, long long t, int rounds, int 
 	__syncthreads();
 }
 
-// Phase 2 item w of round ro (bjacobi.cu phase2_item in FP32), on one half of
-// the CTA: the two halves take alternate items, each with its own planes and
-// named barrier.
-__device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int np, int kp, const float2* src,
+// Phase 2 item w of round ro (bjacobi.cu phase2_item in FP32), on one thread
+// group of the CTA, with its own planes and named barrier.
+__device__ void phase2_item32(Shared32& sh, int g, int w, int ro, int nb, int np, int kp, const float2* src,
 		float2* dst, float2* V, const float2* Qr) {
-	const int lt = threadIdx.x & (kThreads / 2 - 1);
-	float* xr = sh.pl[6 * half + 0];
-	float* xi = sh.pl[6 * half + 1];
-	float* ar = sh.pl[6 * half + 2];
-	float* ai = sh.pl[6 * half + 3];
-	float* br = sh.pl[6 * half + 4];
-	float* bi = sh.pl[6 * half + 5];
+	const int lt = threadIdx.x & (kGT - 1);
+	float* xr = sh.pl[6 * g + 0];
+	float* xi = sh.pl[6 * g + 1];
+	float* ar = sh.pl[6 * g + 2];
+	float* ai = sh.pl[6 * g + 3];
+	float* br = sh.pl[6 * g + 4];
+	float* bi = sh.pl[6 * g + 5];
 	const int nA2 = np * (np - 1);
-	constexpr int NH = MS * MS / (kThreads / 2);  // elements per thread and operand
-	float cr[2][2], ci[2][2];
+	constexpr int NH = MS * MS / kGT;  // elements per thread and operand
+	float cr[4][2], ci[4][2];
 	if (w < nA2) {
 		const int jr = w / (np - 1);
 		int jc = w % (np - 1);
@@ -397,14 +400,14 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 		float2 lx[NH], la[NH], lb[NH];
 #pragma unroll
 		for (int it = 0; it < NH; it++) {
-			const int e = it * (kThreads / 2) + lt, i = e / MS, l = e % MS;
+			const int e = it * kGT + lt, i = e / MS, l = e % MS;
 			lx[it] = __ldcg(src + (long long)gidx(i, Pr, Qr_) * kp + gidx(l, Pc, Qc));
 			la[it] = __ldcg(Qr + (size_t)jr * MS * MS + e);
 			lb[it] = __ldcg(Qr + (size_t)jc * MS * MS + e);
 		}
 #pragma unroll
 		for (int it = 0; it < NH; it++) {
-			const int e = it * (kThreads / 2) + lt, o = (e / MS) * LD + e % MS;
+			const int e = it * kGT + lt, o = (e / MS) * LD + e % MS;
 			xr[o] = lx[it].x;
 			xi[o] = lx[it].y;
 			ar[o] = la[it].x;
@@ -412,26 +415,26 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 			br[o] = lb[it].x;
 			bi[o] = lb[it].y;
 		}
-		half_sync(half);
-		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // T = X Qc
-		half_sync(half);
+		group_sync(g);
+		group_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // T = X Qc
+		group_sync(g);
 #pragma unroll
-		for (int r = 0; r < 2; r++)
+		for (int r = 0; r < 4; r++)
 #pragma unroll
 			for (int c = 0; c < 2; c++) {
 				int row, col;
-				half_rc(lt, r, c, row, col);
+				group_rc(lt, r, c, row, col);
 				xr[row * LD + col] = cr[r][c];
 				xi[row * LD + col] = ci[r][c];
 			}
-		half_sync(half);
-		half_gemm(lt, ar, ai, 1, LD, true, xr, xi, cr, ci);  // Qr^H T
+		group_sync(g);
+		group_gemm(lt, ar, ai, 1, LD, true, xr, xi, cr, ci);  // Qr^H T
 #pragma unroll
-		for (int r = 0; r < 2; r++)
+		for (int r = 0; r < 4; r++)
 #pragma unroll
 			for (int c = 0; c < 2; c++) {
 				int row, col;
-				half_rc(lt, r, c, row, col);
+				group_rc(lt, r, c, row, col);
 				dst[(long long)gidx(row, Pr, Qr_) * kp + gidx(col, Pc, Qc)] = make_float2(cr[r][c], ci[r][c]);
 			}
 	} else {
@@ -441,30 +444,30 @@ __device__ void phase2_item32(Shared32& sh, int half, int w, int ro, int nb, int
 		float2 lx[NH], lb[NH];
 #pragma unroll
 		for (int it = 0; it < NH; it++) {
-			const int e = it * (kThreads / 2) + lt, i = e / MS, l = e % MS;
+			const int e = it * kGT + lt, i = e / MS, l = e % MS;
 			lx[it] = __ldcg(V + (long long)(rb * MS + i) * kp + gidx(l, Pc, Qc));
 			lb[it] = __ldcg(Qr + (size_t)jc * MS * MS + e);
 		}
 #pragma unroll
 		for (int it = 0; it < NH; it++) {
-			const int e = it * (kThreads / 2) + lt, o = (e / MS) * LD + e % MS;
+			const int e = it * kGT + lt, o = (e / MS) * LD + e % MS;
 			xr[o] = lx[it].x;
 			xi[o] = lx[it].y;
 			br[o] = lb[it].x;
 			bi[o] = lb[it].y;
 		}
-		half_sync(half);
-		half_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // V Qc
+		group_sync(g);
+		group_gemm(lt, xr, xi, LD, 1, false, br, bi, cr, ci);  // V Qc
 #pragma unroll
-		for (int r = 0; r < 2; r++)
+		for (int r = 0; r < 4; r++)
 #pragma unroll
 			for (int c = 0; c < 2; c++) {
 				int row, col;
-				half_rc(lt, r, c, row, col);
+				group_rc(lt, r, c, row, col);
 				V[(long long)(rb * MS + row) * kp + gidx(col, Pc, Qc)] = make_float2(cr[r][c], ci[r][c]);
 			}
 	}
-	half_sync(half);
+	group_sync(g);
 }
 
 // The cooperative solve: bjacobi_kernel of bjacobi.cu in FP32 (one CTA per SM). A_r lives in
@@ -517,18 +520,18 @@ __global__ void __launch_bounds__(kThreads, 1) bjacobi32_kernel(float2* A0, floa
 			float2* dst = bufs[t % 3];
 			// items handed out by the round's counter; the next index is fetched
 			// while the current item is processed
-			const int half = tid / (kThreads / 2), lt = tid & (kThreads / 2 - 1);
+			const int g = tid / kGT, lt = tid & (kGT - 1);
 			int* ctr = p2ctr + ((t - 1) & 3);
-			if (lt == 0) sh.next[half] = atomicAdd(ctr, 1);
-			half_sync(half);
-			int w = sh.next[half];
+			if (lt == 0) sh.next[g] = atomicAdd(ctr, 1);
+			group_sync(g);
+			int w = sh.next[g];
 			while (w < nW) {
 				int wn = 0;
 				if (lt == 0) wn = atomicAdd(ctr, 1);
-				phase2_item32(sh, half, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
-				if (lt == 0) sh.next[half] = wn;
-				half_sync(half);
-				w = sh.next[half];
+				phase2_item32(sh, g, w, ro, nb, np, kp, src, dst, V, Qbuf + ((t + 1) & 1) * qstride);
+				if (lt == 0) sh.next[g] = wn;
+				group_sync(g);
+				w = sh.next[g];
 			}
 		}
 		const bool sweep_end = do_p1 && (t % rounds == rounds - 1);
