@@ -89,16 +89,18 @@ def test_rotation_tensor_cores(sx, sy, k):
     assert np.median(diff) < 1e-4
 
 
-def test_fp32_block_jacobi_canonical():
+@pytest.mark.parametrize("sx,k", [(128, 320), (128, 1024)])
+def test_fp32_block_jacobi_canonical(sx, k):
     """k >= 256: the FP32 form solves the overlap eigenproblem by block Jacobi
     in single precision (stopping at a rotation tangent of 1e-3). The result is
     the canonical orthonormalisation Psi' = Psi V L^{-1/2} of stateset.cpp:136-232
     up to the FP32 accuracy: with M = Psi'^H Psi dx^2 = L^{1/2} V^H, M M^H is
     diagonal and its diagonal holds the eigenvalues of S. These checks do not
-    depend on the gaps between eigenvalues (the eigenvectors themselves do)."""
-    sx = sy = 128
-    k = 320
-    c, dx = _ctx(sx, sy, k, seed=11)
+    depend on the gaps between eigenvalues (the eigenvectors themselves do).
+    k = 1024 has more block products per round than the phase-2 CTAs take in
+    eight turns, so the phase-1 CTAs take products as well."""
+    sy = sx
+    c, dx = _ctx(sx, sy, k, seed=11 + k)
     psi0 = c.download().reshape(k, -1)
     S = (psi0.conj() @ psi0.T) * dx * dx
     S0 = np.abs(S - np.diag(np.diag(S))) / np.sqrt(np.outer(np.diag(S).real, np.diag(S).real))
