@@ -114,9 +114,12 @@ def test_fp32_block_jacobi_canonical(sx, k):
     off = np.max(np.abs(MM - np.diag(lam)) / np.sqrt(np.outer(lam, lam)))
     ev = np.linalg.eigvalsh(S)
     lam_err = np.max(np.abs(lam - ev) / ev)
-    print(f"FP32 block Jacobi k={k}: orthonormality {dev:.2e}, off-diagonal {np.max(S0):.1e} -> {off:.2e}, "
-          f"eigenvalues {lam_err:.2e}")
-    assert dev < TOL_ORTHO
+    # the overlap's split-BF16 error (TOL_S relative to the diagonal) reaches
+    # the output's Gram matrix scaled by 1 / lambda_min through W = V L^{-1/2}
+    tol_dev = 2 * TOL_S * np.max(np.diag(S).real) / ev.min()
+    print(f"FP32 block Jacobi k={k}: orthonormality {dev:.2e} (bound {tol_dev:.1e}), off-diagonal "
+          f"{np.max(S0):.1e} -> {off:.2e}, eigenvalues {lam_err:.2e}")
+    assert dev < tol_dev
     assert np.all(np.diff(lam) > -1e-4 * lam[1:])  # ascending, as the sort leaves them
     assert off < 1e-4
     assert lam_err < 1e-4
