@@ -281,8 +281,9 @@ def config_block(form):
 
 # DRAM bytes (read + write) per launch of the phase's dominant kernel, from ncu
 # captures of `python bench.py --steps 1 --warmup 1 --form mixed` on the dot
-# workload (the block Jacobi matrices stay in L2, so the figure is small).
-PROFILED_TRAFFIC = {"eigensolve_fp64": 11.24e6}
+# workload (the block Jacobi matrices stay in L2, so the figures are small):
+# bjacobi32_kernel 4.24 + 1.06 MB, bjacobi_kernel 8.46 + 3.05 MB.
+PROFILED_TRAFFIC = {"eigensolve_fp32": 5.30e6, "eigensolve_fp64": 11.51e6}
 
 
 def max_over_ranks(x, dist, device):
@@ -452,7 +453,8 @@ def main():
     roof = phase_rooflines(rh, fp64_peak, fp32_peak)
     dom = max(roof, key=lambda n: roof[n]["ms_per_solve"])
     roofline = {key: roof[dom][key] for key in ("bound", "achieved", "peak", "unit", "frac")}
-    roofline.update({"traffic": PROFILED_TRAFFIC.get(dom), "kernel": dom, "peak_source": roof[dom]["peak_source"]})
+    traffic = PROFILED_TRAFFIC.get(dom) if args.workload == "dot" else None
+    roofline.update({"traffic": traffic, "kernel": dom, "peak_source": roof[dom]["peak_source"]})
 
     cpu = None
     if rank == 0 and args.workload == "dot":
