@@ -3,9 +3,10 @@
 // The FP32 form's overlap is accurate to about 1e-5 (split-BF16 tensor-core
 // contraction) and its eigensolve stops at a largest rotation tangent of 1e-3,
 // so FP64 arithmetic buys nothing there. This is the schedule of bjacobi.cu —
-// round-robin pairs of 16-index blocks, 32 x 32 subproblems swept on 16 CTAs
-// (cross pairs only except every 16th round), phase 1 of round t pipelined
-// against phase 2 of round t - 1, one grid barrier per round — in single
+// round-robin pairs of 16-index blocks, 32 x 32 subproblems swept by one CTA
+// per pair (k_p / 32 of them; cross pairs only except every 16th round),
+// phase 1 of round t pipelined against phase 2 of round t - 1 (here on four
+// 128-thread groups per CTA), one grid barrier per round — in single
 // precision: the rotation set-up uses the hardware square root and reciprocal
 // square root directly (no Newton refinement), and the block products are
 // FFMA. Its latency chains are the short ones of FP32, which is what the
