@@ -10,6 +10,7 @@ import numpy as np
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 import bench  # noqa: E402
+from itp2d_b200 import capi  # noqa: E402
 
 
 def _with(name):
@@ -48,3 +49,36 @@ def test_bumpy_potential_is_seeded_gaussian_sum():
         assert "6th-order" in cfg["workload"]
     finally:
         _with("dot")
+
+
+def test_phase_rooflines_arithmetic():
+    """Per-phase rooflines from synthetic per-solve stats: algorithmic bytes and
+    flops over the phase time, split by precision, eigensolve flops scaled by
+    the sweeps of that precision."""
+    import json
+    import os
+    _with("dot")
+    w = bench.WORKLOAD
+    k, G, m = w["num_states"], w["sx"] * w["sy"], w["halforder"]
+    stats = {(p, ph): (0.0, 0) for p in ("fp64", "fp32") for ph in capi.PHASES}
+    stats[("fp64", "propagate")] = (10.0, 5)
+    stats[("fp64", "overlap")] = (4.0, 5)
+    stats[("fp32", "eigensolve")] = (20.0, 10)
+    r = {"stats": stats, "sweeps": {"fp64": 0.0, "fp32": 40.0}}
+    roof = bench.phase_rooflines(r, fp64_peak=40.0, fp32_peak=80.0)
+    assert set(roof) == {"propagate_fp64", "overlap_fp64", "eigensolve_fp32"}  # phases with calls only
+    try:  # the measured copy bandwidth, else the benchmark's stated fallback
+        hbm = json.load(open(os.path.join(bench.ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except (OSError, KeyError, ValueError):
+        hbm = 6650.0
+    p = roof["propagate_fp64"]
+    assert abs(p["achieved"] - k * G * 16 * (2 * m * (m + 2) + (m - 1)) * 5 / 10e-3 / 1e9) < 1e-6 * p["achieved"]
+    assert abs(p["frac"] - p["achieved"] / hbm) < 1e-12 and p["unit"] == "GB/s"
+    o = roof["overlap_fp64"]
+    assert abs(o["achieved"] - 4 * k * k * G * 5 / 4e-3 / 1e12) < 1e-9 * o["achieved"]
+    assert o["peak"] == 40.0 and o["bound"] == "tensor"
+    e = roof["eigensolve_fp32"]
+    kp = (k + 31) // 32 * 32
+    flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp * 40.0
+    assert abs(e["achieved"] - flops / 20e-3 / 1e12) < 1e-9 * e["achieved"]
+    assert e["peak"] == 80.0 and e["bound"] == "fp32" and e["sweeps_per_solve"] == 40.0
