@@ -203,6 +203,16 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
  * No counterpart in the reference. */
 int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double* evals, double* evecs);
 
+/* Adds Gaussian impurities to a potential on the device:
+ * V[y][x] += sum_j A_j exp(-r_j^2 / (2 w_j^2)), with r_j the distance of the
+ * cell-centred grid point (x_i = (2i + 1 - sx) dx / 2) from impurity j, in
+ * list order at every point — GaussianImpurities::add_noise (noise.cpp:24-40)
+ * for a whole impurity list. impurities holds n rows (x, y, A, w) and V holds
+ * sx * sy doubles; both must be device (or managed) memory, otherwise
+ * ITP2D_E_INVALID. Asynchronous on cuda_stream (NULL: the default stream). */
+int itp2d_add_gaussian_impurities(int sx, int sy, double dx, int n, const double* impurities, double* V,
+		void* cuda_stream);
+
 /* Measures the FP64 tensor-core (DMMA) throughput of the current device in
  * TFLOP/s with a register-only kernel: the roofline denominator of the FP64
  * contractions. Diagnostic; no reference counterpart. */

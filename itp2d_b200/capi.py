@@ -82,6 +82,7 @@ def lib():
         L.itp2d_device_fp32_peak.argtypes = [dp]
         L.itp2d_hermitian_eigensolve.argtypes = [i, dp, dp, dp]
         L.itp2d_device_fp64_peak.argtypes = [dp]
+        L.itp2d_add_gaussian_impurities.argtypes = [i, i, C.c_double, i, vp, vp, vp]
         L.itp2d_status_string.argtypes = [i]
         L.itp2d_status_string.restype = C.c_char_p
         _lib = L
@@ -102,6 +103,16 @@ def device_fp32_peak() -> float:
     t = C.c_double(0.0)
     _check(lib().itp2d_device_fp32_peak(C.byref(t)), "itp2d_device_fp32_peak")
     return t.value
+
+
+def add_gaussian_impurities(sx: int, sy: int, dx: float, impurities_ptr: int, n: int, V_ptr: int,
+                            stream: int = 0) -> None:
+    """V += Gaussian impurities on the device (itp2d_add_gaussian_impurities);
+    impurities_ptr points to n rows (x, y, A, w) and V_ptr to sx * sy doubles,
+    both device memory (for example torch tensors' data_ptr())."""
+    _check(lib().itp2d_add_gaussian_impurities(sx, sy, dx, n, C.c_void_p(impurities_ptr), C.c_void_p(V_ptr),
+                                               C.c_void_p(stream) if stream else None),
+           "itp2d_add_gaussian_impurities")
 
 
 def device_fp64_peak() -> float:
