@@ -439,3 +439,17 @@ def bumpy_potential(g: Grid, nbumps: int, seed: int, amp=(0.8, 1.2), width=0.1, 
     for j in range(nbumps):
         out += A[j] * np.exp(-((x - c[j, 0]) ** 2 + (y - c[j, 1]) ** 2) / (2 * width * width))
     return out
+
+
+def gaussian_impurities(g: Grid, impurities: np.ndarray, V: np.ndarray) -> np.ndarray:
+    """V plus the impurities (rows x, y, A, w) added one at a time in list order,
+    each as A*exp(-0.5*(r2/w2)) with r = impurity - grid point
+    (GaussianImpurities::add_noise, noise.cpp:24-40, on the grid of
+    datalayout.cpp:21-36). V is [sy][sx]; returns a new array."""
+    out = np.array(V, dtype=np.float64, copy=True)
+    px, py = g.posx[None, :], g.posy[:, None]
+    for cx, cy, A, w in np.asarray(impurities, dtype=np.float64):
+        rx = cx - px
+        ry = cy - py
+        out += A * np.exp(-0.5 * ((rx * rx + ry * ry) / (w * w)))
+    return out

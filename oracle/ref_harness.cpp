@@ -316,4 +316,19 @@ void refsys_times(void* h, double* t) {
 	t[6] = sys->get_convtest_time();
 }
 
+/* V += the impurities of imp (rows x, y, A, w), one GaussianImpurities::add_noise
+ * call each in list order (noise.cpp:24-40) on a DataLayout(sx, sy, dx); the RNG
+ * only satisfies the constructor and is never drawn from. */
+void ref_add_gaussian_impurities(int sx, int sy, double dx, int n, const double* imp, double* V) {
+	DataLayout dl(static_cast<size_t>(sx), static_cast<size_t>(sy), dx);
+	RNG rng(1UL);
+	GaussianImpurities g(0.0, 0.0, 0.0, 0.0, rng);
+	std::vector<double> params(2);
+	for (int j = 0; j < n; j++) {
+		params[0] = imp[4 * j + 2];
+		params[1] = imp[4 * j + 3];
+		g.add_noise(imp[4 * j], imp[4 * j + 1], params, dl, V);
+	}
+}
+
 } // extern "C"

@@ -67,12 +67,24 @@ def lib():
         L.refsys_last_energies.restype = i
         L.refsys_get_states.argtypes = [vp, dp]
         L.refsys_times.argtypes = [vp, dp]
+        L.ref_add_gaussian_impurities.argtypes = [i, i, d, i, dp, dp]
+        L.ref_add_gaussian_impurities.restype = None
         _lib = L
     return _lib
 
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def add_gaussian_impurities(sx: int, sy: int, dx: float, impurities: np.ndarray, V: np.ndarray) -> np.ndarray:
+    """V plus the impurities (rows x, y, A, w) through the reference's
+    GaussianImpurities::add_noise (noise.cpp:24-40); returns a new [sy][sx] array."""
+    imp = np.ascontiguousarray(impurities, dtype=np.float64).reshape(-1, 4)
+    out = np.ascontiguousarray(V, dtype=np.float64).copy()
+    assert out.shape == (sy, sx)
+    lib().ref_add_gaussian_impurities(sx, sy, dx, imp.shape[0], _dp(imp), _dp(out))
+    return out
 
 
 class RefSysParams(C.Structure):

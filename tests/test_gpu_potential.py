@@ -1,24 +1,19 @@
 """Gaussian impurity potentials built on the device (itp2d_add_gaussian_impurities)
-against the reference's host loop restated in numpy: GaussianImpurities::add_noise
-(noise.cpp:24-40) called once per impurity in list order, on the cell-centred grid
-of DataLayout (datalayout.cpp:21-35)."""
+against the oracle's restatement of the reference's host loop
+(GaussianImpurities::add_noise, noise.cpp:24-40, once per impurity in list order
+on the cell-centred grid of datalayout.cpp:21-35), which tests/test_oracle.py pins
+to the compiled reference."""
 import numpy as np
 import pytest
 
 from itp2d_b200 import capi
+from oracle import itp_oracle as O
 
 pytestmark = pytest.mark.gpu
 
 
 def _host_loop(V0, sx, sy, dx, imp):
-    V = V0.copy()
-    x = (2 * np.arange(sx) + 1 - sx) * dx / 2
-    y = (2 * np.arange(sy) + 1 - sy) * dx / 2
-    for cx, cy, A, w in imp:
-        rx = cx - x[None, :]
-        ry = cy - y[:, None]
-        V += A * np.exp(-0.5 * ((rx * rx + ry * ry) / (w * w)))
-    return V
+    return O.gaussian_impurities(O.Grid(sx, sy, dx), imp, V0)
 
 
 @pytest.mark.parametrize("sx,sy,n", [(96, 80, 300), (512, 512, 400)])

@@ -271,3 +271,21 @@ def test_restatement_matches_golden_fixtures(path):
     assert np.max(np.abs(mean.real - z["E"]) / np.abs(z["E"])) < 1e-13
     ortho, _ = O.orthonormalize(g, z["prop"])
     assert 1 - O.subspace_cosines(g, ortho, z["ortho"]).min() < 1e-12
+
+
+def test_gaussian_impurities_restatement_matches_reference(refkit_available):
+    """The numpy restatement of GaussianImpurities::add_noise (noise.cpp:24-40)
+    against the compiled reference on the same impurity list: bit-identical
+    (same operations in the same order, glibc exp on both sides)."""
+    if not refkit_available:
+        pytest.skip("oracle/_ref not built")
+    g = O.Grid.from_length(40, 28, 12.0)
+    rng = np.random.default_rng(7)
+    n = 60
+    imp = np.column_stack([rng.uniform(-6, 6, n), rng.uniform(-4, 4, n), rng.uniform(0.5, 1.5, n),
+                           rng.uniform(0.1, 0.3, n)])
+    V0 = O.harmonic(g)
+    ours = O.gaussian_impurities(g, imp, V0)
+    ref = R.add_gaussian_impurities(g.sx, g.sy, g.dx, imp, V0)
+    assert np.max(np.abs(ours - ref)) <= 1e-15 * np.max(np.abs(ref))
+    assert np.max(np.abs(ours - V0)) > 0.5  # the impurities are there
