@@ -215,6 +215,22 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
                 E=E, converged_mask=None, e2e_times=e2e_times, system=s)
 
 
+def host_description(threads: int) -> str:
+    """CPU model, logical cores and the reference's thread settings, for the
+    CPU-baseline record."""
+    model = "unknown CPU"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return (f"{model}, {os.cpu_count()} logical cores, {threads} OpenMP threads, "
+            f"OPENBLAS_NUM_THREADS={os.environ.get('OPENBLAS_NUM_THREADS', 'unset')}")
+
+
 def cpu_reference_sample(psi, iters=1, threads=None):
     """The itp2d reference (oracle/_ref) timed on the host cores for `iters`
     ITP iterations of the workload; returns seconds per iteration."""
@@ -257,7 +273,7 @@ def reference_arm(args):
     cores = os.cpu_count()
     sample = (f"{args.steps} single ITP iterations (propagate + orthonormalise + energies) of the workload, "
               f"{t_iter:.2f} s each; converged states/s extrapolated as {FP64_CONVERGED} converged states over "
-              f"{FP64_SOLVE_STEPS} iterations of the same algorithm")
+              f"{FP64_SOLVE_STEPS} iterations of the same algorithm; host: {host_description(cores)}")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_iter * FP64_SOLVE_STEPS * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -465,7 +481,8 @@ def main():
                    "sample": f"{args.cpu_iters} ITP iteration(s) of the workload with the reference compiled "
                              f"from its sources (substitute FFT, OpenBLAS, default orthonormalisation), "
                              f"{cs['sec_per_iter']:.2f} s/iteration, "
-                             f"extrapolated over {FP64_SOLVE_STEPS} iterations / {FP64_CONVERGED} converged states"}
+                             f"extrapolated over {FP64_SOLVE_STEPS} iterations / {FP64_CONVERGED} converged states; "
+                             f"host: {host_description(cs['threads'])}"}
 
     e2e_solve = statistics.mean(rh["e2e_times"])
     h2d = k * G * 16
