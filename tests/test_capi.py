@@ -30,3 +30,16 @@ def test_invalid_arguments_rejected_before_device_use():
     assert L.itp2d_ctx_create(22, 16, 0.1, 4, 0, 0.0, 1, 0, None, ctypes.byref(out)) == capi.E_UNSUPPORTED
     assert L.itp2d_ctx_create(8192, 16, 0.1, 4, 1, 1.0, 1, 0, None, ctypes.byref(out)) == capi.E_UNSUPPORTED
     assert L.itp2d_propagate(None) == capi.E_INVALID
+
+
+def test_impurity_arguments_rejected_before_device_use():
+    L = capi.lib()
+    V = ctypes.c_void_p(1)  # never dereferenced: every case below returns before a CUDA call
+    imp = ctypes.c_void_p(1)
+    add = L.itp2d_add_gaussian_impurities
+    assert add(0, 16, 0.1, 1, imp, V, None) == capi.E_INVALID       # empty grid
+    assert add(16, 16, 0.0, 1, imp, V, None) == capi.E_INVALID      # dx <= 0
+    assert add(16, 16, 0.1, -1, imp, V, None) == capi.E_INVALID     # negative count
+    assert add(16, 16, 0.1, 1, None, V, None) == capi.E_INVALID     # no impurity list
+    assert add(16, 16, 0.1, 1, imp, None, None) == capi.E_INVALID   # no potential
+    assert add(16, 16, 0.1, 0, None, V, None) == capi.OK            # nothing to add
