@@ -2,23 +2,27 @@
 B200, mixed (FP32 sweeps + FP64 refinement) and plain FP64 forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dot|bumpy]
+                    [--workload bumpy|dot] [--form both|mixed|fp64]
 
-Workload "dot" (the default, the magnetic quantum dot): V = r^2/2, B = 1 (linear gauge), periodic
-256 x 256 grid of side 14, k = 500 states from seeded complex Gaussian noise,
-4th-order multi-product split (halforder 2) at eps = 0.05, canonical
-orthonormalisation every step. A solve runs ITP iterations until the 250
-lowest states change their energy by less than 1e-9 between iterations
-(the reference's abschange(1e-9) as timestep and final test). One benchmark
-step is one such solve from the same initial states; "converged states" are
-the states passing the final test (for the mixed form, only those whose
-energy also agrees with the plain FP64 solve within 1e-9).
+Workload "bumpy" (the default, the bumpy dot): V = r^2/2 plus 400 Gaussian
+bumps (amplitude uniform in [0.8, 1.2], width 0.1, centres uniform in |x|,
+|y| < 6, seeded), B = 0.5 (linear gauge), periodic 512 x 512 grid of side 16,
+k = 2000 states from seeded complex Gaussian noise, 6th-order multi-product
+split (halforder 3) at eps = 0.05, canonical orthonormalisation every step,
+until the 1000 lowest states change their energy by less than 1e-9 between
+iterations (the reference's abschange(1e-9) as time-step and final test).
 
-Workload "bumpy" (the bumpy dot): V = r^2/2 plus 400 Gaussian bumps (amplitude
-uniform in [0.8, 1.2], width 0.1, centres uniform in |x|, |y| < 6, seeded),
-B = 0.5, periodic 512 x 512 grid of side 16, k = 2000 states, 6th-order split
-(halforder 3) at eps = 0.05, until the 1000 lowest pass abschange(1e-9). The
-reference CPU arm is not timed for it (one reference iteration takes minutes).
+Workload "dot" (the magnetic dot): V = r^2/2, B = 1, periodic 256 x 256 grid
+of side 14, k = 500, 4th-order split (halforder 2), eps = 0.05, the 250 lowest
+states.
+
+One benchmark step is one whole solve of the headline form from the same
+initial states (inputs resident in device memory). The headline is the mixed
+form; "converged states" are the states passing the final test whose energy
+also agrees with the plain FP64 solve within 1e-9. The FP64 form runs once as
+warm-up and min(K, 2) times timed, beside it; the end-to-end figure times
+min(K, 3) solves through the native driver with the initial states copied
+from pinned host memory and energies plus states copied back.
 
 Multi-GPU (torchrun): independent replicas, one solve per rank (weak scaling).
 """
@@ -42,17 +46,17 @@ METRIC = "Converged states/s at |ΔE|≤1e-9, mixed vs plain FP64 (1 B200); p50/
 UNIT = "converged states/s"
 WORKLOADS = {
     "dot": dict(name="magnetic dot", sx=256, sy=256, length=14.0, B=1.0, halforder=2, num_states=500, wanted=250,
-                eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240601),
+                eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240601,
+                golden="solve_magnetic_dot_256_k500.json"),
+    # fp64_solve: iterations and converged states of the FP64 form's solve of
+    # these initial states (the reference's algorithm), compared with every
+    # run's own FP64 solve (fp64_solve_check in the output line)
     "bumpy": dict(name="bumpy dot", sx=512, sy=512, length=16.0, B=0.5, halforder=3, num_states=2000, wanted=1000,
                   eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240602,
-                  bumps=dict(n=400, amp=(0.8, 1.2), width=0.1, box=6.0, seed=20240603)),
+                  bumps=dict(n=400, amp=(0.8, 1.2), width=0.1, box=6.0, seed=20240603),
+                  fp64_solve=(14, 1110), ortho_sample=(500, 256, 128)),
 }
-WORKLOAD = WORKLOADS["dot"]
-# Solve length and converged count of the plain FP64 form on the initial states above
-# (measured by this benchmark's own FP64 solve and re-checked every run); used only to
-# extrapolate the reference CPU arm, which times a bounded sample of iterations.
-FP64_SOLVE_STEPS = 33
-FP64_CONVERGED = 285
+WORKLOAD = WORKLOADS["bumpy"]
 
 
 def extra_potential():
@@ -157,8 +161,8 @@ def alg_bytes_split(w, b):
     return w["num_states"] * G * b * (2 * m * (m + 2) + (m - 1))
 
 
-def run_form(form, psi, K, W, torch, stream, e2e_buf):
-    """W warm-up solves, K timed solves (inputs resident), K end-to-end solves."""
+def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
+    """W warm-up solves, K timed solves (inputs resident), Ke2e end-to-end solves."""
     from itp2d_b200 import capi, system
     w = WORKLOAD
     k = w["num_states"]
@@ -201,7 +205,7 @@ def run_form(form, psi, K, W, torch, stream, e2e_buf):
     # end to end: host inputs copied in, energies and states copied out, per solve
     e2e_times = []
     Eh = np.empty(k)
-    for _ in range(K):
+    for _ in range(Ke2e):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s.reset(psi)           # H2D of the initial states from pinned memory
@@ -227,58 +231,142 @@ def host_description(threads: int) -> str:
                     break
     except OSError:
         pass
-    return (f"{model}, {os.cpu_count()} logical cores, {threads} OpenMP threads, "
-            f"OPENBLAS_NUM_THREADS={os.environ.get('OPENBLAS_NUM_THREADS', 'unset')}")
+    return (f"{model}, {os.cpu_count()} logical cores, {threads} OpenMP threads, BLAS calls outside OpenMP "
+            f"regions (HighMem ZGEMM, ZHEEV) on {threads} threads, inside them on 1")
 
 
-def cpu_reference_sample(psi, iters=1, threads=None):
-    """The itp2d reference (oracle/_ref) timed on the host cores for `iters`
-    ITP iterations of the workload; returns seconds per iteration."""
+def reference_solve():
+    """Length and yield of the plain FP64 solve of the workload: (iterations,
+    converged states, where the figures come from)."""
+    w = WORKLOAD
+    if w.get("golden"):
+        g = json.load(open(os.path.join(ROOT, "tests", "golden", w["golden"])))
+        return g["iterations"], g["converged"], f"the reference's own solve ({w['golden']})"
+    it, conv = w["fp64_solve"]
+    return it, conv, ("this benchmark's FP64 form, the reference's algorithm (checked every run as "
+                      "fp64_solve_check); the reference's own solve is out of reach at this size")
+
+
+def _noise_states(k, sy, sx, dx, seed):
+    rng = np.random.default_rng(seed)
+    psi = rng.standard_normal((k, sy, sx)) + 1j * rng.standard_normal((k, sy, sx))
+    return psi / (np.sqrt(np.sum(np.abs(psi) ** 2, axis=(1, 2))) * dx)[:, None, None]
+
+
+def cpu_reference_sample(threads=None, extras=False):
+    """One bounded sample of a reference ITP iteration (itpsystem.cpp:407-470)
+    on the host cores, with the reference compiled from its sources
+    (oracle/_ref). Returns the measured parts and the iteration time they
+    extrapolate to, or None without the library.
+
+    * propagate + energies: `threads` states of the full grid, one per OpenMP
+      thread (ITPSystem::propagate and calculate_energies loop over states,
+      itpsystem.cpp:243-256,473-511): scaled by k / threads;
+    * orthonormalisation (StateSet::orthonormalize, HighMem, stateset.cpp:136-232):
+      k_o states on a grid of G_o points, with the reference's own phase timers;
+      its overlap dots and ZGEMM lincomb scale as k^2 G and ZHEEV as k^3. The
+      magnetic dot runs it at full size (k_o = k, G_o = G), the bumpy dot at
+      k_o = 500 on 256 x 128.
+    With extras, the Default (per-grid-point ZGEMV) orthonormalisation is timed
+    too where it runs at full size, and the reference's substitute FFT is timed
+    against numpy's pocketfft on the same lines (both one thread)."""
     from oracle import refkit as R
     w = WORKLOAD
     if not R.available():
         return None
-    threads = threads or os.cpu_count() or 1
-    ref = R.RefSystem(w["sx"], w["sy"], w["length"], 0, w["B"], w["halforder"], w["num_states"], w["wanted"],
-                      [w["eps"]], eps_divisor=5.0, timestep_test=w["test"], final_test=w["test"],
-                      potential=w["potential"], init_states=psi, threads=threads, highmem=False)
+    T = threads or os.cpu_count() or 1
+    k, sx, sy, L = w["num_states"], w["sx"], w["sy"], w["length"]
+    G, dx = sx * sy, L / sx
+    t_start = time.perf_counter()
+    kit = R.RefKit(sx, sy, L, 0, w["B"], w["halforder"], w["eps"], T, potential=w["potential"],
+                   extra_potential=extra_potential(), threads=T)
+    st = _noise_states(T, sy, sx, dx, 1)
+    kit.set_states(st)
     t0 = time.perf_counter()
-    for _ in range(iters):
-        ref.step()
-    dt = (time.perf_counter() - t0) / iters
-    ph = ref.times()
-    ref.close()
-    return dict(sec_per_iter=dt, threads=threads, phases=ph)
+    kit.propagate()
+    t1 = time.perf_counter()
+    kit.energies()
+    t2 = time.perf_counter()
+    out = {"threads": T, "prop_s": t1 - t0, "energies_s": t2 - t1, "states_sampled": T}
+    if extras:
+        kit.set_states(st)
+        t0 = time.perf_counter()
+        kit.transform(2)  # FFTx over the kit's states, serial in the harness
+        t_shim = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        np.fft.fft(st, axis=-1)
+        t_np = time.perf_counter() - t0
+        out["fft_shim_over_pocketfft"] = t_shim / t_np
+    kit.close()
+    ko, sxo, syo = w.get("ortho_sample", (k, sx, sy))
+    Go = sxo * syo
+    algos = [True, False] if (extras and (ko, Go) == (k, G)) else [True]
+    for hm in algos:
+        ok = R.RefKit(sxo, syo, L * sxo / sx, 0, w["B"], w["halforder"], w["eps"], ko, highmem=hm, threads=T)
+        ok.set_states(_noise_states(ko, syo, sxo, dx, 2))
+        ok.orthonormalize()
+        out["ortho_highmem" if hm else "ortho_default"] = ok.ortho_times()
+        ok.close()
+    f2 = (k / ko) ** 2 * (G / Go)
+    f3 = (k / ko) ** 3
+    o = out["ortho_highmem"]
+    out["ortho_sample"] = {"states": ko, "grid": [sxo, syo], "k2G_scale": f2, "k3_scale": f3}
+    out["sec_per_iter"] = ((out["prop_s"] + out["energies_s"]) * k / T + (o["dot"] + o["lincomb"]) * f2
+                           + o["eigensolve"] * f3)
+    if "ortho_default" in out:
+        d = out["ortho_default"]
+        out["sec_per_iter_default_ortho"] = ((out["prop_s"] + out["energies_s"]) * k / T
+                                             + (d["dot"] + d["lincomb"]) * f2 + d["eigensolve"] * f3)
+    out["sample_s"] = time.perf_counter() - t_start
+    return out
+
+
+def describe_sample(cs, iters, conv, src):
+    w = WORKLOAD
+    o = cs["ortho_sample"]
+    full = o["states"] == w["num_states"] and o["grid"] == [w["sx"], w["sy"]]
+    txt = (f"one bounded sample per step of a reference ITP iteration (reference compiled from its sources with a "
+           f"substitute FFT and OpenBLAS 0.3.15): propagation + energies of {cs['states_sampled']} states on the "
+           f"full grid scaled by k/{cs['states_sampled']}, and a HighMem orthonormalisation of "
+           f"{o['states']} states on {o['grid'][0]}x{o['grid'][1]} points"
+           + ("" if full else f" scaled by (k/k_o)^2 (G/G_o) = {o['k2G_scale']:.0f} for its dots and ZGEMM and "
+                              f"(k/k_o)^3 = {o['k3_scale']:.0f} for ZHEEV")
+           + f"; {cs['sec_per_iter']:.1f} s per iteration extrapolated over {iters} iterations and {conv} converged "
+             f"states ({src})")
+    if "sec_per_iter_default_ortho" in cs:
+        txt += f"; the Default (ZGEMV) orthonormalisation gives {cs['sec_per_iter_default_ortho']:.1f} s per iteration"
+    else:
+        txt += ("; the Default (per-grid-point ZGEMV) orthonormalisation streams the k x k matrix once per grid "
+                "point and is slower at this size")
+    if "fft_shim_over_pocketfft" in cs:
+        txt += f"; substitute FFT / numpy pocketfft on the same lines = {cs['fft_shim_over_pocketfft']:.2f}"
+    return txt + f"; host: {host_description(cs['threads'])}"
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if WORKLOAD is not WORKLOADS["dot"]:
-        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU arm is timed on the dot workload "
-                                                              "only (one reference iteration of this one takes "
-                                                              "minutes)"}))
-        return
-    psi, _ = initial_states(pinned=False)
     from oracle import refkit as R
     if not R.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libitp2d_ref.so not built"}))
         return
-    for _ in range(args.warmup):
-        cpu_reference_sample(psi, 1)
-    samples = [cpu_reference_sample(psi, 1)["sec_per_iter"] for _ in range(args.steps)]
-    t_iter = statistics.mean(samples)
-    v = FP64_CONVERGED / (FP64_SOLVE_STEPS * t_iter)
-    cores = os.cpu_count()
-    sample = (f"{args.steps} single ITP iterations (propagate + orthonormalise + energies) of the workload, "
-              f"{t_iter:.2f} s each; converged states/s extrapolated as {FP64_CONVERGED} converged states over "
-              f"{FP64_SOLVE_STEPS} iterations of the same algorithm; host: {host_description(cores)}")
+    iters, conv, src = reference_solve()
+    for i in range(args.warmup):
+        first = cpu_reference_sample(extras=(i == 0))
+    samples = [cpu_reference_sample() for _ in range(args.steps)]
+    t_iter = statistics.mean(c["sec_per_iter"] for c in samples)
+    if args.warmup == 0:
+        first = samples[0]
+    first = dict(first, sec_per_iter=t_iter)
+    v = conv / (iters * t_iter)
+    cores = samples[0]["threads"]
+    sample = describe_sample(first, iters, conv, src)
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": t_iter * FP64_SOLVE_STEPS * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "warmup": args.warmup, "ms_per_step": statistics.mean(c["sample_s"] for c in samples) * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": config_block("reference CPU (OpenMP, OpenBLAS ZGEMM/ZHEEV, substitute FFT)"),
-           "impl": "reference",
+           "impl": "reference", "extrapolated_solve_s": iters * t_iter,
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -295,11 +383,9 @@ def config_block(form):
             "parallelism": "replicas", "l2": f"inputs ({state_mb:.0f} MB of states) exceed the 126 MB L2"}
 
 
-# DRAM bytes (read + write) per launch of the phase's dominant kernel, from ncu
-# captures of `python bench.py --steps 1 --warmup 1 --form mixed` on the dot
-# workload (the block Jacobi matrices stay in L2, so the figures are small):
-# bjacobi32_kernel 4.24 + 1.06 MB, bjacobi_kernel 8.46 + 3.05 MB.
-PROFILED_TRAFFIC = {"eigensolve_fp32": 5.30e6, "eigensolve_fp64": 11.51e6}
+# DRAM bytes (read + write) per launch of a phase's dominant kernel, from ncu
+# captures summarised under profiles/ (per workload; None where no capture).
+PROFILED_TRAFFIC = {"dot": {"eigensolve_fp32": 5.30e6, "eigensolve_fp64": 11.51e6}, "bumpy": {}}
 
 
 def max_over_ranks(x, dist, device):
@@ -332,10 +418,12 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
                  per 16 grid points per upper-triangle tile pair of 128 states
       rotation   FP64: 8 k^2 G flops; FP32: 24 MMAs of 128 x 128 x 16 per 16 states
                  per (128 states x 128 grid points) output tile
-      eigensolve block Jacobi: per sweep (kp/16 - 1) rounds of 32 x 32 block
-                 unitaries applied to both sides of the kp x kp matrix and to the
-                 eigenvector matrix, 3 * 8 * 32 * kp^2 flops per round (DMMA for
-                 FP64 states, FFMA for FP32 states)
+      eigensolve 10 k^3 flops per call (the algorithmic figure of a Hermitian
+                 eigensolve); the block Jacobi method's own work, per sweep
+                 (kp/16 - 1) rounds of 32 x 32 block unitaries applied to both
+                 sides of the kp x kp matrix and to the eigenvector matrix,
+                 3 * 8 * 32 * kp^2 flops per round (DMMA for FP64 states, FFMA
+                 for FP32 states), is reported beside it as method_tflops
     """
     w = WORKLOAD
     k, G, m = w["num_states"], w["sx"] * w["sy"], w["halforder"]
@@ -381,11 +469,27 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
         ms, calls = r["stats"][(prec, "eigensolve")]
         if calls == 0:
             continue
-        ach = sweep_flops * r["sweeps"][prec] / (ms * 1e-3) / 1e12
+        # algorithmic work: about 10 k^3 real flops per Hermitian eigensolve
+        ach = 10.0 * k ** 3 * calls / (ms * 1e-3) / 1e12
+        method = sweep_flops * r["sweeps"][prec] / (ms * 1e-3) / 1e12
         out[f"eigensolve_{prec}"] = {"bound": bound, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                                      "frac": ach / peak, "ms_per_solve": ms, "calls_per_solve": calls,
-                                     "sweeps_per_solve": r["sweeps"][prec], "peak_source": psrc}
+                                     "sweeps_per_solve": r["sweeps"][prec], "method_tflops": method,
+                                     "method_frac": method / peak, "peak_source": psrc}
     return out
+
+
+def fp64_solve_check(r64):
+    """The FP64 form's solve length and yield against the figures the reference
+    arm extrapolates with."""
+    iters, conv, src = reference_solve()
+    got_it, got_conv = r64["steps"][-1], r64["conv"][-1]
+    ok = got_it == iters and got_conv == conv
+    if not ok:
+        sys.stderr.write(f"bench: FP64 solve took {got_it} iterations with {got_conv} converged; the reference "
+                         f"arm extrapolates with {iters} and {conv} ({src})\n")
+    return {"expected_iterations": iters, "expected_converged": conv, "iterations": got_it, "converged": got_conv,
+            "source": src, "ok": ok}
 
 
 def main():
@@ -394,10 +498,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-iters", type=int, default=1)
     ap.add_argument("--form", default="both", choices=["both", "fp64", "mixed"],
                     help="run one form only (profiling); the headline needs both")
-    ap.add_argument("--workload", default="dot", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="bumpy", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample (profiling)")
     args = ap.parse_args()
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]
@@ -412,8 +516,9 @@ def main():
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
+
+        import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from itp2d_b200 import capi
     capi.lib()
@@ -421,68 +526,78 @@ def main():
     psi, pin = initial_states(pinned=True)
     w = WORKLOAD
     k, G = w["num_states"], w["sx"] * w["sy"]
-    e2e_buf = np.empty(2 * k * G)
-    import torch as _t
-    e2e_pin = _t.empty(2 * k * G, dtype=_t.float64, pin_memory=True)
+    e2e_pin = torch.empty(2 * k * G, dtype=torch.float64, pin_memory=True)
     e2e_buf = e2e_pin.numpy()
     fp64_peak = capi.device_fp64_peak()
     fp32_peak = capi.device_fp32_peak()
 
+    forms = ["fp64", "mixed"] if args.form == "both" else [args.form]
     results = {}
     with torch.cuda.stream(stream):
         with ClockSampler(local) as clk:
             if dist:
                 dist.barrier()
-            for form in (["fp64", "mixed"] if args.form == "both" else [args.form]):
-                results[form] = run_form(form, psi, args.steps, args.warmup, torch, stream, e2e_buf)
+            for form in forms:
+                head = form == forms[-1]
+                K = args.steps if head else min(args.steps, 2)
+                W = args.warmup if head else 1
+                results[form] = run_form(form, psi, K, W, min(args.steps, 3) if head else 0, torch, stream,
+                                         e2e_buf)
             if dist:
                 dist.barrier()
     clocks = clk.summary()
 
+    head = forms[-1]
     r64, rmx = results.get("fp64"), results.get("mixed")
     conv_mx = rmx["conv"][-1] if rmx else None
+    dE = None
     if r64 and rmx:
         # mixed converged states: pass the final test and agree with FP64 within 1e-9
         E64, Emx = r64["E"], rmx["E"]
         agree = int(np.sum(np.abs(Emx - E64) <= 1e-9))
         conv_mx = min(rmx["conv"][-1], agree)
+        dE = np.abs(Emx[:w["wanted"]] - E64[:w["wanted"]])
 
     def agg(r, conv):
         return replica_rate(conv, sum(r["times"]), len(r["times"]), world, dist, "cuda")
 
-    v64, s64 = agg(r64, r64["conv"][-1]) if r64 else (-1.0, None)
-    vmx, smx = agg(rmx, conv_mx) if rmx else (-1.0, None)
-    head = "mixed" if vmx >= v64 else "fp64"
+    v64, s64 = agg(r64, r64["conv"][-1]) if r64 else (None, None)
+    vmx, smx = agg(rmx, conv_mx) if rmx else (None, None)
     value, per_solve = (vmx, smx) if head == "mixed" else (v64, s64)
     rh = results[head]
     conv_h = conv_mx if head == "mixed" else r64["conv"][-1]
-    forms = {}
+    forms_out = {}
     if r64:
-        forms["fp64"] = {"value": v64, "converged": r64["conv"][-1], "iterations": r64["steps"][-1],
-                         "sec_per_solve": s64}
+        forms_out["fp64"] = {"value": v64, "converged": r64["conv"][-1], "iterations": r64["steps"][-1],
+                             "sec_per_solve": s64, "timed_solves": len(r64["times"])}
     if rmx:
-        forms["mixed"] = {"value": vmx, "converged": conv_mx, "iterations": rmx["steps"][-1], "sec_per_solve": smx}
+        forms_out["mixed"] = {"value": vmx, "converged": conv_mx, "iterations": rmx["steps"][-1],
+                              "sec_per_solve": smx, "timed_solves": len(rmx["times"])}
         if r64:
-            forms["mixed"]["max_abs_dE_vs_fp64_wanted"] = float(
-                np.max(np.abs(rmx["E"][:w["wanted"]] - r64["E"][:w["wanted"]])))
+            forms_out["mixed"]["over_fp64"] = vmx / v64
+            forms_out["mixed"]["dE_vs_fp64"] = {
+                "max": float(dE.max()), "p99": float(np.quantile(dE, 0.99)), "median": float(np.median(dE)),
+                "above_1e-9": int(np.sum(dE > 1e-9)),
+                "per_state": [float(f"{x:.2g}") for x in dE]}
+    if w.get("golden"):
+        g = np.array(json.load(open(os.path.join(ROOT, "tests", "golden", w["golden"])))["energies"])
+        for f, r in results.items():
+            forms_out[f]["max_abs_dE_vs_reference_solve"] = float(np.max(np.abs(r["E"][:w["wanted"]]
+                                                                               - g[:w["wanted"]])))
 
     roof = phase_rooflines(rh, fp64_peak, fp32_peak)
     dom = max(roof, key=lambda n: roof[n]["ms_per_solve"])
     roofline = {key: roof[dom][key] for key in ("bound", "achieved", "peak", "unit", "frac")}
-    traffic = PROFILED_TRAFFIC.get(dom) if args.workload == "dot" else None
-    roofline.update({"traffic": traffic, "kernel": dom, "peak_source": roof[dom]["peak_source"]})
+    roofline.update({"traffic": PROFILED_TRAFFIC[args.workload].get(dom), "kernel": dom,
+                     "peak_source": roof[dom]["peak_source"]})
 
     cpu = None
-    if rank == 0 and args.workload == "dot":
-        cs = cpu_reference_sample(np.ascontiguousarray(psi), args.cpu_iters)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cs = cpu_reference_sample()
         if cs:
-            cpu = {"value": FP64_CONVERGED / (FP64_SOLVE_STEPS * cs["sec_per_iter"]), "unit": UNIT,
-                   "cores": cs["threads"], "kind": "reference",
-                   "sample": f"{args.cpu_iters} ITP iteration(s) of the workload with the reference compiled "
-                             f"from its sources (substitute FFT, OpenBLAS, default orthonormalisation), "
-                             f"{cs['sec_per_iter']:.2f} s/iteration, "
-                             f"extrapolated over {FP64_SOLVE_STEPS} iterations / {FP64_CONVERGED} converged states; "
-                             f"host: {host_description(cs['threads'])}"}
+            iters, conv, src = reference_solve()
+            cpu = {"value": conv / (iters * cs["sec_per_iter"]), "unit": UNIT, "cores": cs["threads"],
+                   "kind": "reference", "sample": describe_sample(cs, iters, conv, src)}
 
     e2e_solve = statistics.mean(rh["e2e_times"])
     h2d = k * G * 16
@@ -495,16 +610,18 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": conv_h * world / e2e_solve, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "solves": len(rh["e2e_times"])},
         "gpu_launches": int(rh["launches"] * args.steps),
         "clocks": clocks,
-        "forms": forms,
-        "latency_s": {"p50": statistics.median(rh["times"]), "p99": max(rh["times"])},
+        "forms": forms_out,
+        "latency_s": {"p50": statistics.median(rh["times"]), "p99": float(np.quantile(rh["times"], 0.99)),
+                      "note": "spread of identical whole solves; request latency is the serving form's"},
         "phases": roof,
     }
+    if r64:
+        out["fp64_solve_check"] = fp64_solve_check(r64)
     if r64 and rmx:
-        out["phases_other_form"] = phase_rooflines(results["fp64" if head == "mixed" else "mixed"], fp64_peak,
-                                                  fp32_peak)
+        out["phases_other_form"] = phase_rooflines(r64, fp64_peak, fp32_peak)
     if rank == 0:
         print(json.dumps(out))
     if dist:

@@ -140,6 +140,7 @@ void* refkit_create(int sx, int sy, double len, int boundary, double B, int half
 	const size_t ws = std::max(k->T->required_workspace(), k->H.required_workspace() + 1);
 	if (threads < 1) threads = 1;
 	omp_set_num_threads(threads);
+	oracle_set_blas_threads(threads);
 	for (int i = 0; i < threads; i++) k->work.push_back(new StateArray(ws, k->dl));
 	return k;
 }
@@ -233,6 +234,17 @@ void refkit_transform(void* h, int kind) {
 		(*k->states)[i].transform(static_cast<Transform>(kind), k->tr);
 }
 
+/* Accumulated seconds of the last orthonormalisations of the kit's StateSet:
+ * [0] overlap dots, [1] eigensolve, [2] lincomb, [3] total
+ * (StateSet timers, stateset.hpp:77-80). */
+void refkit_ortho_times(void* h, double* t4) {
+	StateSet& st = *static_cast<Kit*>(h)->states;
+	t4[0] = st.get_dot_time();
+	t4[1] = st.get_eigensolve_time();
+	t4[2] = st.get_lincomb_time();
+	t4[3] = st.get_ortho_time();
+}
+
 double refkit_normalization_factor(void* h, int kind) {
 	return static_cast<Kit*>(h)->tr.normalization_factor(static_cast<Transform>(kind));
 }
@@ -265,6 +277,7 @@ void* refsys_create(const RefSysParams* p, const double* extra_potential, const 
 		s->noise = new ArrayNoise(extra_potential, G);
 		P.set_user_noise(*s->noise);
 	}
+	oracle_set_blas_threads(p->threads > 0 ? p->threads : 1);
 	s->sys = new ITPSystem(P);
 	if (init_states) {
 		const size_t G = static_cast<size_t>(p->sx) * static_cast<size_t>(p->sy);

@@ -50,6 +50,8 @@ def lib():
         L.refkit_how_orthonormal.restype = d
         L.refkit_energies.argtypes = [vp, dp, dp, dp]
         L.refkit_transform.argtypes = [vp, i]
+        L.refkit_ortho_times.argtypes = [vp, dp]
+        L.refkit_ortho_times.restype = None
         L.refkit_normalization_factor.argtypes = [vp, i]
         L.refkit_normalization_factor.restype = d
         L.refsys_create.restype = vp
@@ -156,6 +158,13 @@ class RefKit:
 
     def orthonormalize(self) -> int:
         return lib().refkit_orthonormalize(self.h)
+
+    def ortho_times(self) -> dict:
+        """Accumulated seconds of this kit's orthonormalisations, by phase
+        (StateSet timers, stateset.hpp:77-80)."""
+        t = np.empty(4)
+        lib().refkit_ortho_times(self.h, _dp(t))
+        return dict(zip(["dot", "eigensolve", "lincomb", "total"], t.tolist()))
 
     def how_orthonormal(self) -> float:
         return lib().refkit_how_orthonormal(self.h)

@@ -11,6 +11,21 @@
 extern "C" {
 #endif
 
+/* BLAS threading policy of the oracle (shim/blas_threads.c). The reference
+ * calls ZGEMM (HighMem lincomb, stateset.cpp:216-224) and ZHEEV
+ * (eigensolver.hpp:80-84) from one thread, outside its OpenMP loops, and the
+ * level-1/2 routines from inside them. A BLAS built for OpenMP programs runs
+ * the former on every core and the latter on one; the runtime linked here is
+ * a pthreads OpenBLAS, so these two calls are routed through wrappers that
+ * raise its thread count to oracle_blas_threads for the call (and only when
+ * no OpenMP region is active), while everything else stays single-threaded
+ * (OPENBLAS_NUM_THREADS=1). The renaming also applies to the reference's own
+ * zheev_ declaration, which follows the cblas.h include (eigensolver.hpp:41-46). */
+#define cblas_zgemm oracle_cblas_zgemm
+#define zheev_ oracle_zheev
+void oracle_set_blas_threads(int threads);
+int oracle_get_blas_threads(void);
+
 enum CBLAS_ORDER { CblasRowMajor = 101, CblasColMajor = 102 };
 enum CBLAS_TRANSPOSE { CblasNoTrans = 111, CblasTrans = 112, CblasConjTrans = 113 };
 

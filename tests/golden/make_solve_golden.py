@@ -1,0 +1,75 @@
+"""Runs the compiled itp2d reference (oracle/_ref, ``make -C oracle`` first)
+through a whole solve of a benchmark workload and stores its converged
+energies as a golden fixture.
+
+    python tests/golden/make_solve_golden.py [--workload dot|bumpy] [--threads T]
+
+Workloads (bench.py's WORKLOADS, same seeded initial states and potential):
+
+* dot: V = r^2/2, B = 1 (linear gauge), periodic 256 x 256 grid of side 14,
+  k = 500, 4th-order multi-product split at eps = 0.05, abschange(1e-9) as
+  time-step and final test on the 250 lowest states
+  -> solve_magnetic_dot_256_k500.json (a few minutes on 8 cores);
+* bumpy: V = r^2/2 + 400 seeded Gaussian bumps, B = 0.5, periodic 512 x 512
+  grid of side 16, k = 2000, 6th-order split, the 1000 lowest states
+  -> solve_bumpy_dot_512_k2000.json (hours on 8 cores, 17 GB of host memory).
+
+The eps divisor is 5 (the reference default) and the orthonormalisation is
+HighMem (one ZGEMM, stateset.cpp:214-228). The reference's ITPSystem::step
+(itpsystem.cpp:407-470) runs until is_finished(); the sorted energies,
+deviations, iteration count, converged count and the reference's own phase
+times (itpsystem.cpp:551-567) are written after every iteration, so an
+interrupted run leaves its progress behind (``finished`` false).
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+from oracle import refkit as R  # noqa: E402
+
+OUT = {"dot": "solve_magnetic_dot_256_k500.json", "bumpy": "solve_bumpy_dot_512_k2000.json"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="dot", choices=sorted(OUT))
+    ap.add_argument("--threads", type=int, default=os.cpu_count())
+    a = ap.parse_args()
+    w = bench.WORKLOADS[a.workload]
+    bench.WORKLOAD = w
+    psi, _ = bench.initial_states(pinned=False)
+    ref = R.RefSystem(w["sx"], w["sy"], w["length"], 0, w["B"], w["halforder"], w["num_states"], w["wanted"],
+                      [w["eps"]], eps_divisor=5.0, timestep_test=w["test"], final_test=w["test"],
+                      potential=w["potential"], extra_potential=bench.extra_potential(), init_states=psi,
+                      threads=a.threads, highmem=True, max_steps=5000, min_eps=1e-9)
+    del psi
+    path = os.path.join(HERE, OUT[a.workload])
+    t0 = time.perf_counter()
+    iter_s = []
+    while not ref.finished:
+        t1 = time.perf_counter()
+        ref.step()
+        iter_s.append(time.perf_counter() - t1)
+        assert not ref.error_flag
+        E, sig = ref.energies()
+        out = {"workload": bench.config_block("reference")["workload"], "seed": w["seed"],
+               "finished": ref.finished, "iterations": ref.total_steps, "converged": ref.num_converged,
+               "final_eps": ref.eps, "threads": a.threads, "seconds": time.perf_counter() - t0,
+               "seconds_per_iteration": iter_s, "energies": E.tolist(), "sigma": sig.tolist(),
+               "phase_seconds": ref.times()}
+        with open(path, "w") as f:
+            json.dump(out, f)
+        print(f"iteration {ref.total_steps}: eps {ref.eps:.4g}, {iter_s[-1]:.1f} s", flush=True)
+    print(f"wrote {path}: {ref.total_steps} iterations, {ref.num_converged} converged, "
+          f"{time.perf_counter() - t0:.0f} s")
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,30 @@ def _with(name):
     bench.WORKLOAD = bench.WORKLOADS[name]
 
 
+def test_default_workload_is_the_bumpy_dot():
+    import importlib
+    b = importlib.reload(bench)
+    assert b.WORKLOAD is b.WORKLOADS["bumpy"]
+    assert b.WORKLOAD["num_states"] == 2000 and b.WORKLOAD["halforder"] == 3
+
+
+def test_reference_solve_figures():
+    """The magnetic dot extrapolates with the reference's own solve (golden
+    fixture); the bumpy dot with the FP64 form's, which every run checks."""
+    _with("dot")
+    it, conv, src = bench.reference_solve()
+    assert (it, conv) == (32, 288) and "reference's own solve" in src
+    _with("bumpy")
+    try:
+        it, conv, src = bench.reference_solve()
+        assert (it, conv) == bench.WORKLOADS["bumpy"]["fp64_solve"] and "fp64_solve_check" in src
+        r64 = {"steps": [it], "conv": [conv]}
+        assert bench.fp64_solve_check(r64)["ok"]
+        assert not bench.fp64_solve_check({"steps": [it + 1], "conv": [conv]})["ok"]
+    finally:
+        _with("dot")
+
+
 def test_dot_has_no_extra_potential():
     _with("dot")
     assert bench.extra_potential() is None
@@ -78,7 +102,9 @@ def test_phase_rooflines_arithmetic():
     assert abs(o["achieved"] - 4 * k * k * G * 5 / 4e-3 / 1e12) < 1e-9 * o["achieved"]
     assert o["peak"] == 40.0 and o["bound"] == "tensor"
     e = roof["eigensolve_fp32"]
+    # algorithmic: 10 k^3 flops per eigensolve call
+    assert abs(e["achieved"] - 10.0 * k ** 3 * 10 / 20e-3 / 1e12) < 1e-9 * e["achieved"]
     kp = (k + 31) // 32 * 32
     flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp * 40.0
-    assert abs(e["achieved"] - flops / 20e-3 / 1e12) < 1e-9 * e["achieved"]
+    assert abs(e["method_tflops"] - flops / 20e-3 / 1e12) < 1e-9 * e["method_tflops"]
     assert e["peak"] == 80.0 and e["bound"] == "fp32" and e["sweeps_per_solve"] == 40.0

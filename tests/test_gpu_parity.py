@@ -175,11 +175,16 @@ def test_propagate_energies_match_oracle(capi, cfg):
     E, sig, res, Ei = c.energies()
     mean, sd = O.energies(H, ref)
     assert np.max(np.abs(E - mean.real) / np.abs(mean.real)) < 1e-12
-    # residual deviation: ||H psi - E psi|| / ||psi|| agrees with the oracle's
-    hp = H.apply(ref)
-    nr = np.sqrt(np.sum(np.abs(ref) ** 2, axis=(1, 2))) * g.dx
-    r_ref = np.sqrt(np.sum(np.abs(hp - mean.real[:, None, None] * ref) ** 2, axis=(1, 2))) * g.dx
-    assert np.max(np.abs(res - r_ref) / (r_ref + 1e-300)) < 1e-8 or np.all(nr > 0)
+    # residual deviation ||H psi - E psi|| of normalised states (the FP64 form
+    # takes states as normalised, like the reference): the second evaluation
+    # shifts by the first one's energies and has no cancellation
+    pn = ref / (np.sqrt(np.sum(np.abs(ref) ** 2, axis=(1, 2))) * g.dx)[:, None, None]
+    c.upload(pn)
+    c.energies()
+    E2, _, res2, _ = c.energies()
+    hp = H.apply(pn)
+    r_ref = np.sqrt(np.sum(np.abs(hp - E2[:, None, None] * pn) ** 2, axis=(1, 2))) * g.dx
+    assert np.max(np.abs(res2 - r_ref) / r_ref) < 1e-10
 
 
 def test_timestep_change_rebuilds_tables(capi):
@@ -287,7 +292,7 @@ def test_eigensolver_spectral_decomposition(capi):
     assert np.linalg.norm(M - R) < 300 * EPS
 
 
-@pytest.mark.parametrize("n", [3, 64, 255, 256, 600, 1000])
+@pytest.mark.parametrize("n", [3, 64, 255, 256, 600, 1000, 2000])
 def test_eigensolver_random(capi, n):
     rng = np.random.default_rng(n)
     X = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
@@ -295,11 +300,12 @@ def test_eigensolver_random(capi, n):
     ev, U = capi.hermitian_eigensolve(M)
     ref = np.linalg.eigvalsh(M)
     assert np.max(np.abs(ev - ref)) < 1e-13 * np.max(np.abs(ref))
-    assert np.max(np.abs(U.conj().T @ U - np.eye(n))) < 2e-14
+    # rounding of the accumulated rotations grows like sqrt(n) eps
+    assert np.max(np.abs(U.conj().T @ U - np.eye(n))) < max(2e-14, 1e-15 * math.sqrt(n))
     assert np.max(np.abs(M @ U - U * ev[None, :])) < 1e-12 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("n", [300, 520])
+@pytest.mark.parametrize("n", [300, 520, 2000])
 def test_eigensolver_graded_spectrum(capi, n):
     """Overlap-like matrix: eigenvalues exp(-2 eps E) spread over three decades,
     near-degenerate pairs included; absolute accuracy eps-scale, eigenvectors
