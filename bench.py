@@ -214,9 +214,10 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         L.itp2d_system_download_states(s.h, e2e_buf.ctypes.data_as(capi.C.POINTER(capi.C.c_double)))
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    return dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
-                launches=(l1 - l0) / K,
-                E=E, converged_mask=None, e2e_times=e2e_times, system=s)
+    out = dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
+               launches=(l1 - l0) / K, E=E, e2e_times=e2e_times)
+    s.close()
+    return out
 
 
 def host_description(threads: int) -> str:
@@ -492,6 +493,107 @@ def fp64_solve_check(r64):
             "source": src, "ok": ok}
 
 
+def serve_requests(n, seed, rate):
+    """The serving configuration's request stream: Poisson arrivals at `rate`
+    per second; per request B ~ U[0, 5], N in {128, 256, 512} (L = 12),
+    k in {50, 200, 1000} (the lower half wanted), tolerance 1e-6 or 1e-9
+    (abschange), V = omega^2 r^2 / 2 with omega ~ U[0.5, 2] plus 0-50 Gaussian
+    bumps (amplitude U[0.5, 1.5], width U[0.1, 0.3], centres uniform in
+    |x|, |y| < 4), 4th-order split, mixed form."""
+    from itp2d_b200 import capi, system
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    out = []
+    for i in range(n):
+        N = int(rng.choice([128, 256, 512]))
+        k = int(rng.choice([50, 200, 1000]))
+        B = float(rng.uniform(0, 5))
+        tol = float(rng.choice([1e-6, 1e-9]))
+        om = float(rng.uniform(0.5, 2.0))
+        nb = int(rng.integers(0, 51))
+        amp = rng.uniform(0.5, 1.5, nb)
+        wid = rng.uniform(0.1, 0.3, nb)
+        cen = rng.uniform(-4, 4, (nb, 2))
+        dx = 12.0 / N
+        x = (2 * np.arange(N) + 1 - N) * dx / 2
+        V = np.zeros((N, N))
+        for a, w, (cx, cy) in zip(amp, wid, cen):
+            V += a * np.exp(-((x[None, :] - cx) ** 2 + (x[:, None] - cy) ** 2) / (2 * w * w))
+        test = f"abschange({tol})"
+        p = system.Parameters(sx=N, sy=N, length=12.0, B=B, halforder=2, num_states=k, wanted=k // 2,
+                              eps=[0.05], timestep_test=test, final_test=test, max_steps=5000,
+                              potential=f"harmonic({om * om})", seed=seed * 100003 + i,
+                              precision=capi.FP32, fp32_switch=min(1e-7, tol))
+        out.append(dict(t=float(t[i]), params=p, V=V, N=N, k=k, tol=tol))
+    return out
+
+
+def serve_main(args):
+    """Serving form: requests arrive (Poisson, 20/s) while others run; the
+    server admits them by device footprint (budget: 120 GB) with up to 8
+    solves on the device at once. Reports whole-job converged states/s,
+    p50/p99 request latency (arrival to result), and serial plain-FP64 solves
+    of a sample of the same requests on the same GPU for comparison."""
+    import threading
+
+    import torch
+    from itp2d_b200 import capi, system
+    torch.cuda.set_device(0)
+    capi.lib()
+    nreq = args.requests
+    reqs = serve_requests(nreq, 20240605, 20.0)
+    with ClockSampler(0) as clk:
+        srv = system.Server(8, 120e9)
+        ids = [None] * nreq
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i, r in enumerate(reqs):
+                d = r["t"] - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(r["params"], r["V"])
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        res = [srv.wait(i, timeout=3600) for i in ids]
+        st = srv.stats()
+        srv.close()
+        # serial plain-FP64 solves of a sample of the same requests
+        sample = list(range(0, nreq, max(1, nreq // args.serial_sample)))[:args.serial_sample]
+        ser = []
+        for i in sample:
+            p = reqs[i]["params"]
+            q = system.Parameters(**{**p.__dict__, "precision": capi.FP64, "fp32_switch": 0.0})
+            sysm = system.ITPSystem(q, extra_potential=reqs[i]["V"])
+            torch.cuda.synchronize()
+            ta = time.perf_counter()
+            sysm.run()
+            torch.cuda.synchronize()
+            ser.append((time.perf_counter() - ta, sysm.num_converged))
+            sysm.close()
+    lat = np.array([r["t_finish"] - r["t_submit"] for r in res])
+    makespan = max(r["t_finish"] for r in res) - min(r["t_submit"] for r in res)
+    conv = sum(r["converged"] for r in res)
+    ser_t = sum(t for t, _ in ser)
+    ser_c = sum(c for _, c in ser)
+    out = {"metric": METRIC, "value": conv / makespan, "unit": UNIT, "n_gpus": 1, "steps": nreq, "warmup": 0,
+           "ms_per_step": makespan / nreq * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": f"serving: {nreq} requests, Poisson arrivals at 20/s, B~U[0,5], N in {{128,256,512}}, "
+                                  f"k in {{50,200,1000}}, tolerance 1e-6 or 1e-9, 4th-order split, mixed form",
+                      "max_active": 8, "memory_budget_gb": 120},
+           "latency_s": {"p50": float(np.median(lat)), "p99": float(np.quantile(lat, 0.99)),
+                         "max": float(lat.max())},
+           "converged": conv, "makespan_s": makespan,
+           "failed": sum(1 for r in res if r["status"] != 0 or r["error_flag"]),
+           "server": st,
+           "serial_fp64_sample": {"requests": len(ser), "seconds": ser_t, "converged": ser_c,
+                                  "converged_per_s": ser_c / ser_t if ser_t else None},
+           "clocks": clk.summary()}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -502,7 +604,13 @@ def main():
                     help="run one form only (profiling); the headline needs both")
     ap.add_argument("--workload", default="bumpy", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample (profiling)")
+    ap.add_argument("--serve", action="store_true", help="the serving form instead of the bench line")
+    ap.add_argument("--requests", type=int, default=120, help="serving form: number of requests")
+    ap.add_argument("--serial-sample", type=int, default=12, help="serving form: serial FP64 solves timed")
     args = ap.parse_args()
+    if args.serve:
+        serve_main(args)
+        return
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]
     if args.impl == "reference":

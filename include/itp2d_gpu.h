@@ -74,6 +74,16 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary,
 /* Frees every device allocation of the context. */
 int itp2d_ctx_destroy(itp2d_ctx* ctx);
 
+/* Device bytes a context of these arguments allocates (states, matrices,
+ * tables), an upper bound computed without allocating: the admission figure
+ * of the serving loop (itp2d_host.h). -1 for invalid arguments. No reference
+ * counterpart (the reference allocates host memory in StateSet::StateSet,
+ * stateset.cpp:23-44). */
+long long itp2d_ctx_footprint(int sx, int sy, int num_states, int boundary, double B, int halforder);
+
+/* Device bytes the context holds (-1 for NULL). */
+long long itp2d_ctx_device_bytes(itp2d_ctx* ctx);
+
 /* Sets the potential V (sx*sy doubles, y-major) or the null potential when
  * V is NULL. Replaces Potential (potential.cpp:21-63) as seen by
  * ExpPotential and the Hamiltonian. Tables are rebuilt for the current time
@@ -197,9 +207,10 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
  * nothing; its temporaries live in one fixed device array of this library
  * (about 1.6 MB, resident on every GPU that loads the library until exit).
  * n above ITP2D_NOALLOC_MAX_N returns ITP2D_E_INVALID. All calls share that
- * array, so calls that overlap on the GPU race: serialise them. The first
- * call on a device looks up the array's address for that device; make it
- * before any stream capture begins. Runs on the default stream.
+ * array, so calls that overlap on the GPU race: serialise them. Every call
+ * looks up the array's address on the current device (a device reset leaves
+ * no stale address); the first call on a device loads the library's device
+ * code there, so make it before any stream capture begins. Runs on the default stream.
  * No counterpart in the reference. */
 int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double* evals, double* evecs);
 

@@ -95,6 +95,54 @@ const char* itp2d_system_last_error(const itp2d_system* s);
 /* The device context owned by the system (for itp2d_gpu.h calls). */
 struct itp2d_ctx* itp2d_system_context(itp2d_system* s);
 
+/* ---- Serving loop (no reference counterpart; the reference runs one
+ * ITPSystem per process, itp2d.cpp:62-135) ----
+ *
+ * Solve requests (one itp2d_parameters each, plus optional extra potential and
+ * initial states as for itp2d_system_create) are queued as they arrive. Up to
+ * max_active of them run at once, each an ITPSystem on its own CUDA stream,
+ * so their kernels overlap on the device; a request is admitted when its
+ * device footprint (itp2d_ctx_footprint) fits in the part of
+ * memory_budget_bytes that the running ones leave free, oldest first among
+ * those that fit. A finished request frees its slot and memory at once.
+ * Requests larger than the whole budget are refused (ITP2D_E_OOM). */
+typedef struct itp2d_server itp2d_server;
+
+typedef struct {
+	int status;          /* ITP2D_OK, or the status that ended the solve */
+	int error_flag;      /* the driver's error flag (e.g. maximum steps reached) */
+	int iterations;      /* ITP iterations taken */
+	int converged;       /* states passing the final convergence test */
+	int num_energies;    /* entries written to E and sigma (num_states) */
+	double t_submit;     /* seconds on a monotonic clock: submission, */
+	double t_start;      /* start of the solve (admission), */
+	double t_finish;     /* and end of the solve */
+	double footprint_bytes;
+} itp2d_request_info;
+
+typedef struct {
+	int queued, running, peak_running, completed;
+	double bytes_in_use, peak_bytes_in_use, budget_bytes;
+	double busy_seconds;     /* time with at least one solve running */
+	double overlap_seconds;  /* time with two or more solves running at once */
+} itp2d_server_stats;
+
+int itp2d_server_create(int max_active, double memory_budget_bytes, itp2d_server** out);
+/* Queues a request; *id names it in itp2d_server_wait. The arrays are copied. */
+int itp2d_server_submit(itp2d_server* s, const itp2d_parameters* p, const double* extra_potential,
+		const double* init_states, long long* id);
+/* Waits up to timeout_s seconds for request id; ITP2D_E_TIMEOUT if it has not
+ * finished. On success fills info and the sorted energies and deviations
+ * (num_states doubles each; either array may be NULL). */
+int itp2d_server_wait(itp2d_server* s, long long id, double timeout_s, itp2d_request_info* info, double* E,
+		double* sigma);
+/* Drops a finished request's record. */
+int itp2d_server_forget(itp2d_server* s, long long id);
+int itp2d_server_get_stats(itp2d_server* s, itp2d_server_stats* stats);
+const char* itp2d_server_last_error(itp2d_server* s);
+/* Runs the queued and running requests to the end, then frees the server. */
+int itp2d_server_destroy(itp2d_server* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,21 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 // (columns of w.V, kp x kp with kp = k rounded up to even) without the
 // overlap checks unless check != 0.
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
+
+// Users of the cooperative eigensolvers (contexts and the standalone
+// eigensolve entry points). The Jacobi kernels are cooperative launches whose
+// CTAs wait for each other at grid barriers; two of them on different streams
+// could each hold part of the GPU while waiting for the rest. While more than
+// one user is alive, launch_eigh therefore serialises the cooperative kernel
+// process-wide and waits for it before returning.
+void coop_user_enter();
+void coop_user_leave();
+struct CoopUser {
+	CoopUser() { coop_user_enter(); }
+	~CoopUser() { coop_user_leave(); }
+	CoopUser(const CoopUser&) = delete;
+	CoopUser& operator=(const CoopUser&) = delete;
+};
 // Counter block of the Jacobi kernel, in ints: per-sweep rotation counts, the
 // result fields at [max_sweeps] and [max_sweeps + 1], then per-sweep maxima of
 // the rotation tangents as 64-bit words starting at jacobi_tmax_offset(), then

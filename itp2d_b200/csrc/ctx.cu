@@ -108,6 +108,8 @@ struct itp2d_ctx {
 	long long phase_calls_p[10] = {};
 	std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 	std::vector<void*> allocs;
+	size_t device_bytes = 0;  // sum of this context's device allocations
+	itp2d::CoopUser coop;     // counts toward the cooperative-eigensolve serialisation
 };
 
 namespace {
@@ -170,7 +172,10 @@ std::vector<c2<R>> make_ext(int N) {
 void* dalloc(itp2d_ctx* c, size_t bytes, cudaError_t* err) {
 	void* p = nullptr;
 	*err = cudaMalloc(&p, bytes ? bytes : 16);
-	if (*err == cudaSuccess) c->allocs.push_back(p);
+	if (*err == cudaSuccess) {
+		c->allocs.push_back(p);
+		c->device_bytes += bytes ? bytes : 16;
+	}
 	return p;
 }
 
@@ -221,6 +226,7 @@ int upload_table(itp2d_ctx* c, void** dst, const std::vector<double>& h) {
 			return cuda_status(e);
 		}
 		c->table_allocs.push_back(*dst);
+		c->device_bytes += n * sizeof(double);
 	}
 	if (c->precision == ITP2D_FP64) {
 		ITP2D_TRY(cudaMemcpy(*dst, h.data(), n * sizeof(double), cudaMemcpyHostToDevice));
@@ -689,6 +695,31 @@ int itp2d_ctx_destroy(itp2d_ctx* c) {
 	return ITP2D_OK;
 }
 
+long long itp2d_ctx_footprint(int sx, int sy, int num_states, int boundary, double B, int halforder) {
+	if (sx < 2 || sy < 2 || num_states < 1 || halforder < 1) return -1;
+	int dev = 0, sms = 148;
+	if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const long long G = (long long)sx * sy, k = num_states;
+	const bool dm = boundary == ITP2D_DIRICHLET && B != 0;
+	// the allocations of itp2d_ctx_create, term by term
+	long long b = (2 + ((halforder >= 3 || dm) ? 1 : 0)) * G * k * 16;  // psi, acc, work
+	const int nt = overlap_tiles(num_states);
+	const int npairs = nt * (nt + 1) / 2;
+	const int nsplit = std::max(1, std::min((4 * sms) / npairs, (int)std::max(1LL, G / 512)));
+	const int parts = std::max(nsplit, tc_overlap_splits(num_states, G, sms));
+	const long long kp = std::max(bjacobi_padded(num_states), (num_states + 1) & ~1);
+	b += (2 + parts) * k * k * 16 + (tc_supported(num_states, G) ? (long long)tc_wsplit_bytes(num_states) : 0);
+	b += (num_states >= kBlockJacobiMinK ? 4 : 3) * kp * kp * 16 + npairs * 8;
+	if (num_states >= kBlockJacobiMinK) b += (long long)bjacobi_qbuf_elems(num_states) * 16;
+	b += k * std::max(sx, sy) * 5 * 8 * (dm ? 2 : 1) + 5 * k * 8 + 16 * k;
+	// tables: three potential exponentials and a kinetic table per member, the
+	// energy tables, and the line plans (twiddles)
+	b += (4LL * halforder + 4) * G * 8 + 4LL * (sx + sy) * 16 * 4;
+	return b + (64 << 10);
+}
+
+long long itp2d_ctx_device_bytes(itp2d_ctx* c) { return c ? (long long)c->device_bytes : -1; }
+
 int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, double B, int halforder,
 		int precision, void* cuda_stream, itp2d_ctx** out) {
 	if (!out || sx < 2 || sy < 2 || num_states < 1 || !(dx > 0) || halforder < 1 || halforder > 8)
@@ -1102,6 +1133,7 @@ long long itp2d_precision_sweeps(itp2d_ctx* c, int precision) {
 
 int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* evecs) {
 	if (n < 1 || !A || !evals || !evecs) return ITP2D_E_INVALID;
+	CoopUser user;
 	const int kp = std::max(bjacobi_padded(n), (n + 1) & ~1);
 	std::vector<double2> S((size_t)n * n);
 	for (int i = 0; i < n; i++)

@@ -10,6 +10,9 @@
 // phase of A_pq. A rotation is skipped when |A_pq| <= tol sqrt(|A_pp A_qq|),
 // which gives the high relative accuracy Jacobi is known for on positive
 // definite matrices; a sweep without rotations ends the iteration.
+#include <atomic>
+#include <mutex>
+
 #include <cooperative_groups.h>
 
 #include "contract.cuh"
@@ -392,6 +395,14 @@ __global__ void build_w_kernel(const double2* __restrict__ V, int k, int kp, con
 
 size_t jacobi_counters(int max_sweeps) { return jacobi_counter_ints(max_sweeps); }
 
+namespace {
+std::atomic<int> g_coop_users{0};
+std::mutex g_coop_mu;
+}  // namespace
+
+void coop_user_enter() { g_coop_users.fetch_add(1); }
+void coop_user_leave() { g_coop_users.fetch_sub(1); }
+
 cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms,
 		cudaStream_t s) {
 	cudaError_t e = launch_eigh(S, k, w, st, num_sms, s, 1);
@@ -412,6 +423,10 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 	const long long n = (long long)kp * kp;
 	cudaError_t e = cudaMemsetAsync(w.counters, 0, jacobi_counters(w.max_sweeps) * sizeof(int), s);
 	if (e != cudaSuccess) return e;
+	// one cooperative kernel at a time while several users share the device:
+	// held until the kernel below has finished
+	std::unique_lock<std::mutex> serial;
+	if (g_coop_users.load() > 1) serial = std::unique_lock<std::mutex>(g_coop_mu);
 	if (w.f32.A0 && w.Qbuf && w.A2 && k >= kBlockJacobiMinK) {
 		e = launch_bjacobi32(S, k, w, num_sms, s);
 		if (e != cudaSuccess) return e;
@@ -439,6 +454,11 @@ cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num
 		unsigned long long* tmax = reinterpret_cast<unsigned long long*>(w.counters + jacobi_tmax_offset(ms));
 		void* args[] = {&w.A0, &w.A1, &w.V, (void*)&kpv, &ms, &tol, &tau_final, &w.counters, &tmax};
 		e = cudaLaunchCooperativeKernel((void*)jacobi_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
+		if (e != cudaSuccess) return e;
+	}
+	if (serial.owns_lock()) {
+		e = cudaStreamSynchronize(s);
+		serial.unlock();
 		if (e != cudaSuccess) return e;
 	}
 	normalize_columns_kernel<<<(k + 31) / 32, 1024, 0, s>>>(w.V, k, kp);

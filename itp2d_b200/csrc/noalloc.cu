@@ -14,11 +14,11 @@
 // (about 1.6 MB in total) and stays resident on every GPU that loads the
 // library until the process exits. Every call uses the same array, so calls
 // that overlap on the GPU (from several host threads, or on several streams)
-// race and must be serialised by the caller. The first call on a device looks
-// up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture begins.
-#include <mutex>
-
+// race and must be serialised by the caller. Every call looks up the array's
+// device address (cudaGetSymbolAddress) with the calling device current, so a
+// device reset or a re-created primary context never leaves a stale address;
+// the first call on a device also loads this library's device code there, so
+// make that first call before any stream capture begins.
 #include "../../include/itp2d_gpu.h"
 #include "contract.cuh"
 
@@ -50,22 +50,13 @@ constexpr size_t kScratchBytes = kOffStat + align_up(sizeof(EigStatus));
 // to kernels.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
-int scratch_address(int dev, unsigned char** out) {
-	if (dev < 0 || dev >= kMaxDevices) return ITP2D_E_INVALID;
-	std::lock_guard<std::mutex> g(g_mu);
-	if (!g_addr[dev]) {
-		void* p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-		if (e != cudaSuccess || !p) return ITP2D_E_CUDA;
-		g_addr[dev] = p;
-	}
-	*out = static_cast<unsigned char*>(g_addr[dev]);
+// Device address of the scratch array on the current device, looked up on
+// every call (no allocation once the module is loaded on the device).
+int scratch_address(unsigned char** out) {
+	void* p = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+	if (e != cudaSuccess || !p) return ITP2D_E_CUDA;
+	*out = static_cast<unsigned char*>(p);
 	return ITP2D_OK;
 }
 
@@ -105,8 +96,9 @@ extern "C" int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double
 	if (cudaGetDevice(&dev) != cudaSuccess) return ITP2D_E_CUDA;
 	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return ITP2D_E_CUDA;
 	unsigned char* base = nullptr;
-	int st = scratch_address(dev, &base);
+	int st = scratch_address(&base);
 	if (st != ITP2D_OK) return st;
+	itp2d::CoopUser user;
 	double2* in = reinterpret_cast<double2*>(base + kOffIn);
 	double2* S = reinterpret_cast<double2*>(base + kOffS);
 	double2* vec = reinterpret_cast<double2*>(base + kOffVec);

@@ -179,6 +179,7 @@ class ITPSystem {
 	const std::vector<std::vector<double>>& get_energies() const { return energies; }
 	const std::vector<std::vector<double>>& get_standard_deviations() const { return deviations; }
 	double get_sorted_energy(size_t n) const { return sorted[n].first.first; }
+	double get_sorted_deviation(size_t n) const { return sorted[n].first.second; }
 	size_t get_sorted_index(size_t n) const { return sorted[n].second; }
 	const std::vector<double>& get_residuals() const { return residuals; }
 	const std::string& last_error() const { return error_text; }

@@ -216,3 +216,118 @@ class ITPSystem:
 
     def context_handle(self) -> int:
         return _lib().itp2d_system_context(self.h)
+
+
+class _RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("error_flag", C.c_int), ("iterations", C.c_int), ("converged", C.c_int),
+                ("num_energies", C.c_int), ("t_submit", C.c_double), ("t_start", C.c_double),
+                ("t_finish", C.c_double), ("footprint_bytes", C.c_double)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int), ("running", C.c_int), ("peak_running", C.c_int), ("completed", C.c_int),
+                ("bytes_in_use", C.c_double), ("peak_bytes_in_use", C.c_double), ("budget_bytes", C.c_double),
+                ("busy_seconds", C.c_double), ("overlap_seconds", C.c_double)]
+
+
+_server_bound = False
+
+
+def _server_lib():
+    global _server_bound
+    L = _lib()
+    if not _server_bound:
+        vp, i, d, dp = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double)
+        L.itp2d_server_create.argtypes = [i, d, C.POINTER(vp)]
+        L.itp2d_server_submit.argtypes = [vp, C.POINTER(_Params), dp, dp, C.POINTER(C.c_longlong)]
+        L.itp2d_server_wait.argtypes = [vp, C.c_longlong, d, C.POINTER(_RequestInfo), dp, dp]
+        L.itp2d_server_forget.argtypes = [vp, C.c_longlong]
+        L.itp2d_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
+        L.itp2d_server_last_error.argtypes = [vp]
+        L.itp2d_server_last_error.restype = C.c_char_p
+        L.itp2d_server_destroy.argtypes = [vp]
+        L.itp2d_ctx_footprint.argtypes = [i, i, i, i, d, i]
+        L.itp2d_ctx_footprint.restype = C.c_longlong
+        _server_bound = True
+    return L
+
+
+def footprint(params: Parameters) -> int:
+    """Device bytes a solve of these parameters allocates (itp2d_ctx_footprint)."""
+    return _server_lib().itp2d_ctx_footprint(params.sx, params.sy, params.num_states, params.boundary,
+                                             float(params.B), params.halforder)
+
+
+class Server:
+    """The serving loop of include/itp2d_host.h: requests queued as they
+    arrive, admitted by device footprint, up to max_active solves at once on
+    their own streams, each retired when it finishes."""
+
+    def __init__(self, max_active: int, memory_budget_bytes: float):
+        h = C.c_void_p()
+        st = _server_lib().itp2d_server_create(int(max_active), float(memory_budget_bytes), C.byref(h))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_server_create")
+        self.h = h
+        self.k = {}
+
+    def submit(self, params: Parameters, extra_potential=None, init_states=None) -> int:
+        raw = params._raw()
+        ep = ip = None
+        if extra_potential is not None:
+            a = np.ascontiguousarray(extra_potential, dtype=np.float64).reshape(-1)
+            ep = a.ctypes.data_as(C.POINTER(C.c_double))
+        if init_states is not None:
+            b = np.ascontiguousarray(init_states, dtype=np.complex128)
+            ip = b.view(np.float64).ctypes.data_as(C.POINTER(C.c_double))
+        rid = C.c_longlong(0)
+        st = _server_lib().itp2d_server_submit(self.h, C.byref(raw), ep, ip, C.byref(rid))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_server_submit")
+        self.k[rid.value] = params.num_states
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = 3600.0) -> dict:
+        """Sorted energies, deviations and timing of a finished request;
+        raises ITP2DError(E_TIMEOUT) if it does not finish within timeout s."""
+        k = self.k[rid]
+        info = _RequestInfo()
+        E, sig = np.empty(k), np.empty(k)
+        st = _server_lib().itp2d_server_wait(self.h, rid, float(timeout), C.byref(info),
+                                             E.ctypes.data_as(C.POINTER(C.c_double)),
+                                             sig.ctypes.data_as(C.POINTER(C.c_double)))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_server_wait")
+        out = {f: getattr(info, f) for f, _ in _RequestInfo._fields_}
+        out["E"], out["sigma"] = E, sig
+        return out
+
+    def forget(self, rid: int) -> None:
+        _server_lib().itp2d_server_forget(self.h, rid)
+        self.k.pop(rid, None)
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        _server_lib().itp2d_server_get_stats(self.h, C.byref(s))
+        return {f: getattr(s, f) for f, _ in _ServerStats._fields_}
+
+    @property
+    def last_error(self) -> str:
+        return _server_lib().itp2d_server_last_error(self.h).decode()
+
+    def close(self):
+        if getattr(self, "h", None):
+            _server_lib().itp2d_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

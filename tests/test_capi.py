@@ -43,3 +43,52 @@ def test_impurity_arguments_rejected_before_device_use():
     assert add(16, 16, 0.1, 1, None, V, None) == capi.E_INVALID     # no impurity list
     assert add(16, 16, 0.1, 1, imp, None, None) == capi.E_INVALID   # no potential
     assert add(16, 16, 0.1, 0, None, V, None) == capi.OK            # nothing to add
+
+
+def test_library_exports_host_header_symbols():
+    """Every function of include/itp2d_host.h (the native driver and the
+    serving loop) is exported too."""
+    import os
+    import re
+    L = capi.lib()
+    txt = open(os.path.join(capi.ROOT, "include", "itp2d_host.h")).read()
+    names = sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*\**\s+\**(itp2d_[a-z0-9_]+)\s*\(",
+                                  txt, flags=re.M)))
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_footprint_estimate():
+    """itp2d_ctx_footprint counts the state buffers (two, three for
+    halforder >= 3 or Dirichlet with a field) and grows with k and N; it
+    computes without a device."""
+    fp = capi.lib().itp2d_ctx_footprint
+    fp.restype = ctypes.c_longlong
+    fp.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    a = fp(256, 256, 500, 0, 1.0, 2)
+    assert a >= 2 * 256 * 256 * 500 * 16
+    assert fp(256, 256, 500, 0, 1.0, 3) >= 3 * 256 * 256 * 500 * 16
+    assert fp(256, 256, 500, 1, 0.7, 2) >= 3 * 256 * 256 * 500 * 16
+    assert fp(256, 256, 1000, 0, 1.0, 2) > a and fp(512, 512, 500, 0, 1.0, 2) > a
+    assert a < 1.5 * 2 * 256 * 256 * 500 * 16  # states dominate
+    assert fp(1, 16, 4, 0, 0.0, 1) == -1
+
+
+def test_server_refuses_before_device_use():
+    """The serving loop validates and admits on the host: a request larger
+    than the whole budget is refused at submission, before any device call."""
+    from itp2d_b200 import system
+    with system.Server(2, 1e6) as srv:
+        p = system.Parameters(sx=64, sy=64, num_states=16, wanted=8, halforder=2, eps=[0.1])
+        try:
+            srv.submit(p)
+        except capi.ITP2DError as e:
+            assert e.status == capi.E_OOM
+        else:
+            raise AssertionError("oversized request admitted")
+        assert srv.stats()["queued"] == 0 and srv.stats()["completed"] == 0
+    L = capi.lib()
+    out = ctypes.c_void_p()
+    assert L.itp2d_server_create(0, 1e9, ctypes.byref(out)) == capi.E_INVALID
+    assert L.itp2d_server_create(2, 0.0, ctypes.byref(out)) == capi.E_INVALID
