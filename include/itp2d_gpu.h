@@ -155,6 +155,19 @@ int itp2d_set_precision(itp2d_ctx* ctx, int precision);
 enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1 };
 int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
 
+/* FP32 states: orthonormalise canonically only on every canonical_every-th
+ * call and by a second-order Lowdin step in between, W = D (I + E)^{-1/2} with
+ * D = diag(S)^{-1/2} and D S D = I + E, the series cut after E^2 (one k x k
+ * product instead of the k x k eigendecomposition). A step whose E is not
+ * small (largest element 0.05, Frobenius norm 0.25) is canonical anyway. The
+ * Lowdin step keeps the state order (no sort by overlap eigenvalue) and does
+ * not check the overlap eigenvalues. 0 or 1: always canonical (the default).
+ * FP64 states are always orthonormalised canonically. No reference
+ * counterpart (stateset.cpp:136-232 is the canonical form). */
+int itp2d_set_fp32_orthonormalization(itp2d_ctx* ctx, int canonical_every);
+/* Number of canonical and of Lowdin orthonormalisations since creation. */
+int itp2d_orthonormalization_counts(itp2d_ctx* ctx, long long* canonical, long long* lowdin);
+
 /* Overlap matrix of the resident states, S_ij = <psi_i|psi_j> dx^2
  * (row-major, num_states^2 interleaved complex doubles), computed by the
  * engine itp2d_orthonormalize would use; the states are not changed.

@@ -40,6 +40,9 @@ typedef struct {
 	char potential[128];
 	char timestep_test[128];
 	char final_test[128];
+	int fp32_canonical_every; /* FP32 form: canonical orthonormalisation on every n-th
+	                             step, second-order Lowdin steps in between
+	                             (itp2d_set_fp32_orthonormalization); 0: always canonical */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

@@ -67,7 +67,8 @@ def lib():
         L.itp2d_synchronize.argtypes = [vp]
         L.itp2d_set_contraction.argtypes = [vp, i]
         L.itp2d_set_precision.argtypes = [vp, i]
-        L.itp2d_set_precision.argtypes = [vp, i]
+        L.itp2d_set_fp32_orthonormalization.argtypes = [vp, i]
+        L.itp2d_orthonormalization_counts.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
@@ -212,9 +213,16 @@ class Context:
         if st != OK:
             raise ITP2DError(st, "itp2d_orthonormalize", bi.value, bv.value)
 
-    def set_precision(self, precision):
-        _check(lib().itp2d_set_precision(self.h, precision), "itp2d_set_precision")
-        self.precision = precision
+    def set_fp32_orthonormalization(self, canonical_every):
+        _check(lib().itp2d_set_fp32_orthonormalization(self.h, int(canonical_every)),
+               "itp2d_set_fp32_orthonormalization")
+
+    def orthonormalization_counts(self):
+        """(canonical, Lowdin) orthonormalisations since creation."""
+        a, b = C.c_longlong(0), C.c_longlong(0)
+        _check(lib().itp2d_orthonormalization_counts(self.h, C.byref(a), C.byref(b)),
+               "itp2d_orthonormalization_counts")
+        return a.value, b.value
 
     def set_precision(self, precision):
         _check(lib().itp2d_set_precision(self.h, precision), "itp2d_set_precision")

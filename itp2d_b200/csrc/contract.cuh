@@ -94,6 +94,21 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 // overlap checks unless check != 0.
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
 
+// Second-order Lowdin orthonormalisation (lowdin.cu): D = diag(S)^{-1/2},
+// E = D S D - I (row-major) and conj(E), stats = {max |E_ij|, sum |E_ij|^2,
+// bad diagonal}; then W = D (I - E/2 + 3/8 E^2) in the rotation layout, with
+// E2 (k x k) as the product's scratch.
+void launch_lowdin_prep(const double2* S, int k, double* D, double2* E, double2* Ec, double* stats,
+		cudaStream_t s);
+void launch_lowdin_w(const double* D, const double2* E, const double2* Ec, double2* E2, int k, double2* W,
+		cudaStream_t s);
+// Largest normalised off-diagonal overlap element and Frobenius norm for which
+// a Lowdin step is taken: the series error 5/16 |E|^3 stays below 5e-3 in the
+// worst case (|E|_2 <= |E|_F) and far below it for the noise-like E of
+// near-converged states.
+constexpr double kLowdinMaxElement = 0.05;
+constexpr double kLowdinMaxFrobenius = 0.25;
+
 // Users of the cooperative eigensolvers (contexts and the standalone
 // eigensolve entry points). The Jacobi kernels are cooperative launches whose
 // CTAs wait for each other at grid barriers; two of them on different streams

@@ -108,6 +108,12 @@ struct itp2d_ctx {
 	long long phase_calls_p[10] = {};
 	std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 	std::vector<void*> allocs;
+	// FP32 form: second-order Lowdin steps between canonical ones
+	int canonical_every = 0;     // 0 or 1: always canonical
+	int since_canonical = 0;     // orthonormalisations since the last canonical one
+	long long ortho_calls[2] = {0, 0};  // canonical, Lowdin
+	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
+	double* hlstat = nullptr;    // pinned copy
 	size_t device_bytes = 0;  // sum of this context's device allocations
 	itp2d::CoopUser coop;     // counts toward the cooperative-eigensolve serialisation
 };
@@ -690,6 +696,7 @@ int itp2d_ctx_destroy(itp2d_ctx* c) {
 	if (c->hstat) cudaFreeHost(c->hstat);
 	if (c->hbuf) cudaFreeHost(c->hbuf);
 	if (c->hflag) cudaFreeHost(c->hflag);
+	if (c->hlstat) cudaFreeHost(c->hlstat);
 	if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 	delete c;
 	return ITP2D_OK;
@@ -785,6 +792,7 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	if (e == cudaSuccess) c->jw.counters = (int*)dalloc(c, jacobi_counters(c->jw.max_sweeps) * sizeof(int), &e);
 	if (e == cudaSuccess) c->dstat = (EigStatus*)dalloc(c, sizeof(EigStatus), &e);
 	if (e == cudaSuccess) c->dnorm = (double*)dalloc(c, sizeof(double), &e);
+	if (e == cudaSuccess) c->lstat = (double*)dalloc(c, 4 * sizeof(double), &e);
 	// energies
 	const int ntiles = std::max(sx, sy);  // upper bound of row or column tiles
 	if (e == cudaSuccess) c->sums = (double*)dalloc(c, (size_t)k * ntiles * 5 * sizeof(double), &e);
@@ -800,6 +808,7 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	}
 	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hstat, sizeof(EigStatus));
 	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hflag, sizeof(int));
+	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hlstat, 4 * sizeof(double));
 	if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hbuf, (size_t)4 * k * sizeof(double));
 	if (e == cudaSuccess) {
 		std::vector<int2> pr;
@@ -974,6 +983,22 @@ int itp2d_set_contraction(itp2d_ctx* c, int engine) {
 	return ITP2D_OK;
 }
 
+int itp2d_set_fp32_orthonormalization(itp2d_ctx* c, int canonical_every) {
+	if (!c || canonical_every < 0) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->canonical_every = canonical_every;
+	c->since_canonical = 0;
+	return ITP2D_OK;
+}
+
+int itp2d_orthonormalization_counts(itp2d_ctx* c, long long* canonical, long long* lowdin) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (canonical) *canonical = c->ortho_calls[0];
+	if (lowdin) *lowdin = c->ortho_calls[1];
+	return ITP2D_OK;
+}
+
 int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 	if (!c || !S) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
@@ -1010,6 +1035,50 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		PhaseTimer t(c, kOverlap);
 		launch_overlap_any(c, tc);
 	}
+	// FP32 form between canonical steps: W = D (I + E)^{-1/2} to second order
+	// when the normalised overlap is close enough to the identity
+	bool lowdin = false;
+	if (!f64 && c->canonical_every > 1 && c->since_canonical + 1 < c->canonical_every) {
+		PhaseTimer t(c, kEigen);
+		launch_lowdin_prep(c->S, c->k, c->jw.evals, c->jw.A0, c->jw.A1, c->lstat, c->stream);
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaMemcpyAsync(c->hlstat, c->lstat, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		const double emax = c->hlstat[0], efro = std::sqrt(c->hlstat[1]);
+		if (c->hlstat[2] == 0.0 && emax < kLowdinMaxElement && efro < kLowdinMaxFrobenius) {
+			launch_lowdin_w(c->jw.evals, c->jw.A0, c->jw.A1, c->jw.V, c->k, c->W, c->stream);
+			c->launches += 3;
+			lowdin = true;
+		}
+		c->launches += 1;
+	}
+	if (lowdin) {
+		c->since_canonical++;
+		c->ortho_calls[1]++;
+		c->last_sweeps = 0;
+		{
+			PhaseTimer t(c, kRotate);
+			if (tc)
+				launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
+						c->stream);
+			else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
+			c->launches += tc ? 2 : 1;
+		}
+		if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		if (tc && *c->hflag != ITP2D_OK) {
+			const int f = *c->hflag;
+			ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+			return f;
+		}
+		void* sw = c->psi;
+		c->psi = c->acc;
+		c->acc = sw;
+		return ITP2D_OK;
+	}
+	c->since_canonical = 0;
+	c->ortho_calls[0]++;
 	{
 		PhaseTimer t(c, kEigen);
 		// FP32 states: the overlap is accurate to about 1e-5; a final tangent of

@@ -267,6 +267,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 	check(itp2d_ctx_create(p.sx, p.sy, dl.dx, p.num_states, p.boundary, p.B, p.halforder, precision, stream, &ctx),
 			"itp2d_ctx_create");
 	check(itp2d_set_timing(ctx, 1), "itp2d_set_timing");
+	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
 	check(itp2d_set_potential(ctx, null_potential ? nullptr : V.data()), "itp2d_set_potential");
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	initial_states = params.initial_states;
@@ -590,6 +591,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->recover = 0;
 	p->precision = ITP2D_FP64;
 	p->fp32_switch = 0.0;
+	p->fp32_canonical_every = 0;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
 	std::strcpy(p->final_test, "relstdev(1e-3,0)");

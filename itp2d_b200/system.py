@@ -22,6 +22,7 @@ class _Params(C.Structure):
         ("max_steps", C.c_int), ("min_eps", C.c_double), ("seed", C.c_ulong), ("ortho_algorithm", C.c_int),
         ("recover", C.c_int), ("precision", C.c_int), ("fp32_switch", C.c_double),
         ("potential", C.c_char * 128), ("timestep_test", C.c_char * 128), ("final_test", C.c_char * 128),
+        ("fp32_canonical_every", C.c_int),
     ]
 
 
@@ -80,6 +81,7 @@ class Parameters:
     recover: bool = False
     precision: int = capi.FP64
     fp32_switch: float = 0.0
+    fp32_canonical_every: int = 0
     potential: str = "harmonic"
     timestep_test: str = "relstdev(1e-3,1e-4)"
     final_test: str = "relstdev(1e-3,0)"
@@ -88,7 +90,8 @@ class Parameters:
         p = _Params()
         _lib().itp2d_parameters_default(C.byref(p))
         for k in ["sx", "sy", "length", "boundary", "B", "halforder", "num_states", "wanted", "ignore_lowest",
-                  "eps_divisor", "max_steps", "min_eps", "seed", "ortho_algorithm", "precision", "fp32_switch"]:
+                  "eps_divisor", "max_steps", "min_eps", "seed", "ortho_algorithm", "precision", "fp32_switch",
+                  "fp32_canonical_every"]:
             setattr(p, k, getattr(self, k))
         p.exhaust_eps, p.recover = int(self.exhaust_eps), int(self.recover)
         if len(self.eps) > 16:

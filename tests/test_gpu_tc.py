@@ -143,3 +143,60 @@ def test_tensor_core_solve_matches_fp64_engine():
         print(f"engine {engine}: {s.total_steps} steps")
         res[engine] = s.energies()[0][:6]
     assert np.max(np.abs(res[capi.CONTRACT_AUTO] - res[capi.CONTRACT_FP64])) < 1e-9
+
+
+def _near_orthonormal(sx, sy, k, seed, delta, L=10.0):
+    """FP32 context holding k states that are orthonormal up to perturbations
+    of relative size delta (the situation after one propagation step), with
+    the FP64 states they came from."""
+    from oracle import itp_oracle as O
+    g = O.Grid(sx, sy, L / sx)
+    psi = O.gaussian_states(g, k, seed)
+    q, _ = np.linalg.qr(psi.reshape(k, -1).T)
+    base = (q.T / g.dx).reshape(k, sy, sx)
+    rng = np.random.default_rng(seed + 1)
+    pert = rng.standard_normal((k, sy, sx)) + 1j * rng.standard_normal((k, sy, sx))
+    pert *= delta / (np.sqrt(np.sum(np.abs(pert) ** 2, axis=(1, 2)))[:, None, None] * g.dx)
+    scale = np.exp(-0.1 * np.arange(k))[:, None, None]  # graded norms, like exp(-eps E)
+    psi = (base + pert) * scale
+    c = capi.Context(sx, sy, g.dx, k, precision=capi.FP32)
+    c.upload(psi)
+    return c, g, psi
+
+
+@pytest.mark.parametrize("k,delta", [(64, 1e-3), (300, 3e-4)])
+def test_lowdin_step_orthonormalises(k, delta):
+    """Between canonical steps the FP32 form orthonormalises with
+    W = D (I + E)^{-1/2} cut after E^2: the states come out orthonormal to the
+    FP32 contraction accuracy, span the input's subspace, and each output state
+    stays within O(delta) of its (normalised) input state: no reordering."""
+    from oracle import itp_oracle as O
+    c, g, psi = _near_orthonormal(128, 128, k, 7, delta)
+    c.set_fp32_orthonormalization(4)
+    c.orthonormalize()
+    assert c.orthonormalization_counts() == (0, 1)
+    out = c.download()
+    assert O.how_orthonormal(g, out) < TOL_ORTHO
+    ref, _ = O.orthonormalize(g, psi)
+    assert 1 - O.subspace_cosines(g, out, ref).min() < 1e-9
+    nrm = np.sqrt(np.sum(np.abs(psi) ** 2, axis=(1, 2))) * g.dx
+    move = np.sqrt(np.sum(np.abs(out - psi / nrm[:, None, None]) ** 2, axis=(1, 2))) * g.dx
+    assert np.max(move) < 10 * delta
+
+
+def test_lowdin_guard_falls_back_to_canonical():
+    """A set far from orthonormal (random states) is orthonormalised
+    canonically even between canonical steps; every canonical_every-th call is
+    canonical; FP64 states are always canonical."""
+    c, dx = _ctx(64, 64, 40, seed=5)
+    c.set_fp32_orthonormalization(3)
+    c.orthonormalize()  # random states: the guard refuses the Lowdin step
+    assert c.orthonormalization_counts() == (1, 0)
+    c.orthonormalize()  # now near orthonormal: Lowdin
+    c.orthonormalize()  # Lowdin (second since the canonical one)
+    c.orthonormalize()  # third: canonical by the schedule
+    assert c.orthonormalization_counts() == (2, 2)
+    c.set_precision(capi.FP64)
+    c.orthonormalize()
+    c.orthonormalize()
+    assert c.orthonormalization_counts() == (4, 2)
