@@ -245,6 +245,26 @@ int itp2d_device_fp64_peak(double* tflops);
  * the single-precision eigensolver. Diagnostic; no reference counterpart. */
 int itp2d_device_fp32_peak(double* tflops);
 
+/* ---- Batched form: one call over many contexts (independent state sets of
+ * any grid size and state count; no reference counterpart, the reference
+ * runs one state set per process) ----
+ *
+ * itp2d_batch_propagate: itp2d_propagate on every context (each on its own
+ * stream, so the instances' passes overlap on the device).
+ * itp2d_batch_orthonormalize: the canonical orthonormalisation of every
+ * context (StateSet::orthonormalize, stateset.cpp:136-232): the overlaps on
+ * the contexts' streams, then ALL k x k eigenproblems in one launch (one CTA
+ * per instance, cyclic Jacobi; 2 <= k <= 4096), then the rotations. status[i]
+ * (and bad_index[i], bad_value[i] when not NULL) report each instance like
+ * itp2d_orthonormalize; an instance that fails keeps its states.
+ * itp2d_batch_energies: itp2d_energies of every context into E[i], sigma[i]
+ * (and sigma_residual[i] when that array and entry are not NULL).
+ * Contexts must be distinct. */
+int itp2d_batch_propagate(int n, itp2d_ctx* const* ctxs);
+int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* bad_index, double* bad_value);
+int itp2d_batch_energies(int n, itp2d_ctx* const* ctxs, double* const* E, double* const* sigma,
+		double* const* sigma_residual);
+
 /* Short description of a status code. */
 const char* itp2d_status_string(int status);
 

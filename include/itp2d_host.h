@@ -146,6 +146,30 @@ const char* itp2d_server_last_error(itp2d_server* s);
 /* Runs the queued and running requests to the end, then frees the server. */
 int itp2d_server_destroy(itp2d_server* s);
 
+/* ---- Batched form (no reference counterpart) ----
+ *
+ * count independent solves (one itp2d_parameters each, any grid size and
+ * state count >= 2; extra_potentials / init_states may be NULL or hold NULL
+ * entries) stepped together: every iteration runs the unfinished instances'
+ * propagations, overlaps, ONE batched eigensolve launch for all of them, the
+ * rotations and the energies (itp2d_batch_* of itp2d_gpu.h), then each
+ * instance's own convergence tests and time-step schedule. Instances leave
+ * the batch as they finish. */
+typedef struct itp2d_batch itp2d_batch;
+int itp2d_batch_create(int count, const itp2d_parameters* params, const double* const* extra_potentials,
+		const double* const* init_states, itp2d_batch** out);
+/* Up to max_iterations batch iterations, fewer when every instance finishes. */
+int itp2d_batch_run(itp2d_batch* b, int max_iterations);
+/* Instance i: iterations, converged count, error flag, seconds from the
+ * batch's start to the instance's finish (t_finish), sorted energies and
+ * deviations (num_states doubles each; either array may be NULL). */
+int itp2d_batch_result(itp2d_batch* b, int i, itp2d_request_info* info, double* E, double* sigma);
+int itp2d_batch_size(const itp2d_batch* b);
+int itp2d_batch_finished(const itp2d_batch* b);
+int itp2d_batch_stats(const itp2d_batch* b, long long* iterations, double* seconds);
+const char* itp2d_batch_last_error(const itp2d_batch* b);
+int itp2d_batch_destroy(itp2d_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,25 @@ void launch_lowdin_w(const double* D, const double2* E, const double2* Ec, doubl
 constexpr double kLowdinMaxElement = 0.05;
 constexpr double kLowdinMaxFrobenius = 0.25;
 
+// One instance of the batched eigensolver (batch.cu): the k x k overlap S
+// (row-major), work matrices A and V ((k + 1) & ~1 squared), the result
+// W = U Lambda^{-1/2} (rotation layout), ascending eigenvalues and their
+// source indices, the status, and the tangent at which the sweeps stop.
+struct BatchEigItem {
+	const double2* S;
+	double2* A;
+	double2* V;
+	double2* W;
+	double* evals;
+	int* perm;
+	EigStatus* st;
+	int k;
+	int pad;
+	double tau;
+};
+cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, cudaStream_t s);
+int batched_eigensolve_max_k();
+
 // Users of the cooperative eigensolvers (contexts and the standalone
 // eigensolve entry points). The Jacobi kernels are cooperative launches whose
 // CTAs wait for each other at grid barriers; two of them on different streams

@@ -6,6 +6,7 @@
 // ExpKinetic expkinetic.cpp:65-136, Kinetic kinetic.cpp:25-83, Transformer
 // k-tables and normalisations transformer.cpp:66-90) and uploaded once per
 // time step.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1266,3 +1267,181 @@ int itp2d_hermitian_eigensolve(int n, const double* A, double* evals, double* ev
 }
 
 }  // extern "C"
+
+// ---- Batched calls over many contexts (the batched form) ----
+
+namespace {
+
+// Locks the contexts' mutexes in address order (no lock-order inversion
+// between concurrent batches).
+struct BatchLock {
+	std::vector<std::unique_lock<std::mutex>> locks;
+	explicit BatchLock(std::vector<itp2d_ctx*> cs) {
+		std::sort(cs.begin(), cs.end());
+		cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+		for (itp2d_ctx* c : cs) locks.emplace_back(c->mu);
+	}
+};
+
+std::mutex g_batch_mu;               // the process-wide batch stream and staging buffers
+cudaStream_t g_batch_stream = nullptr;
+BatchEigItem* g_items_host = nullptr;  // pinned
+BatchEigItem* g_items_dev = nullptr;
+int g_items_cap = 0;
+
+int batch_resources(int n) {
+	if (!g_batch_stream) ITP2D_TRY(cudaStreamCreateWithFlags(&g_batch_stream, cudaStreamNonBlocking));
+	if (n > g_items_cap) {
+		if (g_items_host) cudaFreeHost(g_items_host);
+		if (g_items_dev) cudaFree(g_items_dev);
+		g_items_host = nullptr;
+		g_items_dev = nullptr;
+		g_items_cap = 0;
+		const int cap = std::max(n, 256);
+		ITP2D_TRY(cudaMallocHost((void**)&g_items_host, cap * sizeof(BatchEigItem)));
+		ITP2D_TRY(cudaMalloc((void**)&g_items_dev, cap * sizeof(BatchEigItem)));
+		g_items_cap = cap;
+	}
+	return ITP2D_OK;
+}
+
+}  // namespace
+
+int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* bad_index, double* bad_value) {
+	if (n < 0 || (n > 0 && (!ctxs || !status))) return ITP2D_E_INVALID;
+	if (n == 0) return ITP2D_OK;
+	for (int i = 0; i < n; i++)
+		if (!ctxs[i] || ctxs[i]->k < 2 || ctxs[i]->k > batched_eigensolve_max_k()) return ITP2D_E_INVALID;
+	BatchLock lk(std::vector<itp2d_ctx*>(ctxs, ctxs + n));
+	std::lock_guard<std::mutex> gb(g_batch_mu);
+	int st = batch_resources(n);
+	if (st) return st;
+	std::vector<cudaEvent_t> ev(n + 1, nullptr);
+	auto cleanup = [&]() {
+		for (cudaEvent_t e : ev)
+			if (e) cudaEventDestroy(e);
+	};
+	for (int i = 0; i <= n; i++) {
+		const cudaError_t e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+		if (e != cudaSuccess) {
+			cleanup();
+			return cuda_status(e);
+		}
+	}
+	// overlaps, each on its context's stream
+	for (int i = 0; i < n; i++) {
+		itp2d_ctx* c = ctxs[i];
+		c->since_canonical = 0;
+		c->ortho_calls[0]++;
+		{
+			PhaseTimer t(c, kOverlap);
+			launch_overlap_any(c, use_tensor_cores(c));
+		}
+		cudaEventRecord(ev[i], c->stream);
+		cudaStreamWaitEvent(g_batch_stream, ev[i], 0);
+		BatchEigItem& it = g_items_host[i];
+		it.S = c->S;
+		it.A = c->jw.A0;
+		it.V = c->jw.V;
+		it.W = c->W;
+		it.evals = c->jw.evals;
+		it.perm = c->jw.perm;
+		it.st = c->dstat;
+		it.k = c->k;
+		it.pad = 0;
+		it.tau = c->precision == ITP2D_FP64 ? 3e-9 : 1e-3;
+	}
+	// every eigenproblem in one launch
+	cudaError_t e = cudaMemcpyAsync(g_items_dev, g_items_host, n * sizeof(BatchEigItem), cudaMemcpyHostToDevice,
+			g_batch_stream);
+	if (e == cudaSuccess) e = launch_batched_eigensolve(g_items_dev, n, 60, g_batch_stream);
+	if (e == cudaSuccess) e = cudaEventRecord(ev[n], g_batch_stream);
+	if (e != cudaSuccess) {
+		cleanup();
+		return cuda_status(e);
+	}
+	// rotations, each on its context's stream after the eigensolve
+	for (int i = 0; i < n; i++) {
+		itp2d_ctx* c = ctxs[i];
+		cudaStreamWaitEvent(c->stream, ev[n], 0);
+		const bool tc = use_tensor_cores(c);
+		{
+			PhaseTimer t(c, kRotate);
+			if (tc)
+				launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
+						c->stream);
+			else if (c->precision == ITP2D_FP64)
+				launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
+			else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
+		}
+		c->launches += (tc ? 2 : 1) + 3;
+		if (tc) cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+		cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream);
+	}
+	for (int i = 0; i < n; i++) {
+		itp2d_ctx* c = ctxs[i];
+		e = cudaStreamSynchronize(c->stream);
+		if (e != cudaSuccess) {
+			cleanup();
+			return cuda_status(e);
+		}
+		const EigStatus hs = *c->hstat;
+		int si = hs.status;
+		if (si == ITP2D_OK && use_tensor_cores(c) && *c->hflag != ITP2D_OK) {
+			si = *c->hflag;
+			cudaMemset(c->dflag, 0, sizeof(int));
+		}
+		status[i] = si;
+		if (bad_index) bad_index[i] = hs.bad_index;
+		if (bad_value) bad_value[i] = hs.bad_value;
+		c->last_sweeps = hs.sweeps;
+		if (hs.sweeps > 0) {
+			c->sweeps_total += hs.sweeps;
+			c->sweeps_p[c->precision == ITP2D_FP64 ? 0 : 1] += hs.sweeps;
+		}
+		if (si == ITP2D_OK) {
+			void* t = c->psi;
+			c->psi = c->acc;
+			c->acc = t;
+		}
+	}
+	cleanup();
+	return ITP2D_OK;
+}
+
+int itp2d_batch_energies(int n, itp2d_ctx* const* ctxs, double* const* E, double* const* sigma,
+		double* const* sigma_residual) {
+	if (n < 0 || (n > 0 && (!ctxs || !E || !sigma))) return ITP2D_E_INVALID;
+	for (int i = 0; i < n; i++)
+		if (!ctxs[i] || !E[i] || !sigma[i]) return ITP2D_E_INVALID;
+	BatchLock lk(std::vector<itp2d_ctx*>(ctxs, ctxs + n));
+	for (int i = 0; i < n; i++) {
+		itp2d_ctx* c = ctxs[i];
+		PhaseTimer t(c, kEnergies);
+		if (c->precision == ITP2D_FP64) energies_impl<double>(c, nullptr, true);
+		else energies_impl<float>(c, nullptr, true);
+		ITP2D_TRY(cudaGetLastError());
+		ITP2D_TRY(cudaMemcpyAsync(c->hbuf, c->dE, (size_t)4 * c->k * sizeof(double), cudaMemcpyDeviceToHost,
+				c->stream));
+		ITP2D_TRY(cudaMemcpyAsync(c->dEshift, c->dE, (size_t)c->k * sizeof(double), cudaMemcpyDeviceToDevice,
+				c->stream));
+	}
+	for (int i = 0; i < n; i++) {
+		itp2d_ctx* c = ctxs[i];
+		ITP2D_TRY(cudaStreamSynchronize(c->stream));
+		const int k = c->k;
+		std::memcpy(E[i], c->hbuf, k * sizeof(double));
+		std::memcpy(sigma[i], c->hbuf + k, k * sizeof(double));
+		if (sigma_residual && sigma_residual[i]) std::memcpy(sigma_residual[i], c->hbuf + 2 * k, k * sizeof(double));
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_batch_propagate(int n, itp2d_ctx* const* ctxs) {
+	if (n < 0 || (n > 0 && !ctxs)) return ITP2D_E_INVALID;
+	for (int i = 0; i < n; i++) {
+		const int st = itp2d_propagate(ctxs[i]);
+		if (st) return st;
+	}
+	return ITP2D_OK;
+}

@@ -345,6 +345,11 @@ void ITPSystem::orthonormalize() {
 	double bv = 0;
 	const int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
 	t_ortho += now_s() - t0;
+	orthonormalized(st, bi, bv);
+}
+
+// The outcome of an orthonormalisation: itpsystem.cpp:258-289.
+void ITPSystem::orthonormalized(int st, int bi, double bv) {
 	if (st == ITP2D_OK) return;
 	if (st == ITP2D_E_NONPOSITIVE_EIGENVALUE) {
 		// itpsystem.cpp:264-281: shrink eps and restart from noise, or stop.
@@ -367,10 +372,18 @@ void ITPSystem::orthonormalize() {
 
 void ITPSystem::calculate_energies() {
 	if (total_step_counter == 0) return;
-	const double t0 = now_s();
 	const size_t k = (size_t)p.num_states;
 	std::vector<double> E(k), s(k), r(k);
+	const double t0 = now_s();
 	check(itp2d_energies(ctx, E.data(), s.data(), r.data(), nullptr), "itp2d_energies");
+	t_conv += now_s() - t0;
+	store_energies(E.data(), s.data(), r.data());
+}
+
+// Sorted (E, sigma, n) tuples and the histories (itpsystem.cpp:473-511).
+void ITPSystem::store_energies(const double* E, const double* s, const double* r) {
+	const double t0 = now_s();
+	const size_t k = (size_t)p.num_states;
 	sorted.resize(k);
 	for (size_t n = 0; n < k; n++) sorted[n] = Esn(std::make_pair(E[n], s[n]), n);
 	std::sort(sorted.begin(), sorted.end());
@@ -474,19 +487,34 @@ void ITPSystem::maybe_switch_precision() {
 
 // itpsystem.cpp:407-470
 void ITPSystem::step() {
-	if (finished) return;
+	if (!step_begin()) return;
+	propagate();
+	orthonormalize();
+	calculate_energies();
+	step_end();
+}
+
+bool ITPSystem::step_begin() {
+	if (finished) return false;
 	if (total_step_counter == 0) t_start = now_s();
 	if (total_step_counter >= p.max_steps) {
 		error_text = "maximum number of total steps reached";
 		error_flag = true;
 		finish();
-		return;
+		return false;
 	}
 	step_counter++;
 	total_step_counter++;
-	propagate();
-	orthonormalize();
-	calculate_energies();
+	return true;
+}
+
+void ITPSystem::energies_computed(const double* E, const double* sigma, const double* residual) {
+	store_energies(E, sigma, residual);
+	step_end();
+}
+
+// The convergence tests and time-step schedule after the energies.
+void ITPSystem::step_end() {
 	if (finished) return;
 	const bool was_fp32 = precision == ITP2D_FP32;
 	maybe_switch_precision();

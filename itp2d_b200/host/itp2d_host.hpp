@@ -165,6 +165,14 @@ class ITPSystem {
 	ITPSystem& operator=(const ITPSystem&) = delete;
 
 	void step();
+	// step() in pieces, for a driver that runs many systems through the
+	// batched device calls (itp2d_batch_*): step_begin() (false: finished),
+	// the device work of propagate / orthonormalize / energies done by the
+	// caller, then orthonormalized() with the orthonormalisation's status and
+	// energies_computed() with the per-state energies in storage order.
+	bool step_begin();
+	void orthonormalized(int status, int bad_index, double bad_value);
+	void energies_computed(const double* E, const double* sigma, const double* residual);
 	void finish();
 	void reset(const double* init_states);
 	bool is_finished() const { return finished; }
@@ -192,6 +200,8 @@ class ITPSystem {
 	void propagate();
 	void orthonormalize();
 	void calculate_energies();
+	void store_energies(const double* E, const double* sigma, const double* residual);
+	void step_end();
 	void check_timestep_convergence();
 	void check_final_convergence();
 	void change_time_step();

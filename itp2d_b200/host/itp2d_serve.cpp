@@ -27,13 +27,9 @@
 
 namespace itp2d {
 
-namespace {
-
-double wall_s() {
+inline double wall_s() {
 	return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
-
-}  // namespace
 
 struct Request {
 	long long id = 0;
@@ -278,6 +274,157 @@ int itp2d_server_destroy(itp2d_server* h) {
 	if (!h) return ITP2D_E_INVALID;
 	delete h->s;  // finishes the queued and running requests first
 	delete h;
+	return ITP2D_OK;
+}
+
+}  // extern "C"
+
+// ---- Batched form: many independent solves stepped together ----
+//
+// Each instance is an ITPSystem (its own context and stream); an iteration of
+// the batch runs every unfinished instance's step through the batched device
+// calls: the propagations (all streams), ONE launch for every instance's
+// overlap eigenproblem between the overlaps and the rotations, and the
+// energies; then each instance's own convergence tests and time-step schedule
+// (itpsystem.cpp:407-470). Finished instances leave the batch.
+
+struct itp2d_batch {
+	std::vector<std::unique_ptr<itp2d::ITPSystem>> sys;
+	std::vector<double> t_finish;
+	long long iterations = 0;
+	double t_start = 0, seconds = 0;
+	std::string err;
+};
+
+extern "C" {
+
+int itp2d_batch_create(int count, const itp2d_parameters* params, const double* const* extra_potentials,
+		const double* const* init_states, itp2d_batch** out) {
+	if (!out || count < 1 || !params) return ITP2D_E_INVALID;
+	*out = nullptr;
+	itp2d_batch* b = new itp2d_batch();
+	try {
+		for (int i = 0; i < count; i++) {
+			const itp2d_parameters& p = params[i];
+			itp2d::Parameters P;
+			P.raw() = p;
+			const size_t G = (size_t)p.sx * (size_t)p.sy;
+			if (extra_potentials && extra_potentials[i])
+				P.user_potential.assign(extra_potentials[i], extra_potentials[i] + G);
+			if (init_states && init_states[i])
+				P.initial_states.assign(init_states[i], init_states[i] + 2 * G * (size_t)p.num_states);
+			if (p.num_states < 2) throw itp2d::GeneralError("batched instances need at least two states");
+			b->sys.emplace_back(new itp2d::ITPSystem(P));
+		}
+	} catch (itp2d::DeviceError& e) {
+		const int st = e.status;
+		delete b;
+		return st;
+	} catch (std::exception&) {
+		delete b;
+		return ITP2D_E_INVALID;
+	}
+	b->t_finish.assign(count, 0.0);
+	*out = b;
+	return ITP2D_OK;
+}
+
+int itp2d_batch_run(itp2d_batch* b, int max_iterations) {
+	if (!b) return ITP2D_E_INVALID;
+	const double t0 = itp2d::wall_s();
+	if (b->iterations == 0) b->t_start = t0;
+	try {
+		for (int it = 0; it < max_iterations; it++) {
+			std::vector<itp2d::ITPSystem*> act;
+			for (auto& s : b->sys)
+				if (s->step_begin()) act.push_back(s.get());
+			if (act.empty()) break;
+			const int n = (int)act.size();
+			std::vector<itp2d_ctx*> ctxs(n);
+			for (int i = 0; i < n; i++) ctxs[i] = act[i]->context();
+			int st = itp2d_batch_propagate(n, ctxs.data());
+			if (st) throw itp2d::DeviceError("itp2d_batch_propagate", st);
+			std::vector<int> ost(n), bi(n);
+			std::vector<double> bv(n);
+			st = itp2d_batch_orthonormalize(n, ctxs.data(), ost.data(), bi.data(), bv.data());
+			if (st) throw itp2d::DeviceError("itp2d_batch_orthonormalize", st);
+			for (int i = 0; i < n; i++) act[i]->orthonormalized(ost[i], bi[i], bv[i]);
+			std::vector<std::vector<double>> E(n), S(n), R(n);
+			std::vector<double*> pe(n), ps(n), pr(n);
+			for (int i = 0; i < n; i++) {
+				const size_t k = (size_t)act[i]->p.num_states;
+				E[i].resize(k);
+				S[i].resize(k);
+				R[i].resize(k);
+				pe[i] = E[i].data();
+				ps[i] = S[i].data();
+				pr[i] = R[i].data();
+			}
+			st = itp2d_batch_energies(n, ctxs.data(), pe.data(), ps.data(), pr.data());
+			if (st) throw itp2d::DeviceError("itp2d_batch_energies", st);
+			const double now = itp2d::wall_s();
+			for (int i = 0; i < n; i++) {
+				act[i]->energies_computed(pe[i], ps[i], pr[i]);
+				if (act[i]->is_finished())
+					for (size_t j = 0; j < b->sys.size(); j++)
+						if (b->sys[j].get() == act[i]) b->t_finish[j] = now - b->t_start;
+			}
+			b->iterations++;
+		}
+	} catch (itp2d::DeviceError& e) {
+		b->err = e.what();
+		return e.status;
+	} catch (std::exception& e) {
+		b->err = e.what();
+		return ITP2D_E_INVALID;
+	}
+	b->seconds += itp2d::wall_s() - t0;
+	return ITP2D_OK;
+}
+
+int itp2d_batch_result(itp2d_batch* b, int i, itp2d_request_info* info, double* E, double* sigma) {
+	if (!b || i < 0 || i >= (int)b->sys.size()) return ITP2D_E_INVALID;
+	itp2d::ITPSystem& s = *b->sys[i];
+	const int k = s.p.num_states;
+	const bool have = s.get_total_step_counter() > 0 && !s.get_energies().empty();
+	if (info) {
+		std::memset(info, 0, sizeof(*info));
+		info->status = ITP2D_OK;
+		info->error_flag = s.get_error_flag() ? 1 : 0;
+		info->iterations = s.get_total_step_counter();
+		info->converged = (int)s.how_many_finally_converged();
+		info->num_energies = have ? k : 0;
+		info->t_finish = b->t_finish[i];
+		info->footprint_bytes = (double)itp2d_ctx_device_bytes(s.context());
+	}
+	for (int n = 0; have && n < k; n++) {
+		if (E) E[n] = s.get_sorted_energy(n);
+		if (sigma) sigma[n] = s.get_sorted_deviation(n);
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_batch_size(const itp2d_batch* b) { return b ? (int)b->sys.size() : -1; }
+
+int itp2d_batch_finished(const itp2d_batch* b) {
+	if (!b) return -1;
+	for (auto& s : b->sys)
+		if (!s->is_finished()) return 0;
+	return 1;
+}
+
+int itp2d_batch_stats(const itp2d_batch* b, long long* iterations, double* seconds) {
+	if (!b) return ITP2D_E_INVALID;
+	if (iterations) *iterations = b->iterations;
+	if (seconds) *seconds = b->seconds;
+	return ITP2D_OK;
+}
+
+const char* itp2d_batch_last_error(const itp2d_batch* b) { return b ? b->err.c_str() : ""; }
+
+int itp2d_batch_destroy(itp2d_batch* b) {
+	if (!b) return ITP2D_E_INVALID;
+	delete b;
 	return ITP2D_OK;
 }
 

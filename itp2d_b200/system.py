@@ -334,3 +334,98 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+_batch_bound = False
+
+
+def _batch_lib():
+    global _batch_bound
+    L = _server_lib()
+    if not _batch_bound:
+        vp, i, d, dp = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double)
+        L.itp2d_batch_create.argtypes = [i, C.POINTER(_Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(vp)]
+        L.itp2d_batch_run.argtypes = [vp, i]
+        L.itp2d_batch_result.argtypes = [vp, i, C.POINTER(_RequestInfo), dp, dp]
+        L.itp2d_batch_size.argtypes = [vp]
+        L.itp2d_batch_finished.argtypes = [vp]
+        L.itp2d_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), dp]
+        L.itp2d_batch_last_error.argtypes = [vp]
+        L.itp2d_batch_last_error.restype = C.c_char_p
+        L.itp2d_batch_destroy.argtypes = [vp]
+        _batch_bound = True
+    return L
+
+
+class Batch:
+    """The batched form of include/itp2d_host.h: many independent solves
+    stepped together, one batched eigensolve launch per iteration."""
+
+    def __init__(self, params: list, extra_potentials=None, init_states=None):
+        n = len(params)
+        raws = (_Params * n)(*[p._raw() for p in params])
+        dp = C.POINTER(C.c_double)
+        keep = []
+
+        def ptrs(arrs, cplx):
+            if arrs is None:
+                return None
+            out = (dp * n)()
+            for j, a in enumerate(arrs):
+                if a is None:
+                    out[j] = None
+                    continue
+                b = np.ascontiguousarray(a, dtype=np.complex128 if cplx else np.float64)
+                keep.append(b)
+                out[j] = (b.view(np.float64) if cplx else b).ctypes.data_as(dp)
+            return out
+        h = C.c_void_p()
+        st = _batch_lib().itp2d_batch_create(n, raws, ptrs(extra_potentials, False), ptrs(init_states, True),
+                                             C.byref(h))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_batch_create")
+        self.h = h
+        self.k = [p.num_states for p in params]
+
+    def run(self, max_iterations: int = 1 << 30):
+        st = _batch_lib().itp2d_batch_run(self.h, int(max_iterations))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_batch_run: " + _batch_lib().itp2d_batch_last_error(self.h).decode())
+
+    def result(self, i: int) -> dict:
+        k = self.k[i]
+        info = _RequestInfo()
+        E, sig = np.empty(k), np.empty(k)
+        st = _batch_lib().itp2d_batch_result(self.h, i, C.byref(info), E.ctypes.data_as(C.POINTER(C.c_double)),
+                                             sig.ctypes.data_as(C.POINTER(C.c_double)))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_batch_result")
+        out = {f: getattr(info, f) for f, _ in _RequestInfo._fields_}
+        out["E"], out["sigma"] = E, sig
+        return out
+
+    @property
+    def finished(self) -> bool:
+        return bool(_batch_lib().itp2d_batch_finished(self.h))
+
+    def stats(self) -> dict:
+        it, sec = C.c_longlong(0), C.c_double(0.0)
+        _batch_lib().itp2d_batch_stats(self.h, C.byref(it), C.byref(sec))
+        return {"iterations": it.value, "seconds": sec.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            _batch_lib().itp2d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
