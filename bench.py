@@ -594,6 +594,86 @@ def serve_main(args):
     print(json.dumps(out))
 
 
+def batch_instances(n, seed):
+    """The batched configuration's instances: N in {64, 96, 128, 160, 192}
+    (L = 12), k uniform in 16..128 (the lower half wanted), V = omega^2 r^2 / 2
+    with omega ~ U[0.5, 2] plus 0-50 Gaussian bumps (amplitude U[0.5, 1.5],
+    width U[0.1, 0.3], centres uniform in |x|, |y| < 4), B ~ U[0, 2],
+    4th-order split, mixed form refined to abschange(1e-8)."""
+    from itp2d_b200 import capi, system
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        N = int(rng.choice([64, 96, 128, 160, 192]))
+        k = int(rng.integers(16, 129))
+        om = float(rng.uniform(0.5, 2.0))
+        nb = int(rng.integers(0, 51))
+        amp, wid = rng.uniform(0.5, 1.5, nb), rng.uniform(0.1, 0.3, nb)
+        cen = rng.uniform(-4, 4, (nb, 2))
+        dx = 12.0 / N
+        x = (2 * np.arange(N) + 1 - N) * dx / 2
+        V = np.zeros((N, N))
+        for a, w, (cx, cy) in zip(amp, wid, cen):
+            V += a * np.exp(-((x[None, :] - cx) ** 2 + (x[:, None] - cy) ** 2) / (2 * w * w))
+        p = system.Parameters(sx=N, sy=N, length=12.0, B=float(rng.uniform(0, 2)), halforder=2, num_states=k,
+                              wanted=k // 2, eps=[0.05], timestep_test="abschange(1e-8)",
+                              final_test="abschange(1e-8)", max_steps=5000, potential=f"harmonic({om * om})",
+                              seed=seed * 7919 + i, precision=capi.FP32, fp32_switch=1e-7)
+        out.append((p, V))
+    return out
+
+
+def batch_main(args):
+    """Batched form: args.instances independent solves stepped together
+    (one batched eigensolve launch per iteration), against the same
+    instances solved one after another by the native driver (a sample)."""
+    import torch
+    from itp2d_b200 import capi, system
+    torch.cuda.set_device(0)
+    capi.lib()
+    inst = batch_instances(args.instances, 20240604)
+    with ClockSampler(0) as clk:
+        warm = system.Batch([p for p, _ in inst[:8]], [v for _, v in inst[:8]])
+        warm.run()
+        warm.close()
+        b = system.Batch([p for p, _ in inst], [v for _, v in inst])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run()
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        res = [b.result(i) for i in range(len(inst))]
+        st = b.stats()
+        b.close()
+        sample = list(range(0, len(inst), max(1, len(inst) // args.serial_sample)))[:args.serial_sample]
+        ser_t, ser_c, bat_c = 0.0, 0, 0
+        for i in sample:
+            p, V = inst[i]
+            s = system.ITPSystem(p, extra_potential=V)
+            torch.cuda.synchronize()
+            ta = time.perf_counter()
+            s.run()
+            torch.cuda.synchronize()
+            ser_t += time.perf_counter() - ta
+            ser_c += s.num_converged
+            bat_c += res[i]["converged"]
+            s.close()
+    conv = sum(r["converged"] for r in res)
+    out = {"metric": METRIC, "value": conv / tb, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+           "ms_per_step": tb * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": f"batched: {len(inst)} independent solves, N in {{64,96,128,160,192}}, L=12, "
+                                  f"k in 16..128, omega^2 r^2/2 + 0-50 bumps, B~U[0,2], 4th-order split, mixed "
+                                  f"form to abschange(1e-8)"},
+           "batch": {"seconds": tb, "converged": conv, "iterations": st["iterations"],
+                     "failed": sum(1 for r in res if r["error_flag"])},
+           "serial_sample": {"instances": len(sample), "seconds": ser_t, "converged": ser_c,
+                             "converged_per_s": ser_c / ser_t if ser_t else None,
+                             "batch_converged_same_instances": bat_c},
+           "clocks": clk.summary()}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -606,10 +686,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample (profiling)")
     ap.add_argument("--serve", action="store_true", help="the serving form instead of the bench line")
     ap.add_argument("--requests", type=int, default=120, help="serving form: number of requests")
-    ap.add_argument("--serial-sample", type=int, default=12, help="serving form: serial FP64 solves timed")
+    ap.add_argument("--serial-sample", type=int, default=12, help="serving/batched form: serial solves timed")
+    ap.add_argument("--batch", action="store_true", help="the batched form instead of the bench line")
+    ap.add_argument("--instances", type=int, default=256, help="batched form: number of instances")
     args = ap.parse_args()
     if args.serve:
         serve_main(args)
+        return
+    if args.batch:
+        batch_main(args)
         return
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]

@@ -230,9 +230,13 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // in by cp.async while the current one is transformed (NBUF = 1 where two
 // tiles do not fit in shared memory).
 // FP32 lines of up to 256 points fit in 80 registers without spills: three
-// CTAs per SM (the shared-memory tiles allow three as well).
+// CTAs per SM (the shared-memory tiles allow three as well). FP32 lines of
+// 512 and 1024 points (32 values per thread) fit in 128 registers without
+// spills when asked to: two CTAs per SM, each with a single tile buffer (two
+// double-buffered CTAs would not fit in shared memory), so one CTA's loads
+// overlap the other's transforms.
 template <class R, int A, int B, int NBUF>
-__global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : 0)
+__global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : (sizeof(R) == 4 ? 2 : 0))
 		col_reg_kernel(ColPassArgs a, int k) {
 	using T = c2<R>;
 	constexpr int N = A * B, W = kThreads / B, LD = W + 1, TS = N * LD;
@@ -544,7 +548,9 @@ template <class R, int A, int B>
 void col_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	constexpr int N = A * B, W = kThreads / B;
 	constexpr size_t tile_bytes = (size_t)N * (W + 1) * sizeof(c2<R>);
-	constexpr int NBUF = (2 * tile_bytes + N * sizeof(c2<R>) <= 220 * 1024) ? 2 : 1;
+	// FP32 lines of 32 values per thread run two single-buffered CTAs per SM
+	constexpr bool two_ctas = sizeof(R) == 4 && A > 16;
+	constexpr int NBUF = (!two_ctas && 2 * tile_bytes + N * sizeof(c2<R>) <= 220 * 1024) ? 2 : 1;
 	const size_t sm = N * sizeof(c2<R>) + NBUF * tile_bytes;
 	opt_in_smem(col_reg_kernel<R, A, B, NBUF>, sm);
 	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
