@@ -265,6 +265,14 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 int itp2d_batch_energies(int n, itp2d_ctx* const* ctxs, double* const* E, double* const* sigma,
 		double* const* sigma_residual);
 
+/* Diagnostic of the bounded device waits: one CTA of the tensor-core kernels'
+ * set-up (tensor memory and mbarriers) waits on a barrier that nothing
+ * completes. Returns ITP2D_E_TIMEOUT when the wait gives up after its limit
+ * (about a second) and the kernel frees its tensor memory and returns, as the
+ * overlap and rotation kernels do on a stalled pipeline; the context stays
+ * usable. No reference counterpart. */
+int itp2d_tc_wait_probe(void);
+
 /* Short description of a status code. */
 const char* itp2d_status_string(int status);
 

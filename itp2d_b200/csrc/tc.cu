@@ -509,11 +509,24 @@ __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned c
 	tc_teardown(sh);
 }
 
+// Diagnostic of the bounded waits: one CTA sets up exactly like the
+// tensor-core kernels (tensor memory allocated, mbarriers initialised), waits
+// on a barrier that nothing completes, records ITP2D_E_TIMEOUT when the wait
+// gives up, frees its tensor memory and returns.
+__global__ void __launch_bounds__(kThreads, 1) tc_wait_probe_kernel(int* err) {
+	TcShared& sh = tc_shared();
+	tc_setup(sh);
+	const bool ok = mbar_wait(smem_u32(&sh.mbar[0]), 0);  // phase 0 is never completed
+	if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicExch(err, ITP2D_E_TIMEOUT);
+	tc_teardown(sh);
+}
+
 size_t tc_smem() { return sizeof(TcShared) + 1024; }
 
 void set_tc_attributes() {
 	cudaFuncSetAttribute(overlap_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
 	cudaFuncSetAttribute(rotate_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
+	cudaFuncSetAttribute(tc_wait_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
 }
 
 }  // namespace
@@ -574,3 +587,19 @@ void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, u
 }
 
 }  // namespace itp2d
+
+int itp2d_tc_wait_probe(void) {
+	int* err = nullptr;
+	if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return ITP2D_E_OOM;
+	int st = ITP2D_E_CUDA;
+	if (cudaMemset(err, 0, sizeof(int)) == cudaSuccess) {
+		itp2d::set_tc_attributes();
+		itp2d::tc_wait_probe_kernel<<<1, itp2d::kThreads, itp2d::tc_smem()>>>(err);
+		int h = -1;
+		if (cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+				cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess)
+			st = h;
+	}
+	cudaFree(err);
+	return st;
+}

@@ -200,3 +200,18 @@ def test_lowdin_guard_falls_back_to_canonical():
     c.orthonormalize()
     c.orthonormalize()
     assert c.orthonormalization_counts() == (4, 2)
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable():
+    """The tensor-core kernels' mbarrier waits are bounded: a CTA set up like
+    them that waits on a barrier nothing completes returns ITP2D_E_TIMEOUT
+    after about a second, having freed its tensor memory; the tensor-core
+    overlap then runs normally on the same device."""
+    import time
+    L = capi.lib()
+    L.itp2d_tc_wait_probe.argtypes = []
+    t0 = time.perf_counter()
+    assert L.itp2d_tc_wait_probe() == capi.E_TIMEOUT
+    print(f"wait gave up after {time.perf_counter() - t0:.2f} s")
+    c, dx = _ctx(64, 64, 20, seed=9)
+    assert _rel(c.overlap_matrix(), _exact_overlap(c, dx)) < TOL_S
