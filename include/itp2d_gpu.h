@@ -237,6 +237,40 @@ int itp2d_hermitian_eigensolve_noalloc(int n, const double* A, double* evals, do
 int itp2d_add_gaussian_impurities(int sx, int sy, double dx, int n, const double* impurities, double* V,
 		void* cuda_stream);
 
+/* Potential of a description in the reference's mini-language, evaluated on
+ * the device at the cell-centred grid points into V (sx * sy doubles, device
+ * or managed memory, y-major): the 14 types of the reference's potential
+ * library with their names, parameter counts, defaults and checks
+ * (parse_potential_description, potentialtypes.cpp:56-100, and the
+ * constructors after it): zero, harmonic, elliptic, prettyhardsquare,
+ * softpentagon, henonheiles/henon, gaussian/gaussianblob,
+ * quartic/quarticoscillator, squareoscillator, power/poweroscillator,
+ * ring/ringpotential, cosh/coshpotential, softstadium, powerstadium.
+ * Formulas follow the reference's operation order without fused
+ * multiply-adds. ITP2D_E_INVALID for an unknown type, a wrong parameter count
+ * or a value the reference rejects. Asynchronous on cuda_stream. */
+int itp2d_evaluate_potential(const char* description, int sx, int sy, double dx, double* V, void* cuda_stream);
+/* The same into a host array V (sx * sy doubles), through temporary device
+ * memory; synchronous. */
+int itp2d_evaluate_potential_host(const char* description, int sx, int sy, double dx, double* V);
+/* Validates a description like itp2d_evaluate_potential (no device call);
+ * *is_null (may be NULL) is 1 for the zero potential. */
+int itp2d_potential_check(const char* description, int* is_null);
+
+/* Impurity shapes of noise.cpp:42-87 added to a potential on the device, for
+ * n impurities in list order at every grid point (rows and V in device or
+ * managed memory):
+ *   ITP2D_IMPURITY_COULOMB:    rows (x, y); V += param1 * (r^2)^(-param0 / 2)
+ *                              (CoulombImpurities: exponent, prefactor)
+ *   ITP2D_IMPURITY_HEMISPHERE: rows (x, y); V += param0 sqrt(1 - d^2 / param1^2)
+ *                              inside radius param1 (HemisphereImpurities)
+ *   ITP2D_IMPURITY_DELTA:      rows (x, y, A); V += A at the nearest grid point
+ *                              (DeltaImpurities, DataLayout::nearest_index)
+ * Gaussian impurities: itp2d_add_gaussian_impurities. */
+enum { ITP2D_IMPURITY_COULOMB = 1, ITP2D_IMPURITY_HEMISPHERE = 2, ITP2D_IMPURITY_DELTA = 3 };
+int itp2d_add_impurities(int shape, int sx, int sy, double dx, int n, const double* rows, double param0,
+		double param1, double* V, void* cuda_stream);
+
 /* Measures the FP64 tensor-core (DMMA) throughput of the current device in
  * TFLOP/s with a register-only kernel: the roofline denominator of the FP64
  * contractions. Diagnostic; no reference counterpart. */

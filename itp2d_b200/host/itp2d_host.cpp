@@ -169,30 +169,17 @@ DataLayout::DataLayout(size_t sx, size_t sy, double d)
 	for (size_t y = 0; y < sy; y++) posy[y] = (double)(2 * (long)y + 1 - (long)sy) * 0.5 * dx;
 }
 
+// The potential of a description (potentialtypes.hpp:96-380), evaluated by
+// the device kernel of itp2d_evaluate_potential_host. Returns false for the
+// null potential.
 bool evaluate_potential(const std::string& desc, const DataLayout& dl, std::vector<double>& out) {
-	const auto p = parse_parameter_string(desc);
-	const std::vector<double>& a = p.second;
+	int is_null = 0;
+	if (itp2d_potential_check(desc.c_str(), &is_null) != ITP2D_OK)
+		throw GeneralError("invalid potential description: " + desc);
 	out.assign(dl.N, 0.0);
-	if (p.first == "zero") return false;
-	auto at = [&](size_t i, double d) { return a.size() > i ? a[i] : d; };
-	for (size_t y = 0; y < dl.sizey; y++)
-		for (size_t x = 0; x < dl.sizex; x++) {
-			double v;
-			if (p.first == "harmonic") {
-				const double px = dl.posx[x] - at(1, 0.0), py = dl.posy[y] - at(2, 0.0);
-				v = 0.5 * at(0, 1.0) * (px * px + py * py);
-			} else if (p.first == "elliptic") {
-				const double px = dl.posx[x], py = dl.posy[y];
-				v = 0.5 * (at(0, 1.0) * px * px + at(1, 1.6180339887498948482) * py * py);
-			} else if (p.first == "gaussian" || p.first == "gaussianblob") {
-				const double px = dl.posx[x] - at(2, 0.0), py = dl.posy[y] - at(3, 0.0);
-				const double s = at(1, 1.0);
-				v = at(0, 1.0) * std::exp(-(px * px + py * py) / (2 * s * s));
-			} else {
-				throw GeneralError("potential type not available in this build: " + desc);
-			}
-			out[y * dl.sizex + x] = v;
-		}
+	if (is_null) return false;
+	const int st = itp2d_evaluate_potential_host(desc.c_str(), (int)dl.sizex, (int)dl.sizey, dl.dx, out.data());
+	if (st != ITP2D_OK) throw DeviceError("itp2d_evaluate_potential_host", st);
 	return true;
 }
 

@@ -123,8 +123,8 @@ struct DataLayout {
 	std::vector<double> posx, posy;
 };
 
-// Potentials of potentialtypes.hpp that the hot-path configurations use:
-// "zero", "harmonic(A[,x0,y0])", "elliptic(Ax,Ay)", "gaussian(A,sigma[,x0,y0])".
+// The potential library of potentialtypes.hpp:96-380 (all 14 types, the
+// reference's names, defaults and checks), evaluated on the device.
 // Returns false for the null potential.
 bool evaluate_potential(const std::string& desc, const DataLayout& dl, std::vector<double>& out);
 

@@ -344,4 +344,27 @@ void ref_add_gaussian_impurities(int sx, int sy, double dx, int n, const double*
 	}
 }
 
+/* V += n impurities of one shape through the reference's add_noise, in list
+ * order (noise.cpp:42-87): shape 1 CoulombImpurities(p0 = exponent,
+ * p1 = prefactor), rows (x, y); 2 HemisphereImpurities(p0 = amplitude,
+ * p1 = radius), rows (x, y); 3 DeltaImpurities, rows (x, y, A). The RNG only
+ * satisfies the constructors and is never drawn from. */
+void ref_add_impurities(int shape, int sx, int sy, double dx, int n, const double* rows, double p0, double p1,
+		double* V) {
+	DataLayout dl(static_cast<size_t>(sx), static_cast<size_t>(sy), dx);
+	RNG rng(1UL);
+	CoulombImpurities coulomb(p0, p1, rng);
+	HemisphereImpurities hemi(p0, p1, rng);
+	DeltaImpurities delta(0.0, 0.0, dl, rng);
+	std::vector<double> none, amp(1);
+	for (int j = 0; j < n; j++) {
+		if (shape == 1) coulomb.add_noise(rows[2 * j], rows[2 * j + 1], none, dl, V);
+		else if (shape == 2) hemi.add_noise(rows[2 * j], rows[2 * j + 1], none, dl, V);
+		else {
+			amp[0] = rows[3 * j + 2];
+			delta.add_noise(rows[3 * j], rows[3 * j + 1], amp, dl, V);
+		}
+	}
+}
+
 } // extern "C"

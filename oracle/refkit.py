@@ -71,6 +71,8 @@ def lib():
         L.refsys_times.argtypes = [vp, dp]
         L.ref_add_gaussian_impurities.argtypes = [i, i, d, i, dp, dp]
         L.ref_add_gaussian_impurities.restype = None
+        L.ref_add_impurities.argtypes = [i, i, i, d, i, dp, d, d, dp]
+        L.ref_add_impurities.restype = None
         _lib = L
     return _lib
 
@@ -86,6 +88,17 @@ def add_gaussian_impurities(sx: int, sy: int, dx: float, impurities: np.ndarray,
     out = np.ascontiguousarray(V, dtype=np.float64).copy()
     assert out.shape == (sy, sx)
     lib().ref_add_gaussian_impurities(sx, sy, dx, imp.shape[0], _dp(imp), _dp(out))
+    return out
+
+
+def add_impurities(shape: int, sx: int, sy: int, dx: float, rows: np.ndarray, p0: float, p1: float,
+                   V: np.ndarray) -> np.ndarray:
+    """V plus n impurities of one shape (1 Coulomb, 2 hemisphere, 3 delta)
+    through the reference's add_noise (noise.cpp:42-87); returns a new array."""
+    width = 3 if shape == 3 else 2
+    r = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, width)
+    out = np.ascontiguousarray(V, dtype=np.float64).copy()
+    lib().ref_add_impurities(shape, sx, sy, dx, r.shape[0], _dp(r), float(p0), float(p1), _dp(out))
     return out
 
 

@@ -92,3 +92,37 @@ def test_server_refuses_before_device_use():
     out = ctypes.c_void_p()
     assert L.itp2d_server_create(0, 1e9, ctypes.byref(out)) == capi.E_INVALID
     assert L.itp2d_server_create(2, 0.0, ctypes.byref(out)) == capi.E_INVALID
+
+
+def test_potential_descriptions_checked_like_the_reference():
+    """itp2d_potential_check applies the reference's names, parameter counts
+    and value checks (potentialtypes.cpp:56-500) without a device."""
+    L = capi.lib()
+    f = L.itp2d_potential_check
+    f.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    good = ["zero", "harmonic", "harmonic(2)", "harmonic(1,0.5,-0.5)", "elliptic(1,2)", "prettyhardsquare(6)",
+            "softpentagon", "henonheiles", "henon(1,-1)", "gaussian(1,2)", "gaussianblob(1,2,0,1)",
+            "quartic(0.1)", "quarticoscillator", "squareoscillator(4)", "power(3)", "poweroscillator(3,2)",
+            "ring", "ring(3,1,2)", "ringpotential(3,1,2,0.5,1)", "cosh(1,2)", "coshpotential",
+            "softstadium", "softstadium(1,2,100)", "softstadium(1,2,100,1,10)", "powerstadium(4)",
+            "powerstadium(1,2,4)"]
+    bad = ["nosuchpotential", "harmonic(1,2)", "harmonic(-1)", "elliptic(1)", "elliptic(-1,1)",
+           "softpentagon(1)", "gaussian(1,0)", "gaussian(-1,1)", "quartic(-1)", "power(2,-1)", "ring(-1,1,2)",
+           "ring(3,0,2)", "ring(3,1)", "cosh(0,1)", "cosh(1,0)", "softstadium(0,2,100)", "softstadium(1,2)",
+           "powerstadium(1,0,4)", "powerstadium(1,2)", "zero(1)", "harmonic(1", "harmonic(a)"]
+    for d in good:
+        n = ctypes.c_int(-1)
+        assert f(d.encode(), ctypes.byref(n)) == capi.OK, d
+        assert n.value == (1 if d == "zero" else 0)
+    for d in bad:
+        assert f(d.encode(), None) == capi.E_INVALID, d
+    # device entry points reject bad arguments before any device call
+    ev = L.itp2d_evaluate_potential
+    ev.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    assert ev(b"foo", 16, 16, 0.1, ctypes.c_void_p(1), None) == capi.E_INVALID
+    assert ev(b"harmonic", 0, 16, 0.1, ctypes.c_void_p(1), None) == capi.E_INVALID
+    add = L.itp2d_add_impurities
+    add.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    assert add(9, 16, 16, 0.1, 1, ctypes.c_void_p(1), 1.0, 1.0, ctypes.c_void_p(1), None) == capi.E_INVALID
+    assert add(1, 16, 16, 0.1, 0, None, 1.0, 1.0, ctypes.c_void_p(1), None) == capi.OK
