@@ -299,6 +299,30 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 int itp2d_batch_energies(int n, itp2d_ctx* const* ctxs, double* const* E, double* const* sigma,
 		double* const* sigma_residual);
 
+/* ---- Device-resident driver loop (no reference counterpart) ----
+ *
+ * Runs ITP iterations of the context without returning to the host until the
+ * time-step test of the driver holds: one CUDA graph launch whose conditional
+ * WHILE node repeats propagate, canonical orthonormalisation (the batched
+ * eigensolver's one-CTA Jacobi), energies, and a device kernel that sorts the
+ * (E, sigma, n) tuples and applies the test at every sorted position against
+ * the previous iteration (itpsystem.cpp:291-330 with the tests of
+ * convergence.cpp:75-199): test 0 abschange(limit), 1 relchange(limit),
+ * 2 absstdev(limit, diff_limit), 3 relstdev(limit, diff_limit). A passing
+ * state's flag is kept by its storage index (flags: k ints, in and out); the
+ * loop ends once the states at sorted positions first .. first + count - 1
+ * are all flagged, on an orthonormalisation failure (*status; the failed
+ * iteration's rotation has then been applied with the previous W), or after
+ * max_iterations. prev_sorted_E / prev_sorted_sigma (may be NULL) are the
+ * previous iteration's sorted values. On return: iterations taken, the last
+ * sorted energies, deviations and storage indices, and the sorted values of
+ * the iteration before it (k each; sorted_index and the prev outputs may be
+ * NULL). The time step does not change inside the loop. */
+int itp2d_run_device_loop(itp2d_ctx* ctx, int max_iterations, int test, double limit, double diff_limit, int first,
+		int count, const double* prev_sorted_E, const double* prev_sorted_sigma, int* flags, int* iterations,
+		int* status, double* sorted_E, double* sorted_sigma, int* sorted_index, double* prev_E_out,
+		double* prev_sigma_out);
+
 /* Diagnostic of the bounded device waits: one CTA of the tensor-core kernels'
  * set-up (tensor memory and mbarriers) waits on a barrier that nothing
  * completes. Returns ITP2D_E_TIMEOUT when the wait gives up after its limit

@@ -70,6 +70,17 @@ int itp2d_system_step(itp2d_system* s);
  * returns ITP2D_OK (check itp2d_system_error_flag). */
 int itp2d_system_run(itp2d_system* s, int max_iterations);
 
+/* Like itp2d_system_run, with the FP64 iterations run on the device: each
+ * phase is one itp2d_run_device_loop (iterations without host round trips
+ * until the time-step test holds) followed by the driver's final test and
+ * time-step schedule; the FP32 phase of the mixed form and time-step tests
+ * other than abschange, relchange, absstdev and relstdev take step() instead.
+ * The energy history keeps only the last two iterations of each device phase.
+ * Runs at most max_phases phases. No reference counterpart. */
+int itp2d_system_run_device(itp2d_system* s, int max_phases);
+/* Iterations taken inside device phases. */
+int itp2d_system_device_iterations(const itp2d_system* s);
+
 int itp2d_system_is_finished(const itp2d_system* s);
 int itp2d_system_error_flag(const itp2d_system* s);
 int itp2d_system_total_steps(const itp2d_system* s);

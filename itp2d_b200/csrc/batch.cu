@@ -37,17 +37,21 @@ struct Rot {
 };
 
 __global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEigItem* __restrict__ items, int n,
-		int max_sweeps) {
+		int max_sweeps, int smem_bytes) {
 	__shared__ Rot rot[kMaxPairs / 4];  // pairs handled per chunk (see below)
 	__shared__ double red[kBThreads / 32];
 	__shared__ int s_bad, s_sweeps;
+	extern __shared__ __align__(16) double2 work[];
 	const BatchEigItem it = items[blockIdx.x];
 	const int k = it.k;
 	const int kp = (k + 1) & ~1;
 	const int np = kp / 2;
 	const int tid = threadIdx.x;
-	double2* A = it.A;
-	double2* V = it.V;
+	// A (and V) in shared memory when they fit in this launch's dynamic
+	// shared memory, else the instance's work matrices in global memory
+	const size_t mat = (size_t)kp * kp * sizeof(double2);
+	double2* A = mat <= (size_t)smem_bytes ? work : it.A;
+	double2* V = 2 * mat <= (size_t)smem_bytes ? work + (size_t)kp * kp : it.V;
 	// A = S (row-major, stride kp), V = I
 	for (int idx = tid; idx < kp * kp; idx += blockDim.x) {
 		const int i = idx / kp, j = idx % kp;
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEi
 	// first offending eigenvalue in ascending order (stateset.cpp:158-172)
 	for (int r = tid; r < k; r += blockDim.x) {
 		const double e = it.evals[r];
-		if (!(e > 0.0) || !isnormal(e)) atomicMin(&s_bad, r);
+		if (!(e > 0.0) || !(e >= 2.2250738585072014e-308) || isinf(e) || e != e) atomicMin(&s_bad, r);
 	}
 	__syncthreads();
 	if (tid == 0) {
@@ -198,9 +202,21 @@ __global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEi
 
 }  // namespace
 
-cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, cudaStream_t s) {
+cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, cudaStream_t s) {
 	if (n <= 0) return cudaSuccess;
-	batched_jacobi_kernel<<<n, kBThreads, 0, s>>>(items, n, max_sweeps);
+	// dynamic shared memory for A and V of the largest instance, up to 200 KB
+	// (instances whose matrices do not fit use their global work matrices)
+	const size_t kp = (size_t)((max_k + 1) & ~1);
+	const size_t want = 2 * kp * kp * sizeof(double2);
+	const size_t one = kp * kp * sizeof(double2);
+	const size_t cap = 200 * 1024;
+	const int smem = (int)(want <= cap ? want : (one <= cap ? one : 0));
+	if (smem > 48 * 1024) {
+		const cudaError_t e = cudaFuncSetAttribute(batched_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				smem);
+		if (e != cudaSuccess) return e;
+	}
+	batched_jacobi_kernel<<<n, kBThreads, smem, s>>>(items, n, max_sweeps, smem);
 	return cudaGetLastError();
 }
 

@@ -125,7 +125,8 @@ struct BatchEigItem {
 	int pad;
 	double tau;
 };
-cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, cudaStream_t s);
+// max_k: the largest k among the items (sizes the shared-memory work area).
+cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, cudaStream_t s);
 int batched_eigensolve_max_k();
 
 // Users of the cooperative eigensolvers (contexts and the standalone

@@ -115,6 +115,7 @@ struct itp2d_ctx {
 	long long ortho_calls[2] = {0, 0};  // canonical, Lowdin
 	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
 	double* hlstat = nullptr;    // pinned copy
+	void* loop_buf = nullptr;    // device driver loop state (itp2d_run_device_loop)
 	size_t device_bytes = 0;  // sum of this context's device allocations
 	itp2d::CoopUser coop;     // counts toward the cooperative-eigensolve serialisation
 };
@@ -1354,7 +1355,9 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 	// every eigenproblem in one launch
 	cudaError_t e = cudaMemcpyAsync(g_items_dev, g_items_host, n * sizeof(BatchEigItem), cudaMemcpyHostToDevice,
 			g_batch_stream);
-	if (e == cudaSuccess) e = launch_batched_eigensolve(g_items_dev, n, 60, g_batch_stream);
+	int max_k = 2;
+	for (int i = 0; i < n; i++) max_k = std::max(max_k, ctxs[i]->k);
+	if (e == cudaSuccess) e = launch_batched_eigensolve(g_items_dev, n, 60, max_k, g_batch_stream);
 	if (e == cudaSuccess) e = cudaEventRecord(ev[n], g_batch_stream);
 	if (e != cudaSuccess) {
 		cleanup();
@@ -1443,5 +1446,217 @@ int itp2d_batch_propagate(int n, itp2d_ctx* const* ctxs) {
 		const int st = itp2d_propagate(ctxs[i]);
 		if (st) return st;
 	}
+	return ITP2D_OK;
+}
+
+// ---- Device-resident driver loop ----
+//
+// ITP iterations that never return to the host until the time-step test
+// holds: one CUDA graph whose conditional WHILE node runs the body
+//   propagate -> overlap -> eigensolve (batch.cu, one CTA; no cooperative
+//   grid barrier inside a graph) -> rotation -> energies -> sort + test
+// and whose last kernel sets the loop condition on the device. The test
+// kernel restates the host driver's step logic for the time-step test
+// (itpsystem.cpp:291-330, convergence.cpp:75-199): the (E, sigma, n) tuples
+// sorted by energy, the test applied at every sorted position against the
+// previous iteration's sorted values, a passing state's flag kept by its
+// storage index, and the loop ending once every wanted position's state is
+// flagged (or on an eigensolver failure, or after max_iterations).
+
+namespace {
+
+constexpr int kLoopThreads = 1024;
+
+// loop[0] iterations done, loop[1] done, loop[2] status, loop[3] history length
+__global__ void __launch_bounds__(kLoopThreads) loop_test_kernel(const double* __restrict__ E,
+		const double* __restrict__ S, int k, int first, int count, int test, double limit, double diff_limit,
+		int max_iterations, double* curE, double* curS, double* prevE, double* prevS, int* idx, int* flags,
+		int* loop, const EigStatus* eig, cudaGraphConditionalHandle h) {
+	__shared__ int s_fail;
+	const int tid = threadIdx.x;
+	if (tid == 0) s_fail = 0;
+	// the previous sorted values become history
+	for (int n = tid; n < k; n += blockDim.x) {
+		prevE[n] = curE[n];
+		prevS[n] = curS[n];
+	}
+	__syncthreads();
+	for (int i = tid; i < k; i += blockDim.x) {
+		const double ei = E[i];
+		int r = 0;
+		for (int j = 0; j < k; j++) {
+			const double ej = E[j];
+			r += (ej < ei || (ej == ei && (S[j] < S[i] || (S[j] == S[i] && j < i)))) ? 1 : 0;
+		}
+		curE[r] = ei;
+		curS[r] = S[i];
+		idx[r] = i;
+	}
+	__syncthreads();
+	const int hist = loop[3] + 1;  // history entries including this iteration
+	for (int n = tid; n < k; n += blockDim.x) {
+		bool pass = false;
+		if (test == 0 || test == 1) {  // abschange, relchange: need two entries
+			if (hist >= 2) {
+				const double d = fabs(curE[n] - prevE[n]);
+				pass = test == 0 ? d < limit : fabs((curE[n] - prevE[n]) / prevE[n]) < limit;
+			}
+		} else if (hist >= 2) {  // absstdev, relstdev (deviation tests need two entries too)
+			const double t = test == 2 ? curS[n] : curS[n] / curE[n];
+			const double p = test == 2 ? prevS[n] : prevS[n] / prevE[n];
+			pass = t < limit || fabs(t - p) < diff_limit;
+		}
+		if (pass) flags[idx[n]] = 1;
+	}
+	__syncthreads();
+	for (int n = first + tid; n < first + count; n += blockDim.x)
+		if (!flags[idx[n]]) atomicOr(&s_fail, 1);
+	__syncthreads();
+	if (tid == 0) {
+		const int it = loop[0] + 1;
+		loop[0] = it;
+		loop[3] = hist;
+		int done = !s_fail;
+		if (eig->status != ITP2D_OK) {
+			loop[2] = eig->status;
+			done = 1;
+		}
+		if (it >= max_iterations) done = 1;
+		loop[1] = done;
+		cudaGraphSetConditional(h, done ? 0u : 1u);
+	}
+}
+
+}  // namespace
+
+int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double limit, double diff_limit, int first,
+		int count, const double* prev_sorted_E, const double* prev_sorted_sigma, int* flags, int* iterations,
+		int* status, double* sorted_E, double* sorted_sigma, int* sorted_index, double* prev_E_out,
+		double* prev_sigma_out) {
+	if (!c || max_iterations < 1 || test < 0 || test > 3 || first < 0 || count < 1 || !flags || !iterations ||
+			!status || !sorted_E || !sorted_sigma)
+		return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	const int k = c->k;
+	if (first + count > k || k < 2 || k > batched_eigensolve_max_k() || !c->eps_set) return ITP2D_E_INVALID;
+	// device loop state: sorted E, sigma (current and previous), sorted index,
+	// flags, loop counters, one eigensolver item
+	if (!c->loop_buf) {
+		const size_t bytes = (size_t)4 * k * sizeof(double) + 2 * (size_t)k * sizeof(int) + 8 * sizeof(int) +
+				sizeof(BatchEigItem) + 64;
+		cudaError_t e = cudaSuccess;
+		c->loop_buf = dalloc(c, bytes, &e);
+		ITP2D_TRY(e);
+	}
+	double* curE = (double*)c->loop_buf;
+	double* curS = curE + k;
+	double* prevE = curS + k;
+	double* prevS = prevE + k;
+	int* idx = (int*)(prevS + k);
+	int* dflags = idx + k;
+	int* loop = dflags + k;
+	BatchEigItem* item = (BatchEigItem*)(((uintptr_t)(loop + 8) + 15) & ~(uintptr_t)15);
+	const bool have_prev = prev_sorted_E && prev_sorted_sigma;
+	std::vector<int> hl = {0, 0, ITP2D_OK, have_prev ? 1 : 0, 0, 0, 0, 0};
+	ITP2D_TRY(cudaMemcpyAsync(loop, hl.data(), 8 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+	ITP2D_TRY(cudaMemcpyAsync(dflags, flags, k * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+	if (have_prev) {
+		ITP2D_TRY(cudaMemcpyAsync(curE, prev_sorted_E, k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+		ITP2D_TRY(cudaMemcpyAsync(curS, prev_sorted_sigma, k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	}
+	BatchEigItem it;
+	it.S = c->S;
+	it.A = c->jw.A0;
+	it.V = c->jw.V;
+	it.W = c->W;
+	it.evals = c->jw.evals;
+	it.perm = c->jw.perm;
+	it.st = c->dstat;
+	it.k = k;
+	it.pad = 0;
+	it.tau = c->precision == ITP2D_FP64 ? 3e-9 : 1e-3;
+	ITP2D_TRY(cudaMemcpyAsync(item, &it, sizeof(it), cudaMemcpyHostToDevice, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+
+	// the graph: a WHILE node whose body is one iteration
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	ITP2D_TRY(cudaGraphCreate(&graph, 0));
+	auto fail = [&](cudaError_t e) {
+		if (exec) cudaGraphExecDestroy(exec);
+		if (graph) cudaGraphDestroy(graph);
+		return cuda_status(e);
+	};
+	cudaGraphConditionalHandle h;
+	cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+	if (e != cudaSuccess) return fail(e);
+	cudaGraphNodeParams np = {};
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = h;
+	np.conditional.type = cudaGraphCondTypeWhile;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	e = cudaGraphAddNode(&node, graph, nullptr, 0, &np);
+	if (e != cudaSuccess) return fail(e);
+	cudaGraph_t body = np.conditional.phGraph_out[0];
+	const bool timing = c->timing;
+	c->timing = false;  // event records are not allowed in a conditional body
+	void* const psi0 = c->psi;
+	void* const acc0 = c->acc;
+	const long long launches0 = c->launches;
+	e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+	if (e == cudaSuccess) {
+		const bool tc = use_tensor_cores(c);
+		if (c->precision == ITP2D_FP64) propagate_fused<double>(c);
+		else propagate_fused<float>(c);
+		launch_overlap_any(c, tc);
+		launch_batched_eigensolve(item, 1, 60, k, c->stream);
+		if (tc)
+			launch_rotate_tc(c->W, (const float2*)c->psi, k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream);
+		else if (c->precision == ITP2D_FP64)
+			launch_rotate(c->W, (const double2*)c->psi, k, c->G, (double2*)c->acc, c->stream);
+		else launch_rotate(c->W, (const float2*)c->psi, k, c->G, (float2*)c->acc, c->stream);
+		std::swap(c->psi, c->acc);
+		if (c->precision == ITP2D_FP64) energies_impl<double>(c, nullptr, true);
+		else energies_impl<float>(c, nullptr, true);
+		cudaMemcpyAsync(c->dEshift, c->dE, (size_t)k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+		// the body starts and ends on the same state buffer
+		if (c->psi != psi0)
+			cudaMemcpyAsync(psi0, c->psi, (size_t)c->G * k * c->es, cudaMemcpyDeviceToDevice, c->stream);
+		loop_test_kernel<<<1, kLoopThreads, 0, c->stream>>>(c->dE, c->dsig, k, first, count, test, limit,
+				diff_limit, max_iterations, curE, curS, prevE, prevS, idx, dflags, loop, c->dstat, h);
+		cudaGraph_t out = nullptr;
+		const cudaError_t e2 = cudaStreamEndCapture(c->stream, &out);
+		e = cudaGetLastError();
+		if (e == cudaSuccess) e = e2;
+	}
+	c->psi = psi0;
+	c->acc = acc0;
+	c->timing = timing;
+	const long long per_iteration = c->launches - launches0 + 1;
+	c->launches = launches0;
+	if (e != cudaSuccess) return fail(e);
+	e = cudaGraphInstantiate(&exec, graph, 0);
+	if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+	std::vector<int> out(8);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), loop, 8 * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(flags, dflags, k * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(sorted_E, curE, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(sorted_sigma, curS, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess && sorted_index)
+		e = cudaMemcpyAsync(sorted_index, idx, k * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess && prev_E_out)
+		e = cudaMemcpyAsync(prev_E_out, prevE, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess && prev_sigma_out)
+		e = cudaMemcpyAsync(prev_sigma_out, prevS, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+	if (e != cudaSuccess) return fail(e);
+	cudaGraphExecDestroy(exec);
+	cudaGraphDestroy(graph);
+	*iterations = out[0];
+	*status = out[2];
+	c->launches += per_iteration * out[0];
+	// the current energies are the shift of the next residual evaluation
 	return ITP2D_OK;
 }

@@ -330,7 +330,11 @@ void ITPSystem::orthonormalize() {
 	const double t0 = now_s();
 	int bi = -1;
 	double bv = 0;
+	long long c0 = 0, c1 = 0;
+	itp2d_orthonormalization_counts(ctx, &c0, nullptr);
 	const int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
+	itp2d_orthonormalization_counts(ctx, &c1, nullptr);
+	last_ortho_canonical = c1 > c0;
 	t_ortho += now_s() - t0;
 	orthonormalized(st, bi, bv);
 }
@@ -447,11 +451,27 @@ void ITPSystem::change_time_step() {
 // The FP32 form switches to FP64 once every wanted energy changes by less than
 // fp32_switch per step, or once the largest change has not decreased for
 // kFp32Stall steps (the FP32 noise floor lies above fp32_switch).
+// With Lowdin steps between canonical ones (fp32_canonical_every > 1) the
+// rule looks at canonical iterations only, comparing with the previous
+// canonical iteration, and one stalled comparison ends the FP32 phase: a
+// Lowdin step does not rotate within the subspace, so its per-state energy
+// changes understate the subspace's progress and would end the phase early.
 void ITPSystem::maybe_switch_precision() {
 	if (precision != ITP2D_FP32 || !(p.fp32_switch > 0) || energies.size() < 2) return;
-	constexpr int kFp32Stall = 3;
-	const auto& a = energies[energies.size() - 1];
-	const auto& b = energies[energies.size() - 2];
+	const bool lowdin = p.fp32_canonical_every > 1;
+	const int kFp32Stall = lowdin ? 1 : 3;
+	if (lowdin) {
+		if (!last_ortho_canonical) return;
+		const std::vector<double> prev = fp32_canonical_energies;
+		fp32_canonical_energies = energies.back();
+		if (prev.empty()) return;
+		fp32_compare_with(energies.back(), prev, kFp32Stall);
+		return;
+	}
+	fp32_compare_with(energies[energies.size() - 1], energies[energies.size() - 2], kFp32Stall);
+}
+
+void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit) {
 	double worst = 0.0;
 	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) {
 		const double d = std::fabs(a[n] - b[n]);
@@ -463,7 +483,7 @@ void ITPSystem::maybe_switch_precision() {
 			fp32_stall = 0;
 			return;
 		}
-		if (++fp32_stall < kFp32Stall) return;
+		if (++fp32_stall < stall_limit) return;
 	}
 	check(itp2d_set_precision(ctx, ITP2D_FP64), "itp2d_set_precision");
 	precision = ITP2D_FP64;
@@ -479,6 +499,76 @@ void ITPSystem::step() {
 	orthonormalize();
 	calculate_energies();
 	step_end();
+}
+
+// Iterations on the device until the time-step test holds
+// (itp2d_run_device_loop), then the host's final test and time-step
+// schedule exactly as after a step() (itpsystem.cpp:454-466). Only for the
+// FP64 sweeps, a time-step test of the four single-limit kinds and without
+// eps exhaustion (which changes eps every step); otherwise one step().
+void ITPSystem::run_device_phase() {
+	if (finished) return;
+	const auto spec = parse_parameter_string(p.timestep_test);
+	static const char* names[] = {"abschange", "relchange", "absstdev", "relstdev"};
+	int test = -1;
+	for (int i = 0; i < 4; i++)
+		if (spec.first == names[i]) test = i;
+	const size_t npar = spec.second.size();
+	const bool ok_params = (test < 2 && npar == 1) || (test >= 2 && (npar == 1 || npar == 2));
+	const int remaining = p.max_steps - total_step_counter;
+	if (precision != ITP2D_FP64 || test < 0 || !ok_params || exhausting || remaining < 1) {
+		step();
+		return;
+	}
+	const double limit = spec.second[0], diff = npar == 2 ? spec.second[1] : 0.0;
+	const size_t k = (size_t)p.num_states;
+	std::vector<int> flags(k);
+	for (size_t i = 0; i < k; i++) flags[i] = timestep_converged[i] ? 1 : 0;
+	const double* pe = energies.empty() || energies.back().empty() ? nullptr : energies.back().data();
+	const double* ps = pe ? deviations.back().data() : nullptr;
+	std::vector<double> E(k), S(k), E0(k), S0(k);
+	std::vector<int> idx(k);
+	int iters = 0, st = ITP2D_OK;
+	if (total_step_counter == 0) t_start = now_s();
+	const double t0 = now_s();
+	check(itp2d_run_device_loop(ctx, remaining, test, limit, diff, p.ignore_lowest, p.wanted, pe, ps, flags.data(),
+				  &iters, &st, E.data(), S.data(), idx.data(), E0.data(), S0.data()),
+			"itp2d_run_device_loop");
+	t_prop += now_s() - t0;
+	device_iterations += iters;
+	if (iters == 0) return;
+	total_step_counter += iters;
+	step_counter += iters;
+	// history: the last two iterations (the ones the tests read); the
+	// intermediate iterations' energies stayed on the device
+	energies.resize(total_step_counter);
+	deviations.resize(total_step_counter);
+	if (iters >= 2 || !pe) {
+		energies[total_step_counter - 2 >= 0 ? total_step_counter - 2 : 0] = E0;
+		deviations[total_step_counter - 2 >= 0 ? total_step_counter - 2 : 0] = S0;
+	}
+	energies.back() = E;
+	deviations.back() = S;
+	sorted.resize(k);
+	for (size_t n = 0; n < k; n++) sorted[n] = Esn(std::make_pair(E[n], S[n]), (size_t)idx[n]);
+	residuals.assign(k, 0.0);
+	for (size_t i = 0; i < k; i++) timestep_converged[i] = flags[i] != 0;
+	if (st != ITP2D_OK) {
+		orthonormalized(st, -1, 0.0);
+		return;
+	}
+	bool all = true;
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
+		if (!timestep_converged[sorted[n].second]) all = false;
+	all_timestep_converged = all;
+	if (all_timestep_converged) {
+		check_final_convergence();
+		if (all_finally_converged) {
+			finish();
+			return;
+		}
+		change_time_step();
+	}
 }
 
 bool ITPSystem::step_begin() {
@@ -532,6 +622,7 @@ void ITPSystem::reset(const double* init) {
 	total_step_counter = step_counter = 0;
 	fp32_best = INFINITY;
 	fp32_stall = 0;
+	fp32_canonical_energies.clear();
 	t_total = t_prop = t_ortho = t_conv = 0;
 	energies.clear();
 	deviations.clear();
@@ -679,6 +770,22 @@ int itp2d_system_run(itp2d_system* s, int max_iterations) {
 	}
 	return ITP2D_OK;
 }
+
+int itp2d_system_run_device(itp2d_system* s, int max_phases) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	try {
+		for (int i = 0; i < max_phases && !s->sys->is_finished(); i++) s->sys->run_device_phase();
+	} catch (itp2d::DeviceError& e) {
+		s->err = e.what();
+		return e.status;
+	} catch (std::exception& e) {
+		s->err = e.what();
+		return ITP2D_E_INVALID;
+	}
+	return ITP2D_OK;
+}
+
+int itp2d_system_device_iterations(const itp2d_system* s) { return s && s->sys ? s->sys->device_iterations : -1; }
 
 int itp2d_system_is_finished(const itp2d_system* s) { return s && s->sys && s->sys->is_finished() ? 1 : 0; }
 int itp2d_system_error_flag(const itp2d_system* s) { return s && s->sys && s->sys->get_error_flag() ? 1 : 0; }

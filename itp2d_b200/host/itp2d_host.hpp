@@ -171,6 +171,11 @@ class ITPSystem {
 	// caller, then orthonormalized() with the orthonormalisation's status and
 	// energies_computed() with the per-state energies in storage order.
 	bool step_begin();
+	// Iterations on the device until the time-step test holds, then the
+	// host's final test and time-step schedule (FP64 sweeps; otherwise one
+	// step()).
+	void run_device_phase();
+	int device_iterations = 0;  // iterations run by run_device_phase
 	void orthonormalized(int status, int bad_index, double bad_value);
 	void energies_computed(const double* E, const double* sigma, const double* residual);
 	void finish();
@@ -207,6 +212,7 @@ class ITPSystem {
 	void change_time_step();
 	void init_states();
 	void maybe_switch_precision();
+	void fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit);
 	void check(int status, const char* where);
 
 	DataLayout dl;
@@ -222,6 +228,8 @@ class ITPSystem {
 	int total_step_counter = 0, step_counter = 0;
 	double fp32_best = INFINITY;  // smallest per-step energy change seen in the FP32 form
 	int fp32_stall = 0;           // FP32 steps since that change last decreased
+	bool last_ortho_canonical = true;               // the last orthonormalisation's form
+	std::vector<double> fp32_canonical_energies;    // energies of the last canonical FP32 iteration
 	double eps = 0;
 	std::list<double> eps_values;
 	std::vector<Esn> sorted;

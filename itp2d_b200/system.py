@@ -39,6 +39,8 @@ def _lib():
         for n in ["itp2d_system_destroy", "itp2d_system_step"]:
             getattr(L, n).argtypes = [vp]
         L.itp2d_system_run.argtypes = [vp, i]
+        L.itp2d_system_run_device.argtypes = [vp, i]
+        L.itp2d_system_device_iterations.argtypes = [vp]
         L.itp2d_system_reset.argtypes = [vp, dp]
         for n in ["itp2d_system_is_finished", "itp2d_system_error_flag", "itp2d_system_total_steps",
                   "itp2d_system_num_converged", "itp2d_system_in_fp32"]:
@@ -161,6 +163,16 @@ class ITPSystem:
         st = _lib().itp2d_system_run(self.h, int(max_iterations))
         if st != capi.OK:
             raise capi.ITP2DError(st, "itp2d_system_run: " + self.last_error)
+
+    def run_device(self, max_phases=1 << 30):
+        """Solve with the FP64 iterations on the device (itp2d_system_run_device)."""
+        st = _lib().itp2d_system_run_device(self.h, int(max_phases))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_run_device: " + self.last_error)
+
+    @property
+    def device_iterations(self) -> int:
+        return _lib().itp2d_system_device_iterations(self.h)
 
     @property
     def finished(self) -> bool:

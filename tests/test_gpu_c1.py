@@ -1,7 +1,7 @@
 """Configuration C1 on the GPU: V = r^2/2, B = 0, Dirichlet box of side 12 on
-128 x 128 (DST-II/III lines), k = 64, 2nd-order split at eps = 0.02 halved when
-the wanted states stall (abschange(1e-10)), final test absstdev(1e-6) (the
-deviation of a converged state sits at its FP64 cancellation floor, about 1e-7),
+128 x 128 (DST-II/III lines), k = 64, 2nd-order split at eps = 0.02,
+relstdev(1e-5) as time-step and final test (the deviation of a converged
+state sits at its FP64 cancellation floor, near 1e-6),
 the 55 states of the levels E = 1..10 wanted (the 64 states end inside the
 11-fold level E = 11).
 
@@ -40,7 +40,7 @@ def analytic(n):
     return np.array(out[:n])
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed"])
+@pytest.mark.parametrize("form", ["fp64", "mixed", "fp64_device"])
 def test_c1_solve(form):
     import torch
     if not torch.cuda.is_available():
@@ -53,10 +53,16 @@ def test_c1_solve(form):
                           halforder=w["halforder"], num_states=w["num_states"], wanted=w["wanted"], eps=[w["eps"]],
                           eps_divisor=w["eps_divisor"], timestep_test=w["timestep_test"],
                           final_test=w["final_test"], max_steps=20000, potential=w["potential"],
-                          precision=capi.FP64 if form == "fp64" else capi.FP32,
+                          precision=capi.FP32 if form == "mixed" else capi.FP64,
                           fp32_switch=1e-7 if form == "mixed" else 0.0)
     s = system.ITPSystem(p, init_states=g.c1_states())
-    s.run()
+    if form == "fp64_device":
+        # iterations on the device until the time-step test holds (one CUDA
+        # graph with a conditional loop), the final test on the host
+        s.run_device()
+        assert s.device_iterations == s.total_steps
+    else:
+        s.run()
     assert s.finished and not s.error_flag, s.last_error
     E = s.energies()[0]
     n = w["wanted"]

@@ -35,13 +35,19 @@ def setup():
     return bench, psi, ref
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed"])
+@pytest.mark.parametrize("form", ["fp64", "mixed", "fp64_device"])
 def test_solve_matches_reference_solve(setup, form):
+    """fp64_device: the same FP64 solve with its iterations in a device-side
+    loop (itp2d_system_run_device), the time-step test evaluated on the GPU."""
     bench, psi, ref = setup
     from itp2d_b200 import system
     w = bench.WORKLOAD
-    s = system.ITPSystem(bench.params(form), init_states=psi)
-    s.run()
+    s = system.ITPSystem(bench.params("fp64" if form == "fp64_device" else form), init_states=psi)
+    if form == "fp64_device":
+        s.run_device()
+        assert s.device_iterations == s.total_steps
+    else:
+        s.run()
     assert s.finished and not s.error_flag, s.last_error
     E = s.energies()[0]
     Eref = np.array(ref["energies"])
@@ -50,7 +56,7 @@ def test_solve_matches_reference_solve(setup, form):
     print(f"{form}: {s.total_steps} iterations (reference {ref['iterations']}), {s.num_converged} converged "
           f"(reference {ref['converged']}), max |dE| over the {n} wanted states {dE.max():.3e}")
     assert dE.max() < 2e-9
-    if form == "fp64":
+    if form.startswith("fp64"):
         # the same algorithm from the same states: the solve length can differ
         # only where an energy change sits at the 1e-9 threshold
         assert abs(s.total_steps - ref["iterations"]) <= 1

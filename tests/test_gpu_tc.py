@@ -177,8 +177,14 @@ def test_lowdin_step_orthonormalises(k, delta):
     assert c.orthonormalization_counts() == (0, 1)
     out = c.download()
     assert O.how_orthonormal(g, out) < TOL_ORTHO
+    # every output state lies in the input's span: its residual outside an
+    # FP64 orthonormal basis of that span is at the FP32 / split-BF16 level
     ref, _ = O.orthonormalize(g, psi)
-    assert 1 - O.subspace_cosines(g, out, ref).min() < 1e-9
+    R = ref.reshape(k, -1)
+    X = out.reshape(k, -1)
+    P = (np.conj(R) @ X.T) * g.dx * g.dx
+    res = X - P.T @ R
+    assert np.max(np.sqrt(np.sum(np.abs(res) ** 2, axis=1)) * g.dx) < 5 * TOL_ORTHO
     nrm = np.sqrt(np.sum(np.abs(psi) ** 2, axis=(1, 2))) * g.dx
     move = np.sqrt(np.sum(np.abs(out - psi / nrm[:, None, None]) ** 2, axis=(1, 2))) * g.dx
     assert np.max(move) < 10 * delta
