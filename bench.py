@@ -55,6 +55,13 @@ WORKLOADS = {
                   eps=0.05, potential="harmonic(1)", test="abschange(1e-9)", seed=20240602,
                   bumps=dict(n=400, amp=(0.8, 1.2), width=0.1, box=6.0, seed=20240603),
                   fp64_solve=(14, 1110), ortho_sample=(500, 256, 128)),
+    # the bumpy dot at k = 256: the same kernel instantiations (512-point
+    # lines, tensor-core contractions, block Jacobi) in about 3 GB of device
+    # memory, the case the ncu captures under profiles/ run on
+    "profile": dict(name="bumpy dot (profiling size)", sx=512, sy=512, length=16.0, B=0.5, halforder=3,
+                    num_states=256, wanted=128, eps=0.05, potential="harmonic(1)", test="abschange(1e-9)",
+                    seed=20240602, bumps=dict(n=400, amp=(0.8, 1.2), width=0.1, box=6.0, seed=20240603),
+                    fp64_solve=(0, 0), ortho_sample=(256, 256, 128)),
 }
 WORKLOAD = WORKLOADS["bumpy"]
 
@@ -339,6 +346,8 @@ def describe_sample(cs, iters, conv, src):
     else:
         txt += ("; the Default (per-grid-point ZGEMV) orthonormalisation streams the k x k matrix once per grid "
                 "point and is slower at this size")
+    share = (cs["prop_s"] + cs["energies_s"]) * w["num_states"] / cs["states_sampled"] / cs["sec_per_iter"]
+    txt += f"; propagation + energies (the FFT work) are {100 * share:.0f}% of the iteration"
     if "fft_shim_over_pocketfft" in cs:
         txt += f"; substitute FFT / numpy pocketfft on the same lines = {cs['fft_shim_over_pocketfft']:.2f}"
     return txt + f"; host: {host_description(cs['threads'])}"

