@@ -165,6 +165,11 @@ int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
  * FP64 states are always orthonormalised canonically. No reference
  * counterpart (stateset.cpp:136-232 is the canonical form). */
 int itp2d_set_fp32_orthonormalization(itp2d_ctx* ctx, int canonical_every);
+/* FP32 states: the canonical orthonormalisation's eigensolve stops at a
+ * largest rotation tangent of tau (default 1e-3; off-diagonal elements of
+ * about tau^2 remain). A looser tau suits the first iterations of a solve,
+ * whose basis the next step replaces. FP64 states are not affected. */
+int itp2d_set_fp32_eig_tolerance(itp2d_ctx* ctx, double tau);
 /* Number of canonical and of Lowdin orthonormalisations since creation. */
 int itp2d_orthonormalization_counts(itp2d_ctx* ctx, long long* canonical, long long* lowdin);
 

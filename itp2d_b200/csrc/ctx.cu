@@ -111,6 +111,7 @@ struct itp2d_ctx {
 	std::vector<void*> allocs;
 	// FP32 form: second-order Lowdin steps between canonical ones
 	int canonical_every = 0;     // 0 or 1: always canonical
+	double fp32_tau = 1e-3;      // FP32 eigensolve: largest rotation tangent at which it stops
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
 	long long ortho_calls[2] = {0, 0};  // canonical, Lowdin
 	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
@@ -993,6 +994,13 @@ int itp2d_set_fp32_orthonormalization(itp2d_ctx* c, int canonical_every) {
 	return ITP2D_OK;
 }
 
+int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
+	if (!c || !(tau > 0.0) || tau > 1.0) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->fp32_tau = tau;
+	return ITP2D_OK;
+}
+
 int itp2d_orthonormalization_counts(itp2d_ctx* c, long long* canonical, long long* lowdin) {
 	if (!c) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
@@ -1086,7 +1094,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		// FP32 states: the overlap is accurate to about 1e-5; a final tangent of
 		// 1e-3 leaves off-diagonal elements of about 1e-6, below that (measured
 		// on the magnetic dot: one more FP32 iteration, 3% less solve time)
-		c->jw.tau_final = f64 ? 0.0 : 1e-3;
+		c->jw.tau_final = f64 ? 0.0 : c->fp32_tau;
 		// FP32 states also solve in FP32, on views of the FP64 buffers the block
 		// path leaves free (A1 holds two FP32 matrices, A2 two more)
 		c->jw.f32 = {};

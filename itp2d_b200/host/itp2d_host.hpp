@@ -229,7 +229,6 @@ class ITPSystem {
 	double fp32_best = INFINITY;  // smallest per-step energy change seen in the FP32 form
 	int fp32_stall = 0;           // FP32 steps since that change last decreased
 	bool last_ortho_canonical = true;               // the last orthonormalisation's form
-	std::vector<double> fp32_canonical_energies;    // energies of the last canonical FP32 iteration
 	double eps = 0;
 	std::list<double> eps_values;
 	std::vector<Esn> sorted;

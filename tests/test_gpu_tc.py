@@ -157,7 +157,7 @@ def _near_orthonormal(sx, sy, k, seed, delta, L=10.0):
     rng = np.random.default_rng(seed + 1)
     pert = rng.standard_normal((k, sy, sx)) + 1j * rng.standard_normal((k, sy, sx))
     pert *= delta / (np.sqrt(np.sum(np.abs(pert) ** 2, axis=(1, 2)))[:, None, None] * g.dx)
-    scale = np.exp(-0.1 * np.arange(k))[:, None, None]  # graded norms, like exp(-eps E)
+    scale = np.exp(-6.0 * np.arange(k) / k)[:, None, None]  # graded norms, like exp(-eps E)
     psi = (base + pert) * scale
     c = capi.Context(sx, sy, g.dx, k, precision=capi.FP32)
     c.upload(psi)
