@@ -8,6 +8,8 @@
 #ifndef ITP2D_HOST_H
 #define ITP2D_HOST_H
 
+#include <signal.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -102,6 +104,35 @@ int itp2d_system_download_states(itp2d_system* s, double* states);
  * (dot), [4] eigensolve, [5] lincomb, [6] energies + convergence tests. The
  * device phases [3..5] come from CUDA events. */
 int itp2d_system_times(itp2d_system* s, double* t7);
+
+/* ---- Signals (itp2d.cpp:40-66; itpsystem.cpp:236-241,407-415) ----
+ * The reference's program traps SIGINT and SIGUSR1 into two process-wide
+ * flags that its ITPSystem reads: a raised abort flag ends the solve at the
+ * top of the next step with the error flag set; a raised save flag has the
+ * states saved at the next check point (after propagation, after the
+ * orthonormalisation, after the energies, at the end of a step) and is
+ * lowered again. itp2d_install_signal_handlers installs those handlers over
+ * this library's own pair of flags (a second SIGINT exits with status 1). */
+int itp2d_install_signal_handlers(void);
+volatile sig_atomic_t* itp2d_abort_flag(void);
+volatile sig_atomic_t* itp2d_save_flag(void);
+
+/* The flags this system reads (ITPSystem's abort_flagptr / save_flagptr,
+ * itpsystem.hpp:59-62): any sig_atomic_t the caller owns, or the two above;
+ * NULL disables either (the default). While either is set the device
+ * phases of itp2d_system_run_device run in chunks of at most 32 iterations
+ * and the flags are read between chunks. */
+int itp2d_system_set_flags(itp2d_system* s, volatile sig_atomic_t* abort_flag, volatile sig_atomic_t* save_flag);
+
+/* save_states (itpsystem.cpp:374-389) with the datafile replaced by a
+ * callback: states in storage order (num_states*sy*sx interleaved complex
+ * doubles, valid during the call), order = storage indices by ascending
+ * energy (NULL before the first energies), step = iterations taken. */
+typedef void (*itp2d_save_states_fn)(void* user, const double* states, const int* order, int num_states, int sx,
+		int sy, int step);
+int itp2d_system_set_save_callback(itp2d_system* s, itp2d_save_states_fn fn, void* user);
+/* save_states calls made so far (with or without a callback). */
+int itp2d_system_saves(const itp2d_system* s);
 
 /* Last error message of the driver (exception text), or "". */
 const char* itp2d_system_last_error(const itp2d_system* s);

@@ -9,6 +9,8 @@
 #include <sstream>
 #include <thread>
 
+#include <unistd.h>
+
 namespace itp2d {
 
 namespace {
@@ -28,6 +30,8 @@ std::string num(double v) {
 }
 
 const char* kWhitespace = " \t\n";
+// Largest device-loop chunk while abort or save flags are registered.
+const int kFlagChunk = 32;
 
 }  // namespace
 
@@ -504,9 +508,49 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 void ITPSystem::step() {
 	if (!step_begin()) return;
 	propagate();
+	check_save_flag();
 	orthonormalize();
+	check_save_flag();
 	calculate_energies();
+	check_save_flag();
 	step_end();
+	check_save_flag();
+}
+
+// The abort flag raised by a signal handler ends the solve with the error
+// flag set (itpsystem.cpp:409-415).
+bool ITPSystem::check_abort_flag() {
+	if (abort_flag == nullptr || !*abort_flag) return false;
+	if (!finished) {
+		error_text = "aborted: the abort flag was raised";
+		error_flag = true;
+		finish();
+	}
+	return true;
+}
+
+// itpsystem.cpp:236-241
+void ITPSystem::check_save_flag() {
+	if (save_flag != nullptr && *save_flag) {
+		save_states();
+		*save_flag = 0;
+	}
+}
+
+// ITPSystem::save_states(sort = true) (itpsystem.cpp:374-389): the states in
+// storage order with the storage indices in ascending energy (nullptr before
+// the first energies), handed to the save callback.
+void ITPSystem::save_states() {
+	saves++;
+	if (save_fn == nullptr) return;
+	const size_t k = (size_t)p.num_states, n = (size_t)p.sx * p.sy;
+	std::vector<double> host(2 * k * n);
+	download_states(host.data());
+	std::vector<int> order;
+	if (sorted.size() == k)
+		for (size_t i = 0; i < k; i++) order.push_back((int)sorted[i].second);
+	save_fn(save_user, host.data(), order.empty() ? nullptr : order.data(), p.num_states, p.sx, p.sy,
+			total_step_counter);
 }
 
 // Iterations on the device until the time-step test holds
@@ -515,7 +559,8 @@ void ITPSystem::step() {
 // FP64 sweeps, a time-step test of the four single-limit kinds and without
 // eps exhaustion (which changes eps every step); otherwise one step().
 void ITPSystem::run_device_phase() {
-	if (finished) return;
+	if (finished || check_abort_flag()) return;
+	check_save_flag();
 	const auto spec = parse_parameter_string(p.timestep_test);
 	static const char* names[] = {"abschange", "relchange", "absstdev", "relstdev"};
 	int test = -1;
@@ -523,12 +568,15 @@ void ITPSystem::run_device_phase() {
 		if (spec.first == names[i]) test = i;
 	const size_t npar = spec.second.size();
 	const bool ok_params = (test < 2 && npar == 1) || (test >= 2 && (npar == 1 || npar == 2));
-	const int remaining = p.max_steps - total_step_counter;
+	int remaining = p.max_steps - total_step_counter;
 	if (precision != ITP2D_FP64 || test < 0 || !ok_params || exhausting || remaining < 1) {
 		step();
 		return;
 	}
 	const double limit = spec.second[0], diff = npar == 2 ? spec.second[1] : 0.0;
+	// The device loop sees no host flag: with flags registered it runs in
+	// chunks of at most kFlagChunk iterations and the flags are read between.
+	if ((abort_flag != nullptr || save_flag != nullptr) && remaining > kFlagChunk) remaining = kFlagChunk;
 	const size_t k = (size_t)p.num_states;
 	std::vector<int> flags(k);
 	for (size_t i = 0; i < k; i++) flags[i] = timestep_converged[i] ? 1 : 0;
@@ -580,7 +628,7 @@ void ITPSystem::run_device_phase() {
 }
 
 bool ITPSystem::step_begin() {
-	if (finished) return false;
+	if (finished || check_abort_flag()) return false;
 	if (total_step_counter == 0) t_start = now_s();
 	if (total_step_counter >= p.max_steps) {
 		error_text = "maximum number of total steps reached";
@@ -845,6 +893,59 @@ int itp2d_system_times(itp2d_system* s, double* t7) {
 	}
 	return ITP2D_OK;
 }
+
+// Process-wide flags and the handlers that raise them, as the reference's
+// program installs them (itp2d.cpp:40-66): the first SIGINT raises the abort
+// flag, a second one ends the process at once with status 1; SIGUSR1 raises
+// the save flag. Only async-signal-safe calls (write, _exit) in the handlers.
+static volatile sig_atomic_t g_abort_flag = 0;
+static volatile sig_atomic_t g_save_flag = 0;
+
+static void on_sigint(int) {
+	static const char note[] =
+			"\nSIGINT: the solve ends at its next step (states saved first if a save callback is set); "
+			"a second SIGINT exits at once.\n";
+	if (g_abort_flag) _exit(1);
+	if (write(STDERR_FILENO, note, sizeof(note) - 1) < 0) {
+	}
+	g_abort_flag = 1;
+}
+
+static void on_sigusr1(int) {
+	static const char note[] = "\nSIGUSR1: the states are saved at the next check point; the solve continues.\n";
+	if (write(STDERR_FILENO, note, sizeof(note) - 1) < 0) {
+	}
+	g_save_flag = 1;
+}
+
+volatile sig_atomic_t* itp2d_abort_flag(void) { return &g_abort_flag; }
+volatile sig_atomic_t* itp2d_save_flag(void) { return &g_save_flag; }
+
+int itp2d_install_signal_handlers(void) {
+	struct sigaction a;
+	std::memset(&a, 0, sizeof(a));
+	sigemptyset(&a.sa_mask);
+	a.sa_flags = SA_RESTART;
+	a.sa_handler = on_sigint;
+	if (sigaction(SIGINT, &a, nullptr) != 0) return ITP2D_E_INVALID;
+	a.sa_handler = on_sigusr1;
+	if (sigaction(SIGUSR1, &a, nullptr) != 0) return ITP2D_E_INVALID;
+	return ITP2D_OK;
+}
+
+int itp2d_system_set_flags(itp2d_system* s, volatile sig_atomic_t* abort_flag, volatile sig_atomic_t* save_flag) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	s->sys->set_flags(abort_flag, save_flag);
+	return ITP2D_OK;
+}
+
+int itp2d_system_set_save_callback(itp2d_system* s, itp2d_save_states_fn fn, void* user) {
+	if (!s || !s->sys) return ITP2D_E_INVALID;
+	s->sys->set_save_callback(fn, user);
+	return ITP2D_OK;
+}
+
+int itp2d_system_saves(const itp2d_system* s) { return s && s->sys ? s->sys->saves : -1; }
 
 const char* itp2d_system_last_error(const itp2d_system* s) {
 	if (!s) return "";

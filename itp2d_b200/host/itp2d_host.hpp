@@ -5,6 +5,7 @@
 // exactly as in itpsystem.cpp:202-511 and convergence.cpp:28-199.
 #pragma once
 
+#include <csignal>
 #include <cmath>
 #include <list>
 #include <memory>
@@ -199,6 +200,18 @@ class ITPSystem {
 	itp2d_ctx* context() { return ctx; }
 	void download_states(double* out);
 	void times(double* t7);
+	// The flags a signal handler raises (ITPSystem's abort_flagptr and
+	// save_flagptr, itpsystem.hpp:59-62); nullptr disables each.
+	void set_flags(volatile sig_atomic_t* abort, volatile sig_atomic_t* save) {
+		abort_flag = abort;
+		save_flag = save;
+	}
+	// Where save_states writes (the reference's datafile, itpsystem.cpp:374-389).
+	void set_save_callback(itp2d_save_states_fn fn, void* user) {
+		save_fn = fn;
+		save_user = user;
+	}
+	int saves = 0;  // save_states calls made
 	const itp2d_parameters p;
 
   private:
@@ -214,8 +227,15 @@ class ITPSystem {
 	void maybe_switch_precision();
 	void fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit);
 	void check(int status, const char* where);
+	bool check_abort_flag();
+	void check_save_flag();
+	void save_states();
 
 	DataLayout dl;
+	volatile sig_atomic_t* abort_flag = nullptr;
+	volatile sig_atomic_t* save_flag = nullptr;
+	itp2d_save_states_fn save_fn = nullptr;
+	void* save_user = nullptr;
 	std::unique_ptr<ConvergenceTest> ts_test, final_test;
 	std::vector<double> V;
 	bool null_potential = true;

@@ -56,8 +56,39 @@ def _lib():
         L.itp2d_system_last_error.restype = C.c_char_p
         L.itp2d_system_context.argtypes = [vp]
         L.itp2d_system_context.restype = vp
+        L.itp2d_install_signal_handlers.argtypes = []
+        L.itp2d_abort_flag.restype = ip
+        L.itp2d_save_flag.restype = ip
+        L.itp2d_system_set_flags.argtypes = [vp, ip, ip]
+        L.itp2d_system_set_save_callback.argtypes = [vp, _SaveFn, vp]
+        L.itp2d_system_saves.argtypes = [vp]
         _bound = True
     return L
+
+
+# void (*)(void* user, const double* states, const int* order, int k, int sx, int sy, int step);
+# sig_atomic_t is an int on the platforms this library builds for
+_SaveFn = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int,
+                      C.c_int)
+
+
+def install_signal_handlers() -> None:
+    """SIGINT raises the library's abort flag (a second SIGINT exits with
+    status 1), SIGUSR1 its save flag, as the reference's program does
+    (itp2d.cpp:40-66). Replaces Python's own SIGINT handler."""
+    st = _lib().itp2d_install_signal_handlers()
+    if st != capi.OK:
+        raise capi.ITP2DError(st, "itp2d_install_signal_handlers")
+
+
+def abort_flag():
+    """The library's process-wide abort flag (a ctypes int pointer)."""
+    return _lib().itp2d_abort_flag()
+
+
+def save_flag():
+    """The library's process-wide save flag (a ctypes int pointer)."""
+    return _lib().itp2d_save_flag()
 
 
 @dataclass
@@ -231,6 +262,38 @@ class ITPSystem:
 
     def context_handle(self) -> int:
         return _lib().itp2d_system_context(self.h)
+
+    def set_flags(self, abort=None, save=None):
+        """The abort and save flags this system reads (itpsystem.hpp:59-62):
+        ctypes int objects or pointers (abort_flag() / save_flag()), or None."""
+        def ptr(f):
+            if f is None:
+                return None
+            return f if isinstance(f, C.POINTER(C.c_int)) else C.pointer(f)
+        self._flags = (abort, save)  # keeps caller-owned ints alive
+        st = _lib().itp2d_system_set_flags(self.h, ptr(abort), ptr(save))
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_set_flags")
+
+    def set_save_callback(self, fn):
+        """fn(states (k, sy, sx) complex128 copy in storage order, order (storage
+        indices by ascending energy, or None), step) runs where the reference's
+        save_states writes its datafile (itpsystem.cpp:374-389)."""
+        if fn is None:
+            self._save_cb = _SaveFn()
+        else:
+            def cb(_user, states, order, k, sx, sy, step):
+                a = np.ctypeslib.as_array(states, shape=(k * sy * sx * 2,)).view(np.complex128)
+                o = np.ctypeslib.as_array(order, shape=(k,)).copy() if order else None
+                fn(a.reshape(k, sy, sx).copy(), o, step)
+            self._save_cb = _SaveFn(cb)
+        st = _lib().itp2d_system_set_save_callback(self.h, self._save_cb, None)
+        if st != capi.OK:
+            raise capi.ITP2DError(st, "itp2d_system_set_save_callback")
+
+    @property
+    def saves(self) -> int:
+        return _lib().itp2d_system_saves(self.h)
 
 
 class _RequestInfo(C.Structure):
