@@ -790,7 +790,7 @@ def main():
     roof = phase_rooflines(rh, fp64_peak, fp32_peak)
     dom = max(roof, key=lambda n: roof[n]["ms_per_solve"])
     roofline = {key: roof[dom][key] for key in ("bound", "achieved", "peak", "unit", "frac")}
-    roofline.update({"traffic": PROFILED_TRAFFIC[args.workload].get(dom), "kernel": dom,
+    roofline.update({"traffic": PROFILED_TRAFFIC.get(args.workload, {}).get(dom), "kernel": dom,
                      "peak_source": roof[dom]["peak_source"]})
 
     cpu = None

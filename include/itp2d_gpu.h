@@ -46,9 +46,13 @@ enum { ITP2D_PERIODIC = 0, ITP2D_DIRICHLET = 1 };
 enum { ITP2D_FP64 = 0, ITP2D_FP32 = 1 };
 
 /* Orthonormalisation algorithm, enum OrthoAlgorithm of itp2d_common.hpp:53.
- * Both select the same out-of-place device path; the argument is accepted
- * for interface compatibility. */
-enum { ITP2D_ORTHO_DEFAULT = 0, ITP2D_ORTHO_HIGHMEM = 1 };
+ * DEFAULT and HIGHMEM select the same out-of-place canonical device path; the
+ * argument is accepted for interface compatibility. CHOLESKY (no reference
+ * counterpart) orthonormalises in Gram-Schmidt order instead: S = L L^H,
+ * psi'_n = sum_{i <= n} conj((L^{-1})_{n,i}) psi_i; the state order is kept and
+ * a non-positive pivot of L is reported as ITP2D_E_NONPOSITIVE_EIGENVALUE with
+ * the pivot's index and value. */
+enum { ITP2D_ORTHO_DEFAULT = 0, ITP2D_ORTHO_HIGHMEM = 1, ITP2D_ORTHO_CHOLESKY = 2 };
 
 /* Transform kinds in the order of enum Transform (transformer.hpp:32-34). */
 enum {
@@ -165,13 +169,21 @@ int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
  * FP64 states are always orthonormalised canonically. No reference
  * counterpart (stateset.cpp:136-232 is the canonical form). */
 int itp2d_set_fp32_orthonormalization(itp2d_ctx* ctx, int canonical_every);
+/* The orthonormalisation between the canonical calls of
+ * itp2d_set_fp32_orthonormalization: ITP2D_BETWEEN_LOWDIN (the default, taken
+ * only while the overlap is close to the identity) or ITP2D_BETWEEN_CHOLESKY
+ * (Gram-Schmidt order, ITP2D_ORTHO_CHOLESKY; taken whenever the overlap's
+ * Cholesky factorisation succeeds, canonical otherwise). */
+enum { ITP2D_BETWEEN_LOWDIN = 0, ITP2D_BETWEEN_CHOLESKY = 1 };
+int itp2d_set_fp32_between(itp2d_ctx* ctx, int method);
 /* FP32 states: the canonical orthonormalisation's eigensolve stops at a
  * largest rotation tangent of tau (default 1e-3; off-diagonal elements of
  * about tau^2 remain). A looser tau suits the first iterations of a solve,
  * whose basis the next step replaces. FP64 states are not affected. */
 int itp2d_set_fp32_eig_tolerance(itp2d_ctx* ctx, double tau);
-/* Number of canonical and of Lowdin orthonormalisations since creation. */
-int itp2d_orthonormalization_counts(itp2d_ctx* ctx, long long* canonical, long long* lowdin);
+/* Number of canonical, Lowdin and Cholesky orthonormalisations since
+ * creation; any pointer may be NULL. */
+int itp2d_orthonormalization_counts(itp2d_ctx* ctx, long long* canonical, long long* lowdin, long long* cholesky);
 
 /* Overlap matrix of the resident states, S_ij = <psi_i|psi_j> dx^2
  * (row-major, num_states^2 interleaved complex doubles), computed by the

@@ -43,8 +43,10 @@ typedef struct {
 	char timestep_test[128];
 	char final_test[128];
 	int fp32_canonical_every; /* FP32 form: canonical orthonormalisation on every n-th
-	                             step, second-order Lowdin steps in between
+	                             step, fp32_between steps in between
 	                             (itp2d_set_fp32_orthonormalization); 0: always canonical */
+	int fp32_between;         /* ITP2D_BETWEEN_LOWDIN (0) or ITP2D_BETWEEN_CHOLESKY
+	                             (itp2d_set_fp32_between) */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

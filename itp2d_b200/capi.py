@@ -23,7 +23,8 @@ E_NONPOSITIVE_EIGENVALUE, E_NONNORMAL_EIGENVALUE, E_EIGENSOLVER = 4, 5, 6
 E_TIMEOUT, E_UNSUPPORTED = 7, 8
 PERIODIC, DIRICHLET = 0, 1
 FP64, FP32 = 0, 1
-ORTHO_DEFAULT, ORTHO_HIGHMEM = 0, 1
+ORTHO_DEFAULT, ORTHO_HIGHMEM, ORTHO_CHOLESKY = 0, 1, 2
+BETWEEN_LOWDIN, BETWEEN_CHOLESKY = 0, 1
 CONTRACT_AUTO, CONTRACT_FP64 = 0, 1
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
@@ -68,7 +69,8 @@ def lib():
         L.itp2d_set_contraction.argtypes = [vp, i]
         L.itp2d_set_precision.argtypes = [vp, i]
         L.itp2d_set_fp32_orthonormalization.argtypes = [vp, i]
-        L.itp2d_orthonormalization_counts.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.itp2d_orthonormalization_counts.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 3
+        L.itp2d_set_fp32_between.argtypes = [vp, i]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
@@ -217,12 +219,16 @@ class Context:
         _check(lib().itp2d_set_fp32_orthonormalization(self.h, int(canonical_every)),
                "itp2d_set_fp32_orthonormalization")
 
+    def set_fp32_between(self, method):
+        """BETWEEN_LOWDIN or BETWEEN_CHOLESKY between the canonical calls."""
+        _check(lib().itp2d_set_fp32_between(self.h, int(method)), "itp2d_set_fp32_between")
+
     def orthonormalization_counts(self):
-        """(canonical, Lowdin) orthonormalisations since creation."""
-        a, b = C.c_longlong(0), C.c_longlong(0)
-        _check(lib().itp2d_orthonormalization_counts(self.h, C.byref(a), C.byref(b)),
+        """(canonical, Lowdin, Cholesky) orthonormalisations since creation."""
+        a, b, c = C.c_longlong(0), C.c_longlong(0), C.c_longlong(0)
+        _check(lib().itp2d_orthonormalization_counts(self.h, C.byref(a), C.byref(b), C.byref(c)),
                "itp2d_orthonormalization_counts")
-        return a.value, b.value
+        return a.value, b.value, c.value
 
     def set_precision(self, precision):
         _check(lib().itp2d_set_precision(self.h, precision), "itp2d_set_precision")

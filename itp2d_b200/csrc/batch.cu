@@ -26,6 +26,11 @@ namespace {
 
 constexpr int kBThreads = 512;
 constexpr int kMaxPairs = 2048;  // k_p / 2 for k up to 4096
+// A pair is not rotated when |A_pq| <= kSkipBelow sqrt(|A_pp A_qq|): such an
+// element is at the rounding level of the diagonal. A lower threshold never
+// ends for (numerically) degenerate diagonal pairs, whose rotation is a
+// 45-degree one that leaves an off-diagonal element of the same rounding size.
+constexpr double kSkipBelow = 1e-15;
 
 __device__ __forceinline__ int rr_player(int pos, int r, int npos) {
 	return pos == 0 ? 0 : ((pos - 1 + r) % (npos - 1)) + 1;
@@ -83,7 +88,7 @@ __global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEi
 						const double a = A[(size_t)p * kp + p].x, b = A[(size_t)q * kp + q].x;
 						const double2 cpq = A[(size_t)p * kp + q];
 						const double g = hypot(cpq.x, cpq.y);
-						if (g > 1e-300 && g > 1e-18 * sqrt(fabs(a) * fabs(b))) {
+						if (g > 1e-300 && g > kSkipBelow * sqrt(fabs(a) * fabs(b))) {
 							// real problem [[a, g], [g, b]]: t = sign(z) / (|z| + sqrt(1 + z^2)), z = (b - a) / 2g
 							const double z = 0.5 * (b - a) / g;
 							const double t = (z >= 0 ? 1.0 : -1.0) / (fabs(z) + sqrt(1.0 + z * z));

@@ -109,6 +109,13 @@ void launch_lowdin_w(const double* D, const double2* E, const double2* Ec, doubl
 constexpr double kLowdinMaxElement = 0.05;
 constexpr double kLowdinMaxFrobenius = 0.25;
 
+// Cholesky orthonormalisation (cholesky.cu): W = L^{-H} with S = L L^H, in
+// k x k buffers A (factor, overwritten) and X (inverse), Linv 32 x 32; st
+// receives ITP2D_E_NONPOSITIVE_EIGENVALUE and the pivot on failure.
+int launch_cholesky_w(const double2* S, int k, double2* A, double2* X, double2* Linv, double2* W, EigStatus* st,
+		cudaStream_t s);
+int cholesky_launches(int k);
+
 // One instance of the batched eigensolver (batch.cu): the k x k overlap S
 // (row-major), work matrices A and V ((k + 1) & ~1 squared), the result
 // W = U Lambda^{-1/2} (rotation layout), ascending eigenvalues and their

@@ -109,11 +109,12 @@ struct itp2d_ctx {
 	long long phase_calls_p[10] = {};
 	std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 	std::vector<void*> allocs;
-	// FP32 form: second-order Lowdin steps between canonical ones
+	// FP32 form: Lowdin or Cholesky steps between canonical ones
 	int canonical_every = 0;     // 0 or 1: always canonical
+	int between = ITP2D_BETWEEN_LOWDIN;
 	double fp32_tau = 1e-3;      // FP32 eigensolve: largest rotation tangent at which it stops
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
-	long long ortho_calls[2] = {0, 0};  // canonical, Lowdin
+	long long ortho_calls[3] = {0, 0, 0};  // canonical, Lowdin, Cholesky
 	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
 	double* hlstat = nullptr;    // pinned copy
 	void* loop_buf = nullptr;    // device driver loop state (itp2d_run_device_loop)
@@ -1001,11 +1002,19 @@ int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
 	return ITP2D_OK;
 }
 
-int itp2d_orthonormalization_counts(itp2d_ctx* c, long long* canonical, long long* lowdin) {
+int itp2d_set_fp32_between(itp2d_ctx* c, int method) {
+	if (!c || (method != ITP2D_BETWEEN_LOWDIN && method != ITP2D_BETWEEN_CHOLESKY)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->between = method;
+	return ITP2D_OK;
+}
+
+int itp2d_orthonormalization_counts(itp2d_ctx* c, long long* canonical, long long* lowdin, long long* cholesky) {
 	if (!c) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
 	if (canonical) *canonical = c->ortho_calls[0];
 	if (lowdin) *lowdin = c->ortho_calls[1];
+	if (cholesky) *cholesky = c->ortho_calls[2];
 	return ITP2D_OK;
 }
 
@@ -1026,8 +1035,55 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 	return ITP2D_OK;
 }
 
+// psi <- psi W by the rotation engine of the precision (into acc, swapped on
+// success); the tensor-core rotation's status when it fails.
+static int rotate_states(itp2d_ctx* c, bool tc) {
+	const bool f64 = c->precision == ITP2D_FP64;
+	{
+		PhaseTimer t(c, kRotate);
+		if (tc)
+			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream);
+		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
+		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
+		c->launches += tc ? 2 : 1;
+	}
+	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaGetLastError());
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	if (tc && *c->hflag != ITP2D_OK) {
+		const int f = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+		return f;
+	}
+	void* sw = c->psi;
+	c->psi = c->acc;
+	c->acc = sw;
+	return ITP2D_OK;
+}
+
+// W = L^{-H} from the overlap in c->S (cholesky.cu). ITP2D_OK, or the
+// failing pivot in *bad_index / *bad_value with the states unchanged.
+static int cholesky_w(itp2d_ctx* c, int* bad_index, double* bad_value) {
+	{
+		PhaseTimer t(c, kEigen);
+		const int st = launch_cholesky_w(c->S, c->k, c->jw.A0, c->jw.A1, c->jw.V, c->W, c->dstat, c->stream);
+		if (st != ITP2D_OK) return st;
+		c->launches += cholesky_launches(c->k);
+	}
+	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	const EigStatus s = *c->hstat;
+	c->last_sweeps = 0;
+	if (s.status != ITP2D_OK) {
+		if (bad_index) *bad_index = s.bad_index;
+		if (bad_value) *bad_value = s.bad_value;
+	}
+	return s.status;
+}
+
 int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_value) {
-	if (!c || (algo != ITP2D_ORTHO_DEFAULT && algo != ITP2D_ORTHO_HIGHMEM)) return ITP2D_E_INVALID;
+	if (!c || (algo != ITP2D_ORTHO_DEFAULT && algo != ITP2D_ORTHO_HIGHMEM && algo != ITP2D_ORTHO_CHOLESKY))
+		return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
 	if (bad_index) *bad_index = -1;
 	if (bad_value) *bad_value = 0.0;
@@ -1045,10 +1101,24 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		PhaseTimer t(c, kOverlap);
 		launch_overlap_any(c, tc);
 	}
+	if (algo == ITP2D_ORTHO_CHOLESKY) {
+		const int st = cholesky_w(c, bad_index, bad_value);
+		if (st != ITP2D_OK) return st;
+		c->ortho_calls[2]++;
+		return rotate_states(c, tc);
+	}
+	const bool between = !f64 && c->canonical_every > 1 && c->since_canonical + 1 < c->canonical_every;
+	// FP32 form between canonical steps, Gram-Schmidt order: taken whenever
+	// the factorisation succeeds (canonical below otherwise)
+	if (between && c->between == ITP2D_BETWEEN_CHOLESKY && cholesky_w(c, nullptr, nullptr) == ITP2D_OK) {
+		c->since_canonical++;
+		c->ortho_calls[2]++;
+		return rotate_states(c, tc);
+	}
 	// FP32 form between canonical steps: W = D (I + E)^{-1/2} to second order
 	// when the normalised overlap is close enough to the identity
 	bool lowdin = false;
-	if (!f64 && c->canonical_every > 1 && c->since_canonical + 1 < c->canonical_every) {
+	if (between && c->between == ITP2D_BETWEEN_LOWDIN) {
 		PhaseTimer t(c, kEigen);
 		launch_lowdin_prep(c->S, c->k, c->jw.evals, c->jw.A0, c->jw.A1, c->lstat, c->stream);
 		ITP2D_TRY(cudaGetLastError());
@@ -1066,26 +1136,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		c->since_canonical++;
 		c->ortho_calls[1]++;
 		c->last_sweeps = 0;
-		{
-			PhaseTimer t(c, kRotate);
-			if (tc)
-				launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
-						c->stream);
-			else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
-			c->launches += tc ? 2 : 1;
-		}
-		if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-		ITP2D_TRY(cudaGetLastError());
-		ITP2D_TRY(cudaStreamSynchronize(c->stream));
-		if (tc && *c->hflag != ITP2D_OK) {
-			const int f = *c->hflag;
-			ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
-			return f;
-		}
-		void* sw = c->psi;
-		c->psi = c->acc;
-		c->acc = sw;
-		return ITP2D_OK;
+		return rotate_states(c, tc);
 	}
 	c->since_canonical = 0;
 	c->ortho_calls[0]++;

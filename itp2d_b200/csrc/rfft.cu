@@ -224,7 +224,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Column pass, in place: tiles of W = 256 / B columns x N rows of one state
-// staged in shared memory ([y][c], row stride W + 1); each column line is
+// staged in shared memory ([y][c], row stride W + 1); tile tl covers columns
+// (tl mod nct) W .. of state tl / nct, so the CTAs running at one time read
+// the neighbouring column strips of the same rows (whole DRAM rows rather
+// than one W-column strip of many states); each column line is
 // transformed by B threads of one warp, using the line's own column of the
 // tile as its exchange area. Persistent; with NBUF = 2 the next tile is copied
 // in by cp.async while the current one is transformed (NBUF = 1 where two
@@ -253,8 +256,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : (s
 	T* data = reinterpret_cast<T*>(a.data);
 	// copies tile tl into dst (asynchronously when NBUF = 2); columns beyond sx read as zero
 	auto fetch = [&](T* dst, long long tl) {
-		const long long state = tl % k;
-		const int col0 = (int)(tl / k) * W;
+		const long long state = tl / nct;
+		const int col0 = (int)(tl % nct) * W;
 		const int ncols = min(W, sx - col0);
 		const T* src = data + state * a.G + col0;
 #pragma unroll
@@ -284,8 +287,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : (s
 			fetch(tile, tl);
 			__syncthreads();
 		}
-		const long long state = tl % k;
-		const int col0 = (int)(tl / k) * W;
+		const long long state = tl / nct;
+		const int col0 = (int)(tl % nct) * W;
 		const int ncols = min(W, sx - col0);
 		T v[A];
 #pragma unroll
@@ -425,8 +428,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : 0)
 	const T* psi_all = reinterpret_cast<const T*>(a.psi);
 	const T* src_all = a.src ? reinterpret_cast<const T*>(a.src) : psi_all;
 	auto fetch = [&](T* dst, long long tl) {
-		const long long state = tl % k;
-		const int col0 = (int)(tl / k) * W;
+		const long long state = tl / nct;
+		const int col0 = (int)(tl % nct) * W;
 		const int ncols = min(W, sx - col0);
 		const T* src = src_all + state * a.G + col0;
 #pragma unroll
@@ -457,8 +460,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : 0)
 			fetch(tile, tl);
 			__syncthreads();
 		}
-		const long long state = tl % k;
-		const int ct = (int)(tl / k);
+		const long long state = tl / nct;
+		const int ct = (int)(tl % nct);
 		const int col0 = ct * W;
 		const int ncols = min(W, sx - col0);
 		const long long base = state * a.G + col0;

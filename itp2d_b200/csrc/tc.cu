@@ -56,7 +56,8 @@ constexpr int kPlaneBytes = TM * KT * 2;               // 4 KB: one BF16 plane o
 constexpr int kOperandBytes = 6 * kPlaneBytes;         // 24 KB: re/im x hi/mid/lo
 constexpr int kRawRowBytes = KT * 8;                   // 128 B: 16 complex FP32
 constexpr int kTmemCols = 512;
-constexpr long long kSpinLimit = 1LL << 24;            // ~1 s with the back-off below
+constexpr long long kSpinLimit = 1LL << 24;            // back-stop on the number of polls
+constexpr unsigned long long kWaitNs = 1000000000ULL;  // a wait gives up after 1 s
 
 // Shared memory map (bytes from the 1024-aligned base).
 //   overlap:  planes[2] x (A, B) 96 KB | raw[3] x (A, B) 96 KB
@@ -110,8 +111,16 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
 	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
-// Bounded wait for the phase with the given parity. Returns false on time-out.
+__device__ __forceinline__ unsigned long long global_ns() {
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Bounded wait for the phase with the given parity: false once kWaitNs of
+// wall time (or kSpinLimit polls) passed without the phase completing.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+	const unsigned long long t0 = global_ns();
 	for (long long i = 0; i < kSpinLimit; i++) {
 		uint32_t done;
 		asm volatile(
@@ -122,7 +131,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
 				: "r"(mbar), "r"(parity)
 				: "memory");
 		if (done) return true;
-		if (i > 64) __nanosleep(64);
+		if (i > 64) {
+			__nanosleep(64);
+			if ((i & 255) == 0 && global_ns() - t0 > kWaitNs) return false;
+		}
 	}
 	return false;
 }

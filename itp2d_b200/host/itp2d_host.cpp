@@ -32,6 +32,9 @@ std::string num(double v) {
 const char* kWhitespace = " \t\n";
 // Largest device-loop chunk while abort or save flags are registered.
 const int kFlagChunk = 32;
+// FP32 noise floor of the per-step energy change, in single-precision
+// roundings of the largest wanted energy.
+const double kFp32FloorUlps = 64.0;
 
 }  // namespace
 
@@ -259,6 +262,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 			"itp2d_ctx_create");
 	check(itp2d_set_timing(ctx, 1), "itp2d_set_timing");
 	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
+	check(itp2d_set_fp32_between(ctx, p.fp32_between), "itp2d_set_fp32_between");
 	check(itp2d_set_potential(ctx, null_potential ? nullptr : V.data()), "itp2d_set_potential");
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	initial_states = params.initial_states;
@@ -335,21 +339,20 @@ void ITPSystem::orthonormalize() {
 	int bi = -1;
 	double bv = 0;
 	long long c0 = 0, c1 = 0;
+	const bool cholesky_between = p.fp32_canonical_every > 1 && p.fp32_between == ITP2D_BETWEEN_CHOLESKY;
 	if (precision == ITP2D_FP32) {
-		bool early = energies.size() < 2;
-		if (!early) {
-			const auto& a = energies[energies.size() - 1];
-			const auto& b = energies[energies.size() - 2];
-			double worst = 0.0;
-			for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++)
-				worst = std::max(worst, std::fabs(a[n] - b[n]));
-			early = !(worst < 1e-2);
-		}
+		bool early;
+		if (cholesky_between)
+			early = canonical_prev.empty() ||
+					!(wanted_change(canonical_last, canonical_prev, canonical_step_last - canonical_step_prev) < 1e-2);
+		else
+			early = energies.size() < 2 ||
+					!(wanted_change(energies[energies.size() - 1], energies[energies.size() - 2], 1) < 1e-2);
 		check(itp2d_set_fp32_eig_tolerance(ctx, early ? 0.05 : 1e-3), "itp2d_set_fp32_eig_tolerance");
 	}
-	itp2d_orthonormalization_counts(ctx, &c0, nullptr);
+	itp2d_orthonormalization_counts(ctx, &c0, nullptr, nullptr);
 	const int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
-	itp2d_orthonormalization_counts(ctx, &c1, nullptr);
+	itp2d_orthonormalization_counts(ctx, &c1, nullptr, nullptr);
 	last_ortho_canonical = c1 > c0;
 	t_ortho += now_s() - t0;
 	orthonormalized(st, bi, bv);
@@ -408,6 +411,12 @@ void ITPSystem::store_energies(const double* E, const double* s, const double* r
 		nd[n] = sorted[n].first.second;
 		residuals[n] = r[sorted[n].second];
 	}
+	if (precision == ITP2D_FP32 && last_ortho_canonical) {
+		canonical_prev.swap(canonical_last);
+		canonical_last = ne;
+		canonical_step_prev = canonical_step_last;
+		canonical_step_last = total_step_counter;
+	}
 	t_conv += now_s() - t0;
 }
 
@@ -465,8 +474,11 @@ void ITPSystem::change_time_step() {
 // threshold per step (the FP32 sweep floor), continue in FP64, which refines
 // the eigenpairs to the FP64 fixed point.
 // The FP32 form switches to FP64 once every wanted energy changes by less than
-// fp32_switch per step, or once the largest change has not decreased for
-// kFp32Stall steps (the FP32 noise floor lies above fp32_switch).
+// fp32_switch per step, once the largest change is within kFp32FloorUlps
+// single-precision roundings of the largest wanted energy and has not halved
+// since the previous comparison (it converges by about a factor of ten per
+// step until it meets the FP32 noise floor), or once it has not decreased for
+// a few comparisons (the FP32 noise floor lies above fp32_switch).
 // With Lowdin steps between canonical ones (fp32_canonical_every > 1) the
 // rule skips the Lowdin iterations (a Lowdin step does not rotate within the
 // subspace, so its per-state energy changes understate the subspace's
@@ -476,20 +488,47 @@ void ITPSystem::change_time_step() {
 // The eigensolve tolerance of the FP32 canonical steps is loose (largest
 // rotation tangent 0.05) while the energies still move by more than 1e-2 per
 // step: the basis those steps produce is replaced on the next step anyway.
+//
+// With Cholesky steps between canonical ones the per-state energies of a
+// Cholesky step are those of a Gram-Schmidt basis of the subspace, not of its
+// Ritz-like canonical basis, so the rule compares each canonical iteration
+// with the previous canonical one (the change divided by the iterations
+// between them).
 void ITPSystem::maybe_switch_precision() {
 	if (precision != ITP2D_FP32 || !(p.fp32_switch > 0) || energies.size() < 2) return;
-	const bool lowdin = p.fp32_canonical_every > 1;
-	if (lowdin && !last_ortho_canonical) return;
-	fp32_compare_with(energies[energies.size() - 1], energies[energies.size() - 2], lowdin ? 2 : 3);
+	const bool between = p.fp32_canonical_every > 1;
+	if (between && !last_ortho_canonical) return;
+	if (between && p.fp32_between == ITP2D_BETWEEN_CHOLESKY) {
+		if (canonical_prev.empty()) return;
+		fp32_compare_with(canonical_last, canonical_prev, 2, canonical_step_last - canonical_step_prev);
+		return;
+	}
+	fp32_compare_with(energies[energies.size() - 1], energies[energies.size() - 2], between ? 2 : 3, 1);
 }
 
-void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit) {
+// Largest change per iteration of the wanted sorted energies between a and b,
+// taken `steps` iterations apart (infinite if any is NaN).
+double ITPSystem::wanted_change(const std::vector<double>& a, const std::vector<double>& b, int steps) const {
 	double worst = 0.0;
 	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) {
 		const double d = std::fabs(a[n] - b[n]);
 		worst = (d >= 0.0) ? std::max(worst, d) : INFINITY;  // NaN never counts as converged
 	}
-	if (!(worst < p.fp32_switch)) {
+	return worst / std::max(steps, 1);
+}
+
+void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit,
+		int steps) {
+	const double worst = wanted_change(a, b, steps);
+	const double prev = fp32_last;
+	fp32_last = worst;
+	// near the FP32 noise floor (kFp32FloorUlps single-precision roundings of
+	// the largest wanted energy) a change that no longer halves per step means
+	// the FP32 phase has reached that floor
+	double emax = 0.0;
+	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) emax = std::max(emax, std::fabs(a[n]));
+	const bool at_floor = worst < kFp32FloorUlps * 0x1p-24 * emax && worst > 0.5 * prev;
+	if (!(worst < p.fp32_switch) && !at_floor) {
 		if (worst < fp32_best) {
 			fp32_best = worst;
 			fp32_stall = 0;
@@ -677,7 +716,11 @@ void ITPSystem::reset(const double* init) {
 	exhausting = p.exhaust_eps != 0;
 	total_step_counter = step_counter = 0;
 	fp32_best = INFINITY;
+	fp32_last = INFINITY;
 	fp32_stall = 0;
+	canonical_last.clear();
+	canonical_prev.clear();
+	canonical_step_last = canonical_step_prev = 0;
 	t_total = t_prop = t_ortho = t_conv = 0;
 	energies.clear();
 	deviations.clear();
@@ -753,6 +796,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->precision = ITP2D_FP64;
 	p->fp32_switch = 0.0;
 	p->fp32_canonical_every = 0;
+	p->fp32_between = ITP2D_BETWEEN_LOWDIN;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
 	std::strcpy(p->final_test, "relstdev(1e-3,0)");

@@ -225,7 +225,8 @@ class ITPSystem {
 	void change_time_step();
 	void init_states();
 	void maybe_switch_precision();
-	void fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit);
+	void fp32_compare_with(const std::vector<double>& a, const std::vector<double>& b, int stall_limit, int steps);
+	double wanted_change(const std::vector<double>& a, const std::vector<double>& b, int steps) const;
 	void check(int status, const char* where);
 	bool check_abort_flag();
 	void check_save_flag();
@@ -248,7 +249,11 @@ class ITPSystem {
 	int total_step_counter = 0, step_counter = 0;
 	double fp32_best = INFINITY;  // smallest per-step energy change seen in the FP32 form
 	int fp32_stall = 0;           // FP32 steps since that change last decreased
+	double fp32_last = INFINITY;  // the previous comparison's change
 	bool last_ortho_canonical = true;               // the last orthonormalisation's form
+	// sorted energies of the last two canonical FP32 iterations and their steps
+	std::vector<double> canonical_last, canonical_prev;
+	int canonical_step_last = 0, canonical_step_prev = 0;
 	double eps = 0;
 	std::list<double> eps_values;
 	std::vector<Esn> sorted;

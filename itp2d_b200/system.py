@@ -22,7 +22,7 @@ class _Params(C.Structure):
         ("max_steps", C.c_int), ("min_eps", C.c_double), ("seed", C.c_ulong), ("ortho_algorithm", C.c_int),
         ("recover", C.c_int), ("precision", C.c_int), ("fp32_switch", C.c_double),
         ("potential", C.c_char * 128), ("timestep_test", C.c_char * 128), ("final_test", C.c_char * 128),
-        ("fp32_canonical_every", C.c_int),
+        ("fp32_canonical_every", C.c_int), ("fp32_between", C.c_int),
     ]
 
 
@@ -115,6 +115,7 @@ class Parameters:
     precision: int = capi.FP64
     fp32_switch: float = 0.0
     fp32_canonical_every: int = 0
+    fp32_between: int = capi.BETWEEN_LOWDIN
     potential: str = "harmonic"
     timestep_test: str = "relstdev(1e-3,1e-4)"
     final_test: str = "relstdev(1e-3,0)"
@@ -124,7 +125,7 @@ class Parameters:
         _lib().itp2d_parameters_default(C.byref(p))
         for k in ["sx", "sy", "length", "boundary", "B", "halforder", "num_states", "wanted", "ignore_lowest",
                   "eps_divisor", "max_steps", "min_eps", "seed", "ortho_algorithm", "precision", "fp32_switch",
-                  "fp32_canonical_every"]:
+                  "fp32_canonical_every", "fp32_between"]:
             setattr(p, k, getattr(self, k))
         p.exhaust_eps, p.recover = int(self.exhaust_eps), int(self.recover)
         if len(self.eps) > 16:

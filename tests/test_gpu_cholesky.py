@@ -1,0 +1,144 @@
+"""Cholesky (Gram-Schmidt order) orthonormalisation, ITP2D_ORTHO_CHOLESKY and
+the FP32 form's Cholesky steps between canonical ones (csrc/cholesky.cu).
+
+No reference counterpart (the reference orthonormalises canonically,
+stateset.cpp:136-232), so the checks are against numpy's Cholesky
+factorisation of the same overlap: psi'_n = sum_{i <= n} conj((L^-1)_{n,i})
+psi_i with S = L L^H, S = Psi^H Psi dx^2.
+"""
+import numpy as np
+import pytest
+
+from itp2d_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+
+
+def _states(sx, sy, k, seed, L=10.0, width2=8.0):
+    """Seeded complex Gaussian noise under a Gaussian envelope of variance
+    width2 (None: flat, for k close to the number of grid points)."""
+    dx = L / sx
+    rng = np.random.default_rng(seed)
+    x = (np.arange(sx) - sx / 2) * dx
+    y = (np.arange(sy) - sy / 2) * dx
+    env = 1.0 if width2 is None else np.exp(-0.5 * (y[:, None] ** 2 + x[None, :] ** 2) / width2)
+    psi = (rng.standard_normal((k, sy, sx)) + 1j * rng.standard_normal((k, sy, sx))) * env
+    return psi, dx
+
+
+def _gram_schmidt(psi, dx):
+    k = psi.shape[0]
+    P = psi.reshape(k, -1)
+    S = (P.conj() @ P.T) * dx * dx
+    Linv = np.linalg.inv(np.linalg.cholesky(S))
+    return (Linv @ P).reshape(psi.shape)  # row n: sum_i Linv[n, i] psi_i
+
+
+def _gram(out, dx):
+    X = out.reshape(out.shape[0], -1)
+    return (X.conj() @ X.T) * dx * dx
+
+
+# k = 5: one partial panel; 70, 130: ragged last panels; 1000, 2000: many
+# panels (2000 = the bumpy dot's state count). Flat noise on 4096 grid points
+# keeps the overlap's condition number near ((1 + r) / (1 - r))^2 with
+# r = sqrt(k / 4096), about 32 at k = 2000.
+@pytest.mark.parametrize("sx,sy,k", [(16, 16, 5), (48, 40, 70), (64, 64, 130), (64, 64, 1000), (64, 64, 2000)])
+def test_cholesky_fp64_matches_numpy(sx, sy, k):
+    psi, dx = _states(sx, sy, k, seed=k, width2=None)
+    c = capi.Context(sx, sy, dx, k)
+    c.upload(psi)
+    c.orthonormalize(capi.ORTHO_CHOLESKY)
+    assert c.orthonormalization_counts() == (0, 0, 1)
+    out = c.download()
+    ref = _gram_schmidt(psi, dx)
+    err = np.max(np.abs(out - ref)) / np.max(np.abs(ref))
+    orth = np.max(np.abs(_gram(out, dx) - np.eye(k)))
+    print(f"Cholesky FP64 {sx}x{sy} k={k}: max |out - numpy| / max |numpy| {err:.2e}, orthonormality {orth:.2e}")
+    assert err < 1e-10
+    assert orth < 1e-11
+    # the state order is kept: output n has no component along inputs > n
+    # (the first output is the first input, normalised)
+    n0 = np.sqrt(np.sum(np.abs(psi[0]) ** 2)) * dx
+    assert np.max(np.abs(out[0] - psi[0] / n0)) < 1e-12 * np.max(np.abs(psi[0] / n0))
+
+
+def test_cholesky_zero_state_reports_pivot_and_keeps_states():
+    psi, dx = _states(32, 32, 40, seed=3)
+    psi[37] = 0.0  # S is singular at row 37: pivot exactly 0
+    c = capi.Context(32, 32, dx, 40)
+    c.upload(psi)
+    with pytest.raises(capi.ITP2DError) as e:
+        c.orthonormalize(capi.ORTHO_CHOLESKY)
+    assert e.value.status == capi.E_NONPOSITIVE_EIGENVALUE
+    assert e.value.bad_index == 37 and e.value.bad_value == 0.0
+    assert np.array_equal(c.download(), psi)
+    # the context stays usable: without the zero state it succeeds
+    psi[37] = psi[36] * 0.5 + psi[3]
+    c.upload(psi)
+    c.orthonormalize(capi.ORTHO_CHOLESKY)
+    assert np.max(np.abs(_gram(c.download(), dx) - np.eye(40))) < 1e-11
+
+
+def test_fp32_form_cholesky_between_canonical_steps():
+    """FP32 states with canonical_every = 3 and Cholesky in between: the
+    schedule is canonical, Cholesky, Cholesky, canonical, ...; the Cholesky
+    steps give states orthonormal to the FP32 contraction accuracy that agree
+    with numpy's Gram-Schmidt of the same FP32 states."""
+    sx = sy = 64
+    k = 96
+    psi, dx = _states(sx, sy, k, seed=11)
+    c = capi.Context(sx, sy, dx, k, precision=capi.FP32)
+    c.set_fp32_orthonormalization(3)
+    c.set_fp32_between(capi.BETWEEN_CHOLESKY)
+    c.upload(psi)
+    c.orthonormalize()
+    assert c.orthonormalization_counts() == (1, 0, 0)
+    for n in range(2):
+        before = c.download()  # the FP32 values, widened exactly
+        c.orthonormalize()
+        assert c.orthonormalization_counts() == (1, 0, n + 1)
+        out = c.download()
+        assert np.max(np.abs(_gram(out, dx) - np.eye(k))) < 2e-5
+        ref = _gram_schmidt(before, dx)
+        assert np.max(np.abs(out - ref)) / np.max(np.abs(ref)) < 1e-4
+    c.orthonormalize()
+    assert c.orthonormalization_counts() == (2, 0, 2)
+    with pytest.raises(capi.ITP2DError):
+        c.set_fp32_between(7)
+
+
+def test_mixed_solve_with_cholesky_steps_matches_fp64():
+    """A whole FP32-form solve with Cholesky steps between canonical ones
+    (every third canonical) reaches the FP64 form's energies: the FP64
+    refinement ends the solve with the reference's canonical steps."""
+    from itp2d_b200 import system
+    common = dict(sx=64, sy=64, length=10.0, boundary=capi.PERIODIC, B=0.5, halforder=2, num_states=40,
+                  wanted=20, eps=[0.05], timestep_test="abschange(1e-9)", final_test="abschange(1e-9)",
+                  potential="harmonic(1)", max_steps=3000)
+    psi, _ = _states(64, 64, 40, seed=5)
+    ref = system.ITPSystem(system.Parameters(**common), init_states=psi)
+    ref.run()
+    mixed = system.ITPSystem(system.Parameters(precision=capi.FP32, fp32_switch=1e-7, fp32_canonical_every=3,
+                                               fp32_between=capi.BETWEEN_CHOLESKY, **common), init_states=psi)
+    mixed.run()
+    assert ref.finished and not ref.error_flag and mixed.finished and not mixed.error_flag
+    import ctypes as C
+    n = [C.c_longlong(0) for _ in range(3)]
+    assert capi.lib().itp2d_orthonormalization_counts(C.c_void_p(mixed.context_handle()),
+                                                     *[C.byref(v) for v in n]) == capi.OK
+    c0, c1, c2 = (v.value for v in n)
+    print(f"mixed with Cholesky: {mixed.total_steps} iterations (canonical {c0}, Cholesky {c2}); "
+          f"FP64 form {ref.total_steps}")
+    assert c2 > 0 and c1 == 0
+    E64, Em = ref.energies()[0][:20], mixed.energies()[0][:20]
+    assert np.max(np.abs(E64 - Em)) < 1e-8
+    ref.close()
+    mixed.close()

@@ -174,7 +174,7 @@ def test_lowdin_step_orthonormalises(k, delta):
     c, g, psi = _near_orthonormal(128, 128, k, 7, delta)
     c.set_fp32_orthonormalization(4)
     c.orthonormalize()
-    assert c.orthonormalization_counts() == (0, 1)
+    assert c.orthonormalization_counts() == (0, 1, 0)
     out = c.download()
     assert O.how_orthonormal(g, out) < TOL_ORTHO
     # every output state lies in the input's span: its residual outside an
@@ -197,15 +197,15 @@ def test_lowdin_guard_falls_back_to_canonical():
     c, dx = _ctx(64, 64, 40, seed=5)
     c.set_fp32_orthonormalization(3)
     c.orthonormalize()  # random states: the guard refuses the Lowdin step
-    assert c.orthonormalization_counts() == (1, 0)
+    assert c.orthonormalization_counts() == (1, 0, 0)
     c.orthonormalize()  # now near orthonormal: Lowdin
     c.orthonormalize()  # Lowdin (second since the canonical one)
     c.orthonormalize()  # third: canonical by the schedule
-    assert c.orthonormalization_counts() == (2, 2)
+    assert c.orthonormalization_counts() == (2, 2, 0)
     c.set_precision(capi.FP64)
     c.orthonormalize()
     c.orthonormalize()
-    assert c.orthonormalization_counts() == (4, 2)
+    assert c.orthonormalization_counts() == (4, 2, 0)
 
 
 def test_bounded_wait_gives_up_and_device_stays_usable():
@@ -218,6 +218,9 @@ def test_bounded_wait_gives_up_and_device_stays_usable():
     L.itp2d_tc_wait_probe.argtypes = []
     t0 = time.perf_counter()
     assert L.itp2d_tc_wait_probe() == capi.E_TIMEOUT
-    print(f"wait gave up after {time.perf_counter() - t0:.2f} s")
+    waited = time.perf_counter() - t0
+    print(f"wait gave up after {waited:.2f} s")
+    # the wait is bounded by the global timer (1 s), not by a poll count
+    assert 0.9 < waited < 10.0
     c, dx = _ctx(64, 64, 20, seed=9)
     assert _rel(c.overlap_matrix(), _exact_overlap(c, dx)) < TOL_S
