@@ -156,6 +156,17 @@ int itp2d_set_precision(itp2d_ctx* ctx, int precision);
  * ITP2D_CONTRACT_FP64 always uses FP64 arithmetic (DMMA). FP64 states always
  * use FP64 arithmetic. No reference counterpart (the reference is FP64 only;
  * stateset.cpp:146-154 and 214-228 compute these products with ZHERK/ZGEMM). */
+/* Rayleigh-Ritz step on orthonormal states (no reference counterpart; the
+ * reference's energies are per-state expectation values, itpsystem.cpp:483-494):
+ * the projected Hamiltonian H_ij = <psi_i|H psi_j> dx^2 (Hamiltonian passes
+ * of itp2d_energies, FP64 contraction), its eigendecomposition
+ * H = U diag(theta) U^H by the Jacobi eigensolver, and psi'_n =
+ * sum_i U_{i,n} psi_i. ritz_values (k doubles, ascending, may be NULL)
+ * receives theta. The states must be orthonormal (after
+ * itp2d_orthonormalize); the result is orthonormal to the rotation's
+ * accuracy and its energies are the Ritz values. */
+int itp2d_rayleigh_ritz(itp2d_ctx* ctx, double* ritz_values);
+
 enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1 };
 int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
 

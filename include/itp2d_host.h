@@ -47,6 +47,8 @@ typedef struct {
 	                             (itp2d_set_fp32_orthonormalization); 0: always canonical */
 	int fp32_between;         /* ITP2D_BETWEEN_LOWDIN (0) or ITP2D_BETWEEN_CHOLESKY
 	                             (itp2d_set_fp32_between) */
+	int switch_rayleigh_ritz; /* FP32 form: 1 = one Rayleigh-Ritz step (itp2d_rayleigh_ritz)
+	                             after the first FP64 orthonormalisation of the refinement */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

@@ -71,6 +71,7 @@ def lib():
         L.itp2d_set_fp32_orthonormalization.argtypes = [vp, i]
         L.itp2d_orthonormalization_counts.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 3
         L.itp2d_set_fp32_between.argtypes = [vp, i]
+        L.itp2d_rayleigh_ritz.argtypes = [vp, dp]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
@@ -218,6 +219,14 @@ class Context:
     def set_fp32_orthonormalization(self, canonical_every):
         _check(lib().itp2d_set_fp32_orthonormalization(self.h, int(canonical_every)),
                "itp2d_set_fp32_orthonormalization")
+
+    def rayleigh_ritz(self):
+        """One Rayleigh-Ritz step on the (orthonormal) resident states; returns
+        the ascending Ritz values."""
+        theta = np.empty(self.k)
+        _check(lib().itp2d_rayleigh_ritz(self.h, theta.ctypes.data_as(C.POINTER(C.c_double))),
+               "itp2d_rayleigh_ritz")
+        return theta
 
     def set_fp32_between(self, method):
         """BETWEEN_LOWDIN or BETWEEN_CHOLESKY between the canonical calls."""

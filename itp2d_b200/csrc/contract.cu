@@ -48,8 +48,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // stages of complex-interleaved rows (pitch kPad elements: conflict-free
 // fragment loads): cp.async fetches step s + 1 while the DMMAs of step s run.
 template <class T>
-__global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi, int k, long long G,
-		const int2* __restrict__ pairs, long long chunk, double2* __restrict__ part) {
+__global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi, const T* __restrict__ psib, int k,
+		long long G, const int2* __restrict__ pairs, long long chunk, double2* __restrict__ part) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	T* stage = reinterpret_cast<T*>(smem_raw);  // [2][A rows kBM | B rows kBN][kPad]
 	constexpr int SS = (kBM + kBN) * kPad;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) overlap_kernel(const T* __restrict__ psi,
 			T* db = st + (kBM + lrow) * kPad + lseg + q;
 			if (gg < g1 && ia < k) cp_async_elem<T>(da, psi + (long long)ia * G + gg);
 			else *da = T{0, 0};
-			if (gg < g1 && jb < k) cp_async_elem<T>(db, psi + (long long)jb * G + gg);
+			if (gg < g1 && jb < k) cp_async_elem<T>(db, psib + (long long)jb * G + gg);
 			else *db = T{0, 0};
 		}
 	};
@@ -305,13 +305,13 @@ int overlap_tiles(int k) { return (k + kBM - 1) / kBM; }
 
 template <class T>
 void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
-		double2* part, double dx2, double2* S, cudaStream_t s) {
+		double2* part, double dx2, double2* S, cudaStream_t s, const T* psib) {
 	long long chunk = (G + nsplit - 1) / nsplit;
 	chunk = ((chunk + kBK - 1) / kBK) * kBK;
 	const int used = (int)((G + chunk - 1) / chunk);
 	const size_t sm = (size_t)2 * (kBM + kBN) * kPad * sizeof(T);
 	cudaFuncSetAttribute(overlap_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-	overlap_kernel<T><<<dim3(npairs, used), 256, sm, s>>>(psi, k, G, pairs, chunk, part);
+	overlap_kernel<T><<<dim3(npairs, used), 256, sm, s>>>(psi, psib ? psib : psi, k, G, pairs, chunk, part);
 	launch_overlap_finish(part, k, used, dx2, S, s);
 }
 
@@ -343,9 +343,9 @@ void launch_convert(const void* in, int in_fp64, void* out, long long n, cudaStr
 }
 
 template void launch_overlap<double2>(const double2*, int, long long, const int2*, int, int, double2*, double,
-		double2*, cudaStream_t);
+		double2*, cudaStream_t, const double2*);
 template void launch_overlap<float2>(const float2*, int, long long, const int2*, int, int, double2*, double,
-		double2*, cudaStream_t);
+		double2*, cudaStream_t, const float2*);
 template void launch_rotate<double2>(const double2*, const double2*, int, long long, double2*, cudaStream_t);
 template void launch_rotate<float2>(const double2*, const float2*, int, long long, float2*, cudaStream_t);
 template void launch_normalize1<double2>(double2*, long long, double, double*, cudaStream_t);

@@ -7,9 +7,11 @@ namespace itp2d {
 
 int overlap_tiles(int k);
 // T = double2 (FP64 states) or float2 (FP32 states); products and sums in FP64.
+// S = Psi^H Psib dx^2 from its upper triangle, mirrored Hermitian (psib null:
+// Psi itself; otherwise Psib = H Psi for a Hermitian H).
 template <class T>
 void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
-		double2* part, double dx2, double2* S, cudaStream_t s);
+		double2* part, double dx2, double2* S, cudaStream_t s, const T* psib = nullptr);
 template <class T>
 void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s);
 // Sums the nsplit partial k x k blocks of part (upper triangle i <= j used),
@@ -93,6 +95,10 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 // (columns of w.V, kp x kp with kp = k rounded up to even) without the
 // overlap checks unless check != 0.
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
+// Rayleigh-Ritz: eigenpairs of the Hermitian H (k x k, consumed) with
+// W[:, n] = V[:, p(n)] (unit columns, ascending eigenvalues in w.evals, any
+// sign) for the rotation psi' = psi W.
+cudaError_t launch_ritz(double2* H, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms, cudaStream_t s);
 
 // Second-order Lowdin orthonormalisation (lowdin.cu): D = diag(S)^{-1/2},
 // E = D S D - I (row-major) and conj(E), stats = {max |E_ij|, sum |E_ij|^2,

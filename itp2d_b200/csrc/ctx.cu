@@ -115,6 +115,7 @@ struct itp2d_ctx {
 	double fp32_tau = 1e-3;      // FP32 eigensolve: largest rotation tangent at which it stops
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
 	long long ortho_calls[3] = {0, 0, 0};  // canonical, Lowdin, Cholesky
+	long long ritz_calls = 0;              // Rayleigh-Ritz steps
 	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
 	double* hlstat = nullptr;    // pinned copy
 	void* loop_buf = nullptr;    // device driver loop state (itp2d_run_device_loop)
@@ -1193,6 +1194,43 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	c->psi = c->acc;
 	c->acc = t;
 	return ITP2D_OK;
+}
+
+int itp2d_rayleigh_ritz(itp2d_ctx* c, double* ritz_values) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (c->k < 2) return ITP2D_E_INVALID;
+	const bool f64 = c->precision == ITP2D_FP64;
+	// H psi into the second buffer (psi is not changed)
+	int st = f64 ? energies_impl<double>(c, c->acc, false) : energies_impl<float>(c, c->acc, false);
+	if (st) return st;
+	{
+		PhaseTimer t(c, kOverlap);
+		// projected Hamiltonian psi^H (H psi) dx^2, FP64 products for either precision
+		if (f64)
+			launch_overlap((const double2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
+					c->dx * c->dx, c->S, c->stream, (const double2*)c->acc);
+		else
+			launch_overlap((const float2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part,
+					c->dx * c->dx, c->S, c->stream, (const float2*)c->acc);
+		c->launches += 2;
+	}
+	{
+		PhaseTimer t(c, kEigen);
+		c->jw.tau_final = 0.0;
+		c->jw.f32 = {};
+		ITP2D_TRY(launch_ritz(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
+		c->launches += 6;
+	}
+	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	const EigStatus es = *c->hstat;
+	if (es.status != ITP2D_OK) return es.status;
+	if (ritz_values)
+		ITP2D_TRY(cudaMemcpy(ritz_values, c->jw.evals, (size_t)c->k * sizeof(double), cudaMemcpyDeviceToHost));
+	st = rotate_states(c, use_tensor_cores(c));
+	if (st == ITP2D_OK) c->ritz_calls++;
+	return st;
 }
 
 int itp2d_set_precision(itp2d_ctx* c, int precision) {

@@ -391,6 +391,16 @@ __global__ void build_w_kernel(const double2* __restrict__ V, int k, int kp, con
 	}
 }
 
+// W[i][n] = V[i][perm[n]]: the Ritz vectors' coefficients, ascending Ritz values.
+__global__ void ritz_w_kernel(const double2* __restrict__ V, int k, int kp, const int* __restrict__ perm, double2* W) {
+	const long long n2 = (long long)k * k;
+	for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+			idx += (long long)gridDim.x * blockDim.x) {
+		const int i = (int)(idx / k), n = (int)(idx % k);
+		W[idx] = __ldcg(V + (long long)i * kp + perm[n]);
+	}
+}
+
 }  // namespace
 
 size_t jacobi_counters(int max_sweeps) { return jacobi_counter_ints(max_sweeps); }
@@ -410,6 +420,15 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 	const long long n2 = (long long)k * k;
 	const int kp = jacobi_kp(w, k);
 	build_w_kernel<<<(unsigned)std::min<long long>((n2 + 255) / 256, 4096), 256, 0, s>>>(w.V, k, kp, w.evals,
+			w.perm, W);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_ritz(double2* H, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms, cudaStream_t s) {
+	cudaError_t e = launch_eigh(H, k, w, st, num_sms, s, 0);
+	if (e != cudaSuccess) return e;
+	const long long n2 = (long long)k * k;
+	ritz_w_kernel<<<(unsigned)std::min<long long>((n2 + 255) / 256, 4096), 256, 0, s>>>(w.V, k, jacobi_kp(w, k),
 			w.perm, W);
 	return cudaGetLastError();
 }

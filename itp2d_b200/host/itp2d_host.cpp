@@ -351,9 +351,14 @@ void ITPSystem::orthonormalize() {
 		check(itp2d_set_fp32_eig_tolerance(ctx, early ? 0.05 : 1e-3), "itp2d_set_fp32_eig_tolerance");
 	}
 	itp2d_orthonormalization_counts(ctx, &c0, nullptr, nullptr);
-	const int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
+	int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
 	itp2d_orthonormalization_counts(ctx, &c1, nullptr, nullptr);
 	last_ortho_canonical = c1 > c0;
+	if (st == ITP2D_OK && ritz_pending && precision == ITP2D_FP64) {
+		ritz_pending = false;
+		st = itp2d_rayleigh_ritz(ctx, nullptr);
+		if (st == ITP2D_OK) ritz_steps++;
+	}
 	t_ortho += now_s() - t0;
 	orthonormalized(st, bi, bv);
 }
@@ -540,6 +545,7 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 	precision = ITP2D_FP64;
 	step_counter = 0;
 	all_timestep_converged = false;
+	ritz_pending = p.switch_rayleigh_ritz != 0;
 	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
 }
 
@@ -717,6 +723,8 @@ void ITPSystem::reset(const double* init) {
 	total_step_counter = step_counter = 0;
 	fp32_best = INFINITY;
 	fp32_last = INFINITY;
+	ritz_pending = false;
+	ritz_steps = 0;
 	fp32_stall = 0;
 	canonical_last.clear();
 	canonical_prev.clear();
@@ -797,6 +805,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->fp32_switch = 0.0;
 	p->fp32_canonical_every = 0;
 	p->fp32_between = ITP2D_BETWEEN_LOWDIN;
+	p->switch_rayleigh_ritz = 0;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
 	std::strcpy(p->final_test, "relstdev(1e-3,0)");

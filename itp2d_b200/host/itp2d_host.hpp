@@ -211,7 +211,8 @@ class ITPSystem {
 		save_fn = fn;
 		save_user = user;
 	}
-	int saves = 0;  // save_states calls made
+	int saves = 0;       // save_states calls made
+	int ritz_steps = 0;  // Rayleigh-Ritz steps taken (switch_rayleigh_ritz)
 	const itp2d_parameters p;
 
   private:
@@ -250,6 +251,7 @@ class ITPSystem {
 	double fp32_best = INFINITY;  // smallest per-step energy change seen in the FP32 form
 	int fp32_stall = 0;           // FP32 steps since that change last decreased
 	double fp32_last = INFINITY;  // the previous comparison's change
+	bool ritz_pending = false;    // a Rayleigh-Ritz step after the next FP64 orthonormalisation
 	bool last_ortho_canonical = true;               // the last orthonormalisation's form
 	// sorted energies of the last two canonical FP32 iterations and their steps
 	std::vector<double> canonical_last, canonical_prev;

@@ -22,7 +22,7 @@ class _Params(C.Structure):
         ("max_steps", C.c_int), ("min_eps", C.c_double), ("seed", C.c_ulong), ("ortho_algorithm", C.c_int),
         ("recover", C.c_int), ("precision", C.c_int), ("fp32_switch", C.c_double),
         ("potential", C.c_char * 128), ("timestep_test", C.c_char * 128), ("final_test", C.c_char * 128),
-        ("fp32_canonical_every", C.c_int), ("fp32_between", C.c_int),
+        ("fp32_canonical_every", C.c_int), ("fp32_between", C.c_int), ("switch_rayleigh_ritz", C.c_int),
     ]
 
 
@@ -116,6 +116,7 @@ class Parameters:
     fp32_switch: float = 0.0
     fp32_canonical_every: int = 0
     fp32_between: int = capi.BETWEEN_LOWDIN
+    switch_rayleigh_ritz: bool = False
     potential: str = "harmonic"
     timestep_test: str = "relstdev(1e-3,1e-4)"
     final_test: str = "relstdev(1e-3,0)"
@@ -128,6 +129,7 @@ class Parameters:
                   "fp32_canonical_every", "fp32_between"]:
             setattr(p, k, getattr(self, k))
         p.exhaust_eps, p.recover = int(self.exhaust_eps), int(self.recover)
+        p.switch_rayleigh_ritz = int(self.switch_rayleigh_ritz)
         if len(self.eps) > 16:
             raise ValueError("at most 16 explicit time steps")
         p.num_eps = len(self.eps)
