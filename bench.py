@@ -8,9 +8,12 @@ Workload "bumpy" (the default, the bumpy dot): V = r^2/2 plus 400 Gaussian
 bumps (amplitude uniform in [0.8, 1.2], width 0.1, centres uniform in |x|,
 |y| < 6, seeded), B = 0.5 (linear gauge), periodic 512 x 512 grid of side 16,
 k = 2000 states from seeded complex Gaussian noise, 6th-order multi-product
-split (halforder 3) at eps = 0.05, canonical orthonormalisation every step,
-until the 1000 lowest states change their energy by less than 1e-9 between
-iterations (the reference's abschange(1e-9) as time-step and final test).
+split (halforder 3) at eps = 0.05, until the 1000 lowest states change their
+energy by less than 1e-9 between iterations (the reference's abschange(1e-9)
+as time-step and final test). The FP64 form orthonormalises canonically every
+step (the reference's algorithm); the mixed form's FP32 phase does so on every
+third iteration with Cholesky steps in between, and its FP64 refinement
+canonically.
 
 Workload "dot" (the magnetic dot): V = r^2/2, B = 1, periodic 256 x 256 grid
 of side 14, k = 500, 4th-order split (halforder 2), eps = 0.05, the 250 lowest
@@ -151,15 +154,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# The mixed form's FP32 phase: a canonical orthonormalisation on every third
+# iteration and Cholesky (Gram-Schmidt order) ones in between.
+MIXED_CANONICAL_EVERY = 3
+
+
 def params(form: str):
     from itp2d_b200 import capi, system
     w = WORKLOAD
+    mixed = form == "mixed"
     return system.Parameters(sx=w["sx"], sy=w["sy"], length=w["length"], B=w["B"], halforder=w["halforder"],
                              num_states=w["num_states"], wanted=w["wanted"], eps=[w["eps"]],
                              timestep_test=w["test"], final_test=w["test"], max_steps=5000,
                              potential=w["potential"],
-                             precision=capi.FP32 if form == "mixed" else capi.FP64,
-                             fp32_switch=1e-7 if form == "mixed" else 0.0)
+                             precision=capi.FP32 if mixed else capi.FP64,
+                             fp32_switch=1e-7 if mixed else 0.0,
+                             fp32_canonical_every=MIXED_CANONICAL_EVERY if mixed else 0,
+                             fp32_between=capi.BETWEEN_CHOLESKY)
 
 
 def alg_bytes_split(w, b):

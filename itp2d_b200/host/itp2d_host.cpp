@@ -35,6 +35,11 @@ const int kFlagChunk = 32;
 // FP32 noise floor of the per-step energy change, in single-precision
 // roundings of the largest wanted energy.
 const double kFp32FloorUlps = 64.0;
+// The FP32 switch rule reads the energy change over this many iterations
+// (per iteration): below the visible FP32 floor the subspace keeps converging,
+// and the longer span delays the switch by the iterations that the FP64
+// refinement would otherwise spend at several times the cost.
+const size_t kFp32Span = 3;
 
 }  // namespace
 
@@ -494,11 +499,11 @@ void ITPSystem::change_time_step() {
 // rotation tangent 0.05) while the energies still move by more than 1e-2 per
 // step: the basis those steps produce is replaced on the next step anyway.
 //
-// With Cholesky steps between canonical ones the per-state energies of a
-// Cholesky step are those of a Gram-Schmidt basis of the subspace, not of its
-// Ritz-like canonical basis, so the rule compares each canonical iteration
-// with the previous canonical one (the change divided by the iterations
-// between them).
+// The change is taken over kFp32Span iterations. With Cholesky steps between
+// canonical ones the per-state energies of a Cholesky step are those of a
+// Gram-Schmidt basis of the subspace, not of its Ritz-like canonical basis,
+// so the rule compares each canonical iteration with the previous canonical
+// one (the change divided by the iterations between them).
 void ITPSystem::maybe_switch_precision() {
 	if (precision != ITP2D_FP32 || !(p.fp32_switch > 0) || energies.size() < 2) return;
 	const bool between = p.fp32_canonical_every > 1;
@@ -508,7 +513,9 @@ void ITPSystem::maybe_switch_precision() {
 		fp32_compare_with(canonical_last, canonical_prev, 2, canonical_step_last - canonical_step_prev);
 		return;
 	}
-	fp32_compare_with(energies[energies.size() - 1], energies[energies.size() - 2], between ? 2 : 3, 1);
+	const size_t n = energies.size();
+	const int span = (int)std::min<size_t>(kFp32Span, n - 1);
+	fp32_compare_with(energies[n - 1], energies[n - 1 - span], between ? 2 : 3, span);
 }
 
 // Largest change per iteration of the wanted sorted energies between a and b,
