@@ -49,6 +49,9 @@ typedef struct {
 	                             (itp2d_set_fp32_between) */
 	int switch_rayleigh_ritz; /* FP32 form: 1 = one Rayleigh-Ritz step (itp2d_rayleigh_ritz)
 	                             after the first FP64 orthonormalisation of the refinement */
+	double fp32_eps_factor;   /* FP32 form: the FP32 sweeps propagate with time step
+	                             eps * fp32_eps_factor (0 or 1: eps); the FP64 refinement
+	                             and every convergence test use eps */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

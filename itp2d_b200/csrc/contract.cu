@@ -303,6 +303,30 @@ __global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, 
 
 int overlap_tiles(int k) { return (k + kBM - 1) / kBM; }
 
+int overlap_splits(int k, long long G, int num_sms) {
+	const int nt = overlap_tiles(k);
+	const long long npairs = (long long)nt * (nt + 1) / 2;
+	// two CTAs per SM (80 KB of stages each for FP64 states); up to 16 splits
+	// of at least 512 grid points; the first count whose grid fills its last
+	// wave to 95 % or more, else the best-filled one (k = 2000: 528 tile pairs
+	// fill 1.78 waves unsplit, 5 splits fill 8.92 waves)
+	const long long slots = 2LL * num_sms;
+	const long long most = std::max(1LL, std::min(16LL, G / 512));
+	long long best = 1;
+	double best_fill = 0.0;
+	for (long long ns = 1; ns <= most; ns++) {
+		const long long ctas = npairs * ns;
+		const long long waves = (ctas + slots - 1) / slots;
+		const double fill = (double)ctas / (double)(waves * slots);
+		if (fill > best_fill + 1e-9) {
+			best = ns;
+			best_fill = fill;
+		}
+		if (fill >= 0.95) break;
+	}
+	return (int)best;
+}
+
 template <class T>
 void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
 		double2* part, double dx2, double2* S, cudaStream_t s, const T* psib) {

@@ -6,6 +6,8 @@
 namespace itp2d {
 
 int overlap_tiles(int k);
+// Grid splits of the FP64 overlap for k states on G points.
+int overlap_splits(int k, long long G, int num_sms);
 // T = double2 (FP64 states) or float2 (FP32 states); products and sums in FP64.
 // S = Psi^H Psib dx^2 from its upper triangle, mirrored Hermitian (psib null:
 // Psi itself; otherwise Psib = H Psi for a Hermitian H).

@@ -717,7 +717,7 @@ long long itp2d_ctx_footprint(int sx, int sy, int num_states, int boundary, doub
 	long long b = (2 + ((halforder >= 3 || dm) ? 1 : 0)) * G * k * 16;  // psi, acc, work
 	const int nt = overlap_tiles(num_states);
 	const int npairs = nt * (nt + 1) / 2;
-	const int nsplit = std::max(1, std::min((4 * sms) / npairs, (int)std::max(1LL, G / 512)));
+	const int nsplit = overlap_splits(num_states, G, sms);
 	const int parts = std::max(nsplit, tc_overlap_splits(num_states, G, sms));
 	const long long kp = std::max(bjacobi_padded(num_states), (num_states + 1) & ~1);
 	b += (2 + parts) * k * k * 16 + (tc_supported(num_states, G) ? (long long)tc_wsplit_bytes(num_states) : 0);
@@ -771,9 +771,7 @@ int itp2d_ctx_create(int sx, int sy, double dx, int num_states, int boundary, do
 	// overlap / eigensolver buffers
 	const int nt = overlap_tiles(k);
 	c->npairs = nt * (nt + 1) / 2;
-	// split-K count: the largest that keeps the grid within two waves of two
-	// CTAs per SM (a third, nearly empty wave costs a third of the kernel)
-	c->nsplit = std::max(1, std::min((4 * c->num_sms) / c->npairs, (int)std::max(1LL, c->G / 512)));
+	c->nsplit = overlap_splits(k, c->G, c->num_sms);
 	const int kp = std::max(bjacobi_padded(k), (k + 1) & ~1);  // covers the scalar and block layouts
 	if (e == cudaSuccess) c->S = (double2*)dalloc(c, (size_t)k * k * sizeof(double2), &e);
 	c->tc_nsplit = tc_overlap_splits(k, c->G, c->num_sms);
