@@ -25,6 +25,7 @@ PERIODIC, DIRICHLET = 0, 1
 FP64, FP32 = 0, 1
 ORTHO_DEFAULT, ORTHO_HIGHMEM, ORTHO_CHOLESKY = 0, 1, 2
 BETWEEN_LOWDIN, BETWEEN_CHOLESKY = 0, 1
+COL_SMEM, COL_TMA = 0, 1
 CONTRACT_AUTO, CONTRACT_FP64 = 0, 1
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
@@ -72,6 +73,8 @@ def lib():
         L.itp2d_orthonormalization_counts.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 3
         L.itp2d_set_fp32_between.argtypes = [vp, i]
         L.itp2d_rayleigh_ritz.argtypes = [vp, dp]
+        L.itp2d_set_column_variant.argtypes = [vp, i]
+        L.itp2d_column_variant.argtypes = [vp]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
         L.itp2d_launch_count.restype = C.c_longlong
@@ -219,6 +222,14 @@ class Context:
     def set_fp32_orthonormalization(self, canonical_every):
         _check(lib().itp2d_set_fp32_orthonormalization(self.h, int(canonical_every)),
                "itp2d_set_fp32_orthonormalization")
+
+    def set_column_variant(self, variant):
+        """Column pass of 256/512-point lines: COL_SMEM, COL_TMA, or -1 (tuned)."""
+        _check(lib().itp2d_set_column_variant(self.h, int(variant)), "itp2d_set_column_variant")
+
+    @property
+    def column_variant(self) -> int:
+        return lib().itp2d_column_variant(self.h)
 
     def rayleigh_ritz(self):
         """One Rayleigh-Ritz step on the (orthonormal) resident states; returns

@@ -116,6 +116,10 @@ struct itp2d_ctx {
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
 	long long ortho_calls[3] = {0, 0, 0};  // canonical, Lowdin, Cholesky
 	long long ritz_calls = 0;              // Rayleigh-Ritz steps
+	// register-FFT column pass variant per precision (kColRegSmem / kColTma):
+	// -1 until tuned at the first time step of that precision
+	int col_variant[2] = {-1, -1};
+	int col_forced = -1;  // itp2d_set_column_variant
 	double* lstat = nullptr;     // device: max |E|, |E|_F^2, bad diagonal
 	double* hlstat = nullptr;    // pinned copy
 	void* loop_buf = nullptr;    // device driver loop state (itp2d_run_device_loop)
@@ -487,8 +491,42 @@ void col_pass(itp2d_ctx* c, const LinePlan& lp, void* data, const void* mul2d, c
 	a.sx = c->sx; a.sy = c->sy; a.G = c->G;
 	a.cols_per_tile = col_tile_cols(line_len(lp), sizeof(c2<R>), c->sx);
 	a.lp = lp;
+	const int v = c->col_forced >= 0 ? c->col_forced : c->col_variant[c->precision];
+	a.variant = v >= 0 ? v : kColRegSmem;
+	a.err = c->dflag;
 	launch_col_pass<R>(a, c->k, nullptr, c->stream);
 	c->launches++;
+}
+
+// Times the column pass variants on the spare state buffer (its contents are
+// scratch between calls) with the first member's kinetic table, on up to 128
+// states, and keeps the fastest for this precision.
+template <class R>
+int tune_columns(itp2d_ctx* c) {
+	if (c->boundary != ITP2D_PERIODIC || c->members.empty()) return ITP2D_OK;
+	const MemberTables& mt = c->members[0];
+	ColPassArgs a;
+	a.data = c->acc;
+	a.mul2d = c->B == 0 ? mt.kmul : nullptr;
+	a.mul1d = c->B == 0 ? nullptr : mt.ky;
+	a.mode = 0;
+	a.sx = c->sx; a.sy = c->sy; a.G = c->G;
+	const LinePlan& ly = plan(c, 1, 0);
+	a.cols_per_tile = col_tile_cols(line_len(ly), sizeof(c2<R>), c->sx);
+	a.lp = ly;
+	a.err = c->dflag;
+	const int v = tune_col_pass_reg<R>(a, std::min(c->k, 128), c->stream);
+	c->col_variant[c->precision] = v >= 0 ? v : kColRegSmem;
+	ITP2D_TRY(cudaGetLastError());
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	// a time-out of the TMA variant during tuning is reported, not hidden
+	ITP2D_TRY(cudaMemcpy(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost));
+	if (*c->hflag != ITP2D_OK) {
+		const int f = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+		return f;
+	}
+	return ITP2D_OK;
 }
 
 // One SecondOrderSplit member t applied to `src`, result in `dst`, optionally
@@ -857,7 +895,23 @@ int itp2d_set_time_step(itp2d_ctx* c, double eps) {
 	std::lock_guard<std::mutex> g(c->mu);
 	c->eps = eps;
 	c->eps_set = true;
-	return rebuild_tables(c);
+	const int st = rebuild_tables(c);
+	if (st || c->col_variant[c->precision] >= 0) return st;
+	return c->precision == ITP2D_FP64 ? tune_columns<double>(c) : tune_columns<float>(c);
+}
+
+int itp2d_set_column_variant(itp2d_ctx* c, int variant) {
+	if (!c || variant < -1 || variant >= kColVariants) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->col_forced = variant;
+	return ITP2D_OK;
+}
+
+int itp2d_column_variant(itp2d_ctx* c) {
+	if (!c) return -1;
+	std::lock_guard<std::mutex> g(c->mu);
+	const int v = c->col_forced >= 0 ? c->col_forced : c->col_variant[c->precision];
+	return v >= 0 ? v : kColRegSmem;
 }
 
 int itp2d_upload_states(itp2d_ctx* c, const double* h) {
@@ -924,8 +978,15 @@ int itp2d_energies(itp2d_ctx* c, double* E, double* sigma, double* sres, double*
 		// the current energies are the shift of the next residual evaluation
 		ITP2D_TRY(cudaMemcpyAsync(c->dEshift, c->dE, (size_t)c->k * sizeof(double), cudaMemcpyDeviceToDevice,
 				c->stream));
+		// status of the bounded waits of the passes since the last check
+		ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	}
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	if (*c->hflag != ITP2D_OK) {
+		const int f = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+		return f;
+	}
 	const int k = c->k;
 	std::memcpy(E, c->hbuf, k * sizeof(double));
 	std::memcpy(sigma, c->hbuf + k, k * sizeof(double));
@@ -1745,12 +1806,18 @@ int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double lim
 		e = cudaMemcpyAsync(prev_E_out, prevE, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
 	if (e == cudaSuccess && prev_sigma_out)
 		e = cudaMemcpyAsync(prev_sigma_out, prevS, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
 	if (e != cudaSuccess) return fail(e);
 	cudaGraphExecDestroy(exec);
 	cudaGraphDestroy(graph);
 	*iterations = out[0];
 	*status = out[2];
+	if (*c->hflag != ITP2D_OK) {
+		// a bounded wait of a pass inside the loop ran out
+		*status = *c->hflag;
+		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
+	}
 	c->launches += per_iteration * out[0];
 	// the current energies are the shift of the next residual evaluation
 	return ITP2D_OK;

@@ -23,6 +23,11 @@
 // tables applied as in RowPassArgs / ColPassArgs.
 #include "split.cuh"
 
+#include "../../include/itp2d_gpu.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <mutex>
 #include <set>
@@ -106,11 +111,11 @@ __device__ __forceinline__ void dft_reg(c2<R>* v) {
 	});
 }
 
-// Transform of one line held as v[a] = x[t + B a]. xb: the line's exchange
-// area (N elements, element stride es); xtw: w_N^(b k1) at [k1 * B + b]
-// (forward sign). On return v[a] = X[t + B a].
-template <class R, int A, int B, int SIGN>
-__device__ __forceinline__ void line_fft(c2<R>* v, int t, c2<R>* xb, int es, const c2<R>* xtw) {
+// Transform of one line held as v[a] = x[t + B a]. xb(i): the line's
+// exchange area, element i = 0..N-1 (a reference into shared memory); xtw:
+// w_N^(b k1) at [k1 * B + b] (forward sign). On return v[a] = X[t + B a].
+template <class R, int A, int B, int SIGN, class XB>
+__device__ __forceinline__ void line_fft_x(c2<R>* v, int t, XB&& xb, const c2<R>* xtw) {
 	constexpr int S2 = A / B;
 	dft_reg<R, A, SIGN>(v);
 	sfor<A - 1>([&](auto K) {
@@ -122,7 +127,7 @@ __device__ __forceinline__ void line_fft(c2<R>* v, int t, c2<R>* xb, int es, con
 	__syncwarp();  // earlier readers of xb are done
 	sfor<A>([&](auto K) {
 		constexpr int k1 = K;
-		xb[(k1 * B + (t ^ (k1 & (B - 1)))) * es] = v[k1];
+		xb(k1 * B + (t ^ (k1 & (B - 1)))) = v[k1];
 	});
 	__syncwarp();
 	c2<R> u[A];
@@ -131,13 +136,19 @@ __device__ __forceinline__ void line_fft(c2<R>* v, int t, c2<R>* xb, int es, con
 		const int k1 = t + B * i;
 		sfor<B>([&](auto Bi) {
 			constexpr int b = Bi;
-			u[i * B + b] = xb[(k1 * B + (b ^ t)) * es];
+			u[i * B + b] = xb(k1 * B + (b ^ t));
 		});
 		dft_reg<R, B, SIGN>(u + i * B);
 	});
 	sfor<S2>([&](auto I) {
 		sfor<B>([&](auto K2) { v[I + S2 * K2] = u[I * B + K2]; });
 	});
+}
+
+// The same with the exchange area at xb[i * es].
+template <class R, int A, int B, int SIGN>
+__device__ __forceinline__ void line_fft(c2<R>* v, int t, c2<R>* xb, int es, const c2<R>* xtw) {
+	line_fft_x<R, A, B, SIGN>(v, t, [=](int i) -> c2<R>& { return xb[i * es]; }, xtw);
 }
 
 template <class R, int A, int B>
@@ -320,6 +331,188 @@ __global__ void __launch_bounds__(kThreads, (sizeof(R) == 4 && A <= 16) ? 3 : (s
 		if (NBUF == 2) cur ^= 1;
 	}
 	if (NBUF == 2) cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Column pass with TMA tile movement (kColTma).
+//
+// A tile is one 128-byte wide strip of a state: W = 128 / sizeof(complex)
+// columns (16 FP32, 8 FP64) by all N rows, brought into shared memory by
+// cp.async.bulk.tensor (a 3-D tensor map over k x sy x sx in 8-byte units,
+// boxes of 16 units x min(N, 256) rows, 128-byte swizzle) and written back by
+// the same engine after the in-place transform. S = 3 slots form a ring: the
+// tile two steps ahead is in flight while one is transformed. One thread
+// (the leader, thread 0, also a transform thread) issues the copies: after
+// every transform thread has written tile j back (mbarrier `done`), it
+// stores tile j, then refills the slot of tile j - 1 (whose store has
+// finished reading) with tile j - 1 + S. Transform threads only wait for
+// `full` of their next tile, so no block-wide barrier sits in the loop.
+// Column line `line` of a tile is transformed by B threads of one warp as in
+// col_reg_kernel, using its own column of the slot as the exchange area.
+// Every wait is bounded (one second of global time); on time-out the kernel
+// records ITP2D_E_TIMEOUT in *err, waits (bounded) for its copies in flight
+// and returns.
+
+constexpr unsigned long long kTmaWaitNs = 1000000000ULL;
+
+__device__ __forceinline__ uint32_t sh_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtime_ns() {
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t mb, uint32_t parity) {
+	uint32_t ok;
+	asm volatile(
+			"{\n\t.reg .pred P1;\n\t"
+			"mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+			"selp.b32 %0, 1, 0, P1;\n\t}\n"
+			: "=r"(ok)
+			: "r"(mb), "r"(parity)
+			: "memory");
+	return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false on time-out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mb, uint32_t parity) {
+	if (mbar_try(mb, parity)) return true;
+	const unsigned long long t0 = gtime_ns();
+	for (long long i = 0; i < (1LL << 26); i++) {
+		if (mbar_try(mb, parity)) return true;
+		__nanosleep(32);
+		if ((i & 63) == 0 && gtime_ns() - t0 > kTmaWaitNs) return false;
+	}
+	return false;
+}
+
+__device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t mb) {
+	asm volatile(
+			"cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+			"[%5];" ::"r"(dst),
+			"l"(map), "r"(x), "r"(y), "r"(z), "r"(mb)
+			: "memory");
+}
+
+__device__ __forceinline__ void tma_store3(const CUtensorMap* map, int x, int y, int z, uint32_t src) {
+	asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+			"r"(x), "r"(y), "r"(z), "r"(src)
+			: "memory");
+}
+
+// Byte offset of element (row r, column c) of a tile: 128-byte rows, the
+// 16-byte chunk index of row r XORed with r mod 8 (the TMA 128-byte swizzle).
+template <int ES>
+__device__ __forceinline__ uint32_t swz(int r, int c) {
+	const int byte = c * ES;
+	return (uint32_t)(r * 128 + ((((byte >> 4) ^ (r & 7))) << 4) + (byte & 15));
+}
+
+template <class R, int A, int B, int S>
+__global__ void __launch_bounds__((128 / (2 * (int)sizeof(R))) * B)
+		col_tma_kernel(const __grid_constant__ CUtensorMap map, ColPassArgs a, int k) {
+	using T = c2<R>;
+	constexpr int ES = (int)sizeof(T), N = A * B, W = 128 / ES, NT = W * B;
+	constexpr int TILE = N * 128, BOX = N < 256 ? N : 256, U = ES / 8;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	unsigned char* base =
+			reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+	T* xtw = reinterpret_cast<T*>(base + S * TILE);
+	unsigned long long* full = reinterpret_cast<unsigned long long*>(xtw + N);
+	unsigned long long* done = full + S;
+	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
+	const bool leader = threadIdx.x == 0;
+	if (leader) {
+		for (int s = 0; s < S; s++) {
+			asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_u32(full + s)), "r"(1) : "memory");
+			asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_u32(done + s)), "r"(NT) : "memory");
+		}
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+	const int sx = a.sx;
+	const int nct = (sx + W - 1) / W;
+	const long long total = (long long)k * nct;
+	auto tile_of = [&](long long j) { return (long long)blockIdx.x + j * gridDim.x; };
+	int issued[S], seen[S];  // leader: loads issued and done phases seen per slot
+#pragma unroll
+	for (int s = 0; s < S; s++) issued[s] = seen[s] = 0;
+	auto load = [&](int s, long long tl) {
+		const int st = (int)(tl / nct), x = (int)(tl % nct) * W * U;
+		asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sh_u32(full + s)), "r"(TILE)
+				: "memory");
+#pragma unroll
+		for (int h = 0; h < N / BOX; h++) tma_load3(sh_u32(base + s * TILE + h * BOX * 128), &map, x, h * BOX, st,
+				sh_u32(full + s));
+		issued[s]++;
+	};
+	if (leader) {
+		asm volatile("prefetch.tensormap [%0];" ::"l"(&map) : "memory");
+		for (int s = 0; s < S; s++)
+			if (tile_of(s) < total) load(s, tile_of(s));
+	}
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
+	const R* m2 = reinterpret_cast<const R*>(a.mul2d);
+	const R* m1 = reinterpret_cast<const R*>(a.mul1d);
+	bool ok = true;
+	long long j = 0;
+	for (; tile_of(j) < total; j++) {
+		const long long tl = tile_of(j);
+		const int s = (int)(j % S);
+		const uint32_t par = (uint32_t)((j / S) & 1);
+		if (!mbar_wait_bounded(sh_u32(full + s), par)) {
+			ok = false;
+			break;
+		}
+		unsigned char* tile = base + s * TILE;
+		auto X = [&](int r) -> T& { return *reinterpret_cast<T*>(tile + swz<ES>(r, line)); };
+		const int col0 = (int)(tl % nct) * W;
+		T v[A];
+#pragma unroll
+		for (int i = 0; i < A; i++) v[i] = X(t + B * i);
+		if (a.mode == 0 || a.mode == 1) line_fft_x<R, A, B, -1>(v, t, X, xtw);
+		if (a.mode == 0) {
+			const bool valid = col0 + line < sx;
+#pragma unroll
+			for (int i = 0; i < A; i++) {
+				const int y = t + B * i;
+				const R f = !valid ? (R)0 : (m2 ? m2[y * sx + col0 + line] : m1[y]);
+				v[i] = cscale(v[i], f);
+			}
+		}
+		if (a.mode == 0 || a.mode == 2) line_fft_x<R, A, B, 1>(v, t, X, xtw);
+		__syncwarp();
+#pragma unroll
+		for (int i = 0; i < A; i++) X(t + B * i) = v[i];
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sh_u32(done + s)) : "memory");
+		if (leader) {
+			if (!mbar_wait_bounded(sh_u32(done + s), par)) {
+				ok = false;
+				break;
+			}
+			seen[s]++;
+			const int st = (int)(tl / nct), x = (int)(tl % nct) * W * U;
+#pragma unroll
+			for (int h = 0; h < N / BOX; h++) tma_store3(&map, x, h * BOX, st, sh_u32(tile + h * BOX * 128));
+			asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+			if (j >= 1) {
+				// the slot of tile j - 1: its store (the older group) has read it
+				asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+				const int s1 = (int)((j - 1) % S);
+				if (tile_of(j - 1 + S) < total) load(s1, tile_of(j - 1 + S));
+			}
+		}
+	}
+	if (!ok) atomicExch(a.err, ITP2D_E_TIMEOUT);
+	if (leader) {
+		// copies still in flight: loads not yet consumed (error path only), then
+		// every store
+		for (int s = 0; s < S; s++)
+			if (issued[s] > seen[s]) mbar_wait_bounded(sh_u32(full + s), (uint32_t)((issued[s] - 1) & 1));
+		asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+	}
 }
 
 // Energy sums of one element: Re, Im <psi|h>, <h|h>, |h - es psi|^2, <psi|psi>.
@@ -560,6 +753,65 @@ void col_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	col_reg_kernel<R, A, B, NBUF><<<grid_for(col_reg_kernel<R, A, B, NBUF>, sm, tiles), kThreads, sm, s>>>(a, k);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void* p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+				q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+	});
+	return fn;
+}
+
+constexpr int kTmaStages = 3;
+
+// Tensor map of a k x sy x sx complex state array in 8-byte units, boxes of
+// 16 units (128 bytes) by min(N, 256) rows, 128-byte swizzle.
+template <class R>
+bool encode_state_map(CUtensorMap* m, void* data, int sx, int sy, int k) {
+	auto enc = tensor_map_encoder();
+	if (!enc) return false;
+	constexpr int U = (int)sizeof(c2<R>) / 8;
+	const cuuint64_t dims[3] = {(cuuint64_t)sx * U, (cuuint64_t)sy, (cuuint64_t)k};
+	const cuuint64_t strides[2] = {(cuuint64_t)sx * U * 8, (cuuint64_t)sx * sy * U * 8};
+	const cuuint32_t box[3] = {16, (cuuint32_t)std::min(sy, 256), 1};
+	const cuuint32_t estr[3] = {1, 1, 1};
+	return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, data, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+	               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+	               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA column pass (lines of 256 or 512 points); false when it does not
+// apply (no tensor-map encoder, data not 16-byte aligned, rows not a
+// multiple of 16 bytes, no error word).
+template <class R, int A, int B>
+bool col_tma(const ColPassArgs& a, int k, cudaStream_t s) {
+	constexpr int N = A * B, ES = (int)sizeof(c2<R>), W = 128 / ES, S = kTmaStages;
+	static_assert(N <= 512, "three 128-byte tiles of the line must fit in shared memory");
+	if (a.sy != N || !a.err || (reinterpret_cast<uintptr_t>(a.data) & 15) || ((long long)a.sx * ES) % 16) return false;
+	CUtensorMap map;
+	if (!encode_state_map<R>(&map, a.data, a.sx, a.sy, k)) return false;
+	const size_t sm = 1024 + (size_t)S * N * 128 + N * sizeof(c2<R>) + 2 * S * sizeof(unsigned long long);
+	opt_in_smem(col_tma_kernel<R, A, B, S>, sm);
+	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
+	static int sms = 0;
+	if (!sms) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	}
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_tma_kernel<R, A, B, S>, W * B, sm);
+	const int grid = (int)std::max(1LL, std::min((long long)std::max(1, per_sm) * std::max(1, sms), tiles));
+	col_tma_kernel<R, A, B, S><<<grid, W * B, sm, s>>>(map, a, k);
+	return true;
+}
+
 template <class R, int A, int B>
 void energy_row_reg(const EnergyRowArgs& a, int k, cudaStream_t s) {
 	constexpr int N = A * B, LPI = kThreads / B;
@@ -650,6 +902,10 @@ bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s) {
 template <class R>
 bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	if (a.lp.kind != 0) return false;
+	if (a.variant == kColTma) {
+		if (a.sy == 256 && col_tma<R, 16, 16>(a, k, s)) return true;
+		if (a.sy == 512 && col_tma<R, 32, 16>(a, k, s)) return true;
+	}
 	switch (a.sy) {
 		case 32: col_reg<R, 8, 4>(a, k, s); return true;
 		case 64: col_reg<R, 8, 8>(a, k, s); return true;
@@ -661,6 +917,49 @@ bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	}
 }
 
+template <class R>
+int tune_col_pass_reg(ColPassArgs a, int k, cudaStream_t s) {
+	if (a.lp.kind != 0 || reg_threads(a.sy) == 0) return -1;
+	if (a.sy != 256 && a.sy != 512) return kColRegSmem;  // the only register variant at other sizes
+	cudaEvent_t e0, e1;
+	if (cudaEventCreate(&e0) != cudaSuccess) return kColRegSmem;
+	if (cudaEventCreate(&e1) != cudaSuccess) {
+		cudaEventDestroy(e0);
+		return kColRegSmem;
+	}
+	int best = kColRegSmem;
+	float best_ms = 0.0f;
+	for (int v = 0; v < kColVariants; v++) {
+		a.variant = v;
+		float ms = 0.0f;
+		bool ran = true;
+		for (int rep = 0; rep < 4 && ran; rep++) {  // the first run is a warm-up
+			cudaEventRecord(e0, s);
+			if (v == kColTma) {
+				ran = (a.sy == 256) ? col_tma<R, 16, 16>(a, k, s) : col_tma<R, 32, 16>(a, k, s);
+			} else {
+				if (a.sy == 256) col_reg<R, 16, 16>(a, k, s);
+				else col_reg<R, 32, 16>(a, k, s);
+			}
+			cudaEventRecord(e1, s);
+			if (cudaEventSynchronize(e1) != cudaSuccess) ran = false;
+			float t = 0.0f;
+			cudaEventElapsedTime(&t, e0, e1);
+			if (rep > 0) ms += t;
+		}
+		if (!ran || cudaGetLastError() != cudaSuccess) continue;
+		if (v == kColRegSmem || ms < best_ms) {
+			best = v;
+			best_ms = ms;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	return best;
+}
+
+template int tune_col_pass_reg<double>(ColPassArgs, int, cudaStream_t);
+template int tune_col_pass_reg<float>(ColPassArgs, int, cudaStream_t);
 template bool launch_row_pass_reg<double>(const RowPassArgs&, int, cudaStream_t);
 template bool launch_row_pass_reg<float>(const RowPassArgs&, int, cudaStream_t);
 template bool launch_col_pass_reg<double>(const ColPassArgs&, int, cudaStream_t);

@@ -40,7 +40,13 @@ struct ColPassArgs {
 	long long G;
 	int cols_per_tile;
 	LinePlan lp;
+	// register-FFT column pass variant (rfft.cu): kColRegSmem stages tiles
+	// through registers, kColTma by TMA (tune_col_pass_reg picks one per size)
+	int variant = 0;
+	int* err = nullptr;  // device status word for the TMA variant's bounded waits
 };
+
+enum { kColRegSmem = 0, kColTma = 1, kColVariants = 2 };
 
 // Energy pass over rows, producing h = H psi pieces and per-tile sums.
 //   src_t: array whose rows are transformed (psi or a partially transformed
@@ -118,6 +124,10 @@ template <class R> void launch_row_pass(const RowPassArgs& a, int k, const void*
 // of two); return false, launching nothing, for other lines.
 template <class R> bool launch_row_pass_reg(const RowPassArgs& a, int k, cudaStream_t s);
 template <class R> bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s);
+// Times the register-FFT column pass variants of `a` (its data pointer is a
+// scratch state array of k states, overwritten) and returns the fastest, or
+// -1 if the size has no register path.
+template <class R> int tune_col_pass_reg(ColPassArgs a, int k, cudaStream_t s);
 // Register-FFT energy passes; they run when the tile size equals
 // energy_row_tile_reg / energy_col_tile_reg (non-zero for supported lines).
 int energy_row_tile_reg(const LinePlan& lp, int sy);

@@ -126,3 +126,28 @@ def test_potential_descriptions_checked_like_the_reference():
                     ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     assert add(9, 16, 16, 0.1, 1, ctypes.c_void_p(1), 1.0, 1.0, ctypes.c_void_p(1), None) == capi.E_INVALID
     assert add(1, 16, 16, 0.1, 0, None, 1.0, 1.0, ctypes.c_void_p(1), None) == capi.OK
+
+
+def test_parameter_defaults_match_the_reference_and_leave_extensions_off():
+    """itp2d_parameters_default gives the reference's defaults
+    (parameters.cpp:25-55) and leaves every extension off: canonical
+    orthonormalisation every step, Lowdin between (unused), no Rayleigh-Ritz
+    step at the switch, FP32 sweeps at the solve's own time step."""
+    from itp2d_b200 import system
+    p = system._Params()
+    system._lib().itp2d_parameters_default(ctypes.byref(p))
+    assert (p.halforder, p.num_states, p.wanted, p.max_steps) == (5, 25, 16, 50)
+    assert p.eps_divisor == 5.0 and p.min_eps == 1e-9
+    assert p.precision == capi.FP64 and p.fp32_switch == 0.0
+    assert p.fp32_canonical_every == 0 and p.fp32_between == capi.BETWEEN_LOWDIN
+    assert p.switch_rayleigh_ritz == 0 and p.fp32_eps_factor == 1.0
+    assert p.timestep_test == b"relstdev(1e-3,1e-4)" and p.final_test == b"relstdev(1e-3,0)"
+
+
+def test_signal_flags_are_process_wide_ints():
+    """The abort and save flags the handlers raise are two distinct
+    sig_atomic_t (int) objects owned by the library, lowered at load."""
+    from itp2d_b200 import system
+    a, s = system.abort_flag(), system.save_flag()
+    assert ctypes.addressof(a.contents) != ctypes.addressof(s.contents)
+    assert a[0] in (0, 1) and s[0] in (0, 1)

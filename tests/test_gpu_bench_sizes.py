@@ -86,6 +86,7 @@ def test_fp64_step_matches_oracle(capi, cfg):
     g, V, psi, bt, B, m, eps = setup(cfg)
     prop, hpsi, pn, E_ref, sd_ref, res_ref = oracle_outputs(cfg)
     c = capi.Context(g.sx, g.sy, g.dx, K, bt, B, m)
+    c.set_column_variant(capi.COL_SMEM)
     c.set_potential(V)
     c.set_time_step(eps)
     c.upload(psi)
@@ -120,6 +121,7 @@ def test_fp32_form_step_matches_fp64_oracle(capi, cfg):
     g, V, psi, bt, B, m, eps = setup(cfg)
     prop, hpsi, pn, E_ref, sd_ref, res_ref = oracle_outputs(cfg)
     c = capi.Context(g.sx, g.sy, g.dx, K, bt, B, m, capi.FP32)
+    c.set_column_variant(capi.COL_SMEM)
     c.set_potential(V)
     c.set_time_step(eps)
     c.upload(psi)
@@ -166,3 +168,58 @@ def test_fp64_step_matches_compiled_reference(capi, cfg):
     c.upload(psi)
     c.apply_hamiltonian()
     assert per_state_rel(c.download(), hpsi) < 1e-12
+
+
+# the grids whose column lines take the TMA pass (256 and 512 points, periodic)
+TMA_SIZES = [c for c in SIZES if c[3] == O.PERIODIC and c[1] in (256, 512)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("cfg", TMA_SIZES, ids=[f"{c[0]}x{c[1]}_B{c[4]}_m{c[5]}" for c in TMA_SIZES])
+def test_tma_column_pass_matches_staged_pass(capi, cfg, precision):
+    """The TMA column pass (tiles moved by cp.async.bulk.tensor through a
+    three-slot ring) gives the same step as the register-staged pass, bit for
+    bit: both run the same line transforms on the same values. Checked on the
+    propagation (mode 0 passes with the kinetic tables) and on the
+    Hamiltonian, with k = 37 states (ragged last tiles of a CTA's ring)."""
+    g, V, psi, bt, B, m, eps = setup(cfg)
+    rng = np.random.default_rng(5)
+    psi = np.concatenate([psi] * 13)[:37] * (1 + 0.1 * rng.standard_normal((37, 1, 1)))
+    out = {}
+    for variant in (capi.COL_SMEM, capi.COL_TMA):
+        c = capi.Context(g.sx, g.sy, g.dx, 37, bt, B, m, capi.FP64 if precision == "fp64" else capi.FP32)
+        c.set_column_variant(variant)
+        assert c.column_variant == variant
+        c.set_potential(V)
+        c.set_time_step(eps)
+        c.upload(psi)
+        c.propagate()
+        a = c.download()
+        c.apply_hamiltonian()
+        out[variant] = (a, c.download(), c.energies()[0])
+        c.close()
+    for x, y in zip(out[capi.COL_SMEM], out[capi.COL_TMA]):
+        assert np.array_equal(x, y)
+    # and the TMA step against the oracle
+    prop = O.MultiProductSplit(g, V, bt, B, m, eps).apply(psi)
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    assert per_state_rel(out[capi.COL_TMA][0], prop) < tol
+
+
+def test_column_variant_is_tuned_at_the_first_time_step(capi):
+    """The first time step of a precision times both column passes at the
+    bumpy-dot grid and keeps one of them; -1 restores the tuned choice after a
+    forced one; out-of-range variants are refused."""
+    g, V, psi, bt, B, m, eps = setup(SIZES[3])
+    c = capi.Context(g.sx, g.sy, g.dx, 64, bt, B, m, capi.FP32)
+    c.set_potential(V)
+    c.set_time_step(eps)
+    tuned = c.column_variant
+    assert tuned in (capi.COL_SMEM, capi.COL_TMA)
+    c.set_column_variant(1 - tuned)
+    assert c.column_variant == 1 - tuned
+    c.set_column_variant(-1)
+    assert c.column_variant == tuned
+    with pytest.raises(capi.ITP2DError):
+        c.set_column_variant(2)
+    print(f"bumpy-dot grid, FP32: column variant {tuned}")
