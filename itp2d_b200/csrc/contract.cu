@@ -169,7 +169,7 @@ __global__ void overlap_finish_kernel(const double2* __restrict__ part, int k, i
 // and 68 (8-byte elements) make the transposed fragment reads conflict-free.
 template <class T>
 __global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__ W, const T* __restrict__ psi,
-		int k, long long G, T* __restrict__ out) {
+		int k, long long G, T* __restrict__ out, int upper) {
 	constexpr int PW = 66, PP = sizeof(T) == 16 ? 66 : 68;
 	constexpr int SW = kBK * PW * (int)sizeof(double2), SP = kBK * PP * (int)sizeof(T);
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -203,11 +203,14 @@ __global__ void __launch_bounds__(256) rotate_kernel(const double2* __restrict__
 			else dp[ii * PP + cc] = T{0, 0};
 		}
 	};
+	// upper-triangular W (Cholesky): rows i > n are zero, so the i range ends
+	// with this tile's last output state
+	const int kend = upper ? min(k, n0 + kBM) : k;
 	int cur = 0;
 	fetch(0, 0);
 	cp_async_commit();
-	for (int i0 = 0; i0 < k; i0 += kBK) {
-		if (i0 + kBK < k) fetch(cur ^ 1, i0 + kBK);
+	for (int i0 = 0; i0 < kend; i0 += kBK) {
+		if (i0 + kBK < kend) fetch(cur ^ 1, i0 + kBK);
 		cp_async_commit();
 		cp_async_wait<1>();
 		__syncthreads();
@@ -345,11 +348,11 @@ void launch_overlap_finish(const double2* part, int k, int nsplit, double dx2, d
 }
 
 template <class T>
-void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s) {
+void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s, bool upper) {
 	const dim3 grid((k + kBM - 1) / kBM, (unsigned)((G + kBN - 1) / kBN));
 	const size_t sm = (size_t)2 * kBK * (66 * sizeof(double2) + (sizeof(T) == 16 ? 66 : 68) * sizeof(T));
 	cudaFuncSetAttribute(rotate_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-	rotate_kernel<T><<<grid, 256, sm, s>>>(W, psi, k, G, out);
+	rotate_kernel<T><<<grid, 256, sm, s>>>(W, psi, k, G, out, upper ? 1 : 0);
 }
 
 template <class T>
@@ -370,8 +373,8 @@ template void launch_overlap<double2>(const double2*, int, long long, const int2
 		double2*, cudaStream_t, const double2*);
 template void launch_overlap<float2>(const float2*, int, long long, const int2*, int, int, double2*, double,
 		double2*, cudaStream_t, const float2*);
-template void launch_rotate<double2>(const double2*, const double2*, int, long long, double2*, cudaStream_t);
-template void launch_rotate<float2>(const double2*, const float2*, int, long long, float2*, cudaStream_t);
+template void launch_rotate<double2>(const double2*, const double2*, int, long long, double2*, cudaStream_t, bool);
+template void launch_rotate<float2>(const double2*, const float2*, int, long long, float2*, cudaStream_t, bool);
 template void launch_normalize1<double2>(double2*, long long, double, double*, cudaStream_t);
 template void launch_normalize1<float2>(float2*, long long, double, double*, cudaStream_t);
 

@@ -14,8 +14,10 @@ int overlap_splits(int k, long long G, int num_sms);
 template <class T>
 void launch_overlap(const T* psi, int k, long long G, const int2* pairs, int npairs, int nsplit,
 		double2* part, double dx2, double2* S, cudaStream_t s, const T* psib = nullptr);
+// out = psi W (FP64 DMMA); upper: W is upper triangular (Cholesky), so output
+// tile n reads only states i < n0 + 64.
 template <class T>
-void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s);
+void launch_rotate(const double2* W, const T* psi, int k, long long G, T* out, cudaStream_t s, bool upper = false);
 // Sums the nsplit partial k x k blocks of part (upper triangle i <= j used),
 // scales by dx2 and writes the full Hermitian S.
 void launch_overlap_finish(const double2* part, int k, int nsplit, double dx2, double2* S, cudaStream_t s);
@@ -29,7 +31,7 @@ void launch_overlap_tc(const float2* psi, int k, long long G, int nsplit, double
 // wsplit: tc_wsplit_bytes(k) bytes of device scratch (W^T split into BF16 planes).
 size_t tc_wsplit_bytes(int k);
 void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit, float2* out,
-		int* err, cudaStream_t s);
+		int* err, cudaStream_t s, bool upper = false);
 
 template <class T>
 void launch_normalize1(T* psi, long long G, double dx, double* tmp, cudaStream_t s);

@@ -1096,15 +1096,18 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 }
 
 // psi <- psi W by the rotation engine of the precision (into acc, swapped on
-// success); the tensor-core rotation's status when it fails.
-static int rotate_states(itp2d_ctx* c, bool tc) {
+// success); the tensor-core rotation's status when it fails. upper: W is
+// upper triangular (Cholesky), each output tile reads only the states up to
+// its own last one (about half the products).
+static int rotate_states(itp2d_ctx* c, bool tc, bool upper = false) {
 	const bool f64 = c->precision == ITP2D_FP64;
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
-			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream);
-		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
-		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
+			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream,
+					upper);
+		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream, upper);
+		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream, upper);
 		c->launches += tc ? 2 : 1;
 	}
 	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1165,7 +1168,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		const int st = cholesky_w(c, bad_index, bad_value);
 		if (st != ITP2D_OK) return st;
 		c->ortho_calls[2]++;
-		return rotate_states(c, tc);
+		return rotate_states(c, tc, true);
 	}
 	const bool between = !f64 && c->canonical_every > 1 && c->since_canonical + 1 < c->canonical_every;
 	// FP32 form between canonical steps, Gram-Schmidt order: taken whenever
@@ -1173,7 +1176,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	if (between && c->between == ITP2D_BETWEEN_CHOLESKY && cholesky_w(c, nullptr, nullptr) == ITP2D_OK) {
 		c->since_canonical++;
 		c->ortho_calls[2]++;
-		return rotate_states(c, tc);
+		return rotate_states(c, tc, true);
 	}
 	// FP32 form between canonical steps: W = D (I + E)^{-1/2} to second order
 	// when the normalised overlap is close enough to the identity

@@ -457,11 +457,13 @@ __global__ void split_w_kernel(const double2* __restrict__ W, int k, int ksteps,
 // Rotation tile: out rows n0.. (state index n), columns gt0.. (grid points).
 // A = W^T from the pre-split planes, B[g][i] = psi_i[g].
 __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned char* __restrict__ wsplit,
-		const float2* __restrict__ psi, int k, long long G, float2* __restrict__ out, int* err) {
+		const float2* __restrict__ psi, int k, long long G, float2* __restrict__ out, int* err, int upper) {
 	TcShared& sh = tc_shared();
 	const int n0 = blockIdx.x * TM;
 	const long long gt0 = (long long)blockIdx.y * TN;
 	const int nsteps = (k + KT - 1) / KT;
+	// upper-triangular W (Cholesky): states i >= n0 + TM do not contribute
+	const int nrun = upper ? (min(k, n0 + TM) + KT - 1) / KT : nsteps;
 	tc_setup(sh);
 	const int tid = threadIdx.x;
 	unsigned char* const base = sh.buf;
@@ -510,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned c
 	};
 	auto a_addr = [&](int s) { return smem_u32(base + kRoA + (s & 3) * kOperandBytes); };
 	auto b_addr = [&](int s) { return smem_u32(base + kRoB + (s & 1) * kOperandBytes); };
-	run_pipeline(sh, nsteps, false, prefetch, convert, a_addr, b_addr, err);
+	run_pipeline(sh, nrun, false, prefetch, convert, a_addr, b_addr, err);
 	if (!sh.abort) {
 		store_tile(sh, [&](int r, int c, double re, double im) {
 			const int n = n0 + r;
@@ -589,13 +591,13 @@ void launch_overlap_tc(const float2* psi, int k, long long G, int nsplit, double
 }
 
 void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit, float2* out,
-		int* err, cudaStream_t s) {
+		int* err, cudaStream_t s, bool upper) {
 	const int nt = (k + TM - 1) / TM, ks = (k + KT - 1) / KT;
 	const long long threads = (long long)nt * ks * 32 * 32;
 	split_w_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(W, k, ks, nt, wsplit);
 	set_tc_attributes();
 	const dim3 grid(nt, (unsigned)((G + TN - 1) / TN));
-	rotate_tc_kernel<<<grid, kThreads, tc_smem(), s>>>(wsplit, psi, k, G, out, err);
+	rotate_tc_kernel<<<grid, kThreads, tc_smem(), s>>>(wsplit, psi, k, G, out, err, upper ? 1 : 0);
 }
 
 }  // namespace itp2d
