@@ -168,8 +168,7 @@ int itp2d_set_precision(itp2d_ctx* ctx, int precision);
 int itp2d_rayleigh_ritz(itp2d_ctx* ctx, double* ritz_values);
 
 /* Column passes of periodic 256- and 512-point lines: tiles staged through
- * registers and shared memory (0), or moved by TMA through a three-slot ring
- * with one (1) or two (2) groups of transform threads per CTA.
+ * registers and shared memory (0) or moved by TMA with a three-slot ring (1).
  * The first itp2d_set_time_step of each precision times both on the spare
  * state buffer and keeps the faster; variant >= 0 forces one, -1 restores the
  * tuned choice. itp2d_column_variant returns the variant in use. */

@@ -25,7 +25,7 @@ PERIODIC, DIRICHLET = 0, 1
 FP64, FP32 = 0, 1
 ORTHO_DEFAULT, ORTHO_HIGHMEM, ORTHO_CHOLESKY = 0, 1, 2
 BETWEEN_LOWDIN, BETWEEN_CHOLESKY = 0, 1
-COL_SMEM, COL_TMA, COL_TMA2 = 0, 1, 2
+COL_SMEM, COL_TMA = 0, 1
 CONTRACT_AUTO, CONTRACT_FP64 = 0, 1
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
@@ -224,7 +224,7 @@ class Context:
                "itp2d_set_fp32_orthonormalization")
 
     def set_column_variant(self, variant):
-        """Column pass of 256/512-point lines: COL_SMEM, COL_TMA, COL_TMA2, or -1 (tuned)."""
+        """Column pass of 256/512-point lines: COL_SMEM, COL_TMA, or -1 (tuned)."""
         _check(lib().itp2d_set_column_variant(self.h, int(variant)), "itp2d_set_column_variant")
 
     @property

@@ -409,28 +409,24 @@ __device__ __forceinline__ uint32_t swz(int r, int c) {
 	return (uint32_t)(r * 128 + ((((byte >> 4) ^ (r & 7))) << 4) + (byte & 15));
 }
 
-template <class R, int A, int B, int S, int H>
-__global__ void __launch_bounds__(H * (128 / (2 * (int)sizeof(R))) * B)
+template <class R, int A, int B, int S>
+__global__ void __launch_bounds__((128 / (2 * (int)sizeof(R))) * B)
 		col_tma_kernel(const __grid_constant__ CUtensorMap map, ColPassArgs a, int k) {
 	using T = c2<R>;
 	constexpr int ES = (int)sizeof(T), N = A * B, W = 128 / ES, NT = W * B;
 	constexpr int TILE = N * 128, BOX = N < 256 ? N : 256, U = ES / 8;
-	static_assert(S <= 4 && H <= S, "slot ring");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	unsigned char* base =
 			reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
 	T* xtw = reinterpret_cast<T*>(base + S * TILE);
 	unsigned long long* full = reinterpret_cast<unsigned long long*>(xtw + N);
 	unsigned long long* done = full + S;
-	__shared__ int sh_issued[4], sh_consumed[4];  // loads issued into / consumed from each slot
 	load_xtw<R, A, B>(xtw, reinterpret_cast<const T*>(a.lp.fft.tw));
-	const int g = threadIdx.x / NT, lt = threadIdx.x % NT;  // group, thread within the group
-	const bool leader = lt == 0;                             // issues its group's copies
-	if (threadIdx.x == 0) {
+	const bool leader = threadIdx.x == 0;
+	if (leader) {
 		for (int s = 0; s < S; s++) {
 			asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_u32(full + s)), "r"(1) : "memory");
 			asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_u32(done + s)), "r"(NT) : "memory");
-			sh_issued[s] = sh_consumed[s] = 0;
 		}
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -439,6 +435,9 @@ __global__ void __launch_bounds__(H * (128 / (2 * (int)sizeof(R))) * B)
 	const int nct = (sx + W - 1) / W;
 	const long long total = (long long)k * nct;
 	auto tile_of = [&](long long j) { return (long long)blockIdx.x + j * gridDim.x; };
+	int issued[S], seen[S];  // leader: loads issued and done phases seen per slot
+#pragma unroll
+	for (int s = 0; s < S; s++) issued[s] = seen[s] = 0;
 	auto load = [&](int s, long long tl) {
 		const int st = (int)(tl / nct), x = (int)(tl % nct) * W * U;
 		asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sh_u32(full + s)), "r"(TILE)
@@ -446,19 +445,19 @@ __global__ void __launch_bounds__(H * (128 / (2 * (int)sizeof(R))) * B)
 #pragma unroll
 		for (int h = 0; h < N / BOX; h++) tma_load3(sh_u32(base + s * TILE + h * BOX * 128), &map, x, h * BOX, st,
 				sh_u32(full + s));
-		atomicAdd(&sh_issued[s], 1);
+		issued[s]++;
 	};
-	if (threadIdx.x == 0) {
+	if (leader) {
 		asm volatile("prefetch.tensormap [%0];" ::"l"(&map) : "memory");
 		for (int s = 0; s < S; s++)
 			if (tile_of(s) < total) load(s, tile_of(s));
 	}
-	const int line = lt / B, t = lt % B;
+	const int line = threadIdx.x / B, t = threadIdx.x % B;
 	const R* m2 = reinterpret_cast<const R*>(a.mul2d);
 	const R* m1 = reinterpret_cast<const R*>(a.mul1d);
 	bool ok = true;
-	// group g takes tiles j = g, g + H, ...; tile j sits in slot j mod S
-	for (long long j = g; tile_of(j) < total; j += H) {
+	long long j = 0;
+	for (; tile_of(j) < total; j++) {
 		const long long tl = tile_of(j);
 		const int s = (int)(j % S);
 		const uint32_t par = (uint32_t)((j / S) & 1);
@@ -493,33 +492,26 @@ __global__ void __launch_bounds__(H * (128 / (2 * (int)sizeof(R))) * B)
 				ok = false;
 				break;
 			}
-			atomicAdd(&sh_consumed[s], 1);
+			seen[s]++;
 			const int st = (int)(tl / nct), x = (int)(tl % nct) * W * U;
 #pragma unroll
 			for (int h = 0; h < N / BOX; h++) tma_store3(&map, x, h * BOX, st, sh_u32(tile + h * BOX * 128));
 			asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-			if (H == 1) {
-				// refill the slot of the previous tile, whose store (the older
-				// group) has finished reading it by now
-				if (j >= 1) {
-					asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-					if (tile_of(j - 1 + S) < total) load((int)((j - 1) % S), tile_of(j - 1 + S));
-				}
-			} else {
-				// another group takes tile j + S next: refill this slot as soon as
-				// its store has read it
-				asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-				if (tile_of(j + S) < total) load(s, tile_of(j + S));
+			if (j >= 1) {
+				// the slot of tile j - 1: its store (the older group) has read it
+				asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+				const int s1 = (int)((j - 1) % S);
+				if (tile_of(j - 1 + S) < total) load(s1, tile_of(j - 1 + S));
 			}
 		}
 	}
 	if (!ok) atomicExch(a.err, ITP2D_E_TIMEOUT);
-	if (leader) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this leader's stores
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		// loads still in flight (error path only) land before the CTA exits
+	if (leader) {
+		// copies still in flight: loads not yet consumed (error path only), then
+		// every store
 		for (int s = 0; s < S; s++)
-			if (sh_issued[s] > sh_consumed[s]) mbar_wait_bounded(sh_u32(full + s), (uint32_t)((sh_issued[s] - 1) & 1));
+			if (issued[s] > seen[s]) mbar_wait_bounded(sh_u32(full + s), (uint32_t)((issued[s] - 1) & 1));
+		asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 	}
 }
 
@@ -797,7 +789,7 @@ bool encode_state_map(CUtensorMap* m, void* data, int sx, int sy, int k) {
 // The TMA column pass (lines of 256 or 512 points); false when it does not
 // apply (no tensor-map encoder, data not 16-byte aligned, rows not a
 // multiple of 16 bytes, no error word).
-template <class R, int A, int B, int H>
+template <class R, int A, int B>
 bool col_tma(const ColPassArgs& a, int k, cudaStream_t s) {
 	constexpr int N = A * B, ES = (int)sizeof(c2<R>), W = 128 / ES, S = kTmaStages;
 	static_assert(N <= 512, "three 128-byte tiles of the line must fit in shared memory");
@@ -805,7 +797,7 @@ bool col_tma(const ColPassArgs& a, int k, cudaStream_t s) {
 	CUtensorMap map;
 	if (!encode_state_map<R>(&map, a.data, a.sx, a.sy, k)) return false;
 	const size_t sm = 1024 + (size_t)S * N * 128 + N * sizeof(c2<R>) + 2 * S * sizeof(unsigned long long);
-	opt_in_smem(col_tma_kernel<R, A, B, S, H>, sm);
+	opt_in_smem(col_tma_kernel<R, A, B, S>, sm);
 	const long long tiles = (long long)k * ((a.sx + W - 1) / W);
 	static int sms = 0;
 	if (!sms) {
@@ -814,10 +806,9 @@ bool col_tma(const ColPassArgs& a, int k, cudaStream_t s) {
 		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
 	int per_sm = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_tma_kernel<R, A, B, S, H>, H * W * B, sm);
-	if (per_sm < 1) return false;
-	const int grid = (int)std::max(1LL, std::min((long long)per_sm * std::max(1, sms), (tiles + H - 1) / H));
-	col_tma_kernel<R, A, B, S, H><<<grid, H * W * B, sm, s>>>(map, a, k);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_tma_kernel<R, A, B, S>, W * B, sm);
+	const int grid = (int)std::max(1LL, std::min((long long)std::max(1, per_sm) * std::max(1, sms), tiles));
+	col_tma_kernel<R, A, B, S><<<grid, W * B, sm, s>>>(map, a, k);
 	return true;
 }
 
@@ -912,12 +903,8 @@ template <class R>
 bool launch_col_pass_reg(const ColPassArgs& a, int k, cudaStream_t s) {
 	if (a.lp.kind != 0) return false;
 	if (a.variant == kColTma) {
-		if (a.sy == 256 && col_tma<R, 16, 16, 1>(a, k, s)) return true;
-		if (a.sy == 512 && col_tma<R, 32, 16, 1>(a, k, s)) return true;
-	}
-	if (a.variant == kColTma2) {
-		if (a.sy == 256 && col_tma<R, 16, 16, 2>(a, k, s)) return true;
-		if (a.sy == 512 && col_tma<R, 32, 16, 2>(a, k, s)) return true;
+		if (a.sy == 256 && col_tma<R, 16, 16>(a, k, s)) return true;
+		if (a.sy == 512 && col_tma<R, 32, 16>(a, k, s)) return true;
 	}
 	switch (a.sy) {
 		case 32: col_reg<R, 8, 4>(a, k, s); return true;
@@ -949,9 +936,7 @@ int tune_col_pass_reg(ColPassArgs a, int k, cudaStream_t s) {
 		for (int rep = 0; rep < 4 && ran; rep++) {  // the first run is a warm-up
 			cudaEventRecord(e0, s);
 			if (v == kColTma) {
-				ran = (a.sy == 256) ? col_tma<R, 16, 16, 1>(a, k, s) : col_tma<R, 32, 16, 1>(a, k, s);
-			} else if (v == kColTma2) {
-				ran = (a.sy == 256) ? col_tma<R, 16, 16, 2>(a, k, s) : col_tma<R, 32, 16, 2>(a, k, s);
+				ran = (a.sy == 256) ? col_tma<R, 16, 16>(a, k, s) : col_tma<R, 32, 16>(a, k, s);
 			} else {
 				if (a.sy == 256) col_reg<R, 16, 16>(a, k, s);
 				else col_reg<R, 32, 16>(a, k, s);

@@ -41,13 +41,12 @@ struct ColPassArgs {
 	int cols_per_tile;
 	LinePlan lp;
 	// register-FFT column pass variant (rfft.cu): kColRegSmem stages tiles
-	// through registers, kColTma / kColTma2 by TMA with one / two groups of
-	// transform threads per CTA (tune_col_pass_reg picks one per size)
+	// through registers, kColTma by TMA (tune_col_pass_reg picks one per size)
 	int variant = 0;
 	int* err = nullptr;  // device status word for the TMA variant's bounded waits
 };
 
-enum { kColRegSmem = 0, kColTma = 1, kColTma2 = 2, kColVariants = 3 };
+enum { kColRegSmem = 0, kColTma = 1, kColVariants = 2 };
 
 // Energy pass over rows, producing h = H psi pieces and per-tile sums.
 //   src_t: array whose rows are transformed (psi or a partially transformed

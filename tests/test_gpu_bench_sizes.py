@@ -177,16 +177,16 @@ TMA_SIZES = [c for c in SIZES if c[3] == O.PERIODIC and c[1] in (256, 512)]
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("cfg", TMA_SIZES, ids=[f"{c[0]}x{c[1]}_B{c[4]}_m{c[5]}" for c in TMA_SIZES])
 def test_tma_column_pass_matches_staged_pass(capi, cfg, precision):
-    """The TMA column passes (tiles moved by cp.async.bulk.tensor through a
-    three-slot ring, one or two groups of transform threads per CTA) give the
-    same step as the register-staged pass, bit for bit: both run the same line transforms on the same values. Checked on the
+    """The TMA column pass (tiles moved by cp.async.bulk.tensor through a
+    three-slot ring) gives the same step as the register-staged pass, bit for
+    bit: both run the same line transforms on the same values. Checked on the
     propagation (mode 0 passes with the kinetic tables) and on the
     Hamiltonian, with k = 37 states (ragged last tiles of a CTA's ring)."""
     g, V, psi, bt, B, m, eps = setup(cfg)
     rng = np.random.default_rng(5)
     psi = np.concatenate([psi] * 13)[:37] * (1 + 0.1 * rng.standard_normal((37, 1, 1)))
     out = {}
-    for variant in (capi.COL_SMEM, capi.COL_TMA, capi.COL_TMA2):
+    for variant in (capi.COL_SMEM, capi.COL_TMA):
         c = capi.Context(g.sx, g.sy, g.dx, 37, bt, B, m, capi.FP64 if precision == "fp64" else capi.FP32)
         c.set_column_variant(variant)
         assert c.column_variant == variant
@@ -198,9 +198,8 @@ def test_tma_column_pass_matches_staged_pass(capi, cfg, precision):
         c.apply_hamiltonian()
         out[variant] = (a, c.download(), c.energies()[0])
         c.close()
-    for variant in (capi.COL_TMA, capi.COL_TMA2):
-        for x, y in zip(out[capi.COL_SMEM], out[variant]):
-            assert np.array_equal(x, y)
+    for x, y in zip(out[capi.COL_SMEM], out[capi.COL_TMA]):
+        assert np.array_equal(x, y)
     # and the TMA step against the oracle
     prop = O.MultiProductSplit(g, V, bt, B, m, eps).apply(psi)
     tol = 1e-12 if precision == "fp64" else 2e-5
@@ -216,12 +215,11 @@ def test_column_variant_is_tuned_at_the_first_time_step(capi):
     c.set_potential(V)
     c.set_time_step(eps)
     tuned = c.column_variant
-    assert tuned in (capi.COL_SMEM, capi.COL_TMA, capi.COL_TMA2)
-    other = (tuned + 1) % 3
-    c.set_column_variant(other)
-    assert c.column_variant == other
+    assert tuned in (capi.COL_SMEM, capi.COL_TMA)
+    c.set_column_variant(1 - tuned)
+    assert c.column_variant == 1 - tuned
     c.set_column_variant(-1)
     assert c.column_variant == tuned
     with pytest.raises(capi.ITP2DError):
-        c.set_column_variant(3)
+        c.set_column_variant(2)
     print(f"bumpy-dot grid, FP32: column variant {tuned}")
