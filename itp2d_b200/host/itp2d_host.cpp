@@ -355,8 +355,18 @@ void ITPSystem::orthonormalize() {
 					!(wanted_change(energies[energies.size() - 1], energies[energies.size() - 2], 1) < 1e-2);
 		check(itp2d_set_fp32_eig_tolerance(ctx, early ? 0.05 : 1e-3), "itp2d_set_fp32_eig_tolerance");
 	}
+	int algo = p.ortho_algorithm;
+	if (cholesky_pending && precision == ITP2D_FP64) {
+		// the first FP64 iteration after the FP32 form's switch: its task is to
+		// make the FP32-accurate states orthonormal in FP64, which a canonical
+		// step would do by rotating close pairs (a spurious energy change
+		// that the next step undoes); the canonical steps that follow decide
+		// convergence
+		algo = ITP2D_ORTHO_CHOLESKY;
+		cholesky_pending = false;
+	}
 	itp2d_orthonormalization_counts(ctx, &c0, nullptr, nullptr);
-	int st = itp2d_orthonormalize(ctx, p.ortho_algorithm, &bi, &bv);
+	int st = itp2d_orthonormalize(ctx, algo, &bi, &bv);
 	itp2d_orthonormalization_counts(ctx, &c1, nullptr, nullptr);
 	last_ortho_canonical = c1 > c0;
 	if (st == ITP2D_OK && ritz_pending && precision == ITP2D_FP64) {
@@ -554,6 +564,7 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 	step_counter = 0;
 	all_timestep_converged = false;
 	ritz_pending = p.switch_rayleigh_ritz != 0;
+	cholesky_pending = p.fp32_canonical_every > 1 && p.fp32_between == ITP2D_BETWEEN_CHOLESKY;
 	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
 }
 
@@ -740,6 +751,7 @@ void ITPSystem::reset(const double* init) {
 	fp32_best = INFINITY;
 	fp32_last = INFINITY;
 	ritz_pending = false;
+	cholesky_pending = false;
 	ritz_steps = 0;
 	fp32_stall = 0;
 	canonical_last.clear();

@@ -253,6 +253,7 @@ class ITPSystem {
 	int fp32_stall = 0;           // FP32 steps since that change last decreased
 	double fp32_last = INFINITY;  // the previous comparison's change
 	bool ritz_pending = false;    // a Rayleigh-Ritz step after the next FP64 orthonormalisation
+	bool cholesky_pending = false;  // the next FP64 orthonormalisation by Cholesky (after the switch)
 	bool last_ortho_canonical = true;               // the last orthonormalisation's form
 	// sorted energies of the last two canonical FP32 iterations and their steps
 	std::vector<double> canonical_last, canonical_prev;
