@@ -202,7 +202,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
     def sweeps():
         return {prec: L.itp2d_precision_sweeps(ctx, code) for prec, code in (("fp64", capi.FP64), ("fp32", capi.FP32))}
 
-    p0, l0, w0 = phases(), L.itp2d_launch_count(ctx), sweeps()
+    p0, l0, w0, t0 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -216,7 +216,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         steps.append(s.total_steps)
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
-    p1, l1, w1 = phases(), L.itp2d_launch_count(ctx), sweeps()
+    p1, l1, w1, t1 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
     # per solve: {(precision, phase): (ms, calls)}
     stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
@@ -233,6 +233,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     out = dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
+               tri={p: (t1[p] - t0[p]) / K for p in t1},
                launches=(l1 - l0) / K, E=E, e2e_times=e2e_times)
     s.close()
     return out
@@ -406,7 +407,11 @@ def config_block(form):
 
 # DRAM bytes (read + write) per launch of a phase's dominant kernel, from ncu
 # captures summarised under profiles/ (per workload; None where no capture).
-PROFILED_TRAFFIC = {"dot": {"eigensolve_fp32": 5.30e6, "eigensolve_fp64": 11.51e6}, "bumpy": {}}
+PROFILED_TRAFFIC = {"dot": {"eigensolve_fp32": 5.30e6, "eigensolve_fp64": 11.51e6},
+                    # the FP64 rotation's DRAM bytes per launch measured at k = 256 (2.10 GB:
+                    # the states read and written once), scaled to k = 2000 by the states
+                    # processed
+                    "bumpy": {"rotation_fp64": 2.10e9 * 2000 / 256, "overlap_fp64": 1.13e9 * 2000 / 256}}
 
 
 def max_over_ranks(x, dist, device):
@@ -438,7 +443,9 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
                  FP32 (tensor cores): BF16 MMA work issued, 24 MMAs of 128 x 128 x 16
                  per 16 grid points per upper-triangle tile pair of 128 states
       rotation   FP64: 8 k^2 G flops; FP32: 24 MMAs of 128 x 128 x 16 per 16 states
-                 per (128 states x 128 grid points) output tile
+                 per (128 states x 128 grid points) output tile; a rotation by the
+                 upper-triangular W of a Cholesky step counts only the states up
+                 to each output tile's last one (about half)
       eigensolve 10 k^3 flops per call (the algorithmic figure of a Hermitian
                  eigensolve); the block Jacobi method's own work, per sweep
                  (kp/16 - 1) rounds of 32 x 32 block unitaries applied to both
@@ -457,6 +464,9 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
     mma = 128 * 128 * 16 * 2
     tc_overlap = nt * (nt + 1) // 2 * 24 * mma * ((G + 15) // 16)
     tc_rotation = nt * ((G + 127) // 128) * ((k + 15) // 16) * 24 * mma
+    tc_rotation_tri = sum((min(k, 128 * (t + 1)) + 15) // 16 for t in range(nt)) * ((G + 127) // 128) * 24 * mma
+    nt64 = (k + 63) // 64
+    rotation_tri = 8 * G * sum(64 * min(k, 64 * (t + 1)) for t in range(nt64))
     kp = (k + 31) // 32 * 32
     sweep_flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp
     out = {}
@@ -474,14 +484,16 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
             if calls == 0:
                 continue
             sec = ms * 1e-3
+            total = amount * calls
+            if ph == "rotation" and r.get("tri", {}).get(prec, 0):
+                tri = min(r["tri"][prec], calls)
+                total = amount * (calls - tri) + (tc_rotation_tri if tc else rotation_tri) * tri
             if bound == "hbm":
-                ach, peak, unit, psrc = amount * calls / sec / 1e9, hbm, "GB/s", f"HBM copy ({src})"
+                ach, peak, unit, psrc = total / sec / 1e9, hbm, "GB/s", f"HBM copy ({src})"
             elif bound == "tensor_bf16":
-                ach, peak, unit, psrc = amount * calls / sec / 1e12, bf16, "TFLOP/s", \
-                    f"cuBLAS BF16 sustained ({src})"
+                ach, peak, unit, psrc = total / sec / 1e12, bf16, "TFLOP/s", f"cuBLAS BF16 sustained ({src})"
             else:
-                ach, peak, unit, psrc = amount * calls / sec / 1e12, fp64_peak, "TFLOP/s", \
-                    "FP64 DMMA measured in-run"
+                ach, peak, unit, psrc = total / sec / 1e12, fp64_peak, "TFLOP/s", "FP64 DMMA measured in-run"
             out[f"{ph}_{prec}"] = {"bound": "hbm" if bound == "hbm" else "tensor", "achieved": ach, "peak": peak,
                                    "unit": unit, "frac": ach / peak, "ms_per_solve": ms, "calls_per_solve": calls,
                                    "peak_source": psrc}

@@ -200,6 +200,9 @@ int itp2d_set_fp32_between(itp2d_ctx* ctx, int method);
  * about tau^2 remain). A looser tau suits the first iterations of a solve,
  * whose basis the next step replaces. FP64 states are not affected. */
 int itp2d_set_fp32_eig_tolerance(itp2d_ctx* ctx, double tau);
+/* Rotations by an upper-triangular W (Cholesky steps, about half the
+ * products of a dense rotation) since creation, per precision. */
+int itp2d_triangular_rotations(itp2d_ctx* ctx, long long* fp64, long long* fp32);
 /* Number of canonical, Lowdin and Cholesky orthonormalisations since
  * creation; any pointer may be NULL. */
 int itp2d_orthonormalization_counts(itp2d_ctx* ctx, long long* canonical, long long* lowdin, long long* cholesky);

@@ -74,6 +74,7 @@ def lib():
         L.itp2d_set_fp32_between.argtypes = [vp, i]
         L.itp2d_rayleigh_ritz.argtypes = [vp, dp]
         L.itp2d_set_column_variant.argtypes = [vp, i]
+        L.itp2d_triangular_rotations.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.itp2d_column_variant.argtypes = [vp]
         L.itp2d_overlap_matrix.argtypes = [vp, dp]
         L.itp2d_launch_count.argtypes = [vp]
@@ -142,6 +143,13 @@ def hermitian_eigensolve(A: np.ndarray):
 
 
 PHASES = ["propagate", "overlap", "eigensolve", "rotation", "energies"]
+
+
+def triangular_rotations(handle) -> dict:
+    """Rotations by an upper-triangular W per precision, {"fp64": n, "fp32": n}."""
+    a, b = C.c_longlong(0), C.c_longlong(0)
+    _check(lib().itp2d_triangular_rotations(handle, C.byref(a), C.byref(b)), "itp2d_triangular_rotations")
+    return {"fp64": a.value, "fp32": b.value}
 
 
 def phase_stats(handle) -> dict:

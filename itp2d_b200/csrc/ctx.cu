@@ -116,6 +116,7 @@ struct itp2d_ctx {
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
 	long long ortho_calls[3] = {0, 0, 0};  // canonical, Lowdin, Cholesky
 	long long ritz_calls = 0;              // Rayleigh-Ritz steps
+	long long tri_rot[2] = {0, 0};         // rotations by an upper-triangular W, per precision
 	// register-FFT column pass variant per precision (kColRegSmem / kColTma):
 	// -1 until tuned at the first time step of that precision
 	int col_variant[2] = {-1, -1};
@@ -1062,6 +1063,14 @@ int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
 	return ITP2D_OK;
 }
 
+int itp2d_triangular_rotations(itp2d_ctx* c, long long* fp64, long long* fp32) {
+	if (!c) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	if (fp64) *fp64 = c->tri_rot[ITP2D_FP64];
+	if (fp32) *fp32 = c->tri_rot[ITP2D_FP32];
+	return ITP2D_OK;
+}
+
 int itp2d_set_fp32_between(itp2d_ctx* c, int method) {
 	if (!c || (method != ITP2D_BETWEEN_LOWDIN && method != ITP2D_BETWEEN_CHOLESKY)) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
@@ -1101,6 +1110,7 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 // its own last one (about half the products).
 static int rotate_states(itp2d_ctx* c, bool tc, bool upper = false) {
 	const bool f64 = c->precision == ITP2D_FP64;
+	if (upper) c->tri_rot[c->precision]++;
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
