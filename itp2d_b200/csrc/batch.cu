@@ -1,6 +1,7 @@
 // Batched Hermitian eigensolver: the k x k overlap eigenproblems of many
 // independent state sets (each the ZHEEV call of StateSet::orthonormalize,
-// stateset.cpp:156-176) in one launch, one CTA per instance. Instances of
+// stateset.cpp:156-176) in one persistent launch, one CTA per instance at a
+// time (a work queue hands out the instances). Instances of
 // different k share the launch; no CTA waits for another, so the launch can
 // share the GPU with any other work (unlike the cooperative solvers of
 // jacobi.cu / bjacobi.cu, which serve one large matrix at a time).
@@ -19,6 +20,8 @@
 // (W[i * k + n]: coefficient of state i in output state n).
 #include "../../include/itp2d_gpu.h"
 #include "contract.cuh"
+
+#include <algorithm>
 
 namespace itp2d {
 
@@ -41,13 +44,12 @@ struct Rot {
 	int p, q;             // p < q; p < 0: no rotation
 };
 
-__global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEigItem* __restrict__ items, int n,
-		int max_sweeps, int smem_bytes) {
+// One instance, by the whole CTA.
+__device__ void solve_item(const BatchEigItem& it, int max_sweeps, int smem_bytes) {
 	__shared__ Rot rot[kMaxPairs / 4];  // pairs handled per chunk (see below)
 	__shared__ double red[kBThreads / 32];
 	__shared__ int s_bad, s_sweeps;
 	extern __shared__ __align__(16) double2 work[];
-	const BatchEigItem it = items[blockIdx.x];
 	const int k = it.k;
 	const int kp = (k + 1) & ~1;
 	const int np = kp / 2;
@@ -205,9 +207,28 @@ __global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEi
 	}
 }
 
+// Persistent work queue: every CTA takes the next instance from *next until
+// none is left. The host orders the instances by decreasing k (the longest
+// first), so uneven sizes finish together.
+__global__ void __launch_bounds__(kBThreads) batched_jacobi_kernel(const BatchEigItem* __restrict__ items, int n,
+		int max_sweeps, int smem_bytes, int* next) {
+	__shared__ int s_next;
+	for (;;) {
+		if (threadIdx.x == 0) s_next = atomicAdd(next, 1);
+		__syncthreads();
+		const int q = s_next;
+		__syncthreads();  // every thread has read s_next before it changes
+		if (q >= n) return;
+		const BatchEigItem it = items[q];
+		solve_item(it, max_sweeps, smem_bytes);
+		__syncthreads();
+	}
+}
+
 }  // namespace
 
-cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, cudaStream_t s) {
+cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, int* next,
+		cudaStream_t s) {
 	if (n <= 0) return cudaSuccess;
 	// dynamic shared memory for A and V of the largest instance, up to 200 KB
 	// (instances whose matrices do not fit use their global work matrices)
@@ -221,7 +242,18 @@ cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_
 				smem);
 		if (e != cudaSuccess) return e;
 	}
-	batched_jacobi_kernel<<<n, kBThreads, smem, s>>>(items, n, max_sweeps, smem);
+	static int sms = 0;
+	if (!sms) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	}
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_jacobi_kernel, kBThreads, smem);
+	const int grid = std::max(1, std::min(n, std::max(1, per_sm) * std::max(1, sms)));
+	cudaError_t e = cudaMemsetAsync(next, 0, sizeof(int), s);
+	if (e != cudaSuccess) return e;
+	batched_jacobi_kernel<<<grid, kBThreads, smem, s>>>(items, n, max_sweeps, smem, next);
 	return cudaGetLastError();
 }
 

@@ -142,8 +142,11 @@ struct BatchEigItem {
 	int pad;
 	double tau;
 };
-// max_k: the largest k among the items (sizes the shared-memory work area).
-cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, cudaStream_t s);
+// max_k: the largest k among the items (sizes the shared-memory work area);
+// next: a device int, the work queue's position (reset by the launch). Items
+// in decreasing k balance the CTAs best.
+cudaError_t launch_batched_eigensolve(const BatchEigItem* items, int n, int max_sweeps, int max_k, int* next,
+		cudaStream_t s);
 int batched_eigensolve_max_k();
 
 // Users of the cooperative eigensolvers (contexts and the standalone

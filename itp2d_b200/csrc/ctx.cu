@@ -1458,9 +1458,11 @@ cudaStream_t g_batch_stream = nullptr;
 BatchEigItem* g_items_host = nullptr;  // pinned
 BatchEigItem* g_items_dev = nullptr;
 int g_items_cap = 0;
+int* g_queue_dev = nullptr;  // the batched eigensolver's work-queue position
 
 int batch_resources(int n) {
 	if (!g_batch_stream) ITP2D_TRY(cudaStreamCreateWithFlags(&g_batch_stream, cudaStreamNonBlocking));
+	if (!g_queue_dev) ITP2D_TRY(cudaMalloc((void**)&g_queue_dev, sizeof(int)));
 	if (n > g_items_cap) {
 		if (g_items_host) cudaFreeHost(g_items_host);
 		if (g_items_dev) cudaFree(g_items_dev);
@@ -1521,12 +1523,15 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 		it.pad = 0;
 		it.tau = c->precision == ITP2D_FP64 ? 3e-9 : 1e-3;
 	}
-	// every eigenproblem in one launch
+	// every eigenproblem in one launch, the largest first (the work queue hands
+	// them out in this order)
+	std::stable_sort(g_items_host, g_items_host + n,
+			[](const BatchEigItem& a, const BatchEigItem& b) { return a.k > b.k; });
 	cudaError_t e = cudaMemcpyAsync(g_items_dev, g_items_host, n * sizeof(BatchEigItem), cudaMemcpyHostToDevice,
 			g_batch_stream);
 	int max_k = 2;
 	for (int i = 0; i < n; i++) max_k = std::max(max_k, ctxs[i]->k);
-	if (e == cudaSuccess) e = launch_batched_eigensolve(g_items_dev, n, 60, max_k, g_batch_stream);
+	if (e == cudaSuccess) e = launch_batched_eigensolve(g_items_dev, n, 60, max_k, g_queue_dev, g_batch_stream);
 	if (e == cudaSuccess) e = cudaEventRecord(ev[n], g_batch_stream);
 	if (e != cudaSuccess) {
 		cleanup();
@@ -1636,7 +1641,8 @@ namespace {
 
 constexpr int kLoopThreads = 1024;
 
-// loop[0] iterations done, loop[1] done, loop[2] status, loop[3] history length
+// loop[0] iterations done, loop[1] done, loop[2] status, loop[3] history length,
+// loop[7] the batched eigensolver's work-queue position
 __global__ void __launch_bounds__(kLoopThreads) loop_test_kernel(const double* __restrict__ E,
 		const double* __restrict__ S, int k, int first, int count, int test, double limit, double diff_limit,
 		int max_iterations, double* curE, double* curS, double* prevE, double* prevS, int* idx, int* flags,
@@ -1779,7 +1785,7 @@ int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double lim
 		if (c->precision == ITP2D_FP64) propagate_fused<double>(c);
 		else propagate_fused<float>(c);
 		launch_overlap_any(c, tc);
-		launch_batched_eigensolve(item, 1, 60, k, c->stream);
+		launch_batched_eigensolve(item, 1, 60, k, loop + 7, c->stream);
 		if (tc)
 			launch_rotate_tc(c->W, (const float2*)c->psi, k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream);
 		else if (c->precision == ITP2D_FP64)
