@@ -309,12 +309,14 @@ int overlap_tiles(int k) { return (k + kBM - 1) / kBM; }
 int overlap_splits(int k, long long G, int num_sms) {
 	const int nt = overlap_tiles(k);
 	const long long npairs = (long long)nt * (nt + 1) / 2;
-	// two CTAs per SM (80 KB of stages each for FP64 states); up to 16 splits
-	// of at least 512 grid points; the first count whose grid fills its last
-	// wave to 95 % or more, else the best-filled one (k = 2000: 528 tile pairs
-	// fill 1.78 waves unsplit, 5 splits fill 8.92 waves)
+	// two CTAs per SM (80 KB of stages each for FP64 states); splits of at
+	// least 512 grid points, up to enough for two waves (at least 16); the
+	// first count whose grid fills its last wave to 95 % or more, else the
+	// best-filled one (k = 2000: 528 tile pairs fill 1.78 waves unsplit, 5
+	// splits fill 8.92 waves; a few tile pairs take as many splits as fill
+	// the GPU)
 	const long long slots = 2LL * num_sms;
-	const long long most = std::max(1LL, std::min(16LL, G / 512));
+	const long long most = std::max(1LL, std::min(G / 512, std::max(16LL, 2 * slots / npairs)));
 	long long best = 1;
 	double best_fill = 0.0;
 	for (long long ns = 1; ns <= most; ns++) {
