@@ -46,7 +46,10 @@ typedef struct {
 	                             step, fp32_between steps in between
 	                             (itp2d_set_fp32_orthonormalization); 0: always canonical */
 	int fp32_between;         /* ITP2D_BETWEEN_LOWDIN (0) or ITP2D_BETWEEN_CHOLESKY
-	                             (itp2d_set_fp32_between) */
+	                             (itp2d_set_fp32_between); with Cholesky the energies of the
+	                             Cholesky iterations are not computed (their history entries
+	                             repeat the previous ones) and the first FP64 iteration after
+	                             the switch is a Cholesky step too */
 	int switch_rayleigh_ritz; /* FP32 form: 1 = one Rayleigh-Ritz step (itp2d_rayleigh_ritz)
 	                             after the first FP64 orthonormalisation of the refinement */
 	double fp32_eps_factor;   /* FP32 form: the FP32 sweeps propagate with time step

@@ -403,6 +403,19 @@ void ITPSystem::orthonormalized(int st, int bi, double bv) {
 void ITPSystem::calculate_energies() {
 	if (total_step_counter == 0) return;
 	const size_t k = (size_t)p.num_states;
+	// FP32 form with Cholesky steps: nothing reads the energies of a Cholesky
+	// iteration (the switch rule and the eigensolve tolerance compare
+	// canonical iterations, the convergence tests run in FP64), so they are
+	// not computed; the history repeats the previous iteration's entry
+	if (precision == ITP2D_FP32 && p.fp32_canonical_every > 1 && p.fp32_between == ITP2D_BETWEEN_CHOLESKY &&
+			!last_ortho_canonical && total_step_counter >= 2 && energies.size() >= (size_t)total_step_counter - 1 &&
+			energies[total_step_counter - 2].size() == k) {
+		energies.resize(total_step_counter);
+		deviations.resize(total_step_counter);
+		energies[total_step_counter - 1] = energies[total_step_counter - 2];
+		deviations[total_step_counter - 1] = deviations[total_step_counter - 2];
+		return;
+	}
 	std::vector<double> E(k), s(k), r(k);
 	const double t0 = now_s();
 	check(itp2d_energies(ctx, E.data(), s.data(), r.data(), nullptr), "itp2d_energies");
