@@ -202,7 +202,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
     def sweeps():
         return {prec: L.itp2d_precision_sweeps(ctx, code) for prec, code in (("fp64", capi.FP64), ("fp32", capi.FP32))}
 
-    p0, l0, w0, t0 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
+    p0, l0, w0, tr0 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -216,7 +216,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         steps.append(s.total_steps)
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
-    p1, l1, w1, t1 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
+    p1, l1, w1, tr1 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
     # per solve: {(precision, phase): (ms, calls)}
     stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
@@ -233,7 +233,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     out = dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
-               tri={p: (t1[p] - t0[p]) / K for p in t1},
+               tri={p: (tr1[p] - tr0[p]) / K for p in tr1},
                launches=(l1 - l0) / K, E=E, e2e_times=e2e_times)
     s.close()
     return out
