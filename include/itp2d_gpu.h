@@ -170,8 +170,10 @@ int itp2d_rayleigh_ritz(itp2d_ctx* ctx, double* ritz_values);
 /* Column passes of periodic 256- and 512-point lines: tiles staged through
  * registers and shared memory (0) or moved by TMA with a three-slot ring (1).
  * The first itp2d_set_time_step of each precision times both on the spare
- * state buffer and keeps the faster; variant >= 0 forces one, -1 restores the
- * tuned choice. itp2d_column_variant returns the variant in use. */
+ * state buffer and keeps the faster; the choice is kept for the process per
+ * device, precision and grid, so later contexts of the same size reuse it.
+ * variant >= 0 forces one, -1 restores the tuned choice.
+ * itp2d_column_variant returns the variant in use. */
 int itp2d_set_column_variant(itp2d_ctx* ctx, int variant);
 int itp2d_column_variant(itp2d_ctx* ctx);
 

@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <new>
 #include <string>
@@ -898,7 +900,27 @@ int itp2d_set_time_step(itp2d_ctx* c, double eps) {
 	c->eps_set = true;
 	const int st = rebuild_tables(c);
 	if (st || c->col_variant[c->precision] >= 0) return st;
-	return c->precision == ITP2D_FP64 ? tune_columns<double>(c) : tune_columns<float>(c);
+	// one tuning per device, precision and grid for the process: contexts of
+	// the same size (a serving loop, a batch) reuse the choice
+	static std::mutex mu;
+	static std::map<std::tuple<int, int, int, int, int>, int> tuned;
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const auto key = std::make_tuple(dev, c->precision, c->sx, c->sy, c->boundary);
+	{
+		std::lock_guard<std::mutex> lk(mu);
+		const auto it = tuned.find(key);
+		if (it != tuned.end()) {
+			c->col_variant[c->precision] = it->second;
+			return ITP2D_OK;
+		}
+	}
+	const int r = c->precision == ITP2D_FP64 ? tune_columns<double>(c) : tune_columns<float>(c);
+	if (r == ITP2D_OK && c->col_variant[c->precision] >= 0) {
+		std::lock_guard<std::mutex> lk(mu);
+		tuned[key] = c->col_variant[c->precision];
+	}
+	return r;
 }
 
 int itp2d_set_column_variant(itp2d_ctx* c, int variant) {
