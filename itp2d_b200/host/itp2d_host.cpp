@@ -346,22 +346,14 @@ void ITPSystem::orthonormalize() {
 	long long c0 = 0, c1 = 0;
 	const bool cholesky_between = p.fp32_canonical_every > 1 && p.fp32_between == ITP2D_BETWEEN_CHOLESKY;
 	if (precision == ITP2D_FP32) {
-		// the eigensolve of a canonical FP32 step stops at a largest rotation
-		// tangent of 0.2 while no two canonical steps have been compared (with
-		// Cholesky steps in between: the next Cholesky step restores
-		// orthonormality, and these energies are not compared yet), 0.05 while
-		// the energies move by more than 1e-2 per step, 1e-3 after that
-		bool early, first;
-		if (cholesky_between) {
-			first = canonical_prev.empty();
-			early = first ||
+		bool early;
+		if (cholesky_between)
+			early = canonical_prev.empty() ||
 					!(wanted_change(canonical_last, canonical_prev, canonical_step_last - canonical_step_prev) < 1e-2);
-		} else {
-			first = false;
+		else
 			early = energies.size() < 2 ||
 					!(wanted_change(energies[energies.size() - 1], energies[energies.size() - 2], 1) < 1e-2);
-		}
-		check(itp2d_set_fp32_eig_tolerance(ctx, first ? 0.2 : (early ? 0.05 : 1e-3)), "itp2d_set_fp32_eig_tolerance");
+		check(itp2d_set_fp32_eig_tolerance(ctx, early ? 0.05 : 1e-3), "itp2d_set_fp32_eig_tolerance");
 	}
 	int algo = p.ortho_algorithm;
 	if (cholesky_pending && precision == ITP2D_FP64) {
