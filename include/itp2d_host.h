@@ -52,9 +52,9 @@ typedef struct {
 	                             the switch is a Cholesky step too */
 	int switch_rayleigh_ritz; /* FP32 form: 1 = one Rayleigh-Ritz step (itp2d_rayleigh_ritz)
 	                             after the first FP64 orthonormalisation of the refinement */
-	double fp32_eps_factor;   /* FP32 form: the FP32 sweeps propagate with time step
-	                             eps * fp32_eps_factor (0 or 1: eps); the FP64 refinement
-	                             and every convergence test use eps */
+	int fp32_switch_span;     /* FP32 form: iterations over which the switch rule reads the
+	                             energy change (0: 3; 1: consecutive iterations with the
+	                             stall test alone) */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

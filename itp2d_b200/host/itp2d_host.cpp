@@ -269,7 +269,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
 	check(itp2d_set_fp32_between(ctx, p.fp32_between), "itp2d_set_fp32_between");
 	check(itp2d_set_potential(ctx, null_potential ? nullptr : V.data()), "itp2d_set_potential");
-	check(itp2d_set_time_step(ctx, sweep_eps()), "itp2d_set_time_step");
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	initial_states = params.initial_states;
 	if (!initial_states.empty() && initial_states.size() != 2 * dl.N * (size_t)p.num_states)
 		throw GeneralError("initial states have the wrong size");
@@ -497,7 +497,7 @@ void ITPSystem::change_time_step() {
 		finish();
 		return;
 	}
-	check(itp2d_set_time_step(ctx, sweep_eps()), "itp2d_set_time_step");
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	step_counter = 0;
 	all_timestep_converged = false;
 	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
@@ -537,7 +537,8 @@ void ITPSystem::maybe_switch_precision() {
 		return;
 	}
 	const size_t n = energies.size();
-	const int span = (int)std::min<size_t>(kFp32Span, n - 1);
+	const size_t want = p.fp32_switch_span > 0 ? (size_t)p.fp32_switch_span : kFp32Span;
+	const int span = (int)std::min<size_t>(want, n - 1);
 	fp32_compare_with(energies[n - 1], energies[n - 1 - span], between ? 2 : 3, span);
 }
 
@@ -562,7 +563,8 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 	// the FP32 phase has reached that floor
 	double emax = 0.0;
 	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) emax = std::max(emax, std::fabs(a[n]));
-	const bool at_floor = worst < kFp32FloorUlps * 0x1p-24 * emax && worst > 0.5 * prev;
+	// (a span of 1, the consecutive-iteration rule, relies on the stall test alone)
+	const bool at_floor = p.fp32_switch_span != 1 && worst < kFp32FloorUlps * 0x1p-24 * emax && worst > 0.5 * prev;
 	if (!(worst < p.fp32_switch) && !at_floor) {
 		if (worst < fp32_best) {
 			fp32_best = worst;
@@ -573,20 +575,12 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 	}
 	check(itp2d_set_precision(ctx, ITP2D_FP64), "itp2d_set_precision");
 	precision = ITP2D_FP64;
-	check(itp2d_set_time_step(ctx, sweep_eps()), "itp2d_set_time_step");
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	step_counter = 0;
 	all_timestep_converged = false;
 	ritz_pending = p.switch_rayleigh_ritz != 0;
 	cholesky_pending = p.fp32_canonical_every > 1 && p.fp32_between == ITP2D_BETWEEN_CHOLESKY;
 	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
-}
-
-// The time step the sweeps use: eps, or eps * fp32_eps_factor while the FP32
-// form's sweeps run in FP32 (a longer step converges the subspace in fewer
-// FP32 iterations; the FP64 refinement returns to eps and its fixed point).
-double ITPSystem::sweep_eps() const {
-	const double f = p.fp32_eps_factor;
-	return (precision == ITP2D_FP32 && f > 0.0) ? eps * f : eps;
 }
 
 // itpsystem.cpp:407-470
@@ -790,7 +784,7 @@ void ITPSystem::reset(const double* init) {
 		check(itp2d_set_precision(ctx, p.precision), "itp2d_set_precision");
 		precision = p.precision;
 	}
-	check(itp2d_set_time_step(ctx, sweep_eps()), "itp2d_set_time_step");
+	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	if (init) {
 		initial_states.clear();  // a later recovery re-randomises like the reference
 		check(itp2d_upload_states(ctx, init), "itp2d_upload_states");
@@ -847,7 +841,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->fp32_canonical_every = 0;
 	p->fp32_between = ITP2D_BETWEEN_LOWDIN;
 	p->switch_rayleigh_ritz = 0;
-	p->fp32_eps_factor = 1.0;
+	p->fp32_switch_span = 0;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
 	std::strcpy(p->final_test, "relstdev(1e-3,0)");

@@ -230,7 +230,6 @@ class ITPSystem {
 	double wanted_change(const std::vector<double>& a, const std::vector<double>& b, int steps) const;
 	void check(int status, const char* where);
 	bool check_abort_flag();
-	double sweep_eps() const;
 	void check_save_flag();
 	void save_states();
 

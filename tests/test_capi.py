@@ -132,7 +132,7 @@ def test_parameter_defaults_match_the_reference_and_leave_extensions_off():
     """itp2d_parameters_default gives the reference's defaults
     (parameters.cpp:25-55) and leaves every extension off: canonical
     orthonormalisation every step, Lowdin between (unused), no Rayleigh-Ritz
-    step at the switch, FP32 sweeps at the solve's own time step."""
+    step at the switch, the default switch-rule span."""
     from itp2d_b200 import system
     p = system._Params()
     system._lib().itp2d_parameters_default(ctypes.byref(p))
@@ -140,7 +140,7 @@ def test_parameter_defaults_match_the_reference_and_leave_extensions_off():
     assert p.eps_divisor == 5.0 and p.min_eps == 1e-9
     assert p.precision == capi.FP64 and p.fp32_switch == 0.0
     assert p.fp32_canonical_every == 0 and p.fp32_between == capi.BETWEEN_LOWDIN
-    assert p.switch_rayleigh_ritz == 0 and p.fp32_eps_factor == 1.0
+    assert p.switch_rayleigh_ritz == 0 and p.fp32_switch_span == 0
     assert p.timestep_test == b"relstdev(1e-3,1e-4)" and p.final_test == b"relstdev(1e-3,0)"
 
 
