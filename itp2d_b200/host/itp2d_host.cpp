@@ -508,9 +508,8 @@ void ITPSystem::change_time_step() {
 // the eigenpairs to the FP64 fixed point.
 // The FP32 form switches to FP64 once every wanted energy changes by less than
 // fp32_switch per step, once the largest change is within kFp32FloorUlps
-// single-precision roundings of the largest wanted energy and has not halved
-// since the previous comparison (it converges by about a factor of ten per
-// step until it meets the FP32 noise floor), or once it has not decreased for
+// single-precision roundings of the largest wanted energy and has stopped
+// decreasing since the previous comparison, or once it has not decreased for
 // a few comparisons (the FP32 noise floor lies above fp32_switch).
 // With Lowdin steps between canonical ones (fp32_canonical_every > 1) the
 // rule skips the Lowdin iterations (a Lowdin step does not rotate within the
@@ -559,12 +558,13 @@ void ITPSystem::fp32_compare_with(const std::vector<double>& a, const std::vecto
 	const double prev = fp32_last;
 	fp32_last = worst;
 	// near the FP32 noise floor (kFp32FloorUlps single-precision roundings of
-	// the largest wanted energy) a change that no longer halves per step means
-	// the FP32 phase has reached that floor
+	// the largest wanted energy) a change that has stopped decreasing (within
+	// 10 %) means the FP32 phase has reached that floor; a slowly converging
+	// change still decreases
 	double emax = 0.0;
 	for (int n = p.ignore_lowest; n < p.ignore_lowest + p.wanted; n++) emax = std::max(emax, std::fabs(a[n]));
 	// (a span of 1, the consecutive-iteration rule, relies on the stall test alone)
-	const bool at_floor = p.fp32_switch_span != 1 && worst < kFp32FloorUlps * 0x1p-24 * emax && worst > 0.5 * prev;
+	const bool at_floor = p.fp32_switch_span != 1 && worst < kFp32FloorUlps * 0x1p-24 * emax && worst > 0.9 * prev;
 	if (!(worst < p.fp32_switch) && !at_floor) {
 		if (worst < fp32_best) {
 			fp32_best = worst;
