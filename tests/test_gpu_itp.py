@@ -185,6 +185,20 @@ def test_fp32_form_refines_to_fp64(itp):
     assert np.max(np.abs(E64[:6] - O.fock_darwin_spectrum(6, 1.0))) < 1e-3
 
 
+@pytest.mark.parametrize("span", [1, 3])
+def test_fp32_switch_rule_spans_reach_fp64_energies(itp, span):
+    """Either switch rule (consecutive iterations with the stall test, or the
+    change over three iterations with the floor test) ends the FP32 phase and
+    the FP64 refinement reaches the plain FP64 energies."""
+    kw = dict(sx=48, sy=48, length=12.0, B=1.0, halforder=2, num_states=12, wanted=6, eps=[0.1],
+              potential="harmonic(1)", timestep_test="abschange(1e-10)", final_test="abschange(1e-10)",
+              max_steps=600, seed=5)
+    s64 = _solve(itp, **kw)
+    s32 = _solve(itp, **kw, precision=1, fp32_switch=1e-7, fp32_switch_span=span)
+    assert s32.finished and not s32.in_fp32
+    assert np.max(np.abs(s32.energies()[0][:6] - s64.energies()[0][:6])) < 1e-9
+
+
 def test_recovery_from_dependent_states(itp):
     """A rank-deficient start makes the overlap singular; with recover the
     driver shrinks eps and restarts from noise (itpsystem.cpp:264-281)."""
