@@ -177,7 +177,11 @@ int itp2d_rayleigh_ritz(itp2d_ctx* ctx, double* ritz_values);
 int itp2d_set_column_variant(itp2d_ctx* ctx, int variant);
 int itp2d_column_variant(itp2d_ctx* ctx);
 
-enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1 };
+/* Contraction engine: AUTO (FP64 states: DMMA; FP32 states: tensor cores on
+ * operands split into BF16 planes once per contraction), FP64 (DMMA for
+ * either precision), TC_STAGED (tensor cores, operands split inside each CTA;
+ * the same results as AUTO, bit for bit). */
+enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1, ITP2D_CONTRACT_TC_STAGED = 2 };
 int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
 
 /* FP32 states: orthonormalise canonically only on every canonical_every-th

@@ -26,7 +26,7 @@ FP64, FP32 = 0, 1
 ORTHO_DEFAULT, ORTHO_HIGHMEM, ORTHO_CHOLESKY = 0, 1, 2
 BETWEEN_LOWDIN, BETWEEN_CHOLESKY = 0, 1
 COL_SMEM, COL_TMA = 0, 1
-CONTRACT_AUTO, CONTRACT_FP64 = 0, 1
+CONTRACT_AUTO, CONTRACT_FP64, CONTRACT_TC_STAGED = 0, 1, 2
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
 

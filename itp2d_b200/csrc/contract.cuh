@@ -32,6 +32,16 @@ void launch_overlap_tc(const float2* psi, int k, long long G, int nsplit, double
 size_t tc_wsplit_bytes(int k);
 void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit, float2* out,
 		int* err, cudaStream_t s, bool upper = false);
+// The same contractions from pre-split operands (split once per call into
+// device scratch: tc_rows_bytes for the overlap, tc_cols_bytes for the
+// rotation's psi), copied block by block by cp.async.bulk; bit-identical
+// results to launch_overlap_tc / launch_rotate_tc.
+size_t tc_rows_bytes(int k, long long G);
+size_t tc_cols_bytes(int k, long long G);
+void launch_overlap_tc_presplit(const float2* psi, int k, long long G, int nsplit, unsigned char* rows, double2* part,
+		double dx2, double2* S, int* err, cudaStream_t s);
+void launch_rotate_tc_presplit(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit,
+		unsigned char* cols, float2* out, int* err, cudaStream_t s, bool upper = false);
 
 template <class T>
 void launch_normalize1(T* psi, long long G, double dx, double* tmp, cudaStream_t s);

@@ -91,6 +91,9 @@ struct itp2d_ctx {
 	long long sweeps_total = 0;
 	long long sweeps_p[2] = {0, 0};  // by precision: FP64, FP32
 	int engine = ITP2D_CONTRACT_AUTO;
+	unsigned char* tc_rows = nullptr;  // FP32 states pre-split for the overlap (allocated on first use)
+	unsigned char* tc_cols = nullptr;  // and for the rotation's B operand
+	bool tc_staged = false;            // pre-split scratch unavailable: split inside the contraction CTAs
 	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
 	int* dflag = nullptr;  // tensor-core wait time-outs (device)
 	unsigned char* wsplit = nullptr;  // W^T in BF16 planes (tensor-core rotation)
@@ -761,7 +764,12 @@ long long itp2d_ctx_footprint(int sx, int sy, int num_states, int boundary, doub
 	const int nsplit = overlap_splits(num_states, G, sms);
 	const int parts = std::max(nsplit, tc_overlap_splits(num_states, G, sms));
 	const long long kp = std::max(bjacobi_padded(num_states), (num_states + 1) & ~1);
-	b += (2 + parts) * k * k * 16 + (tc_supported(num_states, G) ? (long long)tc_wsplit_bytes(num_states) : 0);
+	// tensor-core scratch of the FP32 form: W^T planes, pre-split states for
+	// the overlap and the rotation (counted whenever the size can use them)
+	b += (2 + parts) * k * k * 16 + (tc_supported(num_states, G) ? (long long)(tc_wsplit_bytes(num_states) +
+	                                                                           tc_rows_bytes(num_states, G) +
+	                                                                           tc_cols_bytes(num_states, G))
+	                                                             : 0);
 	b += (num_states >= kBlockJacobiMinK ? 4 : 3) * kp * kp * 16 + npairs * 8;
 	if (num_states >= kBlockJacobiMinK) b += (long long)bjacobi_qbuf_elems(num_states) * 16;
 	b += k * std::max(sx, sy) * 5 * 8 * (dm ? 2 : 1) + 5 * k * 8 + 16 * k;
@@ -1044,14 +1052,45 @@ int itp2d_transform(itp2d_ctx* c, int kind) {
 namespace {
 
 bool use_tensor_cores(const itp2d_ctx* c) {
-	return c->precision == ITP2D_FP32 && c->engine == ITP2D_CONTRACT_AUTO && tc_supported(c->k, c->G);
+	return c->precision == ITP2D_FP32 && (c->engine == ITP2D_CONTRACT_AUTO || c->engine == ITP2D_CONTRACT_TC_STAGED) &&
+	       tc_supported(c->k, c->G);
+}
+
+// The pre-split scratch of the tensor-core contractions, allocated on first
+// use (FP32 form only); on failure the contractions split inside their CTAs.
+bool presplit_ready(itp2d_ctx* c) {
+	if (c->engine != ITP2D_CONTRACT_AUTO || c->tc_staged) return false;
+	if (c->tc_rows && c->tc_cols) return true;
+	cudaError_t e = cudaSuccess;
+	if (!c->tc_rows) c->tc_rows = (unsigned char*)dalloc(c, tc_rows_bytes(c->k, c->G), &e);
+	if (e == cudaSuccess && !c->tc_cols) c->tc_cols = (unsigned char*)dalloc(c, tc_cols_bytes(c->k, c->G), &e);
+	if (e != cudaSuccess) {
+		cudaGetLastError();  // an allocation failure is not sticky
+		c->tc_staged = true;
+		return false;
+	}
+	return true;
+}
+
+// psi W on the tensor cores into acc (W upper triangular: triangular K range).
+void tc_rotate(itp2d_ctx* c, bool upper) {
+	if (presplit_ready(c))
+		launch_rotate_tc_presplit(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, c->tc_cols, (float2*)c->acc,
+				c->dflag, c->stream, upper);
+	else
+		launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream,
+				upper);
 }
 
 // S = Psi^H Psi dx^2 (full Hermitian, row-major) by the selected engine.
 void launch_overlap_any(itp2d_ctx* c, bool tc) {
 	if (tc)
-		launch_overlap_tc((const float2*)c->psi, c->k, c->G, c->tc_nsplit, c->part, c->dx * c->dx, c->S, c->dflag,
-				c->stream);
+		if (presplit_ready(c))
+			launch_overlap_tc_presplit((const float2*)c->psi, c->k, c->G, c->tc_nsplit, c->tc_rows, c->part,
+					c->dx * c->dx, c->S, c->dflag, c->stream);
+		else
+			launch_overlap_tc((const float2*)c->psi, c->k, c->G, c->tc_nsplit, c->part, c->dx * c->dx, c->S, c->dflag,
+					c->stream);
 	else if (c->precision == ITP2D_FP64)
 		launch_overlap((const double2*)c->psi, c->k, c->G, c->pairs, c->npairs, c->nsplit, c->part, c->dx * c->dx,
 				c->S, c->stream);
@@ -1064,7 +1103,8 @@ void launch_overlap_any(itp2d_ctx* c, bool tc) {
 }  // namespace
 
 int itp2d_set_contraction(itp2d_ctx* c, int engine) {
-	if (!c || (engine != ITP2D_CONTRACT_AUTO && engine != ITP2D_CONTRACT_FP64)) return ITP2D_E_INVALID;
+	if (!c || (engine != ITP2D_CONTRACT_AUTO && engine != ITP2D_CONTRACT_FP64 && engine != ITP2D_CONTRACT_TC_STAGED))
+		return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
 	c->engine = engine;
 	return ITP2D_OK;
@@ -1136,8 +1176,7 @@ static int rotate_states(itp2d_ctx* c, bool tc, bool upper = false) {
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
-			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream,
-					upper);
+			tc_rotate(c, upper);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream, upper);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream, upper);
 		c->launches += tc ? 2 : 1;
@@ -1258,8 +1297,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
-			launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
-					c->stream);
+			tc_rotate(c, false);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
 		c->launches += tc ? 2 : 1;
@@ -1567,8 +1605,7 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 		{
 			PhaseTimer t(c, kRotate);
 			if (tc)
-				launch_rotate_tc(c->W, (const float2*)c->psi, c->k, c->G, c->wsplit, (float2*)c->acc, c->dflag,
-						c->stream);
+				tc_rotate(c, false);
 			else if (c->precision == ITP2D_FP64)
 				launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
 			else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
@@ -1801,6 +1838,7 @@ int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double lim
 	void* const psi0 = c->psi;
 	void* const acc0 = c->acc;
 	const long long launches0 = c->launches;
+	if (use_tensor_cores(c)) presplit_ready(c);  // allocations happen before the capture
 	e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
 	if (e == cudaSuccess) {
 		const bool tc = use_tensor_cores(c);
@@ -1809,7 +1847,7 @@ int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double lim
 		launch_overlap_any(c, tc);
 		launch_batched_eigensolve(item, 1, 60, k, loop + 7, c->stream);
 		if (tc)
-			launch_rotate_tc(c->W, (const float2*)c->psi, k, c->G, c->wsplit, (float2*)c->acc, c->dflag, c->stream);
+			tc_rotate(c, false);
 		else if (c->precision == ITP2D_FP64)
 			launch_rotate(c->W, (const double2*)c->psi, k, c->G, (double2*)c->acc, c->stream);
 		else launch_rotate(c->W, (const float2*)c->psi, k, c->G, (float2*)c->acc, c->stream);

@@ -454,6 +454,206 @@ __global__ void split_w_kernel(const double2* __restrict__ W, int k, int ksteps,
 	put2(out + blk * kOperandBytes, kmaj_off(r, kk), (float)w0.x, (float)w0.y, (float)w1.x, (float)w1.y);
 }
 
+// ---------------------------------------------------------------------------
+// Pre-split operands. The FP32 states are split into the six BF16 planes once
+// per contraction, in the same block layout as split_w_kernel's W^T, so that
+// the contraction kernels only copy 24 KB blocks (one cp.async.bulk each) and
+// issue MMAs: no split work and no block-wide barrier per K step.
+//   rows layout (overlap): block (state tile ti, grid step gs) at
+//     (ti * gsteps + gs) * kOperandBytes; rows = states, K = grid points;
+//   cols layout (rotation's B): block (grid tile gt, state step s) at
+//     (gt * ksteps + s) * kOperandBytes; rows = grid points, K = states.
+// Zero outside k x G. One warp per core matrix (lane = row in group * 4 + K
+// pair), as in split_w_kernel.
+
+__global__ void split_psi_rows_kernel(const float2* __restrict__ psi, int k, long long G, int ntiles,
+		long long gsteps, unsigned char* __restrict__ out) {
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= (long long)ntiles * gsteps * 32) return;
+	const int m = (int)(warp & 31);
+	const long long blk = warp >> 5;
+	const long long gs = blk % gsteps;
+	const int ti = (int)(blk / gsteps);
+	const int rg = m >> 1, kc = m & 1;
+	const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+	const int i = ti * TM + r;
+	const long long g = gs * KT + kk;  // even; G even: g and g + 1 in range together
+	float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+	if (i < k && g < G) v = *reinterpret_cast<const float4*>(psi + (long long)i * G + g);
+	put2(out + blk * kOperandBytes, kmaj_off(r, kk), v.x, v.y, v.z, v.w);
+}
+
+__global__ void split_psi_cols_kernel(const float2* __restrict__ psi, int k, long long G, long long gtiles,
+		int ksteps, unsigned char* __restrict__ out) {
+	const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (warp >= gtiles * ksteps * 32) return;
+	const int m = (int)(warp & 31);
+	const long long blk = warp >> 5;
+	const int s = (int)(blk % ksteps);
+	const long long gt = blk / ksteps;
+	const int rg = m >> 1, kc = m & 1;
+	const int r = rg * 8 + (lane >> 2), kk = kc * 8 + (lane & 3) * 2;
+	const long long g = gt * TN + r;
+	const int i = s * KT + kk;
+	float2 a = make_float2(0.f, 0.f), b = a;
+	if (g < G) {
+		if (i < k) a = psi[(long long)i * G + g];
+		if (i + 1 < k) b = psi[(long long)(i + 1) * G + g];
+	}
+	put2(out + blk * kOperandBytes, kmaj_off(r, kk), a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// Contiguous global -> shared copy (16-byte aligned, size a multiple of 16)
+// completing on an mbarrier's transaction count.
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+			"l"(src), "r"(bytes), "r"(mbar)
+			: "memory");
+}
+
+constexpr int kRing = 4;                      // slots of (A, B) block pairs
+constexpr int kSlotBytes = 2 * kOperandBytes;  // 48 KB
+static_assert(kRing * kSlotBytes <= kBufBytes, "pre-split ring");
+
+// The K loop over pre-split blocks, run by thread 0 alone: block pair s is
+// copied into slot s mod kRing (full[slot] completes when it has landed),
+// its MMAs are issued and committed to empty[slot]; after the MMAs of step s
+// are issued, the slot of step s - 1 is refilled with step s - 1 + kRing once
+// those MMAs have finished reading it. src_a(s) / src_b(s) give the global
+// blocks (src_b null: B reads A's planes). Returns with every MMA complete or
+// with sh.abort set (copies and MMAs in flight drained, bounded).
+template <class SrcA, class SrcB>
+__device__ void run_bulk_pipeline(TcShared& sh, unsigned long long* full, unsigned long long* empty, int nsteps,
+		bool conjA, SrcA src_a, SrcB src_b, int* err) {
+	if (threadIdx.x != 0 || nsteps <= 0) return;
+	unsigned char* const base = sh.buf;
+	auto copy = [&](int st) {
+		const int slot = st % kRing;
+		unsigned char* dst = base + slot * kSlotBytes;
+		const unsigned char* b = src_b(st);
+		const uint32_t fb = smem_u32(&full[slot]);
+		mbar_expect_tx(fb, b ? 2 * kOperandBytes : kOperandBytes);
+		bulk_copy(smem_u32(dst), src_a(st), kOperandBytes, fb);
+		if (b) bulk_copy(smem_u32(dst + kOperandBytes), b, kOperandBytes, fb);
+	};
+	int copied = 0, issued = 0;  // steps copied / whose MMAs were issued
+	for (; copied < nsteps && copied < kRing; copied++) copy(copied);
+	bool ok = true;
+	for (int st = 0; st < nsteps; st++) {
+		const int slot = st % kRing;
+		if (!mbar_wait(smem_u32(&full[slot]), (uint32_t)((st / kRing) & 1))) {
+			ok = false;
+			break;
+		}
+		tc_fence_after();
+		const uint32_t a = smem_u32(base + slot * kSlotBytes);
+		issue_step(sh.tmem_base, a, src_b(st) ? a + kOperandBytes : a, conjA, st == 0);
+		umma_commit(smem_u32(&empty[slot]));
+		issued = st + 1;
+		if (st >= 1 && copied < nsteps) {
+			const int ps = (st - 1) % kRing;
+			if (!mbar_wait(smem_u32(&empty[ps]), (uint32_t)(((st - 1) / kRing) & 1))) {
+				ok = false;
+				break;
+			}
+			copy(copied++);
+		}
+	}
+	if (!ok) {
+		sh.abort = 1;
+		atomicExch(err, ITP2D_E_TIMEOUT);
+		// copies not yet waited for land before the CTA leaves
+		for (int st = issued; st < copied; st++) mbar_wait(smem_u32(&full[st % kRing]), (uint32_t)((st / kRing) & 1));
+	}
+	// the last commit covers every MMA issued before it
+	if (issued > 0 && !mbar_wait(smem_u32(&empty[(issued - 1) % kRing]), (uint32_t)(((issued - 1) / kRing) & 1))) {
+		sh.abort = 1;
+		atomicExch(err, ITP2D_E_TIMEOUT);
+	}
+}
+
+__device__ void init_ring(unsigned long long* full, unsigned long long* empty) {
+	if (threadIdx.x == 0)
+		for (int i = 0; i < kRing; i++) {
+			mbar_init(smem_u32(&full[i]), 1);
+			mbar_init(smem_u32(&empty[i]), 1);
+		}
+}
+
+// Overlap from the rows layout: tile pair (ti <= tj) from blockIdx.x, grid
+// steps [g0 / KT, g1 / KT) from blockIdx.y; the same MMAs in the same order
+// as overlap_tc_kernel.
+__global__ void __launch_bounds__(kThreads, 1) overlap_tc2_kernel(const unsigned char* __restrict__ rows, int k,
+		long long G, int ntiles, long long gsteps, long long chunk, double2* __restrict__ part, int* err) {
+	TcShared& sh = tc_shared();
+	__shared__ alignas(8) unsigned long long full[kRing], empty[kRing];
+	int p = blockIdx.x, ti = 0;
+	while (p >= ntiles - ti) {
+		p -= ntiles - ti;
+		ti++;
+	}
+	const int tj = ti + p;
+	const int i0 = ti * TM, j0 = tj * TN;
+	const long long g0 = (long long)blockIdx.y * chunk;
+	const long long g1 = min(G, g0 + chunk);
+	const int nsteps = (int)((g1 - g0 + KT - 1) / KT);
+	const long long gs0 = g0 / KT;
+	init_ring(full, empty);
+	tc_setup(sh);
+	const bool diag = ti == tj;
+	run_bulk_pipeline(sh, full, empty, nsteps, true,
+			[&](int st) { return rows + ((long long)ti * gsteps + gs0 + st) * kOperandBytes; },
+			[&](int st) -> const unsigned char* {
+				return diag ? nullptr : rows + ((long long)tj * gsteps + gs0 + st) * kOperandBytes;
+			},
+			err);
+	__syncthreads();
+	tc_fence_after();
+	if (!sh.abort) {
+		double2* out = part + (size_t)blockIdx.y * k * k;
+		store_tile(sh, [&](int r, int c, double re, double im) {
+			const int i = i0 + r, j = j0 + c;
+			if (i < k && j < k) out[(size_t)i * k + j] = make_double2(re, im);
+		});
+	}
+	tc_teardown(sh);
+}
+
+// Rotation from pre-split W^T (A) and the cols layout of psi (B); the same
+// MMAs in the same order as rotate_tc_kernel.
+__global__ void __launch_bounds__(kThreads, 1) rotate_tc2_kernel(const unsigned char* __restrict__ wsplit,
+		const unsigned char* __restrict__ cols, int k, long long G, float2* __restrict__ out, int* err, int upper) {
+	TcShared& sh = tc_shared();
+	__shared__ alignas(8) unsigned long long full[kRing], empty[kRing];
+	const int n0 = blockIdx.x * TM;
+	const long long gt = blockIdx.y;
+	const long long gt0 = gt * TN;
+	const int nsteps = (k + KT - 1) / KT;
+	const int nrun = upper ? (min(k, n0 + TM) + KT - 1) / KT : nsteps;
+	const unsigned char* wblk = wsplit + (size_t)blockIdx.x * nsteps * kOperandBytes;
+	const unsigned char* cblk = cols + (size_t)gt * nsteps * kOperandBytes;
+	init_ring(full, empty);
+	tc_setup(sh);
+	run_bulk_pipeline(sh, full, empty, nrun, false, [&](int st) { return wblk + (size_t)st * kOperandBytes; },
+			[&](int st) -> const unsigned char* { return cblk + (size_t)st * kOperandBytes; }, err);
+	__syncthreads();
+	tc_fence_after();
+	if (!sh.abort) {
+		store_tile(sh, [&](int r, int c, double re, double im) {
+			const int n = n0 + r;
+			const long long g = gt0 + c;
+			if (n < k && g < G) out[(long long)n * G + g] = make_float2((float)re, (float)im);
+		});
+	}
+	tc_teardown(sh);
+}
+
 // Rotation tile: out rows n0.. (state index n), columns gt0.. (grid points).
 // A = W^T from the pre-split planes, B[g][i] = psi_i[g].
 __global__ void __launch_bounds__(kThreads, 1) rotate_tc_kernel(const unsigned char* __restrict__ wsplit,
@@ -540,6 +740,8 @@ size_t tc_smem() { return sizeof(TcShared) + 1024; }
 void set_tc_attributes() {
 	cudaFuncSetAttribute(overlap_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
 	cudaFuncSetAttribute(rotate_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
+	cudaFuncSetAttribute(overlap_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
+	cudaFuncSetAttribute(rotate_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
 	cudaFuncSetAttribute(tc_wait_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem());
 }
 
@@ -598,6 +800,42 @@ void launch_rotate_tc(const double2* W, const float2* psi, int k, long long G, u
 	set_tc_attributes();
 	const dim3 grid(nt, (unsigned)((G + TN - 1) / TN));
 	rotate_tc_kernel<<<grid, kThreads, tc_smem(), s>>>(wsplit, psi, k, G, out, err, upper ? 1 : 0);
+}
+
+size_t tc_rows_bytes(int k, long long G) {
+	return (size_t)((k + TM - 1) / TM) * (size_t)((G + KT - 1) / KT) * kOperandBytes;
+}
+
+size_t tc_cols_bytes(int k, long long G) {
+	return (size_t)((G + TN - 1) / TN) * (size_t)((k + KT - 1) / KT) * kOperandBytes;
+}
+
+void launch_overlap_tc_presplit(const float2* psi, int k, long long G, int nsplit, unsigned char* rows, double2* part,
+		double dx2, double2* S, int* err, cudaStream_t s) {
+	const int nt = (k + TM - 1) / TM;
+	const int npairs = nt * (nt + 1) / 2;
+	const long long gsteps = (G + KT - 1) / KT;
+	const long long threads = (long long)nt * gsteps * 32 * 32;
+	split_psi_rows_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(psi, k, G, nt, gsteps, rows);
+	long long chunk = (G + nsplit - 1) / nsplit;
+	chunk = ((chunk + KT - 1) / KT) * KT;
+	const int used = (int)((G + chunk - 1) / chunk);
+	set_tc_attributes();
+	overlap_tc2_kernel<<<dim3(npairs, used), kThreads, tc_smem(), s>>>(rows, k, G, nt, gsteps, chunk, part, err);
+	launch_overlap_finish(part, k, used, dx2, S, s);
+}
+
+void launch_rotate_tc_presplit(const double2* W, const float2* psi, int k, long long G, unsigned char* wsplit,
+		unsigned char* cols, float2* out, int* err, cudaStream_t s, bool upper) {
+	const int nt = (k + TM - 1) / TM, ks = (k + KT - 1) / KT;
+	const long long gtiles = (G + TN - 1) / TN;
+	long long threads = (long long)nt * ks * 32 * 32;
+	split_w_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(W, k, ks, nt, wsplit);
+	threads = gtiles * ks * 32 * 32;
+	split_psi_cols_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(psi, k, G, gtiles, ks, cols);
+	set_tc_attributes();
+	rotate_tc2_kernel<<<dim3(nt, (unsigned)gtiles), kThreads, tc_smem(), s>>>(wsplit, cols, k, G, out, err,
+			upper ? 1 : 0);
 }
 
 }  // namespace itp2d

@@ -89,6 +89,32 @@ def test_rotation_tensor_cores(sx, sy, k):
     assert np.median(diff) < 1e-4
 
 
+# k = 5 and 130: ragged state tiles; 48 x 40 and 56 x 24: a grid that is not
+# a multiple of the 128-point tile; 128 x 128, k = 300: several tile pairs
+@pytest.mark.parametrize("sx,sy,k", [(32, 32, 5), (48, 40, 130), (56, 24, 64), (128, 128, 300)])
+def test_presplit_contractions_match_staged(sx, sy, k):
+    """The tensor-core overlap and rotation from operands split once per call
+    (BF16 planes in global memory, copied block by block by cp.async.bulk)
+    issue the same MMAs in the same order as the kernels that split inside
+    each CTA: the overlap, the canonical orthonormalisation and a Cholesky
+    step (triangular rotation) are bit-identical."""
+    out = {}
+    for engine in (capi.CONTRACT_AUTO, capi.CONTRACT_TC_STAGED):
+        c, dx = _ctx(sx, sy, k, seed=sx + sy + k)
+        c.set_contraction(engine)
+        S = c.overlap_matrix()
+        c.orthonormalize()
+        canon = c.download()
+        c.orthonormalize(capi.ORTHO_CHOLESKY)
+        out[engine] = (S, canon, c.download())
+        c.close()
+    for a, b in zip(out[capi.CONTRACT_AUTO], out[capi.CONTRACT_TC_STAGED]):
+        assert np.array_equal(a, b)
+    # and the pre-split overlap against FP64 products of the same FP32 states
+    c, dx = _ctx(sx, sy, k, seed=sx + sy + k)
+    assert _rel(c.overlap_matrix(), _exact_overlap(c, dx)) < TOL_S
+
+
 @pytest.mark.parametrize("sx,k", [(128, 320), (128, 1024)])
 def test_fp32_block_jacobi_canonical(sx, k):
     """k >= 256: the FP32 form solves the overlap eigenproblem by block Jacobi
