@@ -20,7 +20,17 @@
 //
 // One CTA (8 warps) owns a 128 x 128 output tile in tensor memory (512
 // columns: large-part real, imaginary, small-part real, imaginary). K
-// advances 16 per step (one MMA depth). Per step:
+// advances 16 per step (one MMA depth).
+//
+// Two engines issue the same MMAs in the same order (bit-identical results):
+//   * pre-split (the default): split_psi_rows_kernel / split_psi_cols_kernel
+//     write the planes of the states once per contraction, in the MMA block
+//     layout; overlap_tc2_kernel / rotate_tc2_kernel then run their K loop in
+//     one thread: a cp.async.bulk of each 24 KB block into a ring of four
+//     slots (full mbarrier), the 24 MMAs, tcgen05.commit to the slot's empty
+//     mbarrier, and the refill of the previous step's slot;
+//   * staged (ITP2D_CONTRACT_TC_STAGED): overlap_tc_kernel / rotate_tc_kernel
+//     split inside the CTA. Per step:
 //   * cp.async fetches the FP32 operand tiles of step s + 2 into a ring of
 //     three raw slots (16-byte pieces, XOR-swizzled against bank conflicts);
 //   * all threads split the raw tile of step s into six BF16 planes in the
