@@ -505,7 +505,7 @@ void col_pass(itp2d_ctx* c, const LinePlan& lp, void* data, const void* mul2d, c
 }
 
 // Times the column pass variants on the spare state buffer (its contents are
-// scratch between calls) with the first member's kinetic table, on up to 128
+// scratch between calls) with the first member's kinetic table, on up to 1024
 // states, and keeps the fastest for this precision.
 template <class R>
 int tune_columns(itp2d_ctx* c) {
@@ -521,7 +521,9 @@ int tune_columns(itp2d_ctx* c) {
 	a.cols_per_tile = col_tile_cols(line_len(ly), sizeof(c2<R>), c->sx);
 	a.lp = ly;
 	a.err = c->dflag;
-	const int v = tune_col_pass_reg<R>(a, std::min(c->k, 128), c->stream);
+	// up to 1024 states: enough tiles (32 per state at 512 points) for the
+	// occupancy and tail of a full pass
+	const int v = tune_col_pass_reg<R>(a, std::min(c->k, 1024), c->stream);
 	c->col_variant[c->precision] = v >= 0 ? v : kColRegSmem;
 	ITP2D_TRY(cudaGetLastError());
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
