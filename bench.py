@@ -13,7 +13,8 @@ energy by less than 1e-9 between iterations (the reference's abschange(1e-9)
 as time-step and final test). The FP64 form orthonormalises canonically every
 step (the reference's algorithm); the mixed form's FP32 phase does so on every
 third iteration with Cholesky steps in between, and its FP64 refinement
-canonically.
+canonically, with the refinement's rotations on the int8 tensor cores
+(eight int8 slices per FP64 operand, exact integer sums; FP64 accuracy).
 
 Workload "dot" (the magnetic dot): V = r^2/2, B = 1, periodic 256 x 256 grid
 of side 14, k = 500, 4th-order split (halforder 2), eps = 0.05, the 250 lowest
@@ -157,6 +158,11 @@ class ClockSampler:
 # The mixed form's FP32 phase: a canonical orthonormalisation on every third
 # iteration and Cholesky (Gram-Schmidt order) ones in between.
 MIXED_CANONICAL_EVERY = 3
+# Jacobi sweeps of its canonical steps' eigensolve, finished by a Cholesky
+# step (0: the full eigensolve).
+MIXED_EIG_SWEEPS = 0
+# Rotation engine of its FP64 refinement steps.
+MIXED_FP64_ROTATION = 1  # ITP2D_ROTATION_INT8
 
 
 def params(form: str):
@@ -170,7 +176,9 @@ def params(form: str):
                              precision=capi.FP32 if mixed else capi.FP64,
                              fp32_switch=1e-7 if mixed else 0.0,
                              fp32_canonical_every=MIXED_CANONICAL_EVERY if mixed else 0,
-                             fp32_between=capi.BETWEEN_CHOLESKY)
+                             fp32_between=capi.BETWEEN_CHOLESKY,
+                             fp32_eig_sweeps=MIXED_EIG_SWEEPS if mixed else 0,
+                             fp64_rotation=MIXED_FP64_ROTATION if mixed else capi.ROTATION_DMMA)
 
 
 def alg_bytes_split(w, b):
@@ -203,6 +211,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         return {prec: L.itp2d_precision_sweeps(ctx, code) for prec, code in (("fp64", capi.FP64), ("fp32", capi.FP32))}
 
     p0, l0, w0, tr0 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
+    i80 = L.itp2d_int8_rotations(ctx)
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -217,6 +226,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
     p1, l1, w1, tr1 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
+    i81 = L.itp2d_int8_rotations(ctx)
     # per solve: {(precision, phase): (ms, calls)}
     stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
@@ -233,7 +243,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     out = dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
-               tri={p: (tr1[p] - tr0[p]) / K for p in tr1},
+               tri={p: (tr1[p] - tr0[p]) / K for p in tr1}, int8_rotations=(i81 - i80) / K,
                launches=(l1 - l0) / K, E=E, e2e_times=e2e_times)
     s.close()
     return out
@@ -442,7 +452,11 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
       overlap    FP64: 4 k^2 G flops (Hermitian half, complex MACs, DMMA)
                  FP32 (tensor cores): BF16 MMA work issued, 24 MMAs of 128 x 128 x 16
                  per 16 grid points per upper-triangle tile pair of 128 states
-      rotation   FP64: 8 k^2 G flops; FP32: 24 MMAs of 128 x 128 x 16 per 16 states
+      rotation   FP64: 8 k^2 G flops (DMMA), or with the int8 engine the int8 MMA
+                 work issued, 36 MMAs of 128 x 128 x 32 per 16 states per (128
+                 states x 64 grid points) output tile, against twice the BF16
+                 peak (the int8 MMA rate), its 8 k^2 G FP64-equivalent rate beside
+                 it; FP32: 24 MMAs of 128 x 128 x 16 per 16 states
                  per (128 states x 128 grid points) output tile; a rotation by the
                  upper-triangular W of a Cholesky step counts only the states up
                  to each output tile's last one (about half)
@@ -467,6 +481,9 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
     tc_rotation_tri = sum((min(k, 128 * (t + 1)) + 15) // 16 for t in range(nt)) * ((G + 127) // 128) * 24 * mma
     nt64 = (k + 63) // 64
     rotation_tri = 8 * G * sum(64 * min(k, 64 * (t + 1)) for t in range(nt64))
+    mma8 = 128 * 128 * 32 * 2
+    oz_rotation = nt * ((G + 63) // 64) * ((k + 15) // 16) * 36 * mma8
+    oz_rotation_tri = sum((min(k, 128 * (t + 1)) + 15) // 16 for t in range(nt)) * ((G + 63) // 64) * 36 * mma8
     kp = (k + 31) // 32 * 32
     sweep_flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp
     out = {}
@@ -485,9 +502,20 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
                 continue
             sec = ms * 1e-3
             total = amount * calls
-            if ph == "rotation" and r.get("tri", {}).get(prec, 0):
-                tri = min(r["tri"][prec], calls)
+            tri = min(r.get("tri", {}).get(prec, 0), calls) if ph == "rotation" else 0
+            if tri:
                 total = amount * (calls - tri) + (tc_rotation_tri if tc else rotation_tri) * tri
+            if ph == "rotation" and prec == "fp64" and r.get("int8_rotations", 0) >= calls > 0:
+                # the int8 engine: MMA work issued against the int8 rate
+                fp64_equiv = total / sec / 1e12
+                total = oz_rotation * (calls - tri) + oz_rotation_tri * tri
+                ach = total / sec / 1e12
+                out[f"{ph}_{prec}"] = {"bound": "tensor", "achieved": ach, "peak": 2 * bf16, "unit": "TOP/s",
+                                       "frac": ach / (2 * bf16), "ms_per_solve": ms, "calls_per_solve": calls,
+                                       "engine": "int8 slices", "fp64_equiv_tflops": fp64_equiv,
+                                       "fp64_equiv_frac_of_dmma": fp64_equiv / fp64_peak,
+                                       "peak_source": f"2 x cuBLAS BF16 sustained ({src})"}
+                continue
             if bound == "hbm":
                 ach, peak, unit, psrc = total / sec / 1e9, hbm, "GB/s", f"HBM copy ({src})"
             elif bound == "tensor_bf16":

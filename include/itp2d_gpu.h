@@ -184,6 +184,20 @@ int itp2d_column_variant(itp2d_ctx* ctx);
 enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1, ITP2D_CONTRACT_TC_STAGED = 2 };
 int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
 
+/* Rotation of FP64 states (psi' = psi W of every orthonormalisation):
+ * ITP2D_ROTATION_DMMA (the default: FP64 tensor-core products) or
+ * ITP2D_ROTATION_INT8 (the int8 tensor cores: both operands split into eight
+ * int8 slices under per-row power-of-two scales, the slice products summed
+ * exactly in 32-bit integers and combined in FP64; the result agrees with the
+ * FP64 products to about 1e-15 of the largest output of each row; k < 8300).
+ * INT8 takes 32 bytes per state and grid point of scratch at its first use; where
+ * that cannot be allocated the DMMA rotation runs. FP32 states are not
+ * affected. */
+enum { ITP2D_ROTATION_DMMA = 0, ITP2D_ROTATION_INT8 = 1 };
+int itp2d_set_fp64_rotation(itp2d_ctx* ctx, int engine);
+/* Rotations of FP64 states run on the int8 tensor cores since creation. */
+long long itp2d_int8_rotations(itp2d_ctx* ctx);
+
 /* FP32 states: orthonormalise canonically only on every canonical_every-th
  * call and by a second-order Lowdin step in between, W = D (I + E)^{-1/2} with
  * D = diag(S)^{-1/2} and D S D = I + E, the series cut after E^2 (one k x k
@@ -206,6 +220,18 @@ int itp2d_set_fp32_between(itp2d_ctx* ctx, int method);
  * about tau^2 remain). A looser tau suits the first iterations of a solve,
  * whose basis the next step replaces. FP64 states are not affected. */
 int itp2d_set_fp32_eig_tolerance(itp2d_ctx* ctx, double tau);
+/* FP32 states: the canonical orthonormalisation's eigensolve runs at most
+ * max_sweeps Jacobi sweeps (0, the default: until the tolerance above); a
+ * capped solve is finished by a Cholesky factorisation S' = L L^H of the
+ * overlap of the states rotated onto its approximate eigenvectors V, in
+ * descending eigenvalue order (lowest energy first): W = V L^{-H}. The states
+ * are then orthonormal whatever the remaining off-diagonal elements, and the
+ * rotation is the canonical one up to them. A factorisation that fails
+ * falls back to the full eigensolve. FP64 states are not affected. */
+int itp2d_set_fp32_eig_sweeps(itp2d_ctx* ctx, int max_sweeps);
+/* Canonical orthonormalisations of FP32 states finished by the Cholesky step
+ * (itp2d_set_fp32_eig_sweeps) since creation. */
+long long itp2d_fp32_capped_eigensolves(itp2d_ctx* ctx);
 /* Rotations by an upper-triangular W (Cholesky steps, about half the
  * products of a dense rotation) since creation, per precision. */
 int itp2d_triangular_rotations(itp2d_ctx* ctx, long long* fp64, long long* fp32);

@@ -55,6 +55,11 @@ typedef struct {
 	int fp32_switch_span;     /* FP32 form: iterations over which the switch rule reads the
 	                             energy change (0: 3; 1: consecutive iterations with the
 	                             stall test alone) */
+	int fp32_eig_sweeps;      /* FP32 form: at most this many Jacobi sweeps in a canonical
+	                             step, finished by a Cholesky step
+	                             (itp2d_set_fp32_eig_sweeps); 0: full eigensolve */
+	int fp64_rotation;        /* ITP2D_ROTATION_DMMA (0) or ITP2D_ROTATION_INT8 for the
+	                             rotations of FP64 states (itp2d_set_fp64_rotation) */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libitp2d_b200.so")
 
-SOURCES = ["split.cu", "contract.cu", "jacobi.cu", "ctx.cu", "probe.cu", "noalloc.cu", "bjacobi.cu", "tc.cu", "rfft.cu", "bjacobi32.cu", "potential.cu", "lowdin.cu", "batch.cu", "cholesky.cu"]
+SOURCES = ["split.cu", "contract.cu", "jacobi.cu", "ctx.cu", "probe.cu", "noalloc.cu", "bjacobi.cu", "tc.cu", "rfft.cu", "bjacobi32.cu", "potential.cu", "lowdin.cu", "batch.cu", "cholesky.cu", "oz.cu"]
 HOST_SOURCES = [os.path.join("host", "itp2d_host.cpp"), os.path.join("host", "itp2d_serve.cpp")]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -575,10 +575,10 @@ __global__ void narrow_init_kernel(const double2* __restrict__ S, int k, int kp,
 }
 
 // The FP32 result widened into the FP64 work matrices the sort and the W build
-// read: the diagonal of the final A into A0 (whose result index becomes 0) and
-// V into the FP64 V.
+// read: the diagonal of the final A (all of it with full set) into A0 (whose
+// result index becomes 0) and V into the FP64 V.
 __global__ void widen_result_kernel(const float2* A0f, const float2* A1f, const float2* A2f, const float2* Vf,
-		int kp, int* counters, int max_sweeps, double2* A0, double2* V) {
+		int kp, int* counters, int max_sweeps, double2* A0, double2* V, int full) {
 	const int which = counters[max_sweeps + 1];
 	const float2* A = which == 0 ? A0f : (which == 1 ? A1f : A2f);
 	const long long n = (long long)kp * kp;
@@ -587,7 +587,8 @@ __global__ void widen_result_kernel(const float2* A0f, const float2* A1f, const 
 		const float2 v = Vf[idx];
 		V[idx] = make_double2(v.x, v.y);
 		const int i = (int)(idx / kp), j = (int)(idx % kp);
-		if (i == j) A0[idx] = make_double2(A[idx].x, 0.0);
+		if (full) A0[idx] = make_double2(A[idx].x, i == j ? 0.0 : A[idx].y);
+		else if (i == j) A0[idx] = make_double2(A[idx].x, 0.0);
 	}
 }
 
@@ -618,7 +619,7 @@ cudaError_t launch_bjacobi32(const double2* S, int k, JacobiWork& w, int num_sms
 	e = cudaLaunchCooperativeKernel((void*)bjacobi32_kernel, dim3(blocks), dim3(kThreads), args, smem, s);
 	if (e != cudaSuccess) return e;
 	widen_result_kernel<<<gblocks, 256, 0, s>>>(w.f32.A0, w.f32.A1, w.f32.A2, w.f32.V, kp, w.counters, ms, w.A0,
-			w.V);
+			w.V, w.full_result ? 1 : 0);
 	set_result_index_kernel<<<1, 1, 0, s>>>(w.counters, ms);
 	return cudaGetLastError();
 }

@@ -82,6 +82,9 @@ struct JacobiWork {
 		float2* V = nullptr;
 		float2* Qbuf = nullptr;  // bjacobi_qbuf_elems(k) elements
 	} f32;
+	// FP32 block path: widen all of the final A into A0 (the rotated overlap
+	// that launch_eig_cholesky_prep reads), not only its diagonal.
+	bool full_result = false;
 };
 
 // Smallest k solved by block Jacobi (when JacobiWork::Qbuf is set).
@@ -107,12 +110,32 @@ cudaError_t launch_eigensolve(double2* S, int k, JacobiWork& w, double2* W, EigS
 		cudaStream_t s);
 // Eigenvalues (ascending, w.evals), permutation (w.perm) and eigenvectors
 // (columns of w.V, kp x kp with kp = k rounded up to even) without the
-// overlap checks unless check != 0.
+// overlap checks unless check != 0; check 2 also accepts a solve that ended
+// at w.max_sweeps without converging (sweeps reported as w.max_sweeps).
 cudaError_t launch_eigh(double2* S, int k, JacobiWork& w, EigStatus* st, int num_sms, cudaStream_t s, int check);
+// Finish of a sweep-capped eigensolve (launch_eigh with check 2): with the
+// order p(a) = perm[k - 1 - a] (descending eigenvalue), S_out[a][b] =
+// A[p(a)][p(b)] (the final Jacobi matrix V^H S V, Hermitian part, k x k) and
+// VT[a][i] = V[i][p(a)] (k x k), for W = V_p L^{-H} with S_out = L L^H.
+cudaError_t launch_eig_cholesky_prep(const JacobiWork& w, int k, double2* S_out, double2* VT, cudaStream_t s);
 // Rayleigh-Ritz: eigenpairs of the Hermitian H (k x k, consumed) with
 // W[:, n] = V[:, p(n)] (unit columns, ascending eigenvalues in w.evals, any
 // sign) for the rotation psi' = psi W.
 cudaError_t launch_ritz(double2* H, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms, cudaStream_t s);
+
+// FP64 rotation out_n[g] = sum_i W[i][n] psi_i[g] on the int8 tensor cores
+// (oz.cu): both operands split into 8 int8 slices under per-row power-of-two
+// scales, slice products accumulated exactly in 32 bits, combined in FP64.
+// wsl (oz_w_bytes), psl (oz_psi_bytes) and ebuf (oz_exp_ints) are scratch;
+// a bounded wait that gives up sets *err to ITP2D_E_TIMEOUT. upper: W upper
+// triangular. oz_launches() kernels per call.
+bool oz_supported(int k, long long G);
+size_t oz_w_bytes(int k);
+size_t oz_psi_bytes(int k, long long G);
+size_t oz_exp_ints(int k, long long G);
+void launch_rotate_oz(const double2* W, const double2* psi, int k, long long G, unsigned char* wsl,
+		unsigned char* psl, int* ebuf, double2* out, int* err, cudaStream_t s, bool upper);
+int oz_launches();
 
 // Second-order Lowdin orthonormalisation (lowdin.cu): D = diag(S)^{-1/2},
 // E = D S D - I (row-major) and conj(E), stats = {max |E_ij|, sum |E_ij|^2,

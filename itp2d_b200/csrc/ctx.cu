@@ -97,6 +97,13 @@ struct itp2d_ctx {
 	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
 	int* dflag = nullptr;  // tensor-core wait time-outs (device)
 	unsigned char* wsplit = nullptr;  // W^T in BF16 planes (tensor-core rotation)
+	// FP64 rotation on the int8 tensor cores (allocated on first use)
+	int fp64_rotation = ITP2D_ROTATION_DMMA;
+	bool oz_failed = false;           // its scratch could not be allocated: DMMA
+	unsigned char* oz_w = nullptr;    // W slices
+	unsigned char* oz_psi = nullptr;  // state slices
+	int* oz_e = nullptr;              // row exponents
+	long long oz_calls = 0;
 	int* hflag = nullptr;  // pinned copy
 	// energies
 	double* sums = nullptr;
@@ -118,6 +125,8 @@ struct itp2d_ctx {
 	int canonical_every = 0;     // 0 or 1: always canonical
 	int between = ITP2D_BETWEEN_LOWDIN;
 	double fp32_tau = 1e-3;      // FP32 eigensolve: largest rotation tangent at which it stops
+	int fp32_sweep_cap = 0;      // FP32 canonical eigensolve: sweep cap with Cholesky finish (0: none)
+	long long capped_calls = 0;  // canonical FP32 steps finished by the Cholesky step
 	int since_canonical = 0;     // orthonormalisations since the last canonical one
 	long long ortho_calls[3] = {0, 0, 0};  // canonical, Lowdin, Cholesky
 	long long ritz_calls = 0;              // Rayleigh-Ritz steps
@@ -1127,6 +1136,32 @@ int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
 	return ITP2D_OK;
 }
 
+int itp2d_set_fp64_rotation(itp2d_ctx* c, int engine) {
+	if (!c || (engine != ITP2D_ROTATION_DMMA && engine != ITP2D_ROTATION_INT8)) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->fp64_rotation = engine;
+	return ITP2D_OK;
+}
+
+long long itp2d_int8_rotations(itp2d_ctx* c) {
+	if (!c) return -1;
+	std::lock_guard<std::mutex> g(c->mu);
+	return c->oz_calls;
+}
+
+int itp2d_set_fp32_eig_sweeps(itp2d_ctx* c, int max_sweeps) {
+	if (!c || max_sweeps < 0 || max_sweeps > 60) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->fp32_sweep_cap = max_sweeps;
+	return ITP2D_OK;
+}
+
+long long itp2d_fp32_capped_eigensolves(itp2d_ctx* c) {
+	if (!c) return -1;
+	std::lock_guard<std::mutex> g(c->mu);
+	return c->capped_calls;
+}
+
 int itp2d_triangular_rotations(itp2d_ctx* c, long long* fp64, long long* fp32) {
 	if (!c) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
@@ -1172,21 +1207,44 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 // success); the tensor-core rotation's status when it fails. upper: W is
 // upper triangular (Cholesky), each output tile reads only the states up to
 // its own last one (about half the products).
+// Scratch of the int8 FP64 rotation, allocated at the first use; false (and
+// the DMMA rotation from then on) when it does not fit.
+static bool oz_ready(itp2d_ctx* c) {
+	if (c->fp64_rotation != ITP2D_ROTATION_INT8 || c->oz_failed || !oz_supported(c->k, c->G)) return false;
+	if (c->oz_w && c->oz_psi && c->oz_e) return true;
+	cudaError_t e = cudaSuccess;
+	if (!c->oz_w) c->oz_w = (unsigned char*)dalloc(c, oz_w_bytes(c->k), &e);
+	if (e == cudaSuccess && !c->oz_psi) c->oz_psi = (unsigned char*)dalloc(c, oz_psi_bytes(c->k, c->G), &e);
+	if (e == cudaSuccess && !c->oz_e) c->oz_e = (int*)dalloc(c, oz_exp_ints(c->k, c->G) * sizeof(int), &e);
+	if (e != cudaSuccess) {
+		cudaGetLastError();  // an allocation failure is not sticky
+		c->oz_failed = true;
+		return false;
+	}
+	return true;
+}
+
 static int rotate_states(itp2d_ctx* c, bool tc, bool upper = false) {
 	const bool f64 = c->precision == ITP2D_FP64;
 	if (upper) c->tri_rot[c->precision]++;
+	const bool oz = !tc && f64 && oz_ready(c);
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
 			tc_rotate(c, upper);
+		else if (oz)
+			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_psi, c->oz_e,
+					(double2*)c->acc, c->dflag, c->stream, upper);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream, upper);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream, upper);
-		c->launches += tc ? 2 : 1;
+		c->launches += tc ? 2 : (oz ? oz_launches() : 1);
 	}
-	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	if (oz) c->oz_calls++;
+	const bool flagged = tc || oz;
+	if (flagged) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaGetLastError());
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
-	if (tc && *c->hflag != ITP2D_OK) {
+	if (flagged && *c->hflag != ITP2D_OK) {
 		const int f = *c->hflag;
 		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
 		return f;
@@ -1215,6 +1273,51 @@ static int cholesky_w(itp2d_ctx* c, int* bad_index, double* bad_value) {
 		if (bad_value) *bad_value = s.bad_value;
 	}
 	return s.status;
+}
+
+// Canonical step of FP32 states with a capped eigensolve (fp32_sweep_cap
+// sweeps of the FP32 block Jacobi, then W = V_p L^{-H} from the Cholesky
+// factorisation of the rotated overlap). Runs inside the eigensolve phase
+// timer. *done is false when the path does not apply or the factorisation
+// failed (c->S is intact: the caller runs the full eigensolve); a failed
+// eigenvalue check of the capped solve is returned as its status.
+static int capped_w(itp2d_ctx* c, bool* done, int* sweeps, int* bad_index, double* bad_value) {
+	*done = false;
+	JacobiWork& w = c->jw;
+	if (!w.f32.A0 || c->k < kBlockJacobiMinK) return ITP2D_OK;
+	const int ms = w.max_sweeps;
+	w.max_sweeps = c->fp32_sweep_cap;
+	w.full_result = true;
+	cudaError_t e = launch_eigh(c->S, c->k, w, c->dstat, c->num_sms, c->stream, 2);
+	w.full_result = false;
+	// the rotated overlap into part, V_p^T into A2 (free once the FP32 solve
+	// has widened its result)
+	if (e == cudaSuccess) e = launch_eig_cholesky_prep(w, c->k, c->part, w.A2, c->stream);
+	w.max_sweeps = ms;
+	ITP2D_TRY(e);
+	c->launches += 6;
+	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	const EigStatus es = *c->hstat;
+	if (es.status != ITP2D_OK) {
+		if (bad_index) *bad_index = es.bad_index;
+		if (bad_value) *bad_value = es.bad_value;
+		return es.status;
+	}
+	*sweeps = es.sweeps;
+	const int st = launch_cholesky_w(c->part, c->k, w.A0, w.A1, w.V, c->W, c->dstat, c->stream);
+	if (st != ITP2D_OK) return st;
+	c->launches += cholesky_launches(c->k);
+	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
+	ITP2D_TRY(cudaStreamSynchronize(c->stream));
+	if (c->hstat->status != ITP2D_OK) return ITP2D_OK;  // not positive definite: full eigensolve
+	// W = V_p W': out[i][n] = sum_m VT[m][i] W'[m][n]
+	launch_rotate(w.A2, c->W, c->k, (long long)c->k, w.A1, c->stream);
+	ITP2D_TRY(cudaMemcpyAsync(c->W, w.A1, (size_t)c->k * c->k * sizeof(double2), cudaMemcpyDeviceToDevice,
+			c->stream));
+	c->launches += 1;
+	*done = true;
+	return ITP2D_OK;
 }
 
 int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_value) {
@@ -1276,6 +1379,8 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 	}
 	c->since_canonical = 0;
 	c->ortho_calls[0]++;
+	bool capped = false;
+	int capped_sweeps = 0;
 	{
 		PhaseTimer t(c, kEigen);
 		// FP32 states: the overlap is accurate to about 1e-5; a final tangent of
@@ -1293,28 +1398,44 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 			c->jw.f32.V = c->jw.f32.A2 + kp2;
 			c->jw.f32.Qbuf = (float2*)c->jw.Qbuf;
 		}
-		ITP2D_TRY(launch_eigensolve(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
-		c->launches += 6;
+		if (!f64 && c->fp32_sweep_cap > 0) {
+			const int st = capped_w(c, &capped, &capped_sweeps, bad_index, bad_value);
+			if (st != ITP2D_OK) return st;
+		}
+		if (!capped) {
+			ITP2D_TRY(launch_eigensolve(c->S, c->k, c->jw, c->W, c->dstat, c->num_sms, c->stream));
+			c->launches += 6;
+		}
 	}
+	const bool oz = !tc && f64 && oz_ready(c);
 	{
 		PhaseTimer t(c, kRotate);
 		if (tc)
 			tc_rotate(c, false);
+		else if (oz)
+			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_psi, c->oz_e,
+					(double2*)c->acc, c->dflag, c->stream, false);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);
-		c->launches += tc ? 2 : 1;
+		c->launches += tc ? 2 : (oz ? oz_launches() : 1);
 	}
-	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	if (oz) c->oz_calls++;
+	const bool flagged = tc || oz;
+	if (flagged) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaGetLastError());
 	ITP2D_TRY(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(EigStatus), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
-	const EigStatus s = *c->hstat;
+	EigStatus s = *c->hstat;
+	if (capped) {
+		s.sweeps = capped_sweeps;  // the status read is the factorisation's
+		c->capped_calls++;
+	}
 	c->last_sweeps = s.sweeps;
 	if (s.sweeps > 0) {
 		c->sweeps_total += s.sweeps;
 		c->sweeps_p[f64 ? 0 : 1] += s.sweeps;
 	}
-	if (tc && *c->hflag != ITP2D_OK) {
+	if (flagged && *c->hflag != ITP2D_OK) {
 		const int f = *c->hflag;
 		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
 		return f;

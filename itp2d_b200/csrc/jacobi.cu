@@ -365,7 +365,9 @@ __global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* _
 		s.bad_value = 0.0;
 		s.pad = 0;
 		s.sweeps = counters[max_sweeps];
-		if (s.sweeps < 0) {
+		if (s.sweeps < 0 && check == 2) {
+			s.sweeps = max_sweeps;  // a capped solve: the caller finishes it
+		} else if (s.sweeps < 0) {
 			s.status = ITP2D_E_EIGENSOLVER;
 		} else if (first_bad < k) {
 			const int n = first_bad;
@@ -375,6 +377,26 @@ __global__ void eig_sort_kernel(const double2* __restrict__ A0, const double2* _
 			s.bad_value = v;
 		}
 		*st = s;
+	}
+}
+
+// S_out[a][b] = (A[p(a)][p(b)] + conj(A[p(b)][p(a)])) / 2 and VT[a][i] =
+// V[i][p(a)], p(a) = perm[k - 1 - a]: the overlap of the states rotated onto
+// the columns of V, largest eigenvalue (lowest energy) first.
+__global__ void eig_cholesky_prep_kernel(const double2* __restrict__ A0, const double2* __restrict__ A1,
+		const double2* __restrict__ A2, const double2* __restrict__ V, const int* __restrict__ perm,
+		const int* __restrict__ counters, int max_sweeps, int k, int kp, double2* __restrict__ S_out,
+		double2* __restrict__ VT) {
+	const int which = counters[max_sweeps + 1];
+	const double2* A = which == 0 ? A0 : (which == 1 ? A1 : A2);
+	const long long n2 = (long long)k * k;
+	for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n2;
+			idx += (long long)gridDim.x * blockDim.x) {
+		const int a = (int)(idx / k), b = (int)(idx % k);
+		const int pa = perm[k - 1 - a], pb = perm[k - 1 - b];
+		const double2 x = __ldcg(A + (long long)pa * kp + pb), y = __ldcg(A + (long long)pb * kp + pa);
+		S_out[idx] = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+		VT[idx] = __ldcg(V + (long long)b * kp + pa);
 	}
 }
 
@@ -430,6 +452,13 @@ cudaError_t launch_ritz(double2* H, int k, JacobiWork& w, double2* W, EigStatus*
 	const long long n2 = (long long)k * k;
 	ritz_w_kernel<<<(unsigned)std::min<long long>((n2 + 255) / 256, 4096), 256, 0, s>>>(w.V, k, jacobi_kp(w, k),
 			w.perm, W);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_eig_cholesky_prep(const JacobiWork& w, int k, double2* S_out, double2* VT, cudaStream_t s) {
+	const long long n2 = (long long)k * k;
+	eig_cholesky_prep_kernel<<<(unsigned)std::min<long long>((n2 + 255) / 256, 4096), 256, 0, s>>>(w.A0, w.A1, w.A2,
+			w.V, w.perm, w.counters, w.max_sweeps, k, jacobi_kp(w, k), S_out, VT);
 	return cudaGetLastError();
 }
 

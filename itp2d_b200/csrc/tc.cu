@@ -53,10 +53,13 @@
 
 #include "../../include/itp2d_gpu.h"
 #include "contract.cuh"
+#include "tcgen05.cuh"
 
 namespace itp2d {
 
 namespace {
+
+using namespace tcg;
 
 constexpr int TM = 128;                                // tile rows (M)
 constexpr int TN = 128;                                // tile cols (N)
@@ -66,8 +69,6 @@ constexpr int kPlaneBytes = TM * KT * 2;               // 4 KB: one BF16 plane o
 constexpr int kOperandBytes = 6 * kPlaneBytes;         // 24 KB: re/im x hi/mid/lo
 constexpr int kRawRowBytes = KT * 8;                   // 128 B: 16 complex FP32
 constexpr int kTmemCols = 512;
-constexpr long long kSpinLimit = 1LL << 24;            // back-stop on the number of polls
-constexpr unsigned long long kWaitNs = 1000000000ULL;  // a wait gives up after 1 s
 
 // Shared memory map (bytes from the 1024-aligned base).
 //   overlap:  planes[2] x (A, B) 96 KB | raw[3] x (A, B) 96 KB
@@ -84,74 +85,8 @@ static_assert(kOvRaw + 3 * kOvRawSlot <= kBufBytes, "overlap shared memory");
 static_assert(kRoRaw + 3 * kRoRawSlot <= kBufBytes, "rotation shared memory");
 static_assert(8 * 32 * 33 * 16 <= kBufBytes, "epilogue staging");
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// Shared-memory matrix descriptor: K-major, no swizzle, version 1.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-	const uint64_t lbo = 128, sbo = 256;
-	uint64_t d = 0;
-	d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-	d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-	d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-	d |= (uint64_t)1 << 46;
-	return d;
-}
-
 // Instruction descriptor: BF16 x BF16 -> F32, K-major A and B, M = 128, N = 128.
-__host__ __device__ constexpr uint32_t idesc(bool negate_a) {
-	return (1u << 4) | (1u << 7) | (1u << 10) | ((negate_a ? 1u : 0u) << 13) | ((uint32_t)(TN >> 3) << 17) |
-	       ((uint32_t)(TM >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
-	const uint32_t z = 0;
-	asm volatile(
-			"{\n\t.reg .pred p;\n\t"
-			"setp.ne.b32 p, %4, 0;\n\t"
-			"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-			:
-			: "r"(tmem_d), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-	unsigned long long t;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-	return t;
-}
-
-// Bounded wait for the phase with the given parity: false once kWaitNs of
-// wall time (or kSpinLimit polls) passed without the phase completing.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-	const unsigned long long t0 = global_ns();
-	for (long long i = 0; i < kSpinLimit; i++) {
-		uint32_t done;
-		asm volatile(
-				"{\n\t.reg .pred P1;\n\t"
-				"mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-				"selp.b32 %0, 1, 0, P1;\n\t}\n"
-				: "=r"(done)
-				: "r"(mbar), "r"(parity)
-				: "memory");
-		if (done) return true;
-		if (i > 64) {
-			__nanosleep(64);
-			if ((i & 255) == 0 && global_ns() - t0 > kWaitNs) return false;
-		}
-	}
-	return false;
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__host__ __device__ constexpr uint32_t idesc(bool negate_a) { return idesc_bf16(TN, negate_a); }
 
 // 16-byte global -> shared copy; src_bytes = 0 writes zeros without reading.
 __device__ __forceinline__ void cp16(uint32_t dst, const void* src, int src_bytes) {
@@ -160,22 +95,6 @@ __device__ __forceinline__ void cp16(uint32_t dst, const void* src, int src_byte
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-	uint32_t r[32];
-	asm volatile(
-			"tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-			"{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-			"%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-			: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-			  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-			  "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-			  "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-			: "r"(taddr));
-	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-	for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
-}
 
 // Byte offset of element (row r, k) of a K-major no-swizzle 128 x 16 plane:
 // core matrix (r / 8, k / 8) at ((r / 8) * 2 + k / 8) * 128, rows 16 B apart.
@@ -229,10 +148,10 @@ __device__ __forceinline__ void issue_step(uint32_t tmem, uint32_t abase, uint32
 		const uint64_t br = sdesc(bbase + q * kPlaneBytes), bi = sdesc(bbase + (3 + q) * kPlaneBytes);
 		// (a) A B:        re = ar br - ai bi,  im = ar bi + ai br
 		// (b) conj(A) B:  re = ar br + ai bi,  im = ar bi - ai br
-		umma(cre, ar, br, id, acc);
-		umma(cre, ai, bi, conjA ? id : idn, 1u);
-		umma(cim, ar, bi, id, acc);
-		umma(cim, ai, br, conjA ? idn : id, 1u);
+		umma_f16(cre, ar, br, id, acc);
+		umma_f16(cre, ai, bi, conjA ? id : idn, 1u);
+		umma_f16(cim, ar, bi, id, acc);
+		umma_f16(cim, ai, br, conjA ? idn : id, 1u);
 	}
 }
 
@@ -249,12 +168,7 @@ __device__ TcShared& tc_shared() {
 }
 
 __device__ void tc_setup(TcShared& sh) {
-	if (threadIdx.x < 32) {
-		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem_base)),
-				"r"(kTmemCols)
-				: "memory");
-		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-	}
+	if (threadIdx.x < 32) tmem_alloc(&sh.tmem_base, kTmemCols);
 	if (threadIdx.x == 0) {
 		mbar_init(smem_u32(&sh.mbar[0]), 1);
 		mbar_init(smem_u32(&sh.mbar[1]), 1);
@@ -269,9 +183,7 @@ __device__ void tc_setup(TcShared& sh) {
 __device__ void tc_teardown(TcShared& sh) {
 	tc_fence_before();
 	__syncthreads();
-	if (threadIdx.x < 32)
-		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh.tmem_base), "r"(kTmemCols)
-				: "memory");
+	if (threadIdx.x < 32) tmem_dealloc(sh.tmem_base, kTmemCols);
 }
 
 // The step pipeline. prefetch(s) issues the cp.async copies of step s (called
@@ -513,18 +425,6 @@ __global__ void split_psi_cols_kernel(const float2* __restrict__ psi, int k, lon
 		if (i + 1 < k) b = psi[(long long)(i + 1) * G + g];
 	}
 	put2(out + blk * kOperandBytes, kmaj_off(r, kk), a.x, a.y, b.x, b.y);
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-}
-
-// Contiguous global -> shared copy (16-byte aligned, size a multiple of 16)
-// completing on an mbarrier's transaction count.
-__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
-	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-			"l"(src), "r"(bytes), "r"(mbar)
-			: "memory");
 }
 
 constexpr int kRing = 4;                      // slots of (A, B) block pairs

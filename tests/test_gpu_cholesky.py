@@ -145,3 +145,102 @@ def test_mixed_solve_with_cholesky_steps_matches_fp64():
     assert np.max(np.abs(E64 - Em)) < 1e-8
     ref.close()
     mixed.close()
+
+
+def _span_distance(a, b, dx):
+    """Largest norm of a state of a outside the span of b (b orthonormal in FP64)."""
+    k = a.shape[0]
+    A, B = a.reshape(k, -1), b.reshape(k, -1)
+    C = (B.conj() @ A.T) * dx * dx          # C[j, n] = <b_j|a_n>
+    R = A - C.T @ B
+    return float(np.max(np.sqrt(np.sum(np.abs(R) ** 2, axis=1)) * dx))
+
+
+@pytest.mark.parametrize("cap", [1, 2, 60])
+def test_fp32_capped_eigensolve_is_finished_by_cholesky(cap):
+    """FP32 canonical step with the eigensolve capped at `cap` sweeps (k = 300:
+    the block Jacobi path): the states come out orthonormal to the FP32
+    contraction accuracy, span the input's space, and the solve reports at most
+    `cap` sweeps. Rotated states of a nearly diagonal overlap (propagated
+    eigenstate-like inputs) agree with the uncapped canonical step's."""
+    sx = sy = 64
+    k = 300
+    psi, dx = _states(sx, sy, k, seed=21, width2=None)
+    c = capi.Context(sx, sy, dx, k, precision=capi.FP32)
+    c.set_fp32_eig_sweeps(cap)
+    c.upload(psi)
+    before = c.download()
+    c.orthonormalize()
+    out = c.download()
+    assert c.orthonormalization_counts() == (1, 0, 0)
+    assert c.capped_eigensolves() == 1
+    assert 1 <= c.last_sweeps <= cap
+    orth = np.max(np.abs(_gram(out, dx) - np.eye(k)))
+    ref = _gram_schmidt(before, dx)
+    span = _span_distance(out, ref, dx)
+    print(f"capped FP32 eigensolve, {cap} sweeps max ({c.last_sweeps} run): orthonormality {orth:.1e}, "
+          f"span distance {span:.1e}")
+    assert orth < 2e-5
+    assert span < 1e-4
+    # a second step on orthonormal states (overlap I plus FP32 noise, whose
+    # eigenvectors are arbitrary): still orthonormal, same span
+    c.orthonormalize()
+    again = c.download()
+    assert c.capped_eigensolves() == 2
+    assert np.max(np.abs(_gram(again, dx) - np.eye(k))) < 2e-5
+    assert _span_distance(again, ref, dx) < 1e-4
+
+
+def test_fp32_capped_eigensolve_matches_canonical_on_a_near_diagonal_overlap():
+    """States that are nearly orthogonal with distinct norms (the overlap of
+    propagated, almost converged states: diagonal plus small couplings): the
+    capped step's states equal the canonical ones up to phase, to the FP32
+    accuracy, in the same (descending-norm) order."""
+    sx = sy = 64
+    k = 300
+    basis, dx = _states(sx, sy, k, seed=5, width2=None)
+    basis = _gram_schmidt(basis, dx)
+    rng = np.random.default_rng(9)
+    scale = np.exp(-0.05 * np.arange(k))                 # e^{-eps E_n}: distinct, well separated
+    mix = np.eye(k) + 1e-3 * (rng.standard_normal((k, k)) + 1j * rng.standard_normal((k, k)))
+    psi = (scale[:, None] * mix) @ basis.reshape(k, -1)
+    psi = psi.reshape(basis.shape)
+    outs = {}
+    for cap in (0, 2):
+        c = capi.Context(sx, sy, dx, k, precision=capi.FP32)
+        c.set_fp32_eig_sweeps(cap)
+        c.upload(psi)
+        c.orthonormalize()
+        outs[cap] = c.download()
+        assert c.capped_eigensolves() == (1 if cap else 0)
+    A, B = outs[0].reshape(k, -1), outs[2].reshape(k, -1)
+    # canonical: ascending eigenvalue order; capped: descending
+    X = (A[::-1].conj() @ B.T) * dx * dx
+    d = np.abs(np.diag(X))
+    print(f"near-diagonal overlap: min |<canonical_n|capped_n>| {d.min():.7f}")
+    assert np.min(d) > 1 - 1e-4
+
+
+def test_mixed_solve_with_capped_eigensolves_matches_fp64():
+    """A whole FP32-form solve whose canonical steps cap the eigensolve at two
+    sweeps (k = 260: the block Jacobi path) reaches the FP64 form's energies."""
+    from itp2d_b200 import system
+    common = dict(sx=64, sy=64, length=10.0, boundary=capi.PERIODIC, B=0.5, halforder=2, num_states=260,
+                  wanted=60, eps=[0.05], timestep_test="abschange(1e-9)", final_test="abschange(1e-9)",
+                  potential="harmonic(1)", max_steps=3000)
+    psi, _ = _states(64, 64, 260, seed=8)
+    ref = system.ITPSystem(system.Parameters(**common), init_states=psi)
+    ref.run()
+    mixed = system.ITPSystem(system.Parameters(precision=capi.FP32, fp32_switch=1e-7, fp32_canonical_every=3,
+                                               fp32_between=capi.BETWEEN_CHOLESKY, fp32_eig_sweeps=2, **common),
+                             init_states=psi)
+    mixed.run()
+    assert ref.finished and not ref.error_flag and mixed.finished and not mixed.error_flag
+    capped = capi.lib().itp2d_fp32_capped_eigensolves(mixed.context_handle())
+    print(f"mixed with capped eigensolves: {mixed.total_steps} iterations ({capped} capped); "
+          f"FP64 form {ref.total_steps}")
+    assert capped > 0
+    E64, Em = ref.energies()[0][:60], mixed.energies()[0][:60]
+    assert np.max(np.abs(E64 - Em)) < 1e-8
+    ref.close()
+    mixed.close()
