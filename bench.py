@@ -13,8 +13,9 @@ energy by less than 1e-9 between iterations (the reference's abschange(1e-9)
 as time-step and final test). The FP64 form orthonormalises canonically every
 step (the reference's algorithm); the mixed form's FP32 phase does so on every
 third iteration with Cholesky steps in between, and its FP64 refinement
-canonically, with the refinement's rotations on the int8 tensor cores
-(eight int8 slices per FP64 operand, exact integer sums; FP64 accuracy).
+canonically, with the refinement's overlaps and rotations on the int8 tensor
+cores (eight int8 slices per FP64 operand, exact integer sums; FP64
+accuracy).
 
 Workload "dot" (the magnetic dot): V = r^2/2, B = 1, periodic 256 x 256 grid
 of side 14, k = 500, 4th-order split (halforder 2), eps = 0.05, the 250 lowest
@@ -162,7 +163,7 @@ MIXED_CANONICAL_EVERY = 3
 # step (0: the full eigensolve).
 MIXED_EIG_SWEEPS = 0
 # Rotation engine of its FP64 refinement steps.
-MIXED_FP64_ROTATION = 1  # ITP2D_ROTATION_INT8
+MIXED_FP64_ENGINE = 1  # ITP2D_FP64_INT8
 
 
 def params(form: str):
@@ -178,7 +179,7 @@ def params(form: str):
                              fp32_canonical_every=MIXED_CANONICAL_EVERY if mixed else 0,
                              fp32_between=capi.BETWEEN_CHOLESKY,
                              fp32_eig_sweeps=MIXED_EIG_SWEEPS if mixed else 0,
-                             fp64_rotation=MIXED_FP64_ROTATION if mixed else capi.ROTATION_DMMA)
+                             fp64_engine=MIXED_FP64_ENGINE if mixed else capi.FP64_DMMA)
 
 
 def alg_bytes_split(w, b):
@@ -211,7 +212,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         return {prec: L.itp2d_precision_sweeps(ctx, code) for prec, code in (("fp64", capi.FP64), ("fp32", capi.FP32))}
 
     p0, l0, w0, tr0 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
-    i80 = L.itp2d_int8_rotations(ctx)
+    i80 = L.itp2d_int8_contractions(ctx)
     for _ in range(K):
         s.reset(psi)
         torch.cuda.synchronize()
@@ -226,7 +227,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         conv.append(s.num_converged)
         assert not s.error_flag, s.last_error
     p1, l1, w1, tr1 = phases(), L.itp2d_launch_count(ctx), sweeps(), capi.triangular_rotations(ctx)
-    i81 = L.itp2d_int8_rotations(ctx)
+    i81 = L.itp2d_int8_contractions(ctx)
     # per solve: {(precision, phase): (ms, calls)}
     stats = {key: ((p1[key][0] - p0[key][0]) / K, (p1[key][1] - p0[key][1]) / K) for key in p1}
     E, sig, res, idx = s.energies()
@@ -243,7 +244,7 @@ def run_form(form, psi, K, W, Ke2e, torch, stream, e2e_buf):
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     out = dict(times=times, steps=steps, conv=conv, stats=stats, sweeps={p: (w1[p] - w0[p]) / K for p in w1},
-               tri={p: (tr1[p] - tr0[p]) / K for p in tr1}, int8_rotations=(i81 - i80) / K,
+               tri={p: (tr1[p] - tr0[p]) / K for p in tr1}, int8_contractions=(i81 - i80) / K,
                launches=(l1 - l0) / K, E=E, e2e_times=e2e_times)
     s.close()
     return out
@@ -449,7 +450,9 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
     Algorithmic work per call:
       propagate  k G b [2 m (m + 2) + (m - 1)] bytes (b = 16 FP64, 8 FP32)
       energies   5 k G b bytes
-      overlap    FP64: 4 k^2 G flops (Hermitian half, complex MACs, DMMA)
+      overlap    FP64: 4 k^2 G flops (Hermitian half, complex MACs, DMMA), or with
+                 the int8 engine 36 MMAs of 128 x 128 x 32 per 16 grid points per
+                 (128 x 64 states) tile pair of the upper triangle
                  FP32 (tensor cores): BF16 MMA work issued, 24 MMAs of 128 x 128 x 16
                  per 16 grid points per upper-triangle tile pair of 128 states
       rotation   FP64: 8 k^2 G flops (DMMA), or with the int8 engine the int8 MMA
@@ -484,6 +487,9 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
     mma8 = 128 * 128 * 32 * 2
     oz_rotation = nt * ((G + 63) // 64) * ((k + 15) // 16) * 36 * mma8
     oz_rotation_tri = sum((min(k, 128 * (t + 1)) + 15) // 16 for t in range(nt)) * ((G + 63) // 64) * 36 * mma8
+    ntj = (k + 63) // 64
+    oz_overlap = sum(ntj - 2 * t for t in range(nt)) * ((G + 15) // 16) * 36 * mma8
+    int8 = r.get("int8_contractions", 0) > 0
     kp = (k + 31) // 32 * 32
     sweep_flops = (kp // 16 - 1) * 3 * 8 * 32 * kp * kp
     out = {}
@@ -505,10 +511,13 @@ def phase_rooflines(r, fp64_peak, fp32_peak):
             tri = min(r.get("tri", {}).get(prec, 0), calls) if ph == "rotation" else 0
             if tri:
                 total = amount * (calls - tri) + (tc_rotation_tri if tc else rotation_tri) * tri
-            if ph == "rotation" and prec == "fp64" and r.get("int8_rotations", 0) >= calls > 0:
+            if ph in ("rotation", "overlap") and prec == "fp64" and int8:
                 # the int8 engine: MMA work issued against the int8 rate
                 fp64_equiv = total / sec / 1e12
-                total = oz_rotation * (calls - tri) + oz_rotation_tri * tri
+                if ph == "rotation":
+                    total = oz_rotation * (calls - tri) + oz_rotation_tri * tri
+                else:
+                    total = oz_overlap * calls
                 ach = total / sec / 1e12
                 out[f"{ph}_{prec}"] = {"bound": "tensor", "achieved": ach, "peak": 2 * bf16, "unit": "TOP/s",
                                        "frac": ach / (2 * bf16), "ms_per_solve": ms, "calls_per_solve": calls,

@@ -184,19 +184,21 @@ int itp2d_column_variant(itp2d_ctx* ctx);
 enum { ITP2D_CONTRACT_AUTO = 0, ITP2D_CONTRACT_FP64 = 1, ITP2D_CONTRACT_TC_STAGED = 2 };
 int itp2d_set_contraction(itp2d_ctx* ctx, int engine);
 
-/* Rotation of FP64 states (psi' = psi W of every orthonormalisation):
- * ITP2D_ROTATION_DMMA (the default: FP64 tensor-core products) or
- * ITP2D_ROTATION_INT8 (the int8 tensor cores: both operands split into eight
- * int8 slices under per-row power-of-two scales, the slice products summed
- * exactly in 32-bit integers and combined in FP64; the result agrees with the
- * FP64 products to about 1e-15 of the largest output of each row; k < 8300).
- * INT8 takes 32 bytes per state and grid point of scratch at its first use; where
- * that cannot be allocated the DMMA rotation runs. FP32 states are not
- * affected. */
-enum { ITP2D_ROTATION_DMMA = 0, ITP2D_ROTATION_INT8 = 1 };
-int itp2d_set_fp64_rotation(itp2d_ctx* ctx, int engine);
-/* Rotations of FP64 states run on the int8 tensor cores since creation. */
-long long itp2d_int8_rotations(itp2d_ctx* ctx);
+/* Engine of the overlap S = Psi^H Psi dx^2 and the rotation psi' = psi W of
+ * itp2d_orthonormalize on FP64 states: ITP2D_FP64_DMMA (the default: FP64
+ * tensor-core products) or ITP2D_FP64_INT8 (the int8 tensor cores: both
+ * operands split into eight int8 slices under per-row power-of-two scales,
+ * the slice products summed exactly in 32-bit integers and combined in FP64;
+ * the results agree with FP64 products to about 1e-15 of the largest output
+ * of each row; k < 8300). INT8 takes about 48 bytes per state and grid point
+ * of scratch at its first use; where that cannot be allocated the DMMA
+ * contractions run. FP32 states, the Rayleigh-Ritz step and the batched and
+ * device-loop forms are not affected. */
+enum { ITP2D_FP64_DMMA = 0, ITP2D_FP64_INT8 = 1 };
+int itp2d_set_fp64_engine(itp2d_ctx* ctx, int engine);
+/* Overlaps and rotations of FP64 states run on the int8 tensor cores since
+ * creation. */
+long long itp2d_int8_contractions(itp2d_ctx* ctx);
 
 /* FP32 states: orthonormalise canonically only on every canonical_every-th
  * call and by a second-order Lowdin step in between, W = D (I + E)^{-1/2} with

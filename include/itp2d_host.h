@@ -58,8 +58,8 @@ typedef struct {
 	int fp32_eig_sweeps;      /* FP32 form: at most this many Jacobi sweeps in a canonical
 	                             step, finished by a Cholesky step
 	                             (itp2d_set_fp32_eig_sweeps); 0: full eigensolve */
-	int fp64_rotation;        /* ITP2D_ROTATION_DMMA (0) or ITP2D_ROTATION_INT8 for the
-	                             rotations of FP64 states (itp2d_set_fp64_rotation) */
+	int fp64_engine;        /* ITP2D_FP64_DMMA (0) or ITP2D_FP64_INT8 for the
+	                             rotations of FP64 states (itp2d_set_fp64_engine) */
 } itp2d_parameters;
 
 typedef struct itp2d_system itp2d_system;

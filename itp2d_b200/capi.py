@@ -27,7 +27,7 @@ ORTHO_DEFAULT, ORTHO_HIGHMEM, ORTHO_CHOLESKY = 0, 1, 2
 BETWEEN_LOWDIN, BETWEEN_CHOLESKY = 0, 1
 COL_SMEM, COL_TMA = 0, 1
 CONTRACT_AUTO, CONTRACT_FP64, CONTRACT_TC_STAGED = 0, 1, 2
-ROTATION_DMMA, ROTATION_INT8 = 0, 1
+FP64_DMMA, FP64_INT8 = 0, 1
 TRANSFORMS = ["FFT", "iFFT", "FFTx", "iFFTx", "FFTy", "iFFTy", "DST", "iDST", "DSTx", "iDSTx",
               "DSTy", "iDSTy", "DCT", "iDCT", "DCTx", "iDCTx", "DCTy", "iDCTy"]
 
@@ -74,9 +74,9 @@ def lib():
         L.itp2d_orthonormalization_counts.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 3
         L.itp2d_set_fp32_between.argtypes = [vp, i]
         L.itp2d_set_fp32_eig_sweeps.argtypes = [vp, i]
-        L.itp2d_set_fp64_rotation.argtypes = [vp, i]
-        L.itp2d_int8_rotations.argtypes = [vp]
-        L.itp2d_int8_rotations.restype = C.c_longlong
+        L.itp2d_set_fp64_engine.argtypes = [vp, i]
+        L.itp2d_int8_contractions.argtypes = [vp]
+        L.itp2d_int8_contractions.restype = C.c_longlong
         L.itp2d_fp32_capped_eigensolves.argtypes = [vp]
         L.itp2d_fp32_capped_eigensolves.restype = C.c_longlong
         L.itp2d_rayleigh_ritz.argtypes = [vp, dp]
@@ -263,13 +263,13 @@ class Context:
         Cholesky step (0: full eigensolve)."""
         _check(lib().itp2d_set_fp32_eig_sweeps(self.h, int(max_sweeps)), "itp2d_set_fp32_eig_sweeps")
 
-    def set_fp64_rotation(self, engine):
-        """ROTATION_DMMA (default) or ROTATION_INT8 for the rotation of FP64 states."""
-        _check(lib().itp2d_set_fp64_rotation(self.h, int(engine)), "itp2d_set_fp64_rotation")
+    def set_fp64_engine(self, engine):
+        """FP64_DMMA (default) or FP64_INT8 for the rotation of FP64 states."""
+        _check(lib().itp2d_set_fp64_engine(self.h, int(engine)), "itp2d_set_fp64_engine")
 
-    def int8_rotations(self) -> int:
+    def int8_contractions(self) -> int:
         """Rotations of FP64 states run on the int8 tensor cores since creation."""
-        return lib().itp2d_int8_rotations(self.h)
+        return lib().itp2d_int8_contractions(self.h)
 
     def capped_eigensolves(self) -> int:
         """Canonical FP32 steps finished by the Cholesky step since creation."""

@@ -123,18 +123,24 @@ cudaError_t launch_eig_cholesky_prep(const JacobiWork& w, int k, double2* S_out,
 // sign) for the rotation psi' = psi W.
 cudaError_t launch_ritz(double2* H, int k, JacobiWork& w, double2* W, EigStatus* st, int num_sms, cudaStream_t s);
 
-// FP64 rotation out_n[g] = sum_i W[i][n] psi_i[g] on the int8 tensor cores
-// (oz.cu): both operands split into 8 int8 slices under per-row power-of-two
-// scales, slice products accumulated exactly in 32 bits, combined in FP64.
-// wsl (oz_w_bytes), psl (oz_psi_bytes) and ebuf (oz_exp_ints) are scratch;
-// a bounded wait that gives up sets *err to ITP2D_E_TIMEOUT. upper: W upper
-// triangular. oz_launches() kernels per call.
+// FP64 rotation out_n[g] = sum_i W[i][n] psi_i[g] and overlap S = Psi^H Psi
+// dx^2 on the int8 tensor cores (oz.cu): both operands split into 8 int8
+// slices under per-row power-of-two scales, slice products accumulated
+// exactly in 32 bits, combined in FP64. wsl (oz_w_bytes), scratch
+// (oz_scratch_bytes) and ebuf (oz_exp_ints) are scratch; a bounded wait that
+// gives up sets *err to ITP2D_E_TIMEOUT. upper: W upper triangular. The
+// overlap writes nsplit (oz_overlap_splits, at most max_splits) partial
+// blocks into part and sums them into S (launch_overlap_finish).
+// oz_launches() kernels per call of either.
 bool oz_supported(int k, long long G);
 size_t oz_w_bytes(int k);
-size_t oz_psi_bytes(int k, long long G);
+size_t oz_scratch_bytes(int k, long long G);
 size_t oz_exp_ints(int k, long long G);
 void launch_rotate_oz(const double2* W, const double2* psi, int k, long long G, unsigned char* wsl,
-		unsigned char* psl, int* ebuf, double2* out, int* err, cudaStream_t s, bool upper);
+		unsigned char* scratch, int* ebuf, double2* out, int* err, cudaStream_t s, bool upper);
+int oz_overlap_splits(int k, long long G, int num_sms, int max_splits);
+void launch_overlap_oz(const double2* psi, int k, long long G, int nsplit, unsigned char* scratch, int* ebuf,
+		double2* part, double dx2, double2* S, int* err, cudaStream_t s);
 int oz_launches();
 
 // Second-order Lowdin orthonormalisation (lowdin.cu): D = diag(S)^{-1/2},

@@ -97,11 +97,12 @@ struct itp2d_ctx {
 	int tc_nsplit = 1;  // grid chunks of the tensor-core overlap
 	int* dflag = nullptr;  // tensor-core wait time-outs (device)
 	unsigned char* wsplit = nullptr;  // W^T in BF16 planes (tensor-core rotation)
-	// FP64 rotation on the int8 tensor cores (allocated on first use)
-	int fp64_rotation = ITP2D_ROTATION_DMMA;
-	bool oz_failed = false;           // its scratch could not be allocated: DMMA
+	// FP64 overlap and rotation on the int8 tensor cores (scratch allocated on first use)
+	int fp64_engine = ITP2D_FP64_DMMA;
+	bool oz_failed = false;           // the scratch could not be allocated: DMMA
 	unsigned char* oz_w = nullptr;    // W slices
-	unsigned char* oz_psi = nullptr;  // state slices
+	unsigned char* oz_scratch = nullptr;  // state slices
+	int oz_nsplit = 1;                // grid splits of the int8 overlap
 	int* oz_e = nullptr;              // row exponents
 	long long oz_calls = 0;
 	int* hflag = nullptr;  // pinned copy
@@ -1060,6 +1061,8 @@ int itp2d_transform(itp2d_ctx* c, int kind) {
 	return cuda_status(cudaGetLastError());
 }
 
+static bool oz_ready(itp2d_ctx* c);
+
 namespace {
 
 bool use_tensor_cores(const itp2d_ctx* c) {
@@ -1095,6 +1098,13 @@ void tc_rotate(itp2d_ctx* c, bool upper) {
 
 // S = Psi^H Psi dx^2 (full Hermitian, row-major) by the selected engine.
 void launch_overlap_any(itp2d_ctx* c, bool tc) {
+	if (!tc && c->precision == ITP2D_FP64 && oz_ready(c)) {
+		launch_overlap_oz((const double2*)c->psi, c->k, c->G, c->oz_nsplit, c->oz_scratch, c->oz_e, c->part,
+				c->dx * c->dx, c->S, c->dflag, c->stream);
+		c->launches += oz_launches();
+		c->oz_calls++;
+		return;
+	}
 	if (tc)
 		if (presplit_ready(c))
 			launch_overlap_tc_presplit((const float2*)c->psi, c->k, c->G, c->tc_nsplit, c->tc_rows, c->part,
@@ -1136,14 +1146,14 @@ int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
 	return ITP2D_OK;
 }
 
-int itp2d_set_fp64_rotation(itp2d_ctx* c, int engine) {
-	if (!c || (engine != ITP2D_ROTATION_DMMA && engine != ITP2D_ROTATION_INT8)) return ITP2D_E_INVALID;
+int itp2d_set_fp64_engine(itp2d_ctx* c, int engine) {
+	if (!c || (engine != ITP2D_FP64_DMMA && engine != ITP2D_FP64_INT8)) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);
-	c->fp64_rotation = engine;
+	c->fp64_engine = engine;
 	return ITP2D_OK;
 }
 
-long long itp2d_int8_rotations(itp2d_ctx* c) {
+long long itp2d_int8_contractions(itp2d_ctx* c) {
 	if (!c) return -1;
 	std::lock_guard<std::mutex> g(c->mu);
 	return c->oz_calls;
@@ -1193,9 +1203,10 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 	launch_overlap_any(c, tc);
 	ITP2D_TRY(cudaGetLastError());
 	ITP2D_TRY(cudaMemcpyAsync(S, c->S, (size_t)c->k * c->k * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-	if (tc) ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	// the tensor-core overlaps (BF16 planes, int8 slices) flag a bounded wait that gave up
+	ITP2D_TRY(cudaMemcpyAsync(c->hflag, c->dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
 	ITP2D_TRY(cudaStreamSynchronize(c->stream));
-	if (tc && *c->hflag != ITP2D_OK) {
+	if (*c->hflag != ITP2D_OK) {
 		const int f = *c->hflag;
 		ITP2D_TRY(cudaMemset(c->dflag, 0, sizeof(int)));
 		return f;
@@ -1207,14 +1218,15 @@ int itp2d_overlap_matrix(itp2d_ctx* c, double* S) {
 // success); the tensor-core rotation's status when it fails. upper: W is
 // upper triangular (Cholesky), each output tile reads only the states up to
 // its own last one (about half the products).
-// Scratch of the int8 FP64 rotation, allocated at the first use; false (and
-// the DMMA rotation from then on) when it does not fit.
+// Scratch of the int8 FP64 contractions, allocated at the first use; false
+// (and the DMMA contractions from then on) when it does not fit.
 static bool oz_ready(itp2d_ctx* c) {
-	if (c->fp64_rotation != ITP2D_ROTATION_INT8 || c->oz_failed || !oz_supported(c->k, c->G)) return false;
-	if (c->oz_w && c->oz_psi && c->oz_e) return true;
+	if (c->fp64_engine != ITP2D_FP64_INT8 || c->oz_failed || !oz_supported(c->k, c->G)) return false;
+	if (c->oz_w && c->oz_scratch && c->oz_e) return true;
+	c->oz_nsplit = oz_overlap_splits(c->k, c->G, c->num_sms, std::max(c->nsplit, c->tc_nsplit));
 	cudaError_t e = cudaSuccess;
 	if (!c->oz_w) c->oz_w = (unsigned char*)dalloc(c, oz_w_bytes(c->k), &e);
-	if (e == cudaSuccess && !c->oz_psi) c->oz_psi = (unsigned char*)dalloc(c, oz_psi_bytes(c->k, c->G), &e);
+	if (e == cudaSuccess && !c->oz_scratch) c->oz_scratch = (unsigned char*)dalloc(c, oz_scratch_bytes(c->k, c->G), &e);
 	if (e == cudaSuccess && !c->oz_e) c->oz_e = (int*)dalloc(c, oz_exp_ints(c->k, c->G) * sizeof(int), &e);
 	if (e != cudaSuccess) {
 		cudaGetLastError();  // an allocation failure is not sticky
@@ -1233,7 +1245,7 @@ static int rotate_states(itp2d_ctx* c, bool tc, bool upper = false) {
 		if (tc)
 			tc_rotate(c, upper);
 		else if (oz)
-			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_psi, c->oz_e,
+			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_scratch, c->oz_e,
 					(double2*)c->acc, c->dflag, c->stream, upper);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream, upper);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream, upper);
@@ -1413,7 +1425,7 @@ int itp2d_orthonormalize(itp2d_ctx* c, int algo, int* bad_index, double* bad_val
 		if (tc)
 			tc_rotate(c, false);
 		else if (oz)
-			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_psi, c->oz_e,
+			launch_rotate_oz(c->W, (const double2*)c->psi, c->k, c->G, c->oz_w, c->oz_scratch, c->oz_e,
 					(double2*)c->acc, c->dflag, c->stream, false);
 		else if (f64) launch_rotate(c->W, (const double2*)c->psi, c->k, c->G, (double2*)c->acc, c->stream);
 		else launch_rotate(c->W, (const float2*)c->psi, c->k, c->G, (float2*)c->acc, c->stream);

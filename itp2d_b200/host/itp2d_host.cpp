@@ -269,7 +269,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
 	check(itp2d_set_fp32_between(ctx, p.fp32_between), "itp2d_set_fp32_between");
 	check(itp2d_set_fp32_eig_sweeps(ctx, p.fp32_eig_sweeps), "itp2d_set_fp32_eig_sweeps");
-	check(itp2d_set_fp64_rotation(ctx, p.fp64_rotation), "itp2d_set_fp64_rotation");
+	check(itp2d_set_fp64_engine(ctx, p.fp64_engine), "itp2d_set_fp64_engine");
 	check(itp2d_set_potential(ctx, null_potential ? nullptr : V.data()), "itp2d_set_potential");
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
 	initial_states = params.initial_states;
@@ -845,7 +845,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->switch_rayleigh_ritz = 0;
 	p->fp32_switch_span = 0;
 	p->fp32_eig_sweeps = 0;
-	p->fp64_rotation = ITP2D_ROTATION_DMMA;
+	p->fp64_engine = ITP2D_FP64_DMMA;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");
 	std::strcpy(p->final_test, "relstdev(1e-3,0)");
