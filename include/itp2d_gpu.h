@@ -210,6 +210,10 @@ long long itp2d_int8_contractions(itp2d_ctx* ctx);
  * FP64 states are always orthonormalised canonically. No reference
  * counterpart (stateset.cpp:136-232 is the canonical form). */
 int itp2d_set_fp32_orthonormalization(itp2d_ctx* ctx, int canonical_every);
+/* Moves the next canonical step of that schedule `calls` orthonormalisations
+ * later (the schedule then continues every canonical_every-th call). Called
+ * after itp2d_set_fp32_orthonormalization, which restarts the schedule. */
+int itp2d_set_fp32_canonical_delay(itp2d_ctx* ctx, int calls);
 /* The orthonormalisation between the canonical calls of
  * itp2d_set_fp32_orthonormalization: ITP2D_BETWEEN_LOWDIN (the default, taken
  * only while the overlap is close to the identity) or ITP2D_BETWEEN_CHOLESKY

@@ -58,6 +58,9 @@ typedef struct {
 	int fp32_eig_sweeps;      /* FP32 form: at most this many Jacobi sweeps in a canonical
 	                             step, finished by a Cholesky step
 	                             (itp2d_set_fp32_eig_sweeps); 0: full eigensolve */
+	int fp32_canonical_delay; /* FP32 form: the first canonical step comes this many
+	                             iterations later than fp32_canonical_every puts it
+	                             (itp2d_set_fp32_canonical_delay) */
 	int fp64_engine;        /* ITP2D_FP64_DMMA (0) or ITP2D_FP64_INT8 for the
 	                             rotations of FP64 states (itp2d_set_fp64_engine) */
 } itp2d_parameters;

@@ -1139,6 +1139,13 @@ int itp2d_set_fp32_orthonormalization(itp2d_ctx* c, int canonical_every) {
 	return ITP2D_OK;
 }
 
+int itp2d_set_fp32_canonical_delay(itp2d_ctx* c, int calls) {
+	if (!c || calls < 0) return ITP2D_E_INVALID;
+	std::lock_guard<std::mutex> g(c->mu);
+	c->since_canonical = -calls;
+	return ITP2D_OK;
+}
+
 int itp2d_set_fp32_eig_tolerance(itp2d_ctx* c, double tau) {
 	if (!c || !(tau > 0.0) || tau > 1.0) return ITP2D_E_INVALID;
 	std::lock_guard<std::mutex> g(c->mu);

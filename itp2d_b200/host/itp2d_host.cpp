@@ -267,6 +267,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 			"itp2d_ctx_create");
 	check(itp2d_set_timing(ctx, 1), "itp2d_set_timing");
 	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
+	check(itp2d_set_fp32_canonical_delay(ctx, p.fp32_canonical_delay), "itp2d_set_fp32_canonical_delay");
 	check(itp2d_set_fp32_between(ctx, p.fp32_between), "itp2d_set_fp32_between");
 	check(itp2d_set_fp32_eig_sweeps(ctx, p.fp32_eig_sweeps), "itp2d_set_fp32_eig_sweeps");
 	check(itp2d_set_fp64_engine(ctx, p.fp64_engine), "itp2d_set_fp64_engine");
@@ -787,6 +788,9 @@ void ITPSystem::reset(const double* init) {
 		precision = p.precision;
 	}
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
+	// the FP32 form's canonical schedule restarts with the solve
+	check(itp2d_set_fp32_orthonormalization(ctx, p.fp32_canonical_every), "itp2d_set_fp32_orthonormalization");
+	check(itp2d_set_fp32_canonical_delay(ctx, p.fp32_canonical_delay), "itp2d_set_fp32_canonical_delay");
 	if (init) {
 		initial_states.clear();  // a later recovery re-randomises like the reference
 		check(itp2d_upload_states(ctx, init), "itp2d_upload_states");
@@ -845,6 +849,7 @@ void itp2d_parameters_default(itp2d_parameters* p) {
 	p->switch_rayleigh_ritz = 0;
 	p->fp32_switch_span = 0;
 	p->fp32_eig_sweeps = 0;
+	p->fp32_canonical_delay = 0;
 	p->fp64_engine = ITP2D_FP64_DMMA;
 	std::strcpy(p->potential, "harmonic");
 	std::strcpy(p->timestep_test, "relstdev(1e-3,1e-4)");

@@ -24,7 +24,7 @@ class _Params(C.Structure):
         ("potential", C.c_char * 128), ("timestep_test", C.c_char * 128), ("final_test", C.c_char * 128),
         ("fp32_canonical_every", C.c_int), ("fp32_between", C.c_int), ("switch_rayleigh_ritz", C.c_int),
         ("fp32_switch_span", C.c_int), ("fp32_eig_sweeps", C.c_int),
-        ("fp64_engine", C.c_int),
+        ("fp32_canonical_delay", C.c_int), ("fp64_engine", C.c_int),
     ]
 
 
@@ -121,6 +121,7 @@ class Parameters:
     switch_rayleigh_ritz: bool = False
     fp32_switch_span: int = 0
     fp32_eig_sweeps: int = 0
+    fp32_canonical_delay: int = 0
     fp64_engine: int = capi.FP64_DMMA
     potential: str = "harmonic"
     timestep_test: str = "relstdev(1e-3,1e-4)"
@@ -131,7 +132,7 @@ class Parameters:
         _lib().itp2d_parameters_default(C.byref(p))
         for k in ["sx", "sy", "length", "boundary", "B", "halforder", "num_states", "wanted", "ignore_lowest",
                   "eps_divisor", "max_steps", "min_eps", "seed", "ortho_algorithm", "precision", "fp32_switch",
-                  "fp32_canonical_every", "fp32_between", "fp32_switch_span", "fp32_eig_sweeps", "fp64_engine"]:
+                  "fp32_canonical_every", "fp32_between", "fp32_switch_span", "fp32_eig_sweeps", "fp32_canonical_delay", "fp64_engine"]:
             setattr(p, k, getattr(self, k))
         p.exhaust_eps, p.recover = int(self.exhaust_eps), int(self.recover)
         p.switch_rayleigh_ritz = int(self.switch_rayleigh_ritz)

@@ -143,7 +143,7 @@ def test_parameter_defaults_match_the_reference_and_leave_extensions_off():
     assert p.precision == capi.FP64 and p.fp32_switch == 0.0
     assert p.fp32_canonical_every == 0 and p.fp32_between == capi.BETWEEN_LOWDIN
     assert p.switch_rayleigh_ritz == 0 and p.fp32_switch_span == 0 and p.fp32_eig_sweeps == 0
-    assert p.fp64_engine == 0
+    assert p.fp64_engine == 0 and p.fp32_canonical_delay == 0
     assert p.timestep_test == b"relstdev(1e-3,1e-4)" and p.final_test == b"relstdev(1e-3,0)"
 
 
