@@ -1097,8 +1097,11 @@ void tc_rotate(itp2d_ctx* c, bool upper) {
 }
 
 // S = Psi^H Psi dx^2 (full Hermitian, row-major) by the selected engine.
-void launch_overlap_any(itp2d_ctx* c, bool tc) {
-	if (!tc && c->precision == ITP2D_FP64 && oz_ready(c)) {
+// int8: the FP64 int8 engine may run (itp2d_overlap_matrix and
+// itp2d_orthonormalize; the batched form and the captured device loop keep
+// DMMA: they read no timeout flag, and the loop allocates nothing).
+void launch_overlap_any(itp2d_ctx* c, bool tc, bool int8 = true) {
+	if (int8 && !tc && c->precision == ITP2D_FP64 && oz_ready(c)) {
 		launch_overlap_oz((const double2*)c->psi, c->k, c->G, c->oz_nsplit, c->oz_scratch, c->oz_e, c->part,
 				c->dx * c->dx, c->S, c->dflag, c->stream);
 		c->launches += oz_launches();
@@ -1709,7 +1712,7 @@ int itp2d_batch_orthonormalize(int n, itp2d_ctx* const* ctxs, int* status, int* 
 		c->ortho_calls[0]++;
 		{
 			PhaseTimer t(c, kOverlap);
-			launch_overlap_any(c, use_tensor_cores(c));
+			launch_overlap_any(c, use_tensor_cores(c), false);
 		}
 		cudaEventRecord(ev[i], c->stream);
 		cudaStreamWaitEvent(g_batch_stream, ev[i], 0);
@@ -1986,7 +1989,7 @@ int itp2d_run_device_loop(itp2d_ctx* c, int max_iterations, int test, double lim
 		const bool tc = use_tensor_cores(c);
 		if (c->precision == ITP2D_FP64) propagate_fused<double>(c);
 		else propagate_fused<float>(c);
-		launch_overlap_any(c, tc);
+		launch_overlap_any(c, tc, false);
 		launch_batched_eigensolve(item, 1, 60, k, loop + 7, c->stream);
 		if (tc)
 			tc_rotate(c, false);
