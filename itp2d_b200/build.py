@@ -18,7 +18,8 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libitp2d_b200.so")
 
 SOURCES = ["split.cu", "contract.cu", "jacobi.cu", "ctx.cu", "probe.cu", "noalloc.cu", "bjacobi.cu", "tc.cu", "rfft.cu", "bjacobi32.cu", "potential.cu", "lowdin.cu", "batch.cu", "cholesky.cu", "oz.cu"]
-HOST_SOURCES = [os.path.join("host", "itp2d_host.cpp"), os.path.join("host", "itp2d_serve.cpp")]
+HOST_SOURCES = [os.path.join("host", "itp2d_host.cpp"), os.path.join("host", "itp2d_serve.cpp"),
+                os.path.join("host", "itp2d_datafile.cpp")]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -57,7 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(OBJ, os.path.basename(h).replace(".cpp", ".o"))
         objs.append(obj)
         deps = [src, os.path.join(HERE, "host", "itp2d_host.hpp"), os.path.join(ROOT, "include", "itp2d_gpu.h"),
-                os.path.join(ROOT, "include", "itp2d_host.h")]
+                os.path.join(ROOT, "include", "itp2d_host.h"), os.path.join(ROOT, "include", "itp2d_datafile.h")]
         if force or not os.path.exists(obj) or max(os.path.getmtime(d) for d in deps) > os.path.getmtime(obj):
             cmd = ["g++", *CXX_FLAGS, "-c", src, "-o", obj]
             procs.append((h, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

@@ -6,10 +6,13 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <ctime>
 #include <sstream>
 #include <thread>
 
 #include <unistd.h>
+
+#include "../../include/itp2d_datafile.h"
 
 namespace itp2d {
 
@@ -254,6 +257,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 		if (params.user_potential.size() != dl.N) throw GeneralError("user potential has the wrong size");
 		for (size_t i = 0; i < dl.N; i++) V[i] += params.user_potential[i];
 		null_potential = false;
+		user_noise = true;
 	}
 	for (int i = 0; i < p.num_eps; i++) eps_values.push_back(p.eps[i]);
 	if (!eps_values.empty()) {
@@ -262,6 +266,7 @@ ITPSystem::ITPSystem(const Parameters& params, void* stream)
 	} else {
 		eps = 0.5;  // Parameters::default_initial_eps
 	}
+	eps_history.assign(1, std::make_pair(1, eps));
 	precision = p.precision;
 	check(itp2d_ctx_create(p.sx, p.sy, dl.dx, p.num_states, p.boundary, p.B, p.halforder, precision, stream, &ctx),
 			"itp2d_ctx_create");
@@ -501,6 +506,7 @@ void ITPSystem::change_time_step() {
 		return;
 	}
 	check(itp2d_set_time_step(ctx, eps), "itp2d_set_time_step");
+	eps_history.emplace_back(total_step_counter + 1, eps);
 	step_counter = 0;
 	all_timestep_converged = false;
 	std::fill(timestep_converged.begin(), timestep_converged.end(), false);
@@ -783,6 +789,7 @@ void ITPSystem::reset(const double* init) {
 	} else {
 		eps = 0.5;
 	}
+	eps_history.assign(1, std::make_pair(1, eps));
 	if (precision != p.precision) {
 		check(itp2d_set_precision(ctx, p.precision), "itp2d_set_precision");
 		precision = p.precision;
@@ -990,6 +997,101 @@ int itp2d_system_times(itp2d_system* s, double* t7) {
 		return e.status;
 	}
 	return ITP2D_OK;
+}
+
+// The reference ITPSystem's datafile with --save final states, written at the
+// end of a solve from the driver's records (itpsystem.cpp:69-116 attributes,
+// potential and noise; 113-114, 220-226 time steps; 399-402 histories;
+// 513-531 final states, energies and run attributes).
+int itp2d_system_write_datafile(itp2d_system* s, const char* filename, int clobber, int save_states) {
+	if (!s || !s->sys || !filename) return ITP2D_E_INVALID;
+	itp2d::ITPSystem& sys = *s->sys;
+	const itp2d_parameters& p = sys.p;
+	const itp2d::DataLayout& dl = sys.datalayout();
+	const double t0 = itp2d::now_s();
+	itp2d_datafile* f = nullptr;
+	int st = itp2d_datafile_create(filename, (int)dl.sizex, (int)dl.sizey, dl.dx, clobber, &f);
+	auto ok = [&](int status) {
+		if (st == ITP2D_OK && status != ITP2D_OK) {
+			st = status;
+			s->err = itp2d_datafile_last_error();
+		}
+	};
+	if (st != ITP2D_OK) {
+		s->err = itp2d_datafile_last_error();
+		return st;
+	}
+	char timestring[32] = "";
+	const std::time_t now = std::time(nullptr);
+	std::tm utc;
+	if (gmtime_r(&now, &utc)) std::strftime(timestring, sizeof timestring, "%Y-%m-%d %H:%M:%SZ", &utc);
+	ok(itp2d_datafile_add_attribute_string(f, "program_version", "itp2d_b200"));
+	ok(itp2d_datafile_add_attribute_ulong(f, "random_seed", p.seed));
+	ok(itp2d_datafile_add_attribute_string(f, "start_time", timestring));
+	ok(itp2d_datafile_add_attribute_ulong(f, "num_threads", 1));
+	ok(itp2d_datafile_add_attribute_int(f, "num_states", p.num_states));
+	ok(itp2d_datafile_add_attribute_int(f, "num_wanted_to_converge", p.wanted));
+	ok(itp2d_datafile_add_attribute_int(f, "ignore_lowest", p.ignore_lowest));
+	ok(itp2d_datafile_add_attribute_double(f, "grid_length", dl.lenx));
+	ok(itp2d_datafile_add_attribute_string(f, "grid_boundary_type",
+			p.boundary == ITP2D_DIRICHLET ? "dirichlet" : "periodic"));
+	ok(itp2d_datafile_add_attribute_int(f, "operator_splitting_order", 2 * p.halforder));
+	ok(itp2d_datafile_add_attribute_string(f, "potential", p.potential));
+	ok(itp2d_datafile_add_attribute_string(f, "noise", sys.has_user_noise() ? "user" : "none"));
+	ok(itp2d_datafile_add_attribute_string(f, "impurity_type", "N/A"));
+	ok(itp2d_datafile_add_attribute_string(f, "impurity_distribution", "N/A"));
+	ok(itp2d_datafile_add_attribute_string(f, "impurity_constraint", "none"));
+	ok(itp2d_datafile_add_attribute_string(f, "timestep_convergence_test",
+			sys.timestep_test().get_description().c_str()));
+	ok(itp2d_datafile_add_attribute_string(f, "final_convergence_test",
+			sys.final_convergence_test().get_description().c_str()));
+	ok(itp2d_datafile_add_attribute_double(f, "magnetic_field_strength", p.B));
+	if (!sys.is_null_potential() && sys.get_potential().size() == dl.N)
+		ok(itp2d_datafile_write_potential(f, sys.get_potential().data()));
+	ok(itp2d_datafile_write_noise_realization(f, nullptr, 0));
+	if (!sys.eps_history.empty()) ok(itp2d_datafile_add_attribute_double(f, "initial_time_step", sys.eps_history[0].second));
+	for (const auto& e : sys.eps_history) ok(itp2d_datafile_write_time_step_history(f, e.first, e.second));
+	const auto& E = sys.get_energies();
+	const auto& D = sys.get_standard_deviations();
+	for (size_t i = 0; i < E.size(); i++) ok(itp2d_datafile_write_energy_history(f, E[i].data(), (int)E[i].size(), (int)i));
+	for (size_t i = 0; i < D.size(); i++)
+		ok(itp2d_datafile_write_deviation_history(f, D[i].data(), (int)D[i].size(), (int)i));
+	if (save_states && st == ITP2D_OK) {
+		const size_t k = (size_t)p.num_states;
+		std::vector<double> states(2 * dl.N * k);
+		std::vector<int> order(k);
+		const bool sorted = !E.empty();
+		for (size_t n = 0; sorted && n < k; n++) order[n] = (int)sys.get_sorted_index(n);
+		try {
+			sys.download_states(states.data());
+			ok(itp2d_datafile_write_stateset(f, states.data(), (int)k, sys.get_total_step_counter(),
+					sorted ? order.data() : nullptr));
+		} catch (itp2d::DeviceError& e) {
+			ok(e.status);
+			s->err = e.what();
+		}
+	}
+	if (!E.empty()) ok(itp2d_datafile_write_energies(f, E.back().data(), (int)E.back().size()));
+	if (!D.empty()) ok(itp2d_datafile_write_energy_standard_deviations(f, D.back().data(), (int)D.back().size()));
+	ok(itp2d_datafile_add_attribute_int(f, "num_converged", (int)sys.how_many_finally_converged()));
+	ok(itp2d_datafile_add_attribute_int(f, "error_flag", sys.get_error_flag() ? 1 : 0));
+	ok(itp2d_datafile_add_attribute_int(f, "total_steps_done", sys.get_total_step_counter()));
+	double t[7] = {0, 0, 0, 0, 0, 0, 0};
+	try {
+		sys.times(t);
+	} catch (itp2d::DeviceError& e) {
+		ok(e.status);
+		s->err = e.what();
+	}
+	ok(itp2d_datafile_add_attribute_double(f, "propagation_time", t[1]));
+	ok(itp2d_datafile_add_attribute_double(f, "orthonormalization_time", t[2]));
+	ok(itp2d_datafile_add_attribute_double(f, "dotproduct_time", t[3]));
+	ok(itp2d_datafile_add_attribute_double(f, "eigensolve_time", t[4]));
+	ok(itp2d_datafile_add_attribute_double(f, "lincomb_time", t[5]));
+	ok(itp2d_datafile_add_attribute_double(f, "convtest_time", t[6]));
+	ok(itp2d_datafile_add_attribute_double(f, "io_time", itp2d::now_s() - t0));
+	ok(itp2d_datafile_close(f));
+	return st;
 }
 
 // Process-wide flags and the handlers that raise them, as the reference's

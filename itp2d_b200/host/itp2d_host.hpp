@@ -196,6 +196,12 @@ class ITPSystem {
 	double get_sorted_deviation(size_t n) const { return sorted[n].first.second; }
 	size_t get_sorted_index(size_t n) const { return sorted[n].second; }
 	const std::vector<double>& get_residuals() const { return residuals; }
+	const std::vector<double>& get_potential() const { return V; }
+	bool is_null_potential() const { return null_potential; }
+	bool has_user_noise() const { return user_noise; }  // an extra potential was added
+	const ConvergenceTest& timestep_test() const { return *ts_test; }
+	const ConvergenceTest& final_convergence_test() const { return *final_test; }
+	const DataLayout& datalayout() const { return dl; }
 	const std::string& last_error() const { return error_text; }
 	itp2d_ctx* context() { return ctx; }
 	void download_states(double* out);
@@ -212,6 +218,10 @@ class ITPSystem {
 		save_user = user;
 	}
 	int saves = 0;       // save_states calls made
+	// (first step with the value, time step) at the start and at every change
+	// of the time step: the datafile's time_step_history (itpsystem.cpp:113-114,
+	// 220-226)
+	std::vector<std::pair<int, double>> eps_history;
 	int ritz_steps = 0;  // Rayleigh-Ritz steps taken (switch_rayleigh_ritz)
 	const itp2d_parameters p;
 
@@ -241,6 +251,7 @@ class ITPSystem {
 	std::unique_ptr<ConvergenceTest> ts_test, final_test;
 	std::vector<double> V;
 	bool null_potential = true;
+	bool user_noise = false;
 	std::vector<double> initial_states;
 	itp2d_ctx* ctx = nullptr;
 	int precision = ITP2D_FP64;

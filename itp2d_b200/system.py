@@ -269,6 +269,12 @@ class ITPSystem:
         return dict(zip(["total", "propagation", "orthonormalization", "dot", "eigensolve", "lincomb",
                          "convtest"], t.tolist()))
 
+    def write_datafile(self, filename: str, clobber: bool = False, save_states: bool = True):
+        """The reference's HDF5 datafile of this solve (--save final states):
+        itp2d_system_write_datafile, read back with itp2d_b200.datafile."""
+        from . import datafile
+        datafile.write_system_datafile(self, filename, clobber, save_states)
+
     def context_handle(self) -> int:
         return _lib().itp2d_system_context(self.h)
 
