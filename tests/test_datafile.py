@@ -269,3 +269,59 @@ def test_independent_walk_of_a_written_file(tmp_path):
     assert set(links) == {"deviation_history", "energy_history", "final_energies", "final_energy_standard_deviations",
                           "noise_data", "potential_values", "state_history", "states", "time_step_history"}
     assert len(links) <= 2 * leaf_k and internal_k == 16
+
+
+def _decode_type(b, p):
+    """A datatype message body decoded from the specification's field tables
+    (classes 0, 1, 6 version 1 and 10 version 2), independent of the library."""
+    cls, ver = b[p] & 15, b[p] >> 4
+    size = struct.unpack_from("<I", b, p + 4)[0]
+    if cls == 0:
+        return ("int", size, bool(b[p + 1] & 8)), p + 12
+    if cls == 1:
+        assert b[p + 1:p + 4] == bytes([0x20, 63, 0]) and size == 8
+        return ("double",), p + 20
+    if cls == 6:
+        assert ver == 1
+        n = struct.unpack_from("<H", b, p + 1)[0]
+        q, members = p + 8, []
+        for _ in range(n):
+            end = b.index(b"\0", q)
+            name = b[q:end].decode()
+            q += (end - q + 8) // 8 * 8
+            off = struct.unpack_from("<I", b, q)[0]
+            assert b[q + 4] == 0  # no member dimensions
+            t, q = _decode_type(b, q + 32)
+            members.append((name, off, t))
+        return ("compound", size, members), q
+    if cls == 10:
+        assert ver == 2
+        nd = b[p + 8]
+        dims = struct.unpack_from(f"<{nd}I", b, p + 12)
+        perm = struct.unpack_from(f"<{nd}I", b, p + 12 + 4 * nd)
+        assert perm == tuple(range(nd))
+        t, q = _decode_type(b, p + 12 + 8 * nd)
+        return ("array", size, dims, t), q
+    raise AssertionError(f"class {cls}")
+
+
+def test_compound_and_array_encodings_follow_the_specification(tmp_path):
+    p = str(tmp_path / "t.h5")
+    sx, sy = 5, 3
+    with D.Datafile(p, sx, sy, 0.5, clobber=True) as f:
+        f.write_stateset(np.zeros((2, sy, sx), complex), 1)
+        f.write_time_step_history(1, 0.5)
+        f.write_potential(np.zeros((sy, sx)))
+    dbl = ("double",)
+    cplx = ("compound", 16, [("r", 0, dbl), ("i", 8, dbl)])
+    expect = {
+        "states": ("array", 16 * sx * sy, (sy, sx), cplx),
+        "state_history": ("compound", 8, [("step", 0, ("int", 4, True)), ("index", 4, ("int", 4, True))]),
+        "time_step_history": ("compound", 16, [("step", 0, ("int", 4, True)), ("time_step", 8, dbl)]),
+        "potential_values": ("array", 8 * sx * sy, (sy, sx), dbl),
+    }
+    for name, want in expect.items():
+        body = D.header_message(p, name, MSG_TYPE)
+        got, end = _decode_type(body, 0)
+        assert got == want, name
+        assert len(body) - end < 8  # only the message's padding follows
