@@ -69,6 +69,9 @@ int guarded(F&& f) {
 	} catch (std::bad_alloc&) {
 		g_error = "out of host memory";
 		return ITP2D_E_OOM;
+	} catch (std::exception& e) {  // nothing else may cross the C ABI
+		g_error = e.what();
+		return ITP2D_E_IO;
 	}
 }
 

@@ -1003,8 +1003,22 @@ int itp2d_system_times(itp2d_system* s, double* t7) {
 // end of a solve from the driver's records (itpsystem.cpp:69-116 attributes,
 // potential and noise; 113-114, 220-226 time steps; 399-402 histories;
 // 513-531 final states, energies and run attributes).
+static int write_datafile(itp2d_system* s, const char* filename, int clobber, int save_states);
+
 int itp2d_system_write_datafile(itp2d_system* s, const char* filename, int clobber, int save_states) {
 	if (!s || !s->sys || !filename) return ITP2D_E_INVALID;
+	try {
+		return write_datafile(s, filename, clobber, save_states);
+	} catch (std::bad_alloc&) {
+		s->err = "out of host memory";
+		return ITP2D_E_OOM;
+	} catch (std::exception& e) {
+		s->err = e.what();
+		return ITP2D_E_INVALID;
+	}
+}
+
+static int write_datafile(itp2d_system* s, const char* filename, int clobber, int save_states) {
 	itp2d::ITPSystem& sys = *s->sys;
 	const itp2d_parameters& p = sys.p;
 	const itp2d::DataLayout& dl = sys.datalayout();
@@ -1058,17 +1072,20 @@ int itp2d_system_write_datafile(itp2d_system* s, const char* filename, int clobb
 		ok(itp2d_datafile_write_deviation_history(f, D[i].data(), (int)D[i].size(), (int)i));
 	if (save_states && st == ITP2D_OK) {
 		const size_t k = (size_t)p.num_states;
-		std::vector<double> states(2 * dl.N * k);
-		std::vector<int> order(k);
 		const bool sorted = !E.empty();
-		for (size_t n = 0; sorted && n < k; n++) order[n] = (int)sys.get_sorted_index(n);
 		try {
+			std::vector<double> states(2 * dl.N * k);
+			std::vector<int> order(k);
+			for (size_t n = 0; sorted && n < k; n++) order[n] = (int)sys.get_sorted_index(n);
 			sys.download_states(states.data());
 			ok(itp2d_datafile_write_stateset(f, states.data(), (int)k, sys.get_total_step_counter(),
 					sorted ? order.data() : nullptr));
 		} catch (itp2d::DeviceError& e) {
 			ok(e.status);
 			s->err = e.what();
+		} catch (std::bad_alloc&) {
+			ok(ITP2D_E_OOM);
+			s->err = "out of host memory for the states";
 		}
 	}
 	if (!E.empty()) ok(itp2d_datafile_write_energies(f, E.back().data(), (int)E.back().size()));
