@@ -625,11 +625,18 @@ struct Reader {
 
 	explicit Reader(const char* path) {
 		if (!path) bad_arg("filename is NULL");
+		struct stat sb;
+		if (::stat(path, &sb) == 0 && !S_ISREG(sb.st_mode))
+			io_fail(std::string("datafile '") + path + "' is not a regular file");
 		FILE* fp = std::fopen(path, "rb");
 		if (!fp) io_fail(std::string("cannot open datafile '") + path + "': " + std::strerror(errno));
 		std::fseek(fp, 0, SEEK_END);
 		const long n = std::ftell(fp);
 		std::fseek(fp, 0, SEEK_SET);
+		if (n < 0) {
+			std::fclose(fp);
+			io_fail(std::string("cannot size datafile '") + path + "'");
+		}
 		d.resize(n > 0 ? (size_t)n : 0);
 		const size_t got = d.empty() ? 0 : std::fread(d.data(), 1, d.size(), fp);
 		std::fclose(fp);

@@ -325,3 +325,9 @@ def test_compound_and_array_encodings_follow_the_specification(tmp_path):
         got, end = _decode_type(body, 0)
         assert got == want, name
         assert len(body) - end < 8  # only the message's padding follows
+
+
+def test_reader_refuses_a_directory(tmp_path):
+    with pytest.raises(D.DatafileError) as e:
+        D.read(str(tmp_path), "states")
+    assert e.value.status == D.E_IO
