@@ -370,8 +370,8 @@ void grow(Dataset& d, const std::vector<uint64_t>& want) {
 	for (uint64_t x : nd) n *= x;
 	std::vector<uint8_t> out(n * es, 0);
 	if (nd.size() == 1) {
-		std::memcpy(out.data(), d.data.data(), d.data.size());
-	} else {  // rank 2
+		if (!d.data.empty()) std::memcpy(out.data(), d.data.data(), d.data.size());
+	} else if (d.dims[1] > 0) {  // rank 2
 		for (uint64_t r = 0; r < d.dims[0]; r++)
 			std::memcpy(out.data() + r * nd[1] * es, d.data.data() + r * d.dims[1] * es, d.dims[1] * es);
 	}
@@ -1238,7 +1238,8 @@ int itp2d_datafile_read_values(const char* filename, const char* dataset, double
 		if (ds.present)
 			for (uint64_t i = 0; i < n; i++) r.values(*ds.type, ds.at + i * ds.type->size, v);
 		if (n_values) *n_values = (long long)v.size();
-		if (out) std::memcpy(out, v.data(), std::min<uint64_t>(v.size(), (uint64_t)std::max(0ll, max_values)) * 8);
+		const uint64_t nv = std::min<uint64_t>(v.size(), (uint64_t)std::max(0ll, max_values));
+		if (out && nv) std::memcpy(out, v.data(), nv * 8);
 	});
 }
 
