@@ -24,7 +24,7 @@ _bound = False
 
 class DatafileError(RuntimeError):
     def __init__(self, status: int, what: str):
-        msg = capi.lib().itp2d_datafile_last_error().decode()
+        msg = capi.lib().itp2d_datafile_last_error().decode(errors="replace")
         super().__init__(f"{what}: {msg} (status {status})")
         self.status = status
 
@@ -215,7 +215,7 @@ def string_attribute(filename: str, name: str, obj: str = "/") -> str:
     buf = C.create_string_buffer(65536)
     _check(_lib().itp2d_datafile_read_string_attribute(_b(filename), _b(obj), _b(name), buf, len(buf)),
            f"string_attribute({name})")
-    return buf.value.decode()
+    return buf.value.decode(errors="replace")
 
 
 def header_message(filename: str, obj: str, mtype: int, index: int = 0) -> bytes:

@@ -331,3 +331,30 @@ def test_reader_refuses_a_directory(tmp_path):
     with pytest.raises(D.DatafileError) as e:
         D.read(str(tmp_path), "states")
     assert e.value.status == D.E_IO
+
+
+def test_truncated_and_corrupted_files_fail_cleanly(tmp_path):
+    """Every truncation, and a flipped byte anywhere, gives a status or
+    values, never a crash (the reader bounds-checks every field)."""
+    p = str(tmp_path / "good.h5")
+    with D.Datafile(p, 5, 3, 0.5, clobber=True) as f:
+        f.add_attribute("num_states", 2)
+        f.write_stateset(np.ones((2, 3, 5), complex), 1, [1, 0])
+        f.write_energy_history([1.0, 2.0], 0)
+        f.write_time_step_history(1, 0.5)
+    good = open(p, "rb").read()
+    q = tmp_path / "bad.h5"
+    for cut in range(0, len(good), 37):
+        q.write_bytes(good[:cut])
+        with pytest.raises(D.DatafileError):
+            D.read(str(q), "states")
+    for i in range(0, len(good), 13):
+        b = bytearray(good)
+        b[i] ^= 0xFF
+        q.write_bytes(bytes(b))
+        for call in (lambda: D.read(str(q), "states"), lambda: D.attribute(str(q), "num_states"),
+                     lambda: D.string_attribute(str(q), "description", "states")):
+            try:
+                call()
+            except D.DatafileError:
+                pass
