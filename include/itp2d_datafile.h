@@ -14,10 +14,12 @@
  * "/deviation_history" (steps x states), "/final_energies",
  * "/final_energy_standard_deviations", "/potential_values" (scalar of
  * double[sizey][sizex]), "/noise_data"; complex values are the compound
- * {r, i} of two doubles. Differences: datasets are stored contiguous and
- * uncompressed at their current size (the reference uses 1 x 1 chunks with
- * deflate level 9 and unlimited maximum sizes), the file is rewritten as a
- * whole on every flush, and the "description" texts are this library's own.
+ * {r, i} of two doubles. Datasets are stored contiguous and uncompressed at
+ * their current size unless itp2d_datafile_set_chunking selects the
+ * reference's storage (1 x 1 chunks, deflate, unlimited maximum sizes); the
+ * file is rewritten as a whole on every flush, and the "description" texts
+ * are this library's own. The readers also read chunked, deflated datasets,
+ * so files written by the reference itself can seed --copy-states.
  *
  * All functions return ITP2D_OK or an error status (ITP2D_E_INVALID for bad
  * arguments or a mismatching file, ITP2D_E_IO for file-system or format
@@ -42,6 +44,13 @@ struct itp2d_system;
  * "description" and the attributes grid_sizex, grid_sizey, grid_delta. */
 int itp2d_datafile_create(const char* filename, int sizex, int sizey, double dx, int clobber,
 		itp2d_datafile** out);
+/* Storage of the datasets written from now on (every flush rewrites them
+ * all): deflate_level 0-9 stores them as the reference does (one element per
+ * chunk, deflated at that level, unlimited maximum sizes; the reference uses
+ * 9, datafile.cpp:76-88); a negative level (the default) stores them
+ * contiguous and uncompressed, which is faster to write and read. The scalar
+ * "/potential_values" stays contiguous, as in the reference. */
+int itp2d_datafile_set_chunking(itp2d_datafile* f, int deflate_level);
 /* Writes the whole file as it stands (Datafile::flush, datafile.hpp). */
 int itp2d_datafile_flush(itp2d_datafile* f);
 /* Flushes and frees (Datafile::~Datafile). */

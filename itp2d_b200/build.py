@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     relink = force or procs or not os.path.exists(LIB) or \
         max(os.path.getmtime(o) for o in objs) > os.path.getmtime(LIB)
     if relink:
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl", "-lz"]
         # the host objects are plain g++ output; nvcc links them with the device code
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         if r.returncode != 0:

@@ -37,6 +37,7 @@ def _lib():
         ll, llp = C.c_longlong, C.POINTER(C.c_longlong)
         L.itp2d_datafile_create.argtypes = [s, i, i, d, i, C.POINTER(vp)]
         L.itp2d_datafile_flush.argtypes = [vp]
+        L.itp2d_datafile_set_chunking.argtypes = [vp, i]
         L.itp2d_datafile_close.argtypes = [vp]
         L.itp2d_datafile_add_attribute_int.argtypes = [vp, s, i]
         L.itp2d_datafile_add_attribute_double.argtypes = [vp, s, d]
@@ -88,6 +89,11 @@ class Datafile:
         _check(_lib().itp2d_datafile_create(_b(filename), sx, sy, dx, int(clobber), C.byref(h)),
                "itp2d_datafile_create")
         self.h = h
+
+    def set_chunking(self, deflate_level: int = 9):
+        """The reference's storage from now on: one element per chunk,
+        deflated (a negative level: contiguous, the default)."""
+        _check(_lib().itp2d_datafile_set_chunking(self.h, deflate_level), "set_chunking")
 
     def add_attribute(self, name: str, value, kind: str = None):
         """kind: "int", "double", "ulong" or "string" (default: from the value's type)."""

@@ -42,6 +42,8 @@
 #include <string>
 #include <vector>
 
+#include <zlib.h>
+
 #include "../../include/itp2d_datafile.h"
 #include "../../include/itp2d_gpu.h"
 
@@ -244,14 +246,17 @@ void encode_type(Out& o, const Type& t) {
 	}
 }
 
-// Version 1 dataspace; no dims = scalar. The maximum sizes equal the sizes.
-void encode_space(Out& o, const std::vector<uint64_t>& dims) {
+// Version 1 dataspace; no dims = scalar. The maximum sizes equal the sizes,
+// or are unlimited (extendible, as the reference creates its datasets).
+void encode_space(Out& o, const std::vector<uint64_t>& dims, bool unlimited = false) {
 	o.u8(1);
 	o.u8((unsigned)dims.size());
-	o.u8(0);
+	o.u8(unlimited ? 1 : 0);
 	o.u8(0);
 	o.u32(0);
 	for (uint64_t d : dims) o.u64(d);
+	if (unlimited)
+		for (size_t i = 0; i < dims.size(); i++) o.u64(kUndef);
 }
 
 struct Attr {
@@ -310,7 +315,7 @@ std::vector<uint8_t> object_header(const std::vector<Msg>& msgs) {
 }
 
 constexpr uint16_t kMsgNil = 0x0000, kMsgSpace = 0x0001, kMsgType = 0x0003, kMsgFill = 0x0005,
-		kMsgLayout = 0x0008, kMsgAttr = 0x000c, kMsgCont = 0x0010, kMsgSymtab = 0x0011;
+		kMsgLayout = 0x0008, kMsgFilters = 0x000b, kMsgAttr = 0x000c, kMsgCont = 0x0010, kMsgSymtab = 0x0011;
 constexpr uint8_t kConstant = 0x01;
 
 Msg attr_msg(const Attr& a) {
@@ -387,6 +392,7 @@ struct itp2d_datafile {
 	double dx = 0;
 	std::vector<Attr> root_attrs;
 	std::map<std::string, Dataset> sets;  // by name without '/', sorted like the symbol-table node
+	int deflate = -1;                     // < 0: contiguous datasets; 0-9: chunked, deflated at this level
 
 	void add_root_attr(Attr a) {
 		for (const Attr& b : root_attrs)
@@ -463,16 +469,127 @@ std::vector<uint8_t> layout_msg(uint64_t addr, uint64_t size) {
 	return o.b;
 }
 
-std::vector<Msg> dataset_msgs(const Dataset& d, uint64_t addr) {
+// K of the chunk-index B-trees: a version 0 superblock has no field for it,
+// so readers take the format's default.
+constexpr int kChunkK = 32;
+
+// Chunked storage as the reference's datasets have it (datafile.cpp:76-88):
+// one element per chunk, each deflated, indexed by a version 1 B-tree (type 1)
+// whose nodes hold up to 2K chunks. Returns the bytes to place at `start`;
+// *root receives the B-tree's address (undefined for an empty dataset).
+std::vector<uint8_t> chunk_storage(const Dataset& d, uint64_t start, int level, uint64_t* root) {
+	const size_t rank = d.dims.size();
+	const uint64_t es = d.type->size, n = d.elements();
+	*root = kUndef;
+	Out o;
+	if (n == 0) return o.b;
+	struct Key {
+		uint32_t size;
+		std::vector<uint64_t> off;  // rank offsets, then the element's byte offset
+	};
+	std::vector<Key> keys(n);
+	std::vector<uint64_t> addr(n);
+	std::vector<uint8_t> z(compressBound((uLong)es));
+	std::vector<uint64_t> idx(rank, 0);
+	for (uint64_t e = 0; e < n; e++) {
+		uLongf len = (uLongf)z.size();
+		if (compress2(z.data(), &len, d.data.data() + e * es, (uLong)es, level) != Z_OK) io_fail("deflate failed");
+		addr[e] = start + o.size();
+		o.raw(z.data(), len);
+		keys[e].size = (uint32_t)len;
+		keys[e].off = idx;
+		keys[e].off.push_back(0);
+		for (size_t i = rank; i-- > 0;) {
+			if (++idx[i] < d.dims[i]) break;
+			idx[i] = 0;
+		}
+	}
+	// the right boundary of the last chunk: its offsets plus the chunk dimensions
+	Key right = {0, keys.back().off};
+	for (size_t i = 0; i < rank; i++) right.off[i] += 1;
+	right.off[rank] = es;
+	const size_t ks = 8 + 8 * (rank + 1);
+	const size_t node_bytes = 24 + 2 * kChunkK * 8 + (2 * kChunkK + 1) * ks;
+	auto put_key = [](Out& w, const Key& k) {
+		w.u32(k.size);
+		w.u32(0);  // filter mask: every filter applied
+		for (uint64_t x : k.off) w.u64(x);
+	};
+	o.pad_to(round8(o.size()));
+	// level by level: the children (addresses and left keys) grouped into nodes
+	std::vector<uint64_t> child_addr = addr;
+	std::vector<Key> child_key = keys;
+	for (int lvl = 0;; lvl++) {
+		const size_t per = 2 * kChunkK, nn = (child_addr.size() + per - 1) / per;
+		const uint64_t first = start + o.size();
+		std::vector<uint64_t> node_addr(nn);
+		std::vector<Key> node_key(nn);
+		for (size_t j = 0; j < nn; j++) {
+			node_addr[j] = first + j * node_bytes;
+			const size_t b = j * per, e = std::min(child_addr.size(), b + per);
+			node_key[j] = child_key[b];
+			Out w;
+			w.raw("TREE", 4);
+			w.u8(1);  // chunk index
+			w.u8((unsigned)lvl);
+			w.u16((unsigned)(e - b));
+			w.u64(j > 0 ? first + (j - 1) * node_bytes : kUndef);
+			w.u64(j + 1 < nn ? first + (j + 1) * node_bytes : kUndef);
+			for (size_t c = b; c < e; c++) {
+				put_key(w, child_key[c]);
+				w.u64(child_addr[c]);
+			}
+			put_key(w, e < child_addr.size() ? child_key[e] : right);
+			w.pad_to(node_bytes);
+			o.raw(w.b.data(), w.size());
+		}
+		if (nn == 1) {
+			*root = node_addr[0];
+			break;
+		}
+		child_addr.swap(node_addr);
+		child_key.swap(node_key);
+	}
+	return o.b;
+}
+
+bool is_chunked(const Dataset& d, int level) { return level >= 0 && !d.dims.empty(); }
+
+std::vector<Msg> dataset_msgs(const Dataset& d, uint64_t addr, int level) {
+	const bool chunked = is_chunked(d, level);
 	std::vector<Msg> m;
-	// fill value message version 1: allocation late, fill written if set, default (zero) fill
-	m.push_back({kMsgFill, kConstant, {1, 2, 2, 1, 0, 0, 0, 0}});
+	// fill value message version 1: allocation late (incremental when chunked),
+	// fill written if set, default (zero) fill
+	m.push_back({kMsgFill, kConstant, {1, (uint8_t)(chunked ? 3 : 2), 2, 1, 0, 0, 0, 0}});
 	Out t, s;
 	encode_type(t, *d.type);
-	encode_space(s, d.dims);
+	encode_space(s, d.dims, chunked);
 	m.push_back({kMsgType, kConstant, t.b});
 	m.push_back({kMsgSpace, 0, s.b});
-	m.push_back({kMsgLayout, kConstant, layout_msg(d.data.empty() ? kUndef : addr, d.data.size())});
+	if (chunked) {
+		Out l;
+		l.u8(3);  // version 3
+		l.u8(2);  // chunked
+		l.u8((unsigned)d.dims.size() + 1);
+		l.u64(addr);
+		for (size_t i = 0; i < d.dims.size(); i++) l.u32(1);
+		l.u32(d.type->size);
+		m.push_back({kMsgLayout, kConstant, l.b});
+		Out f;  // filter pipeline version 1: deflate at `level`
+		f.u8(1);
+		f.u8(1);
+		f.zeros(6);
+		f.u16(1);  // deflate
+		f.u16(8);  // name length, padded
+		f.u16(0);  // mandatory
+		f.u16(1);  // one client value
+		f.name8("deflate");
+		f.u32((uint32_t)level);
+		f.u32(0);  // padding after an odd number of values
+		m.push_back({kMsgFilters, kConstant, f.b});
+	} else {
+		m.push_back({kMsgLayout, kConstant, layout_msg(d.data.empty() ? kUndef : addr, d.data.size())});
+	}
 	for (const Attr& a : d.attrs) m.push_back(attr_msg(a));
 	return m;
 }
@@ -505,12 +622,18 @@ std::vector<uint8_t> itp2d_datafile::serialise() const {
 	std::vector<size_t> hdr_bytes;
 	for (const auto& kv : sets) {
 		a_hdr.push_back(at);
-		hdr_bytes.push_back(object_header(dataset_msgs(kv.second, 0)).size());
+		hdr_bytes.push_back(object_header(dataset_msgs(kv.second, 0, deflate)).size());
 		at = round8(at + hdr_bytes.back());
 	}
+	std::vector<std::vector<uint8_t>> chunks;  // chunked storage of each dataset
+	std::vector<uint64_t> a_layout;
 	for (const auto& kv : sets) {
 		a_raw.push_back(at);
-		at = round8(at + kv.second.data.size());
+		uint64_t la = kv.second.data.empty() ? kUndef : at;
+		chunks.emplace_back();
+		if (is_chunked(kv.second, deflate)) chunks.back() = chunk_storage(kv.second, at, deflate, &la);
+		a_layout.push_back(la);
+		at = round8(at + (is_chunked(kv.second, deflate) ? chunks.back().size() : kv.second.data.size()));
 	}
 	const uint64_t eof = at;
 
@@ -589,7 +712,7 @@ std::vector<uint8_t> itp2d_datafile::serialise() const {
 	size_t i = 0;
 	for (const auto& kv : sets) {
 		f.pad_to(a_hdr[i]);
-		const auto h = object_header(dataset_msgs(kv.second, a_raw[i]));
+		const auto h = object_header(dataset_msgs(kv.second, a_layout[i], deflate));
 		if (h.size() != hdr_bytes[i]) io_fail("internal: header size changed");
 		f.raw(h.data(), h.size());
 		i++;
@@ -597,7 +720,10 @@ std::vector<uint8_t> itp2d_datafile::serialise() const {
 	i = 0;
 	for (const auto& kv : sets) {
 		f.pad_to(a_raw[i]);
-		f.raw(kv.second.data.data(), kv.second.data.size());
+		if (is_chunked(kv.second, deflate))
+			f.raw(chunks[i].data(), chunks[i].size());
+		else
+			f.raw(kv.second.data.data(), kv.second.data.size());
 		i++;
 	}
 	f.pad_to(eof);
@@ -826,6 +952,7 @@ struct Reader {
 					p += nb;
 				}
 				m.type = decode_type(p, depth + 1);
+				if ((uint64_t)m.offset + m.type->size > size) io_fail("datafile corrupt: compound member outside");
 				t->members.push_back(std::move(m));
 			}
 			break;
@@ -838,6 +965,12 @@ struct Reader {
 			p += 4 * nd;
 			if (version < 3) p += 4 * nd;  // permutation indices
 			t->base = decode_type(p, depth + 1);
+			uint64_t cnt = 1;
+			for (uint32_t x : t->dims) {
+				cnt *= x;
+				if (cnt > 0xffffffffull) io_fail("datafile corrupt: array datatype too large");
+			}
+			if (t->base->size == 0 || cnt * t->base->size != size) io_fail("datafile corrupt: array datatype size");
 			break;
 		}
 		default:
@@ -871,7 +1004,126 @@ struct Reader {
 		bool present = false;
 	};
 
-	Data dataset(const char* name) const {
+	// Deflate (filter 1) is the one filter read; the pipeline's filter ids in order.
+	std::vector<unsigned> filters(const std::vector<RawMsg>& m) const {
+		std::vector<unsigned> ids;
+		const RawMsg* f = find(m, kMsgFilters);
+		if (!f) return ids;
+		const int v = (int)uint(f->at, 1), nf = (int)uint(f->at + 1, 1);
+		uint64_t p = f->at + (v == 1 ? 8 : 2);
+		for (int i = 0; i < nf; i++) {
+			const unsigned id = (unsigned)uint(p, 2);
+			uint64_t name_len = 0;
+			p += 2;
+			if (v == 1 || id >= 256) {
+				name_len = uint(p, 2);
+				p += 2;
+			}
+			const uint64_t nvals = uint(p + 2, 2);
+			p += 4;
+			p += v == 1 ? round8(name_len) : name_len;
+			p += 4 * nvals + (v == 1 && (nvals & 1) ? 4 : 0);
+			ids.push_back(id);
+		}
+		return ids;
+	}
+
+	// Chunks of a version 1 B-tree (type 1): offsets (rank + 1 values, the
+	// last the element's byte offset), stored size, filter mask, address.
+	struct Chunk {
+		std::vector<uint64_t> off;
+		uint64_t size, mask, addr;
+	};
+	void chunk_tree(uint64_t rel, int nd, std::vector<Chunk>& out, int depth) const {
+		if (depth > 64) io_fail("datafile corrupt: chunk B-tree too deep");
+		const uint64_t at = abs(rel);
+		expect(at, "TREE");
+		if (uint(at + 4, 1) != 1) io_fail("datafile corrupt: not a chunk B-tree");
+		const int level = (int)uint(at + 5, 1);
+		const uint64_t n = uint(at + 6, 2);
+		const uint64_t ks = 8 + 8 * (uint64_t)nd;
+		for (uint64_t i = 0; i < n; i++) {
+			const uint64_t key = at + 24 + i * (ks + 8);
+			const uint64_t child = uint(key + ks, 8);
+			if (level > 0) {
+				chunk_tree(child, nd, out, depth + 1);
+				continue;
+			}
+			Chunk c;
+			c.size = uint(key, 4);
+			c.mask = uint(key + 4, 4);
+			for (int j = 0; j < nd; j++) c.off.push_back(uint(key + 8 + 8 * j, 8));
+			c.addr = child;
+			out.push_back(c);
+			if (out.size() > (uint64_t)1 << 32) io_fail("datafile corrupt: too many chunks");
+		}
+	}
+
+	// Number of elements of a dataspace, refusing products that overflow or
+	// exceed what one read can hold (2^40 bytes at the given element size).
+	static uint64_t element_count(const std::vector<uint64_t>& dims, uint64_t es) {
+		uint64_t n = 1;
+		for (uint64_t x : dims) {
+			if (x != 0 && n > ((uint64_t)1 << 40) / x) io_fail("dataset too large to read");
+			n *= x;
+		}
+		if (es != 0 && n > ((uint64_t)1 << 40) / es) io_fail("dataset too large to read");
+		return n;
+	}
+
+	// The elements of a chunked dataset, decompressed and placed row-major
+	// into one buffer (unwritten chunks read as zero, the default fill).
+	std::vector<uint8_t> gather_chunks(const std::vector<RawMsg>& m, uint64_t tree, const std::vector<uint32_t>& cdims,
+			const std::vector<uint64_t>& dims, uint64_t es) const {
+		const size_t rank = dims.size();
+		if (cdims.size() != rank + 1) io_fail("chunk dimensions do not match the dataspace");
+		const uint64_t n = element_count(dims, es);
+		uint64_t cn = 1;
+		for (size_t i = 0; i < rank; i++) {
+			cn *= cdims[i];
+			if (cn * es > ((uint64_t)1 << 32)) io_fail("chunk too large");
+		}
+		std::vector<uint8_t> out(n * es, 0);
+		if (tree == kUndef || n == 0) return out;
+		const std::vector<unsigned> ids = filters(m);
+		for (unsigned id : ids)
+			if (id != 1) io_fail("filter " + std::to_string(id) + " is not supported (deflate only)");
+		std::vector<Chunk> chunks;
+		chunk_tree(tree, (int)rank + 1, chunks, 0);
+		std::vector<uint8_t> raw(cn * es);
+		for (const Chunk& c : chunks) {
+			const uint64_t at = abs(c.addr);
+			need(at, c.size);
+			const bool deflated = !ids.empty() && !(c.mask & 1);
+			if (deflated) {
+				uLongf len = (uLongf)raw.size();
+				if (uncompress(raw.data(), &len, &d[at], (uLong)c.size) != Z_OK || len != raw.size())
+					io_fail("datafile corrupt: a chunk does not inflate to its size");
+			} else {
+				if (c.size != raw.size()) io_fail("datafile corrupt: chunk of the wrong size");
+				std::memcpy(raw.data(), &d[at], raw.size());
+			}
+			// copy the chunk's part inside the dataset, element by element
+			std::vector<uint64_t> idx(rank, 0);
+			for (uint64_t e = 0; e < cn; e++) {
+				uint64_t lin = 0;
+				bool inside = true;
+				for (size_t i = 0; i < rank; i++) {
+					const uint64_t g = c.off[i] + idx[i];
+					if (g >= dims[i]) inside = false;
+					lin = lin * dims[i] + g;
+				}
+				if (inside) std::memcpy(&out[lin * es], &raw[e * es], es);
+				for (size_t i = rank; i-- > 0;) {
+					if (++idx[i] < cdims[i]) break;
+					idx[i] = 0;
+				}
+			}
+		}
+		return out;
+	}
+
+	Data dataset(const char* name) {
 		const auto m = messages(lookup(name));
 		const RawMsg *t = find(m, kMsgType), *s = find(m, kMsgSpace), *l = find(m, kMsgLayout);
 		if (!t || !s || !l) bad_arg(std::string("'") + (name ? name : "/") + "' is not a dataset");
@@ -879,25 +1131,45 @@ struct Reader {
 		uint64_t p = t->at;
 		out.type = decode_type(p);
 		const bool nonnull = decode_space(s->at, out.dims);
-		uint64_t n = 1;
-		for (uint64_t x : out.dims) n *= x;
+		uint64_t n = element_count(out.dims, out.type->size);
 		if (!nonnull) n = 0;
 		const int lv = (int)uint(l->at, 1);
 		int cls;
 		uint64_t addr = kUndef;
+		uint64_t tree = kUndef;
+		std::vector<uint32_t> cdims;
 		if (lv == 3) {
 			cls = (int)uint(l->at + 1, 1);
 			if (cls == 1) addr = uint(l->at + 2, 8);
 			if (cls == 0) addr = l->at + 4 - base;  // compact: data inside the message
+			if (cls == 2) {
+				const int nd = (int)uint(l->at + 2, 1);
+				tree = uint(l->at + 3, 8);
+				for (int i = 0; i < nd; i++) cdims.push_back((uint32_t)uint(l->at + 11 + 4 * i, 4));
+			}
 		} else if (lv == 1 || lv == 2) {
 			const int nd = (int)uint(l->at + 1, 1);
 			cls = (int)uint(l->at + 2, 1);
 			if (cls == 1) addr = uint(l->at + 8, 8);
 			if (cls == 0) addr = l->at + 8 + 4 * nd + 4 - base;
+			if (cls == 2) {
+				tree = uint(l->at + 8, 8);
+				for (int i = 0; i < nd; i++) cdims.push_back((uint32_t)uint(l->at + 16 + 4 * i, 4));
+			}
 		} else {
 			io_fail("layout message version " + std::to_string(lv) + " is not supported");
 		}
-		if (cls == 2) io_fail("chunked datasets are not supported");
+		if (cls == 2) {
+			if (!cdims.empty() && cdims.back() != out.type->size) io_fail("chunk element size differs from the type");
+			for (size_t i = 0; i + 1 < cdims.size(); i++)
+				if (cdims[i] == 0) io_fail("datafile corrupt: zero chunk dimension");
+			std::vector<uint8_t> all = gather_chunks(m, tree, cdims, out.dims, out.type->size);
+			// the gathered elements are read like contiguous storage placed after the file
+			out.at = d.size();
+			d.insert(d.end(), all.begin(), all.end());
+			out.present = n > 0;
+			return out;
+		}
 		if (n > 0) {
 			if (addr == kUndef) io_fail("dataset has no storage");
 			out.at = abs(addr);
@@ -1070,6 +1342,13 @@ int itp2d_datafile_create(const char* filename, int sizex, int sizey, double dx,
 }
 
 int itp2d_datafile_flush(itp2d_datafile* f) { return guarded([&] { checked(f)->write(); }); }
+
+int itp2d_datafile_set_chunking(itp2d_datafile* f, int deflate_level) {
+	return guarded([&] {
+		if (deflate_level > 9) bad_arg("deflate level above 9");
+		checked(f)->deflate = deflate_level < 0 ? -1 : deflate_level;
+	});
+}
 
 int itp2d_datafile_close(itp2d_datafile* f) {
 	if (!f) return ITP2D_OK;

@@ -39,7 +39,7 @@ def test_library_exports_datafile_header_symbols():
     txt = open(os.path.join(capi.ROOT, "include", "itp2d_datafile.h")).read()
     names = sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*\**\s+\**(itp2d_[a-z0-9_]+)\s*\(",
                                   txt, flags=re.M)))
-    assert len(names) == 25
+    assert len(names) == 26
     lib = capi.lib()
     for n in names:
         assert hasattr(lib, n), n
@@ -358,3 +358,81 @@ def test_truncated_and_corrupted_files_fail_cleanly(tmp_path):
                 call()
             except D.DatafileError:
                 pass
+
+
+def _write_run(path, chunk_level=None):
+    sx, sy, k = 6, 4, 40
+    rng = np.random.default_rng(21)
+    st = _states(rng, k, sy, sx)
+    with D.Datafile(path, sx, sy, 0.5, clobber=True) as f:
+        if chunk_level is not None:
+            f.set_chunking(chunk_level)
+        f.add_attribute("num_states", k)
+        f.write_stateset(st, 3)
+        f.write_stateset(st[::-1], 5, np.arange(k)[::-1])  # 80 chunks: a two-level chunk index
+        for i in range(30):  # 30 x 40 = 1200 chunks of one double
+            f.write_energy_history(rng.normal(size=k), i)
+        f.write_time_step_history(1, 0.5)
+        f.write_energies(rng.normal(size=k))
+        f.write_potential(rng.normal(size=(sy, sx)))
+        f.write_noise_realization([])
+        f.write_state(3, 1, st[7])  # grows states to 4 slots, zero-filled
+    return st
+
+
+def test_chunked_deflated_storage_reads_like_contiguous(tmp_path):
+    """The reference's storage (one element per chunk, deflate 9, unlimited
+    maximum sizes, datafile.cpp:76-88) holds the same values as the
+    contiguous default, and --copy-states reads it."""
+    a, b = str(tmp_path / "contiguous.h5"), str(tmp_path / "chunked.h5")
+    st = _write_run(a)
+    _write_run(b, 9)
+    for name in ["states", "state_history", "energy_history", "time_step_history", "final_energies",
+                 "potential_values", "noise_data"]:
+        assert D.shape(a, name) == D.shape(b, name), name
+        assert np.array_equal(D.read(a, name), D.read(b, name)), name
+    assert np.array_equal(D.init_states(b, 40, 6, 4, 0.5)[1], st[7])
+    # the layout, filter and dataspace messages say what the reference's datasets say
+    lay = D.header_message(b, "energy_history", MSG_LAYOUT)
+    assert lay[:3] == bytes([3, 2, 3]) and struct.unpack_from("<III", lay, 11) == (1, 1, 8)
+    flt = D.header_message(b, "energy_history", 11)
+    assert struct.unpack_from("<HHHH", flt, 8) == (1, 8, 0, 1) and struct.unpack_from("<I", flt, 24)[0] == 9
+    spc = D.header_message(b, "energy_history", MSG_SPACE)
+    assert spc[2] & 1 and struct.unpack_from("<QQ", spc, 24) == (2 ** 64 - 1, 2 ** 64 - 1)
+    assert D.header_message(b, "potential_values", MSG_LAYOUT)[:2] == bytes([3, 1])  # scalar stays contiguous
+
+
+def _inflate_chunks(b, tree, nd, out, es, dims):
+    """Chunk B-tree (type 1) walked from the specification, chunks inflated
+    with Python's zlib and placed by their offsets."""
+    import zlib
+    assert b[tree:tree + 4] == b"TREE" and b[tree + 4] == 1
+    level, n = b[tree + 5], struct.unpack_from("<H", b, tree + 6)[0]
+    ks = 8 + 8 * nd
+    for i in range(n):
+        key = tree + 24 + i * (ks + 8)
+        size, mask = struct.unpack_from("<II", b, key)
+        off = struct.unpack_from(f"<{nd}Q", b, key + 8)
+        child = struct.unpack_from("<Q", b, key + ks)[0]
+        if level:
+            _inflate_chunks(b, child, nd, out, es, dims)
+            continue
+        raw = zlib.decompress(b[child:child + size])
+        assert len(raw) == es and mask == 0
+        lin = 0
+        for d, o in zip(dims, off[:-1]):
+            lin = lin * d + o
+        out[lin * es:(lin + 1) * es] = raw
+
+
+def test_chunk_index_decoded_independently(tmp_path):
+    p = str(tmp_path / "chunked.h5")
+    _write_run(p, 6)
+    b = open(p, "rb").read()
+    lay = D.header_message(p, "energy_history", MSG_LAYOUT)
+    tree = struct.unpack_from("<Q", lay, 3)[0]
+    dims, _ = D.shape(p, "energy_history")
+    out = bytearray(8 * int(np.prod(dims)))
+    _inflate_chunks(b, tree, 3, out, 8, dims)
+    assert np.array_equal(np.frombuffer(bytes(out), dtype="<f8").reshape(dims), D.read(p, "energy_history"))
+    assert b[tree + 5] == 1  # 1200 chunks: leaves under one internal node
