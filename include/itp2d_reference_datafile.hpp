@@ -6,7 +6,8 @@
  * `#include "datafile.hpp"` by this header and `Datafile` by
  * `itp2d_b200::Datafile`; the body of StateSet::init_from_datafile
  * (stateset.cpp:86-109) becomes itp2d_b200::init_from_datafile(*this, name).
- * Same constructor, methods and arguments; a failure throws the reference's
+ * Same constructor, methods, arguments and storage (one element per chunk,
+ * deflate 9); a failure throws the reference's
  * GeneralError with the library's message (the reference rethrows HDF5's
  * exceptions). Link with -litp2d_b200.
  */
@@ -39,6 +40,8 @@ class Datafile {
 	Datafile(std::string filename, DataLayout const& dl, bool clobber = false) : f(NULL), sx(dl.sizex), sy(dl.sizey) {
 		check_datafile(itp2d_datafile_create(filename.c_str(), static_cast<int>(dl.sizex), static_cast<int>(dl.sizey),
 				dl.dx, clobber ? 1 : 0, &f), "Datafile");
+		// the reference's storage: one element per chunk, deflate 9 (datafile.cpp:76-88)
+		check_datafile(itp2d_datafile_set_chunking(f, 9), "Datafile");
 	}
 	~Datafile() { itp2d_datafile_close(f); }
 

@@ -112,6 +112,10 @@ int main(int argc, char** argv) {
 	std::vector<double> fe = read_all(path, "final_energies");
 	expect(fe.size() == N && std::memcmp(&fe[0], &E.back()[0], N * sizeof(double)) == 0, "final_energies");
 	expect(read_all(path, "noise_data").empty(), "noise_data of NoNoise is empty");
+	unsigned char lay[64];
+	int lay_size = 0;
+	itp2d_datafile_header_message(path, "energy_history", 8, 0, lay, sizeof lay, &lay_size);
+	expect(lay_size >= 3 && lay[0] == 3 && lay[1] == 2, "stored chunked, as the reference's datasets");
 	double seed = 0;
 	itp2d_datafile_read_attribute(path, "/", "random_seed", &seed);
 	expect(seed == 12345.0, "random_seed attribute");
